@@ -1,0 +1,144 @@
+"""Runs the compiled reference (oracle/_ref/mapp_ref_harness) on a workload.
+
+Test infrastructure only (the oracle is the checker, never the product).  The
+harness executable links the unmodified reference objects; see
+oracle/ref/harness.cpp for the call sequences it reproduces.  Each run is a
+separate process, so a reference abort cannot take the caller down.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+HARNESS = os.path.join(HERE, "_ref", "mapp_ref_harness")
+
+
+def available() -> bool:
+    return os.path.exists(HARNESS)
+
+
+def _meta(path):
+    out = {}
+    if not os.path.exists(path):
+        return out
+    for line in open(path):
+        parts = line.split()
+        if not parts:
+            continue
+        key, vals = parts[0], parts[1:]
+        nums = []
+        for v in vals:
+            try:
+                nums.append(int(v))
+            except ValueError:
+                nums.append(float(v))
+        out[key] = nums[0] if len(nums) == 1 else nums
+    return out
+
+
+class RefRun:
+    """Builds a command file, runs the harness once and loads every output."""
+
+    def __init__(self, workload: dict, workdir: str | None = None):
+        self.w = workload
+        self.dir = workdir or tempfile.mkdtemp(prefix="mapp_ref_")
+        self.lines = [f"script {workload['script']}"]
+        style = workload["style"]
+        if style.startswith("DMD"):
+            self.lines.append(f"oracle_ff {style}")
+        else:
+            self.lines.append(f"ffcoef_style {style}")
+        self.lines.append("ffcoef " + " ".join(workload["coef"]))
+        self.lines.append("init")
+        self.steps = []
+
+    def _p(self, tag):
+        return os.path.join(self.dir, tag)
+
+    def add(self, line):
+        self.lines.append(line)
+        return self
+
+    def dump(self, tag="s0"):
+        self.steps.append(("dump", tag))
+        return self.add(f"dump {self._p(tag)}")
+
+    def force(self, tag="f0", st_clc=1):
+        self.steps.append(("force", tag))
+        return self.add(f"force {st_clc} {self._p(tag)}")
+
+    def energy(self, tag="e0"):
+        self.steps.append(("energy", tag))
+        return self.add(f"energy {self._p(tag)}")
+
+    def crd(self, tag="crd"):
+        self.steps.append(("crd", tag))
+        return self.add(f"crd {self._p(tag)}")
+
+    def cdot(self, tag="cd"):
+        self.steps.append(("cdot", tag))
+        return self.add(f"cdot {self._p(tag)}")
+
+    def calcg(self, a: np.ndarray, alpha: float, chk=0, tag="g"):
+        ap = self._p(tag + ".a.bin")
+        np.ascontiguousarray(a, dtype=np.float64).tofile(ap)
+        self.steps.append(("calcg", tag))
+        return self.add(f"calcg {chk} {alpha!r} {ap} {self._p(tag)}")
+
+    def setx(self, x: np.ndarray, tag="u"):
+        xp = self._p(tag + ".x_in.bin")
+        np.ascontiguousarray(x, dtype=np.float64).tofile(xp)
+        self.steps.append(("setx", tag))
+        return self.add(f"setx {xp} {self._p(tag)}")
+
+    def setc(self, c: np.ndarray, tag="c"):
+        cp = self._p(tag + ".c_in.bin")
+        np.ascontiguousarray(c, dtype=np.float64).tofile(cp)
+        return self.add(f"setc {cp}")
+
+    def time(self, what: str, reps: int, tag="t"):
+        self.steps.append(("time", tag))
+        return self.add(f"time {what} {reps} {self._p(tag)}")
+
+    def run(self, timeout=600) -> dict:
+        cmd_path = self._p("commands.txt")
+        lines = []
+        for ln in self.lines:
+            if ln.startswith("ffcoef_style "):
+                # EAM / FS use the stock reference classes: create them by script
+                continue
+            lines.append(ln)
+        style = self.w["style"]
+        if not style.startswith("DMD"):
+            # stock style: create the force field with the reference's own "ff" command
+            script2 = self._p("in_stock.mapp")
+            with open(self.w["script"]) as src, open(script2, "w") as dst:
+                dst.write(src.read())
+                dst.write(f"ff {style}\n")
+                dst.write(" ".join(self.w["coef"]) + "\n")
+            lines = [f"script {script2}"] + [ln for ln in lines[1:] if not ln.startswith("ffcoef ")]
+        with open(cmd_path, "w") as fp:
+            fp.write("\n".join(lines) + "\n")
+        proc = subprocess.run([HARNESS, cmd_path], capture_output=True, text=True, timeout=timeout)
+        if proc.returncode != 0:
+            raise RuntimeError(f"reference harness failed ({proc.returncode}):\n{proc.stdout[-2000:]}\n{proc.stderr[-2000:]}")
+        self.stdout = proc.stdout
+        return self.load()
+
+    def load(self) -> dict:
+        res = {}
+        for kind, tag in self.steps:
+            p = self._p(tag)
+            m = _meta(p + ".meta")
+            d = {"meta": m}
+            for fn in os.listdir(self.dir):
+                if fn.startswith(tag + ".") and fn.endswith(".bin") and not fn.endswith("_in.bin") and not fn.endswith(".a.bin"):
+                    name = fn[len(tag) + 1:-4]
+                    dt = np.int32 if name in ("nsize", "nlist", "type", "id", "crd") else np.float64
+                    d[name] = np.fromfile(os.path.join(self.dir, fn), dtype=dt)
+            res[tag] = d
+        return res
