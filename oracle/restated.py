@@ -1,0 +1,256 @@
+"""ctypes wrapper around the C restatement oracle (oracle/mapp_oracle.c).
+
+Test infrastructure only: the checker for the GPU library, never the product.
+``OracleRun`` mirrors the reference harness (oracle/reference.py): it takes a
+workload written by ``mapp_b200.fixtures.write_workload`` and reproduces the
+reference's call sequence (Min_LBFGS::init order) in the restatement.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_mapp.so")
+SRC = os.path.join(HERE, "mapp_oracle.c")
+
+STYLES = {"EAM": 0, "FS": 1, "DMD_I": 2, "DMD_II": 3, "DMD": 4}
+
+
+def build(force=False):
+    """Compile the restatement with the reference's arithmetic flags."""
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(SRC):
+        subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", LIB_PATH, SRC, "-lm"])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+        ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+        L.orc_new.restype = P
+        L.orc_new.argtypes = [C.c_int, C.c_int]
+        L.orc_free.argtypes = [P]
+        L.orc_set_tables.argtypes = [P, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, dp, dp, dp]
+        L.orc_set_fs.argtypes = [P, dp, dp, dp, dp, dp, dp, dp, dp, ip]
+        L.orc_set_dmd.argtypes = [P, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, dp]
+        L.orc_set_atoms.argtypes = [P, C.c_int, dp, C.c_double, dp, C.c_void_p, C.c_void_p]
+        L.orc_init.argtypes = [P]
+        L.orc_update_x.argtypes = [P, dp, C.POINTER(C.c_int)]
+        L.orc_update_c.argtypes = [P, dp]
+        L.orc_counts.argtypes = [P, ip]
+        L.orc_get_x.argtypes = [P, dp]
+        L.orc_get_c.argtypes = [P, dp]
+        L.orc_get_ghost_src.argtypes = [P, ip]
+        L.orc_get_list.argtypes = [P, ip, ip]
+        L.orc_get_cutph.argtypes = [P, dp]
+        L.orc_get_box.argtypes = [P, dp, dp]
+        L.orc_force.argtypes = [P, C.c_int, dp, dp]
+        L.orc_energy.argtypes = [P]
+        L.orc_energy.restype = C.c_double
+        L.orc_create_2nd_neigh_lst.argtypes = [P]
+        L.orc_get_crd.argtypes = [P, ip, C.c_void_p, C.c_void_p]
+        L.orc_c_d_calc.argtypes = [P, dp]
+        L.orc_calc_g.argtypes = [P, C.c_int, C.c_double, dp, dp]
+        L.orc_calc_g.restype = C.c_double
+        L.orc_get_vec.argtypes = [P, C.c_int, dp]
+        L.orc_get_pairs.argtypes = [P, dp]
+        L.orc_gauss_hermite.argtypes = [C.c_int, dp, dp]
+        L.orc_get_dmd_consts.argtypes = [P, dp]
+        L.orc_spline7.argtypes = [C.c_int, C.c_double, dp]
+        L.orc_spline9.argtypes = [C.c_int, C.c_double, dp]
+        _lib = L
+    return _lib
+
+
+def _numbers(lines):
+    return np.array([float(t) for ln in lines for t in ln.split("#")[0].split()], dtype=np.float64)
+
+
+def read_eam_file(path, nt, fs_mode):
+    """Raw columns of a setfl / FS table file in the reference's reading order
+    (one element header line, ff_eam.cpp:692-775): F [nt][nrho],
+    rho [nt][nt][nr] (FS) or [nt][nr] (setfl), r*phi [nt(nt+1)/2][nr]."""
+    with open(path) as fp:
+        lines = fp.readlines()
+    hdr = lines[4].split()
+    nrho, drho, nr, dr = int(hdr[0]), float(hdr[1]), int(hdr[2]), float(hdr[3])
+    v = _numbers(lines[6:])
+    pos = 0
+    F = np.zeros((nt, nrho))
+    rho = np.zeros((nt, nt, nr)) if fs_mode else np.zeros((nt, nr))
+    for i in range(nt):
+        F[i] = v[pos:pos + nrho]
+        pos += nrho
+        if fs_mode:
+            for j in range(nt):
+                rho[i, j] = v[pos:pos + nr]
+                pos += nr
+        else:
+            rho[i] = v[pos:pos + nr]
+            pos += nr
+    ncomp = nt * (nt + 1) // 2
+    rphi = v[pos:pos + ncomp * nr].reshape(ncomp, nr).copy()
+    return dict(nr=nr, dr=dr, nrho=nrho, drho=drho, F=F, rho=rho, rphi=rphi)
+
+
+def read_fs_coeffs(path, nt):
+    rows = []
+    with open(path) as fp:
+        for ln in fp:
+            t = ln.split("#")[0].split()
+            if t:
+                rows.append(t)
+    rows = rows[1:]
+    A = np.array([float(r[0]) for r in rows[:nt]])
+    rows = rows[nt:]
+    t1 = np.array([float(r[0]) for r in rows[:nt * nt]])
+    t2 = np.array([float(r[1]) for r in rows[:nt * nt]])
+    rows = rows[nt * nt:]
+    ncomp = nt * (nt + 1) // 2
+    vals = {}
+    k = 0
+    for i in range(nt):
+        for j in range(i, nt):
+            vals[j * (j + 1) // 2 + i] = [float(x) for x in rows[k]]
+            k += 1
+    arr = np.array([vals[q] for q in range(ncomp)])
+    return dict(A=A, t1=t1, t2=t2, cut_rho=arr[:, 0].copy(), cut_phi=arr[:, 1].copy(), k1=arr[:, 2].copy(),
+                k2=arr[:, 3].copy(), k3=arr[:, 4].copy(), chk=np.ones(ncomp, dtype=np.int32))
+
+
+class Oracle:
+    """One restated MAPP system (Atoms + Neighbor + ForceField)."""
+
+    def __init__(self, workload: dict):
+        L = lib()
+        self.w = workload
+        cfg = workload["cfg"]
+        self.cfg = cfg
+        self.style = workload["style"]
+        self.nt = len(cfg.names)
+        self.dmd = cfg.dmd
+        self.h = L.orc_new(STYLES[self.style], self.nt)
+        coef = workload["coef"]
+        if self.style == "EAM":
+            t = read_eam_file(coef[2], self.nt, coef[1] == "FS")
+            L.orc_set_tables(self.h, t["nr"], t["dr"], t["nrho"], t["drho"], int(coef[1] == "FS"),
+                             np.ascontiguousarray(t["F"]), np.ascontiguousarray(t["rho"]), np.ascontiguousarray(t["rphi"]))
+        elif self.style == "FS":
+            c = read_fs_coeffs(coef[1], self.nt)
+            L.orc_set_fs(self.h, c["A"], c["t1"], c["t2"], c["cut_rho"], c["cut_phi"], c["k1"], c["k2"], c["k3"], c["chk"])
+        else:
+            t = read_eam_file(coef[7], self.nt, coef[6] == "FS")
+            L.orc_set_tables(self.h, t["nr"], t["dr"], t["nrho"], t["drho"], int(coef[6] == "FS"),
+                             np.ascontiguousarray(t["F"]), np.ascontiguousarray(t["rho"]), np.ascontiguousarray(t["rphi"]))
+            L.orc_set_dmd(self.h, float(coef[1]), int(coef[2]), float(coef[3]), float(coef[4]), float(coef[5]),
+                          np.asarray(cfg.masses, dtype=np.float64))
+        H = np.ascontiguousarray(cfg.H().ravel())
+        skin = float(workload.get("skin", 0.5))
+        if self.dmd:
+            x = np.ascontiguousarray(cfg.x_dmd())
+            c = np.ascontiguousarray(cfg.c)
+            L.orc_set_atoms(self.h, cfg.natms, H, skin, x, None, c.ctypes.data)
+            self._keep = (x, c)
+        else:
+            from mapp_b200.fixtures import md_order
+            order = md_order(cfg)
+            s = np.ascontiguousarray(cfg.s[order])
+            ty = np.ascontiguousarray(cfg.type[order].astype(np.int32))
+            L.orc_set_atoms(self.h, cfg.natms, H, skin, s, ty.ctypes.data, None)
+            self._keep = (s, ty)
+        L.orc_init(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_free(self.h)
+            self.h = None
+
+    @property
+    def x_dim(self):
+        return 3 + self.nt if self.dmd else 3
+
+    def counts(self):
+        out = np.zeros(5, dtype=np.int32)
+        lib().orc_counts(self.h, out)
+        return dict(natms=int(out[0]), nph=int(out[1]), npairs=int(out[2]), tot_bin=int(out[3]), comm_need=int(out[4]))
+
+    def x_all(self):
+        c = self.counts()
+        x = np.zeros((c["natms"] + c["nph"]) * self.x_dim)
+        lib().orc_get_x(self.h, x)
+        return x.reshape(-1, self.x_dim)
+
+    def neighbor_list(self):
+        c = self.counts()
+        ns = np.zeros(c["natms"], dtype=np.int32)
+        fl = np.zeros(max(c["npairs"], 1), dtype=np.int32)
+        lib().orc_get_list(self.h, ns, fl)
+        return ns, fl[:c["npairs"]]
+
+    def ghost_src(self):
+        c = self.counts()
+        g = np.zeros(max(c["nph"], 1), dtype=np.int32)
+        lib().orc_get_ghost_src(self.h, g)
+        return g[:c["nph"]]
+
+    def force(self, st_clc=1):
+        c = self.counts()
+        f = np.zeros(c["natms"] * self.x_dim)
+        en = np.zeros(7)
+        lib().orc_force(self.h, st_clc, f, en)
+        return f.reshape(-1, self.x_dim), en
+
+    def energy(self):
+        return lib().orc_energy(self.h)
+
+    def update_x(self, x):
+        r = C.c_int(0)
+        lib().orc_update_x(self.h, np.ascontiguousarray(x, dtype=np.float64).ravel(), C.byref(r))
+        return r.value
+
+    def update_c(self, c):
+        lib().orc_update_c(self.h, np.ascontiguousarray(c, dtype=np.float64).ravel())
+
+    def crd(self):
+        lib().orc_create_2nd_neigh_lst(self.h)
+        c = self.counts()
+        crd = np.zeros(c["natms"] + c["nph"], dtype=np.int32)
+        lib().orc_get_crd(self.h, crd, None, None)
+        return crd
+
+    def c_d(self):
+        c = self.counts()
+        out = np.zeros(c["natms"] * self.nt)
+        lib().orc_c_d_calc(self.h, out)
+        return out.reshape(-1, self.nt)
+
+    def calc_g(self, a, alpha, chk=0):
+        c = self.counts()
+        g = np.zeros(c["natms"] * self.nt)
+        cost = lib().orc_calc_g(self.h, chk, alpha, np.ascontiguousarray(a, dtype=np.float64).ravel(), g)
+        return cost, g.reshape(-1, self.nt)
+
+    def vec(self, which):
+        c = self.counts()
+        n = c["natms"] + c["nph"]
+        out = np.zeros(n * (1 if which == 4 else self.nt))
+        lib().orc_get_vec(self.h, which, out)
+        return out
+
+    def pairs(self):
+        c = self.counts()
+        nt = self.nt
+        n0, n1 = c["npairs"] * nt * nt, c["npairs"] * nt * (nt + 1) // 2
+        out = np.zeros(3 * n0 + 3 * n1)
+        lib().orc_get_pairs(self.h, out)
+        return out
