@@ -1,0 +1,138 @@
+/*
+ * mapp_b200 -- B200-native force-field hot path of MAPP, behind a C ABI.
+ *
+ * One mg_system is one MAPP single-rank system (Atoms + Neighbor + ForceField)
+ * resident on one GPU.  Entry points mirror the reference's own boundary:
+ *
+ *   ForceField  (ff.h:12-29)          coef / init / force_calc / energy_calc /
+ *                                     create_2nd_neigh_lst / c_d_calc / calc_g / fin
+ *   Neighbor    (neighbor.h:46-58)    create_list, neighbor_list, no_pairs
+ *   Atoms       (atoms.h:255-287)     H / skin / per-atom vectors, update_0, update(c)
+ *
+ * so a MAPP ForceField subclass can forward its virtuals one-to-one (see
+ * INTEGRATION.md).  Conventions:
+ *   - every function returns MG_OK (0) or an MG_ERR_* code; mg_last_error()
+ *     returns the message of the last failure on the calling thread (the
+ *     reference prints the same text and exits, error.cpp:29-43);
+ *   - array arguments may be host or device memory (detected per call);
+ *     host arrays are copied through the system's stream;
+ *   - per-atom arrays use the reference's layouts: x is natms * x_dim with
+ *     x_dim = 3 (EAM, FS) or 3 + ntypes (DMD: x y z alpha_1..alpha_n),
+ *     c is natms * ntypes, type is natms ints, f has the layout of x;
+ *   - en_st receives 7 doubles if st_clc != 0 (energy, then the virial
+ *     xx yy zz yz zx xy as in ff_eam.cpp:150-155), else 1.
+ */
+#ifndef MAPP_B200_H
+#define MAPP_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mg_system mg_system;
+
+#define MG_OK 0
+#define MG_ERR_ARG 1          /* bad argument (style name, sizes, null pointer)   */
+#define MG_ERR_FILE 2         /* potential file cannot be opened                  */
+#define MG_ERR_FORMAT 3       /* potential file malformed / ended prematurely     */
+#define MG_ERR_STATE 4        /* call out of order (e.g. force before init)       */
+#define MG_ERR_CUDA 5         /* CUDA runtime error                               */
+#define MG_ERR_CAPACITY 6     /* a device buffer limit could not be met          */
+#define MG_ERR_UNSUPPORTED 7  /* feature not available for this style / form      */
+#define MG_ERR_TIMEOUT 8      /* a bounded device-side wait ran out               */
+
+#define MG_FORM_FP64 0        /* plain form: FP64 arithmetic throughout            */
+#define MG_FORM_FP32 1        /* precision form: FP32 pair/quadrature/spline,
+                                 Kahan-compensated per-site sums, FP64 totals      */
+#define MG_FORM_MLP 2         /* learned form: BF16 MLP replaces DMD quadrature    */
+
+/* ---- library ---------------------------------------------------------- */
+const char* mg_last_error(void);
+int mg_version(void);
+
+/* ---- lifecycle -------------------------------------------------------- */
+/* style: a ForceField style name of ff_styles.h: "EAM", "FS", "DMD_I",
+   "DMD_II" or "DMD" (MAPP::ff_style, MAPP.cpp:243-264). */
+int mg_create(const char* style, int device, mg_system** out);
+int mg_destroy(mg_system* s);
+int mg_set_stream(mg_system* s, void* cuda_stream);
+int mg_set_form(mg_system* s, int form);
+
+/* ---- Atoms ------------------------------------------------------------ */
+/* AtomTypes::add_type (atom_types.cpp): names and masses in type order. */
+int mg_atoms_set_types(mg_system* s, int ntypes, const char* const* names, const double* masses);
+/* Atoms::H (atoms.h:266), 3x3 row-major, lower triangular as ReadCFG::set_box
+   leaves it (read_cfg.cpp:365-460); B = H^-1 is formed as M3INV (init.h:72). */
+int mg_atoms_set_box(mg_system* s, const double* H);
+/* Atoms::skin (atoms.cpp:19, 2908-2915); default 0.5. */
+int mg_atoms_set_skin(mg_system* s, double skin);
+/* Owned atoms in the state ReadCFG leaves them: vector 0 holds FRACTIONAL
+   coordinates s in [0,1) (plus alpha for DMD), then type (MD) or c (DMD). */
+int mg_atoms_set(mg_system* s, int natms, const double* x_frac, const int* type, const double* c);
+/* Atoms::update_0(0,1,...) (atoms.cpp:1780-1865) after the caller wrote the
+   owned Cartesian x (natms * x_dim): skin check against the positions at the
+   last rebuild, then either a ghost refresh or x2s + ghost build + list
+   rebuild.  *rebuilt (may be NULL) reports which. */
+int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt);
+/* Owned c written, then Atoms::update(c_n) ghost refresh. */
+int mg_atoms_update_c(mg_system* s, const double* c);
+/* Owned x (natms * x_dim, Cartesian; a rebuild wraps it into the box). */
+int mg_atoms_get_x(mg_system* s, double* x);
+/* Ghost ("phantom") atoms: x (natms_ph * x_dim) and the owned atom each one
+   images (natms_ph ints); either pointer may be NULL. */
+int mg_atoms_get_ghosts(mg_system* s, double* x, int* owner);
+
+/* ---- ForceField ------------------------------------------------------- */
+/* ForceField::coef(narg, arg) with the reference's arguments, arg[0] being
+   "ff_coef":  EAM  ff_coef {SetFL|FS|FuncFL} file...     (ff_eam.cpp:400-429)
+               FS   ff_coef file                          (ff_fs.cpp:113-335)
+               DMD* ff_coef r_crd n alpha_min alpha_max T {FS|SetFL|FuncFL} file...
+                                                          (ff_dmd_I.cpp:735-796) */
+int mg_ff_coef(mg_system* s, int narg, const char* const* arg);
+/* ForceField::init, then Atoms::ph_setup(1), Neighbor::init,
+   Neighbor::create_list(0,1), Atoms::store_0 -- the order every reference
+   caller uses (min_l-bfgs.cpp:178-182, md_nh.cpp:486-503, clock_bdf.cpp:223-236). */
+int mg_ff_init(mg_system* s);
+/* ForceField::force_calc (ff_eam.cpp:44, ff_fs.cpp:379, ff_dmd_I.cpp:88).
+   f receives the owned forces (natms * x_dim; DMD includes the alpha
+   components). f may be NULL to keep them on the device. */
+int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st);
+/* ForceField::energy_calc (ff_eam.cpp:268, ff_fs.cpp:609, ff_dmd_I.cpp:454). */
+int mg_ff_energy_calc(mg_system* s, double* energy);
+/* ForceField::create_2nd_neigh_lst (ff_dmd_I.cpp:2138-2217). */
+int mg_ff_create_2nd_neigh_lst(mg_system* s);
+/* ForceField::c_d_calc (ff_dmd_I.cpp:2241-2398); c_d receives natms * ntypes
+   (may be NULL). Uses the per-pair densities of the last force_calc. */
+int mg_ff_c_d_calc(mg_system* s, double* c_d);
+/* ForceField::calc_g (ff_dmd_I.cpp:2402-2674): a and g are natms * ntypes;
+   *cost receives the return value; chk != 0 computes the cost only. */
+int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g, double* cost);
+/* ForceField::fin (releases the per-pair scratch and FF vectors). */
+int mg_ff_fin(mg_system* s);
+
+/* ---- Neighbor --------------------------------------------------------- */
+/* Neighbor::create_list(0,1) preceded by x2s and a ghost rebuild, as the
+   rebuild branch of Atoms::update_0 runs it. */
+int mg_neighbor_create_list(mg_system* s);
+/* natms, natms_ph and Neighbor::no_pairs (any pointer may be NULL). */
+int mg_neighbor_counts(mg_system* s, int* natms, int* natms_ph, long long* no_pairs);
+/* Neighbor::neighbor_list_size (natms) and the concatenated per-atom half
+   lists (no_pairs ints, j > i, indices in the reference's owned+ghost index
+   space); the order inside one atom's list is unspecified. */
+int mg_neighbor_get_list(mg_system* s, int* sizes, int* pairs);
+
+/* ---- diagnostics ------------------------------------------------------ */
+/* Per-atom double vectors of the force field, owned + ghost entries:
+   "E", "dE", "ddE", "n", "c_d" (owned only), "rho" (EAM/FS: F'(rho)). */
+int mg_get_vector(mg_system* s, const char* name, double* out);
+/* Per-atom int vectors: "crd" (owned + ghost). */
+int mg_get_int_vector(mg_system* s, const char* name, int* out);
+/* Device time in ms of the last call of each phase, measured with CUDA events
+   on the system's stream: "list", "force", "energy", "c_d", "calc_g". */
+int mg_last_time(mg_system* s, const char* phase, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAPP_B200_H */

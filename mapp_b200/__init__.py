@@ -1,0 +1,269 @@
+"""mapp_b200: B200-native force-field hot path of MAPP (neighbour list,
+EAM / Finnis-Sinclair / DMD energies, forces and chemical potentials).
+
+The compute path is the CUDA library ``libmapp_b200.so`` (C ABI declared in
+``include/mapp_b200.h``).  This module is a thin ctypes mirror of that ABI,
+shaped like the reference's own objects: a :class:`System` holds one MAPP
+system (Atoms + Neighbor + ForceField) and exposes the ForceField virtuals
+(``coef``, ``init``, ``force_calc``, ``energy_calc``, ``create_2nd_neigh_lst``,
+``c_d_calc``, ``calc_g``) and the Atoms updates the reference's callers use
+(``update_0`` via :meth:`System.update_x`, ``update(c)`` via
+:meth:`System.update_c`).  There is no CPU path: without the library or a GPU
+every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmapp_b200.so")
+
+MG_FORM_FP64, MG_FORM_FP32, MG_FORM_MLP = 0, 1, 2
+ERRORS = {1: "ARG", 2: "FILE", 3: "FORMAT", 4: "STATE", 5: "CUDA", 6: "CAPACITY", 7: "UNSUPPORTED", 8: "TIMEOUT"}
+
+# Every exported entry point of include/mapp_b200.h with its ctypes signature.
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+SIGNATURES = {
+    "mg_last_error": (C.c_char_p, []),
+    "mg_version": (C.c_int, []),
+    "mg_create": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "mg_destroy": (C.c_int, [_P]),
+    "mg_set_stream": (C.c_int, [_P, _P]),
+    "mg_set_form": (C.c_int, [_P, C.c_int]),
+    "mg_atoms_set_types": (C.c_int, [_P, C.c_int, C.POINTER(C.c_char_p), _D]),
+    "mg_atoms_set_box": (C.c_int, [_P, _P]),
+    "mg_atoms_set_skin": (C.c_int, [_P, C.c_double]),
+    "mg_atoms_set": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "mg_atoms_update_x": (C.c_int, [_P, _P, _I]),
+    "mg_atoms_update_c": (C.c_int, [_P, _P]),
+    "mg_atoms_get_x": (C.c_int, [_P, _P]),
+    "mg_atoms_get_ghosts": (C.c_int, [_P, _P, _P]),
+    "mg_ff_coef": (C.c_int, [_P, C.c_int, C.POINTER(C.c_char_p)]),
+    "mg_ff_init": (C.c_int, [_P]),
+    "mg_ff_force_calc": (C.c_int, [_P, C.c_int, _P, _D]),
+    "mg_ff_energy_calc": (C.c_int, [_P, _D]),
+    "mg_ff_create_2nd_neigh_lst": (C.c_int, [_P]),
+    "mg_ff_c_d_calc": (C.c_int, [_P, _P]),
+    "mg_ff_calc_g": (C.c_int, [_P, C.c_int, C.c_double, _P, _P, _D]),
+    "mg_ff_fin": (C.c_int, [_P]),
+    "mg_neighbor_create_list": (C.c_int, [_P]),
+    "mg_neighbor_counts": (C.c_int, [_P, _I, _I, C.POINTER(C.c_longlong)]),
+    "mg_neighbor_get_list": (C.c_int, [_P, _P, _P]),
+    "mg_get_vector": (C.c_int, [_P, C.c_char_p, _P]),
+    "mg_get_int_vector": (C.c_int, [_P, C.c_char_p, _P]),
+    "mg_last_time": (C.c_int, [_P, C.c_char_p, _D]),
+}
+
+
+class MGError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mapp_b200 error {ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"mapp_b200 CUDA library not built ({path}); run python -m mapp_b200.build")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    """Pointer of a numpy array, a torch tensor (host or device) or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    raise TypeError(type(a))
+
+
+def _check(rc):
+    if rc != 0:
+        raise MGError(rc, load_library().mg_last_error().decode())
+
+
+class System:
+    """One MAPP system on one GPU, driven through the C ABI."""
+
+    def __init__(self, style: str, device: int = 0):
+        L = load_library()
+        h = C.c_void_p()
+        _check(L.mg_create(style.encode(), device, C.byref(h)))
+        self.h = h
+        self.style = style
+        self.dmd = style.startswith("DMD")
+        self.nt = 0
+        self.natms = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().mg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def x_dim(self):
+        return 3 + self.nt if self.dmd else 3
+
+    # ---- setup -----------------------------------------------------------
+    def set_types(self, names, masses):
+        self.nt = len(names)
+        arr = (C.c_char_p * len(names))(*[n.encode() for n in names])
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        _check(load_library().mg_atoms_set_types(self.h, len(names), arr, m.ctypes.data_as(_D)))
+
+    def set_box(self, H):
+        H = np.ascontiguousarray(H, dtype=np.float64).reshape(9)
+        _check(load_library().mg_atoms_set_box(self.h, H.ctypes.data))
+
+    def set_skin(self, skin):
+        _check(load_library().mg_atoms_set_skin(self.h, float(skin)))
+
+    def set_atoms(self, x_frac, type=None, c=None):
+        x = np.ascontiguousarray(x_frac, dtype=np.float64)
+        self.natms = x.shape[0]
+        t = None if type is None else np.ascontiguousarray(type, dtype=np.int32)
+        cc = None if c is None else np.ascontiguousarray(c, dtype=np.float64)
+        _check(load_library().mg_atoms_set(self.h, self.natms, _ptr(x), _ptr(t), _ptr(cc)))
+
+    def set_stream(self, stream_ptr: int):
+        _check(load_library().mg_set_stream(self.h, stream_ptr))
+
+    def set_form(self, form: int):
+        _check(load_library().mg_set_form(self.h, form))
+
+    def coef(self, args):
+        arr = (C.c_char_p * len(args))(*[a.encode() for a in args])
+        _check(load_library().mg_ff_coef(self.h, len(args), arr))
+
+    def init(self):
+        _check(load_library().mg_ff_init(self.h))
+
+    # ---- ForceField ------------------------------------------------------
+    def force_calc(self, st_clc=1, f=None):
+        """Returns (f, en_st); f may be a preallocated host/device buffer."""
+        out = f if f is not None else np.zeros((self.natms, self.x_dim))
+        en = np.zeros(7)
+        _check(load_library().mg_ff_force_calc(self.h, st_clc, _ptr(out), en.ctypes.data_as(_D)))
+        return out, (en if st_clc else en[:1])
+
+    def energy_calc(self):
+        e = C.c_double(0.0)
+        _check(load_library().mg_ff_energy_calc(self.h, C.byref(e)))
+        return e.value
+
+    def create_2nd_neigh_lst(self):
+        _check(load_library().mg_ff_create_2nd_neigh_lst(self.h))
+
+    def c_d_calc(self, out=None):
+        o = out if out is not None else np.zeros((self.natms, self.nt))
+        _check(load_library().mg_ff_c_d_calc(self.h, _ptr(o)))
+        return o
+
+    def calc_g(self, a, alpha, chk=0, g=None):
+        aa = a if not isinstance(a, np.ndarray) else np.ascontiguousarray(a, dtype=np.float64)
+        gg = g if g is not None else np.zeros((self.natms, self.nt))
+        cost = C.c_double(0.0)
+        _check(load_library().mg_ff_calc_g(self.h, chk, float(alpha), _ptr(aa), _ptr(gg), C.byref(cost)))
+        return cost.value, gg
+
+    def fin(self):
+        _check(load_library().mg_ff_fin(self.h))
+
+    # ---- Atoms -----------------------------------------------------------
+    def update_x(self, x):
+        xx = x if not isinstance(x, np.ndarray) else np.ascontiguousarray(x, dtype=np.float64)
+        r = C.c_int(0)
+        _check(load_library().mg_atoms_update_x(self.h, _ptr(xx), C.byref(r)))
+        return r.value
+
+    def update_c(self, c):
+        cc = c if not isinstance(c, np.ndarray) else np.ascontiguousarray(c, dtype=np.float64)
+        _check(load_library().mg_atoms_update_c(self.h, _ptr(cc)))
+
+    def get_x(self):
+        x = np.zeros((self.natms, self.x_dim))
+        _check(load_library().mg_atoms_get_x(self.h, x.ctypes.data))
+        return x
+
+    def counts(self):
+        n, g, p = C.c_int(0), C.c_int(0), C.c_longlong(0)
+        _check(load_library().mg_neighbor_counts(self.h, C.byref(n), C.byref(g), C.byref(p)))
+        return dict(natms=n.value, nph=g.value, npairs=p.value)
+
+    def ghosts(self):
+        c = self.counts()
+        x = np.zeros((c["nph"], self.x_dim))
+        o = np.zeros(c["nph"], dtype=np.int32)
+        _check(load_library().mg_atoms_get_ghosts(self.h, x.ctypes.data, o.ctypes.data))
+        return x, o
+
+    def neighbor_list(self):
+        c = self.counts()
+        sizes = np.zeros(self.natms, dtype=np.int32)
+        pairs = np.zeros(max(c["npairs"], 1), dtype=np.int32)
+        _check(load_library().mg_neighbor_get_list(self.h, sizes.ctypes.data, pairs.ctypes.data))
+        return sizes, pairs[:c["npairs"]]
+
+    def rebuild_list(self):
+        _check(load_library().mg_neighbor_create_list(self.h))
+
+    def vector(self, name):
+        n = self.natms * (1 if name == "rho" else self.nt)
+        out = np.zeros(n)
+        _check(load_library().mg_get_vector(self.h, name.encode(), out.ctypes.data))
+        return out
+
+    def crd(self):
+        c = self.counts()
+        out = np.zeros(c["natms"] + c["nph"], dtype=np.int32)
+        _check(load_library().mg_get_int_vector(self.h, b"crd", out.ctypes.data))
+        return out
+
+    def last_time(self, phase):
+        ms = C.c_double(0.0)
+        _check(load_library().mg_last_time(self.h, phase.encode(), C.byref(ms)))
+        return ms.value
+
+
+def system_from_workload(w: dict, device: int = 0, skin: float = 0.5) -> System:
+    """Build and init a System from a workload written by mapp_b200.fixtures."""
+    from .fixtures import md_order
+
+    cfg = w["cfg"]
+    s = System(w["style"], device)
+    s.set_types(cfg.names, cfg.masses)
+    s.set_box(cfg.H())
+    s.set_skin(skin)
+    if cfg.dmd:
+        s.set_atoms(cfg.x_dmd(), c=cfg.c)
+    else:
+        order = md_order(cfg)
+        s.set_atoms(cfg.s[order], type=cfg.type[order])
+    s.coef(w["coef"])
+    s.init()
+    return s

@@ -1,0 +1,1219 @@
+// Host side of the mapp_b200 C ABI: potential readers, spline construction,
+// cut-offs, ghost / neighbour-list rebuild orchestration and the ForceField
+// entry points.  Numbers that decide list membership (B, cut_ph_s, cut_sk_sq,
+// table coefficients) are computed here in plain IEEE double in the
+// reference's operation order, so they equal the reference's bit for bit.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/mapp_b200.h"
+#include "mg_internal.h"
+#include "mg_reduce.cuh"
+
+using namespace mg;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CU(call)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) return fail(MG_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                         \
+    } while (0)
+
+#define CHK(call)             \
+    do {                      \
+        int r_ = (call);      \
+        if (r_) return r_;    \
+    } while (0)
+
+template <class T>
+int dalloc(T** p, size_t n)
+{
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(MG_ERR_CAPACITY, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    }
+    return MG_OK;
+}
+
+// grow keeping the first `keep` elements
+template <class T>
+int dgrow(T** p, size_t n, size_t keep, cudaStream_t st)
+{
+    T* q = nullptr;
+    cudaError_t e = cudaMalloc((void**)&q, (n ? n : 1) * sizeof(T));
+    if (e != cudaSuccess) return fail(MG_ERR_CAPACITY, "cudaMalloc of %zu bytes failed", n * sizeof(T));
+    if (*p && keep) {
+        e = cudaMemcpyAsync(q, *p, keep * sizeof(T), cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return fail(MG_ERR_CUDA, "grow copy: %s", cudaGetErrorString(e));
+        cudaStreamSynchronize(st);
+    }
+    if (*p) cudaFree(*p);
+    *p = q;
+    return MG_OK;
+}
+
+bool is_device_ptr(const void* p)
+{
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// ---- splines: interpolate (ff_eam.cpp:1323-1352) and interpolate_m
+// (ff_dmd_I.cpp:1794-1836), on rows of `w` doubles ---------------------------
+void spline_cubic(int n, double delta, double* s, int w)
+{
+    auto S = [&](int i, int k) -> double& { return s[(size_t)i * w + k]; };
+    S(0, 1) = S(1, 0) - S(0, 0);
+    S(1, 1) = 0.5 * (S(2, 0) - S(0, 0));
+    S(n - 2, 1) = 0.5 * (S(n - 1, 0) - S(n - 3, 0));
+    S(n - 1, 1) = S(n - 1, 0) - S(n - 2, 0);
+    for (int i = 2; i < n - 2; i++) S(i, 1) = ((S(i - 2, 0) - S(i + 2, 0)) + 8.0 * (S(i + 1, 0) - S(i - 1, 0))) / 12.0;
+    for (int i = 0; i < n - 1; i++) {
+        S(i, 2) = 3.0 * (S(i + 1, 0) - S(i, 0)) - 2.0 * S(i, 1) - S(i + 1, 1);
+        S(i, 3) = S(i, 1) + S(i + 1, 1) - 2.0 * (S(i + 1, 0) - S(i, 0));
+    }
+    S(n - 1, 2) = 0.0;
+    S(n - 1, 3) = 0.0;
+}
+
+void spline7(int n, double delta, double* s, int w)
+{
+    spline_cubic(n, delta, s, w);
+    for (int i = 0; i < n; i++) {
+        s[(size_t)i * w + 4] = s[(size_t)i * w + 1] / delta;
+        s[(size_t)i * w + 5] = 2.0 * s[(size_t)i * w + 2] / delta;
+        s[(size_t)i * w + 6] = 3.0 * s[(size_t)i * w + 3] / delta;
+    }
+}
+
+void spline9(int n, double delta, double* s, int w)
+{
+    spline_cubic(n, delta, s, w);
+    auto S = [&](int i, int k) -> double& { return s[(size_t)i * w + k]; };
+    for (int i = 0; i < n - 1; i++) S(i, 4) = (S(i + 1, 2) - S(i, 2)) / 6.0 - 0.5 * S(i, 3);
+    S(n - 1, 4) = 0.0;
+    for (int i = 0; i < n; i++) {
+        S(i, 5) = S(i, 1) / delta;
+        S(i, 6) = 2.0 * S(i, 2) / delta;
+        S(i, 7) = 3.0 * S(i, 3) / delta;
+        S(i, 8) = 4.0 * S(i, 4) / delta;
+    }
+}
+
+// Gauss-Hermite nodes and weights for weight exp(-x^2), by Newton iteration on
+// the orthonormal Hermite recurrence (Golub-Welsch initial guesses as in the
+// classical "gauher" routine), long double, ascending order.
+void gauss_hermite(int n, double* x_out, double* w_out)
+{
+    const long double pim4 = 0.7511255444649425L;
+    long double x[kMaxQuad], w[kMaxQuad], z = 0, z1, p1, p2, p3, pp = 0;
+    int m = (n + 1) / 2;
+    for (int i = 0; i < m; i++) {
+        if (i == 0) z = sqrtl((long double)(2 * n + 1)) - 1.85575L * powl((long double)(2 * n + 1), -0.16667L);
+        else if (i == 1) z -= 1.14L * powl((long double)n, 0.426L) / z;
+        else if (i == 2) z = 1.86L * z - 0.86L * x[0];
+        else if (i == 3) z = 1.91L * z - 0.91L * x[1];
+        else z = 2.0L * z - x[i - 2];
+        for (int it = 0; it < 100; it++) {
+            p1 = pim4;
+            p2 = 0.0L;
+            for (int j = 0; j < n; j++) {
+                p3 = p2;
+                p2 = p1;
+                p1 = z * sqrtl(2.0L / (j + 1)) * p2 - sqrtl((long double)j / (j + 1)) * p3;
+            }
+            pp = sqrtl(2.0L * n) * p2;
+            z1 = z;
+            z = z1 - p1 / pp;
+            if (fabsl(z - z1) <= 1e-19L * fabsl(z)) break;
+        }
+        x[i] = z;
+        x[n - 1 - i] = -z;
+        w[i] = 2.0L / (pp * pp);
+        w[n - 1 - i] = w[i];
+    }
+    if (n % 2 == 1) x[m - 1] = 0.0L;
+    for (int i = 0; i < n; i++) {
+        x_out[i] = (double)x[n - 1 - i];
+        w_out[i] = (double)w[n - 1 - i];
+    }
+}
+
+// whitespace tokens of a line up to a '#' (MAPP::parse_line, MAPP.cpp:468-521)
+std::vector<std::string> tokens(const std::string& line)
+{
+    std::vector<std::string> out;
+    std::string s = line.substr(0, line.find('#'));
+    std::istringstream is(s);
+    std::string t;
+    while (is >> t) out.push_back(t);
+    return out;
+}
+
+}  // namespace
+
+struct mg_system {
+    int style = 0, form = MG_FORM_FP64, device = 0, nt = 0, x_dim = 3, dmd = 0;
+    std::vector<std::string> names;
+    std::vector<double> masses;
+    bool types_set = false, box_set = false, atoms_set = false, coef_set = false, initialized = false;
+    double H[3][3] = {{0}}, B[3][3] = {{0}}, skin = 0.5;
+    int natms = 0;
+    // tables (host, built by coef)
+    int nr = 0, nrho = 0;
+    double dr = 0, drho = 0;
+    std::vector<double> rhoT, phiT, FT;  // device layouts
+    int Fw = 7;
+    // FS analytic
+    std::vector<double> fsA, fst1, fst2, fs_cut_rho, fs_cut_phi, fsk1, fsk2, fsk3;
+    std::vector<int> fs_chk;
+    // DMD
+    double rsq_crd = 0, alpha_min = 0, alpha_max = 0, T = 0;
+    int nq = 0;
+    double xi[kMaxQuad], w0[kMaxQuad];
+    // derived box/bins
+    int comm_need[3] = {1, 1, 1};
+    double tot_cut_ph = 0;
+    // device
+    Dev d;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    size_t cap = 0;          // per-atom capacity (owned + ghost)
+    int cap_bins = 0;
+    int* flags = nullptr;
+    int* offs = nullptr;
+    void* scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    double* stage = nullptr;  // device staging for host arrays
+    size_t stage_cap = 0;
+    double* red_out = nullptr;  // 8 doubles
+    double* d_rhoT = nullptr;
+    double* d_phiT = nullptr;
+    double* d_FT = nullptr;
+    int* cursor = nullptr;
+    int crd_built = 0;
+    int npair_blocks = 2;
+    long long npairs = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double t_list = 0, t_force = 0, t_energy = 0, t_cd = 0, t_g = 0;
+    long long partial_rows = 0;
+};
+
+namespace {
+
+int check_sys(mg_system* s)
+{
+    if (!s) return fail(MG_ERR_ARG, "null mg_system");
+    if (cudaSetDevice(s->device) != cudaSuccess) return fail(MG_ERR_CUDA, "cudaSetDevice(%d) failed", s->device);
+    return MG_OK;
+}
+
+int stage_in(mg_system* s, const void* src, size_t bytes, const void** dev_out)
+{
+    if (is_device_ptr(src)) {
+        *dev_out = src;
+        return MG_OK;
+    }
+    if (bytes > s->stage_cap) {
+        CHK(dalloc((char**)&s->stage, bytes));
+        s->stage_cap = bytes;
+    }
+    CU(cudaMemcpyAsync(s->stage, src, bytes, cudaMemcpyHostToDevice, s->st));
+    *dev_out = s->stage;
+    return MG_OK;
+}
+
+int copy_out(mg_system* s, void* dst, const void* dev_src, size_t bytes)
+{
+    if (!dst || !bytes) return MG_OK;
+    cudaMemcpyKind k = is_device_ptr(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CU(cudaMemcpyAsync(dst, dev_src, bytes, k, s->st));
+    return MG_OK;
+}
+
+int ensure_partials(mg_system* s, long long rows)
+{
+    if (rows <= s->partial_rows) return MG_OK;
+    long long n = rows + rows / 4 + 64;
+    CHK(dalloc(&s->d.partial, (size_t)n * 8));
+    s->partial_rows = n;
+    return MG_OK;
+}
+
+// per-atom arrays (owned + ghost), keeping rebuild inputs
+int ensure_atoms(mg_system* s, size_t need, size_t keep)
+{
+    if (need <= s->cap) return MG_OK;
+    size_t cap = need + need / 2 + 1024;
+    int nt = s->nt;
+    Dev& d = s->d;
+    CHK(dgrow(&d.sfr, cap, keep, s->st));
+    CHK(dgrow(&d.alpha, cap * nt, keep * nt, s->st));
+    if (s->dmd) CHK(dgrow(&d.c, cap * nt, keep * nt, s->st));
+    else CHK(dgrow(&d.type, cap, keep, s->st));
+    CHK(dgrow(&d.root, cap, keep, s->st));
+    CHK(dgrow(&d.gchain, cap, keep, s->st));
+    CHK(dgrow(&d.pos, cap, keep, s->st));
+    CHK(dalloc(&d.bin, cap));
+    CHK(dalloc(&d.cell_pos, cap));
+    CHK(dalloc(&d.rho, cap));
+    CHK(dalloc(&d.E, cap * nt));
+    CHK(dalloc(&d.dE, cap * nt));
+    CHK(dalloc(&d.ddE, cap * nt));
+    CHK(dalloc(&d.n, cap * nt));
+    CHK(dalloc(&d.s, cap * nt));
+    CHK(dalloc(&d.t, cap * nt));
+    CHK(dalloc(&d.v, cap * nt));
+    CHK(dalloc(&d.crd, cap));
+    CHK(dalloc(&s->flags, cap));
+    CHK(dalloc(&s->offs, cap));
+    size_t tb = scan_temp_bytes((int)cap);
+    if (tb > s->scan_tmp_bytes) {
+        CHK(dalloc((char**)&s->scan_tmp, tb));
+        s->scan_tmp_bytes = tb;
+    }
+    s->cap = cap;
+    return MG_OK;
+}
+
+int ensure_pairs(mg_system* s, int maxnb)
+{
+    Dev& d = s->d;
+    size_t np = (size_t)s->natms * maxnb;
+    CHK(dalloc(&d.nbr, np));
+    CHK(dalloc(&d.pr, np * s->npair_blocks));
+    d.maxnb = maxnb;
+    d.maxp = (long long)np;
+    return MG_OK;
+}
+
+void fill_dev_scalars(mg_system* s)
+{
+    Dev& d = s->d;
+    d.natms = s->natms;
+    d.nt = s->nt;
+    d.x_dim = s->x_dim;
+    d.style = s->style;
+    d.form = s->form;
+    memcpy(d.H, s->H, sizeof(d.H));
+    memcpy(d.B, s->B, sizeof(d.B));
+}
+
+// ForceField::init cut-offs (ff_eam.cpp:360-371, ff_fs.cpp:339-352,
+// ff_dmd_I.cpp:672-682) and Atoms::set_ph (atoms.cpp:249-278); returns ph_cut.
+void compute_cutoffs(mg_system* s)
+{
+    Dev& d = s->d;
+    double skin = s->skin, ph_cut = 0.0;
+    int nt = s->nt, ncomp = nt * (nt + 1) / 2;
+    if (s->style == STYLE_EAM) {
+        for (int i = 0; i < ncomp; i++) d.cut_sk_sq[i] = d.cut_sq + (skin) * (skin) + 2 * sqrt(d.cut_sq) * (skin);
+        ph_cut = sqrt(d.cut_sq);
+    } else if (s->style == STYLE_FS) {
+        for (int i = 0; i < ncomp; i++)
+            if (d.fs_chk[i]) {
+                double a = d.fs_cut_phi[i] * d.fs_cut_phi[i], b = d.fs_cut_rho[i] * d.fs_cut_rho[i];
+                d.fs_cut_sq[i] = a > b ? a : b;
+                d.cut_sk_sq[i] = d.fs_cut_sq[i] + (skin) * (skin) + 2 * sqrt(d.fs_cut_sq[i]) * (skin);
+                double c = sqrt(d.fs_cut_sq[i]);
+                ph_cut = ph_cut > c ? ph_cut : c;
+            } else {
+                d.fs_cut_sq[i] = 0.0;
+                d.cut_sk_sq[i] = 0.0;
+            }
+    } else {
+        for (int i = 0; i < ncomp; i++)
+            d.cut_sk_sq[i] = d.cut_sq_mod + (skin) * (skin) + 2.0 * sqrt(d.cut_sq_mod) * (skin);
+        ph_cut = sqrt(d.cut_sq_mod);
+    }
+    s->tot_cut_ph = ph_cut + skin;
+    for (int i = 0; i < 3; i++) {
+        double tmp = 0.0;
+        for (int j = i; j < 3; j++) tmp += s->B[j][i] * s->B[j][i];
+        d.cut_ph_s[i] = s->tot_cut_ph * sqrt(tmp);
+    }
+    for (int i = 0; i < 3; i++) {
+        d.s_ph_hi[i] = 1.0 - d.cut_ph_s[i];
+        d.s_ph_lo[i] = 0.0 + d.cut_ph_s[i];
+    }
+    for (int i = 0; i < 3; i++) s->comm_need[i] = (int)(d.cut_ph_s[i] / (1.0 - 0.0)) + 1;
+    // Neighbor::create_bin_list (neighbor.cpp:311-330)
+    d.tot_bin = 1;
+    for (int i = 0; i < 3; i++) {
+        d.grid[i] = (int)((2.0 * d.cut_ph_s[i] + 1.0 - 0.0) / d.cut_ph_s[i]) + 1;
+        d.tot_bin *= d.grid[i];
+    }
+    for (int i = 0; i < 3; i++) {
+        int no = 1;
+        for (int j = 0; j < i; j++) no *= d.grid[j];
+        d.denom[i] = no;
+    }
+}
+
+// Atoms::ph_setup (atoms.cpp:317-372), then binning, s2x and the half list.
+// Expects d.sfr (owned, fractional) and root/gchain of owned atoms set.
+int rebuild(mg_system* s)
+{
+    Dev& d = s->d;
+    cudaStream_t st = s->st;
+    CU(cudaEventRecord(s->ev0, st));
+    int natms = s->natms, nph = 0;
+    int lo_dim = 0, hi_dim = natms;
+    fill_dev_scalars(s);
+    CU(cudaMemsetAsync(d.status, 0, 8 * sizeof(int), st));
+    for (int dim = 0; dim < 3; dim++) {
+        for (int dir = 0; dir < 2; dir++) {
+            int lo = lo_dim, hi = hi_dim;
+            for (int pass = 0; pass < s->comm_need[dim]; pass++) {
+                int tmp_r = natms + nph;
+                int n = hi - lo;
+                int count = 0;
+                if (n > 0) {
+                    d.nph = nph;
+                    d.nall = natms + nph;
+                    CU(launch_ghost_flags(d, lo, hi, dim, dir, s->flags, st));
+                    CU(launch_exclusive_scan(s->flags, s->offs, n, s->scan_tmp, s->scan_tmp_bytes, st));
+                    int last[2];
+                    CU(cudaMemcpyAsync(&last[0], s->offs + n - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+                    CU(cudaMemcpyAsync(&last[1], s->flags + n - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+                    CU(cudaStreamSynchronize(st));
+                    count = last[0] + last[1];
+                    if ((size_t)(natms + nph + count) > s->cap) {
+                        // flags/offs are reallocated by ensure_atoms: recompute them after growing
+                        CHK(ensure_atoms(s, natms + nph + count, natms + nph));
+                        CU(launch_ghost_flags(d, lo, hi, dim, dir, s->flags, st));
+                        CU(launch_exclusive_scan(s->flags, s->offs, n, s->scan_tmp, s->scan_tmp_bytes, st));
+                    }
+                    CU(launch_ghost_scatter(d, lo, hi, dim, dir, s->flags, s->offs, natms + nph, st));
+                }
+                nph += count;
+                hi = natms + nph;
+                lo = tmp_r;
+            }
+        }
+        lo_dim = 0;
+        hi_dim = natms + nph;
+    }
+    d.nph = nph;
+    d.nall = natms + nph;
+    int st_h[8];
+    CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (st_h[4]) return fail(MG_ERR_CAPACITY, "ghost image chain deeper than %d swaps (box too small for the cut-off)", kMaxChain);
+    // bins
+    if (d.tot_bin + 1 > s->cap_bins) {
+        CHK(dalloc(&d.cell_count, d.tot_bin + 1));
+        CHK(dalloc(&d.cell_start, d.tot_bin + 1));
+        CHK(dalloc(&s->cursor, d.tot_bin + 1));
+        s->cap_bins = d.tot_bin + 1;
+        size_t tb = scan_temp_bytes(d.tot_bin + 1);
+        if (tb > s->scan_tmp_bytes) {
+            CHK(dalloc((char**)&s->scan_tmp, tb));
+            s->scan_tmp_bytes = tb;
+        }
+    }
+    CU(cudaMemsetAsync(d.cell_count, 0, (d.tot_bin + 1) * sizeof(int), st));
+    CU(launch_bin_and_s2x(d, st));
+    CU(launch_exclusive_scan(d.cell_count, d.cell_start, d.tot_bin + 1, s->scan_tmp, s->scan_tmp_bytes, st));
+    CU(cudaMemsetAsync(s->cursor, 0, (d.tot_bin + 1) * sizeof(int), st));
+    CU(launch_cell_fill(d, s->cursor, st));
+    // half list, growing the per-atom capacity on overflow
+    for (int attempt = 0; attempt < 4; attempt++) {
+        CU(cudaMemsetAsync(d.status, 0, 8 * sizeof(int), st));
+        CU(launch_neigh(d, st));
+        CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        if (!st_h[0]) break;
+        int need = st_h[1] + 16;
+        CHK(ensure_pairs(s, need));
+        if (attempt == 3) return fail(MG_ERR_CAPACITY, "neighbour list capacity could not be met");
+    }
+    CU(launch_store_x0(d, st));
+    s->crd_built = 0;
+    CU(cudaEventRecord(s->ev1, st));
+    CU(cudaEventSynchronize(s->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    s->t_list = ms;
+    return MG_OK;
+}
+
+int reduce_to_host(mg_system* s, int rows, int nvals, double* out)
+{
+    CU(launch_reduce_partials(s->d, rows, nvals, s->red_out, s->st));
+    CU(cudaMemcpyAsync(out, s->red_out, nvals * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return MG_OK;
+}
+
+// ---- potential readers -----------------------------------------------------
+
+int read_all(const char* path, std::vector<std::string>& lines)
+{
+    std::ifstream in(path);
+    if (!in) return fail(MG_ERR_FILE, "file %s not found", path);
+    std::string ln;
+    while (std::getline(in, ln)) lines.push_back(ln);
+    return MG_OK;
+}
+
+// setfl / FS table files (ff_eam.cpp:674-879, 883-1108; ff_dmd_I.cpp:1300-1548):
+// four lines (the 4th lists the file's elements), "Nrho drho Nr dr cut", one
+// element header line, then the values.
+int read_tables(mg_system* s, const char* path, bool fs_layout)
+{
+    std::vector<std::string> lines;
+    CHK(read_all(path, lines));
+    if (lines.size() < 6) return fail(MG_ERR_FORMAT, "eam potential file ended immaturely");
+    std::vector<std::string> el = tokens(lines[3]);
+    int nt = s->nt;
+    if ((int)el.size() < 2 || (int)el.size() - 1 < nt) return fail(MG_ERR_FORMAT, "wrong format in eam potential file");
+    int tot = (int)el.size() - 1;
+    std::vector<int> fe(nt);
+    for (int a = 0; a < nt; a++) {
+        int k = 0;
+        while (k < tot && el[k + 1] != s->names[a]) k++;
+        if (k == tot) return fail(MG_ERR_FORMAT, "atom type not found in eam file");
+        fe[a] = k;
+    }
+    std::vector<std::string> h = tokens(lines[4]);
+    if (h.size() != 5) return fail(MG_ERR_FORMAT, "wrong format in eam potential file");
+    int nrho = atoi(h[0].c_str()), nr = atoi(h[2].c_str());
+    double drho = atof(h[1].c_str()), dr = atof(h[3].c_str());
+    if (nr < 5 || nrho < 5) return fail(MG_ERR_FORMAT, "table sizes too small (nr=%d nrho=%d)", nr, nrho);
+    std::vector<double> v;
+    size_t need = fs_layout ? (size_t)tot * nrho + (size_t)tot * tot * nr + (size_t)tot * (tot + 1) / 2 * nr
+                            : (size_t)tot * (nrho + nr) + (size_t)tot * (tot + 1) / 2 * nr;
+    v.reserve(need);
+    for (size_t li = 6; li < lines.size() && v.size() < need; li++)
+        for (const std::string& t : tokens(lines[li])) v.push_back(strtod(t.c_str(), nullptr));
+    if (v.size() < need) return fail(MG_ERR_FORMAT, "eam potential file ended immaturely");
+    s->nr = nr;
+    s->nrho = nrho;
+    s->dr = dr;
+    s->drho = drho;
+    s->Fw = s->dmd ? 9 : 7;
+    int ncomp = nt * (nt + 1) / 2;
+    s->FT.assign((size_t)nt * (nrho + 1) * s->Fw, 0.0);
+    s->rhoT.assign((size_t)nt * nt * nr * 8, 0.0);
+    s->phiT.assign((size_t)ncomp * nr * 8, 0.0);
+    // offsets of each file element's blocks
+    size_t per_el = fs_layout ? (size_t)nrho + (size_t)tot * nr : (size_t)nrho + nr;
+    size_t phi0 = per_el * tot;
+    auto phi_off = [&](int e1, int e2) {  // e1 >= e2
+        return phi0 + ((size_t)e1 * (e1 + 1) / 2 + e2) * nr;
+    };
+    for (int a = 0; a < nt; a++) {
+        const double* Fsrc = v.data() + per_el * fe[a];
+        double* Fd = s->FT.data() + (size_t)a * (nrho + 1) * s->Fw;
+        for (int k = 0; k < nrho; k++) Fd[(size_t)k * s->Fw] = Fsrc[k];
+        if (s->dmd) spline9(nrho, drho, Fd, s->Fw);
+        else spline7(nrho, drho, Fd, s->Fw);
+    }
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b < nt; b++) {
+            // density slot b*nt+a: FS block [a][b]; setfl: the source element's
+            // single density, aliased to every slot of that element
+            const double* src = fs_layout ? v.data() + per_el * fe[a] + nrho + (size_t)fe[b] * nr
+                                          : v.data() + per_el * fe[a] + nrho;
+            double* dst = s->rhoT.data() + (size_t)(b * nt + a) * nr * 8;
+            for (int k = 0; k < nr; k++) dst[(size_t)k * 8] = src[k];
+            spline7(nr, dr, dst, 8);
+        }
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b <= a; b++) {
+            int e1 = fe[a] > fe[b] ? fe[a] : fe[b], e2 = fe[a] > fe[b] ? fe[b] : fe[a];
+            const double* src = v.data() + phi_off(e1, e2);
+            double* dst = s->phiT.data() + (size_t)comp_idx(a, b) * nr * 8;
+            for (int k = 0; k < nr; k++) dst[(size_t)k * 8] = src[k];
+            spline7(nr, dr, dst, 8);
+        }
+    return MG_OK;
+}
+
+// analytic FS coefficient file (ff_fs.cpp:113-335)
+int read_fs_coeffs(mg_system* s, const char* path)
+{
+    std::vector<std::string> lines;
+    CHK(read_all(path, lines));
+    std::vector<std::vector<std::string>> rows;
+    for (const std::string& l : lines) {
+        std::vector<std::string> t = tokens(l);
+        if (!t.empty()) rows.push_back(t);
+    }
+    int nt = s->nt, ncomp = nt * (nt + 1) / 2;
+    size_t r = 0;
+    if (rows.empty() || (int)rows[0].size() != nt)
+        return fail(MG_ERR_FORMAT, "number of types represented and forcefield do not match");
+    std::vector<int> types(nt);
+    for (int i = 0; i < nt; i++) {
+        int k = 0;
+        while (k < nt && s->names[k] != rows[0][i]) k++;
+        if (k == nt) return fail(MG_ERR_FORMAT, "atom type %s not found", rows[0][i].c_str());
+        types[i] = k;
+    }
+    r = 1;
+    Dev& d = s->d;
+    for (int i = 0; i < nt; i++, r++) {
+        if (r >= rows.size() || rows[r].size() != 1) return fail(MG_ERR_FORMAT, "Wrong format in the force filed file");
+        d.fsA[types[i]] = atof(rows[r][0].c_str());
+    }
+    for (int i = 0; i < nt; i++)
+        for (int j = 0; j < nt; j++, r++) {
+            if (r >= rows.size() || rows[r].size() != 2) return fail(MG_ERR_FORMAT, "Wrong format in the force filed file");
+            d.fst1[types[i]][types[j]] = atof(rows[r][0].c_str());
+            d.fst2[types[i]][types[j]] = atof(rows[r][1].c_str());
+        }
+    for (int q = 0; q < 16; q++) d.fs_chk[q] = 0;
+    for (int i = 0; i < nt; i++)
+        for (int j = i; j < nt; j++, r++) {
+            if (r >= rows.size() || rows[r].size() != 5) return fail(MG_ERR_FORMAT, "Wrong format in the force filed file");
+            int c = comp_idx(types[i], types[j]);
+            d.fs_cut_rho[c] = atof(rows[r][0].c_str());
+            d.fs_cut_phi[c] = atof(rows[r][1].c_str());
+            d.fsk1[c] = atof(rows[r][2].c_str());
+            d.fsk2[c] = atof(rows[r][3].c_str());
+            d.fsk3[c] = atof(rows[r][4].c_str());
+            d.fs_chk[c] = 1;
+        }
+    (void)ncomp;
+    return MG_OK;
+}
+
+int upload_tables(mg_system* s)
+{
+    Dev& d = s->d;
+    if (s->style == STYLE_FS) return MG_OK;
+    CHK(dalloc(&s->d_rhoT, s->rhoT.size()));
+    CHK(dalloc(&s->d_phiT, s->phiT.size()));
+    CHK(dalloc(&s->d_FT, s->FT.size()));
+    CU(cudaMemcpy(s->d_rhoT, s->rhoT.data(), s->rhoT.size() * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_phiT, s->phiT.data(), s->phiT.size() * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_FT, s->FT.data(), s->FT.size() * 8, cudaMemcpyHostToDevice));
+    d.rhoT = s->d_rhoT;
+    d.phiT = s->d_phiT;
+    d.FT = s->d_FT;
+    d.Fw = s->Fw;
+    d.nr = s->nr;
+    d.nrho = s->nrho;
+    d.dr = s->dr;
+    d.drho = s->drho;
+    d.dr_inv = 1.0 / s->dr;
+    d.drho_inv = 1.0 / s->drho;
+    return MG_OK;
+}
+
+int timed_begin(mg_system* s)
+{
+    CU(cudaEventRecord(s->ev0, s->st));
+    return MG_OK;
+}
+
+int timed_end(mg_system* s, double* slot)
+{
+    CU(cudaEventRecord(s->ev1, s->st));
+    CU(cudaEventSynchronize(s->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    *slot = ms;
+    return MG_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+const char* mg_last_error(void) { return g_err.c_str(); }
+
+int mg_version(void) { return 100; }
+
+int mg_create(const char* style, int device, mg_system** out)
+{
+    if (!style || !out) return fail(MG_ERR_ARG, "null argument");
+    int st;
+    if (!strcmp(style, "EAM")) st = STYLE_EAM;
+    else if (!strcmp(style, "FS")) st = STYLE_FS;
+    else if (!strcmp(style, "DMD_I")) st = STYLE_DMD_I;
+    else if (!strcmp(style, "DMD_II")) st = STYLE_DMD_II;
+    else if (!strcmp(style, "DMD")) st = STYLE_DMD;
+    else return fail(MG_ERR_ARG, "unknown forcefield: %s", style);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(MG_ERR_CUDA, "no CUDA device available: the mapp_b200 library has no CPU path");
+    }
+    if (device < 0 || device >= ndev) return fail(MG_ERR_ARG, "device %d out of range", device);
+    mg_system* s = new mg_system();
+    s->style = st;
+    s->dmd = st >= STYLE_DMD_I;
+    s->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete s;
+        return fail(MG_ERR_CUDA, "cudaSetDevice failed");
+    }
+    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete s;
+        return fail(MG_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    s->own_stream = true;
+    cudaEventCreate(&s->ev0);
+    cudaEventCreate(&s->ev1);
+    memset(&s->d, 0, sizeof(Dev));
+    int r = dalloc(&s->d.status, 8);
+    if (!r) r = dalloc(&s->red_out, 8);
+    if (r) {
+        delete s;
+        return r;
+    }
+    *out = s;
+    return MG_OK;
+}
+
+int mg_destroy(mg_system* s)
+{
+    if (!s) return MG_OK;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->st);
+    Dev& d = s->d;
+    void* ptrs[] = {d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
+                    d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
+                    d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status,
+                    s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->own_stream && s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return MG_OK;
+}
+
+int mg_set_stream(mg_system* s, void* stream)
+{
+    CHK(check_sys(s));
+    cudaStreamSynchronize(s->st);
+    if (s->own_stream && s->st) cudaStreamDestroy(s->st);
+    s->st = (cudaStream_t)stream;
+    s->own_stream = false;
+    return MG_OK;
+}
+
+int mg_set_form(mg_system* s, int form)
+{
+    CHK(check_sys(s));
+    if (form != MG_FORM_FP64) return fail(MG_ERR_UNSUPPORTED, "form %d is not available in this build", form);
+    s->form = form;
+    return MG_OK;
+}
+
+int mg_atoms_set_types(mg_system* s, int ntypes, const char* const* names, const double* masses)
+{
+    CHK(check_sys(s));
+    if (ntypes < 1 || ntypes > kMaxTypes) return fail(MG_ERR_ARG, "ntypes must be 1..%d", kMaxTypes);
+    if (!names || !masses) return fail(MG_ERR_ARG, "null names / masses");
+    s->nt = ntypes;
+    s->names.clear();
+    s->masses.clear();
+    for (int i = 0; i < ntypes; i++) {
+        if (!names[i]) return fail(MG_ERR_ARG, "null type name");
+        if (masses[i] <= 0.0) return fail(MG_ERR_ARG, "mass cannot be zero");
+        s->names.push_back(names[i]);
+        s->masses.push_back(masses[i]);
+    }
+    s->x_dim = s->dmd ? 3 + ntypes : 3;
+    s->types_set = true;
+    return MG_OK;
+}
+
+int mg_atoms_set_box(mg_system* s, const double* H)
+{
+    CHK(check_sys(s));
+    if (!H) return fail(MG_ERR_ARG, "null H");
+    double A[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) A[i][j] = s->H[i][j] = H[i * 3 + j];
+    for (int i = 0; i < 3; i++)
+        for (int j = i + 1; j < 3; j++)
+            if (A[i][j] != 0.0) return fail(MG_ERR_ARG, "H must be lower triangular (Atoms::H convention)");
+    // M3INV (init.h:72-85)
+    double (*Bm)[3] = s->B;
+    Bm[0][0] = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+    Bm[1][1] = A[2][2] * A[0][0] - A[2][0] * A[0][2];
+    Bm[2][2] = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+    Bm[1][0] = A[1][2] * A[2][0] - A[1][0] * A[2][2];
+    Bm[2][1] = A[2][0] * A[0][1] - A[2][1] * A[0][0];
+    Bm[0][2] = A[0][1] * A[1][2] - A[0][2] * A[1][1];
+    Bm[2][0] = A[1][0] * A[2][1] - A[2][0] * A[1][1];
+    Bm[0][1] = A[2][1] * A[0][2] - A[0][1] * A[2][2];
+    Bm[1][2] = A[0][2] * A[1][0] - A[1][2] * A[0][0];
+    double det = A[0][0] * Bm[0][0] + A[0][1] * Bm[1][0] + A[0][2] * Bm[2][0];
+    if (det == 0.0) return fail(MG_ERR_ARG, "H determinant is zero");
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) Bm[i][j] /= det;
+    s->box_set = true;
+    return MG_OK;
+}
+
+int mg_atoms_set_skin(mg_system* s, double skin)
+{
+    CHK(check_sys(s));
+    if (!(skin >= 0.0)) return fail(MG_ERR_ARG, "skin cannot be negative");
+    s->skin = skin;
+    return MG_OK;
+}
+
+int mg_atoms_set(mg_system* s, int natms, const double* x, const int* type, const double* c)
+{
+    CHK(check_sys(s));
+    if (!s->types_set) return fail(MG_ERR_STATE, "atom types must be set before atoms");
+    if (natms < 0) return fail(MG_ERR_ARG, "natms < 0");
+    if (natms > 0 && !x) return fail(MG_ERR_ARG, "null x");
+    if (natms > 0 && s->dmd && !c) return fail(MG_ERR_ARG, "DMD needs c");
+    if (natms > 0 && !s->dmd && !type) return fail(MG_ERR_ARG, "EAM/FS need type");
+    s->natms = natms;
+    Dev& d = s->d;
+    fill_dev_scalars(s);
+    size_t cap0 = (size_t)natms * 4 + 1024;
+    s->cap = 0;
+    CHK(ensure_atoms(s, cap0, 0));
+    CHK(dalloc(&d.pos0, natms));
+    CHK(dalloc(&d.nnb, natms));
+    CHK(dalloc(&d.ncrd, natms));
+    CHK(dalloc(&d.f, (size_t)natms * s->x_dim));
+    CHK(dalloc(&d.c_d, (size_t)natms * s->nt));
+    CHK(dalloc(&d.a_in, (size_t)natms * s->nt));
+    CHK(dalloc(&d.g, (size_t)natms * s->nt));
+    s->npair_blocks = s->dmd ? 3 * s->nt * s->nt + 3 * (s->nt * (s->nt + 1) / 2) : 2;
+    CHK(ensure_pairs(s, s->dmd ? 96 : 64));
+    d.maxcrd = 32;
+    CHK(dalloc(&d.crdl, (size_t)natms * d.maxcrd));
+    if (natms) {
+        const void* dx = nullptr;
+        CHK(stage_in(s, x, (size_t)natms * s->x_dim * sizeof(double), &dx));
+        CU(launch_split_x(d, (const double*)dx, 1, s->st));
+        if (s->dmd) {
+            CU(cudaMemcpyAsync(d.c, c, (size_t)natms * s->nt * sizeof(double),
+                               is_device_ptr(c) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->st));
+        } else {
+            CU(cudaMemcpyAsync(d.type, type, (size_t)natms * sizeof(int),
+                               is_device_ptr(type) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->st));
+        }
+        CU(cudaStreamSynchronize(s->st));
+    }
+    s->atoms_set = true;
+    s->initialized = false;
+    return MG_OK;
+}
+
+int mg_ff_coef(mg_system* s, int narg, const char* const* arg)
+{
+    CHK(check_sys(s));
+    if (!s->types_set) return fail(MG_ERR_STATE, "atom types must be set before ff_coef");
+    Dev& d = s->d;
+    if (s->style == STYLE_EAM) {
+        if (narg < 3) return fail(MG_ERR_ARG, "wrong coeff command for eam Force Field");
+        if (!strcmp(arg[1], "FS")) {
+            if (narg != 3) return fail(MG_ERR_ARG, "one file is needed for eam");
+            CHK(read_tables(s, arg[2], true));
+        } else if (!strcmp(arg[1], "SetFL")) {
+            if (narg != 3) return fail(MG_ERR_ARG, "one file is needed for eam");
+            CHK(read_tables(s, arg[2], false));
+        } else if (!strcmp(arg[1], "FuncFL")) {
+            return fail(MG_ERR_UNSUPPORTED, "FuncFL tables are not supported by this build; convert to SetFL");
+        } else
+            return fail(MG_ERR_ARG, "wrong coeff command for eam Force Field");
+        // ff_eam.cpp:424-425
+        d.cut_sq = (s->nr - 1.0) * (s->nr - 1.0) * s->dr * s->dr;
+        d.rho_max = (s->nrho - 1.0) * s->drho;
+    } else if (s->style == STYLE_FS) {
+        if (narg != 2) return fail(MG_ERR_ARG, "wrong coeff command for Finnis-Sinclair Force Field");
+        CHK(read_fs_coeffs(s, arg[1]));
+    } else {
+        if (narg < 8) return fail(MG_ERR_ARG, "wrong coeff command for eam Force Field");
+        double kb = 8.617332478e-5, hbar = 6.5821192815e-16;
+        d.rsq_crd = atof(arg[1]);
+        d.rsq_crd *= d.rsq_crd;
+        int n = atoi(arg[2]);
+        if (n < 1 || n > kMaxQuad) return fail(MG_ERR_ARG, "n should be between 1 and 14");
+        s->nq = n;
+        d.nq = n;
+        gauss_hermite(n, d.xi, d.w0);
+        for (int i = 0; i < n; i++) {
+            d.w1[i] = d.w0[i] * d.xi[i];
+            d.w2[i] = d.w0[i] * d.xi[i] * d.xi[i];
+        }
+        d.alpha_min = atof(arg[3]);
+        d.alpha_max = atof(arg[4]);
+        double T = atof(arg[5]);
+        if (!strcmp(arg[6], "FS")) {
+            if (narg != 8) return fail(MG_ERR_ARG, "one file is needed for eam");
+            CHK(read_tables(s, arg[7], true));
+        } else if (!strcmp(arg[6], "SetFL") || !strcmp(arg[6], "FuncFL")) {
+            return fail(MG_ERR_UNSUPPORTED, "DMD styles read FS tables in this build (got %s)", arg[6]);
+        } else
+            return fail(MG_ERR_ARG, "wrong coeff command for eam Force Field");
+        for (int i = 0; i < s->nt; i++) {
+            double mass = s->masses[i];
+            mass *= 1.0364269184093291236e-28;
+            double deb_l = hbar * hbar * 2.0 / (mass * kb * T);
+            d.c0[i] = 1.5 * kb * T * (log(deb_l) - 1.0);
+        }
+        d.kbT = kb * T;
+        d.beta = 1.0 / d.kbT;
+        if (d.alpha_min == 0.0) return fail(MG_ERR_ARG, "minimum alpha cannot be zero");
+        d.rc = (static_cast<double>(s->nr) - 1.0) * s->dr;
+        d.rho_max = (static_cast<double>(s->nrho) - 1.0) * s->drho;
+        d.cut_sq = d.rc * d.rc;
+        double mod_rc = d.rc + d.xi[n - 1] / sqrt(d.alpha_min);
+        d.cut_sq_mod = mod_rc * mod_rc;
+    }
+    s->coef_set = true;
+    s->initialized = false;
+    return MG_OK;
+}
+
+int mg_ff_init(mg_system* s)
+{
+    CHK(check_sys(s));
+    if (!s->types_set || !s->box_set || !s->atoms_set || !s->coef_set)
+        return fail(MG_ERR_STATE, "types, box, atoms and ff_coef must be set before init");
+    CHK(upload_tables(s));
+    fill_dev_scalars(s);
+    compute_cutoffs(s);
+    // owned atoms: root / chain identity, s already in d.sfr
+    {
+        std::vector<int> root(s->natms);
+        for (int i = 0; i < s->natms; i++) root[i] = i;
+        if (s->natms) {
+            CU(cudaMemcpyAsync(s->d.root, root.data(), s->natms * sizeof(int), cudaMemcpyHostToDevice, s->st));
+            CU(cudaMemsetAsync(s->d.gchain, 0, s->natms * sizeof(unsigned long long), s->st));
+        }
+        CU(cudaStreamSynchronize(s->st));
+    }
+    CHK(ensure_partials(s, 2LL * div_up((long long)s->natms * 32, kFFBlock) + div_up((long long)s->natms * 4, kFFBlock) + 8));
+    CHK(rebuild(s));
+    s->initialized = true;
+    return MG_OK;
+}
+
+int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
+{
+    CHK(check_sys(s));
+    if (!s->initialized) return fail(MG_ERR_STATE, "init must run before update_0");
+    Dev& d = s->d;
+    if (s->natms) {
+        const void* dx = nullptr;
+        CHK(stage_in(s, x, (size_t)s->natms * s->x_dim * sizeof(double), &dx));
+        CU(launch_split_x(d, (const double*)dx, 0, s->st));
+    }
+    CU(cudaMemsetAsync(d.status + 5, 0, sizeof(int), s->st));
+    CU(launch_skin_check(d, s->skin * s->skin, d.status + 5, s->st));
+    int flag = 0;
+    CU(cudaMemcpyAsync(&flag, d.status + 5, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    if (flag) {
+        CU(launch_x2s(d, s->st));
+        CHK(rebuild(s));
+    } else {
+        CU(launch_refresh_x(d, s->st));
+    }
+    if (rebuilt) *rebuilt = flag;
+    return MG_OK;
+}
+
+int mg_atoms_update_c(mg_system* s, const double* c)
+{
+    CHK(check_sys(s));
+    if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "c exists only in DMD mode");
+    if (!s->initialized) return fail(MG_ERR_STATE, "init must run first");
+    size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
+    CU(cudaMemcpyAsync(s->d.c, c, bytes, is_device_ptr(c) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->st));
+    CU(launch_refresh_c(s->d, s->st));
+    return MG_OK;
+}
+
+int mg_atoms_get_x(mg_system* s, double* x)
+{
+    CHK(check_sys(s));
+    if (!x) return fail(MG_ERR_ARG, "null x");
+    size_t bytes = (size_t)s->natms * s->x_dim * sizeof(double);
+    if (bytes > s->stage_cap) {
+        CHK(dalloc((char**)&s->stage, bytes));
+        s->stage_cap = bytes;
+    }
+    CU(launch_merge_x(s->d, s->stage, 0, s->natms, s->st));
+    CHK(copy_out(s, x, s->stage, bytes));
+    CU(cudaStreamSynchronize(s->st));
+    return MG_OK;
+}
+
+int mg_atoms_get_ghosts(mg_system* s, double* x, int* owner)
+{
+    CHK(check_sys(s));
+    int nph = s->d.nph;
+    if (x && nph) {
+        size_t bytes = (size_t)nph * s->x_dim * sizeof(double);
+        if (bytes > s->stage_cap) {
+            CHK(dalloc((char**)&s->stage, bytes));
+            s->stage_cap = bytes;
+        }
+        CU(launch_merge_x(s->d, s->stage, s->natms, nph, s->st));
+        CHK(copy_out(s, x, s->stage, bytes));
+    }
+    if (owner && nph) CHK(copy_out(s, owner, s->d.root + s->natms, (size_t)nph * sizeof(int)));
+    CU(cudaStreamSynchronize(s->st));
+    return MG_OK;
+}
+
+int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
+{
+    CHK(check_sys(s));
+    if (!s->initialized) return fail(MG_ERR_STATE, "force_calc before init");
+    Dev& d = s->d;
+    fill_dev_scalars(s);
+    CHK(timed_begin(s));
+    CU(cudaMemsetAsync(d.f, 0, (size_t)s->natms * s->x_dim * sizeof(double), s->st));
+    int rows = 0;
+    if (s->style == STYLE_EAM || s->style == STYLE_FS) {
+        CU(cudaMemsetAsync(d.rho, 0, (size_t)s->natms * sizeof(double), s->st));
+        CU(s->style == STYLE_EAM ? launch_eam_force(d, st_clc, &rows, s->st) : launch_fs_force(d, st_clc, &rows, s->st));
+    } else {
+        CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
+        CU(launch_dmd_force(d, st_clc, &rows, s->st));
+    }
+    double tot[8] = {0};
+    CU(launch_reduce_partials(d, rows, 7, s->red_out, s->st));
+    CHK(timed_end(s, &s->t_force));
+    CU(cudaMemcpyAsync(tot, s->red_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CHK(copy_out(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
+    CU(cudaStreamSynchronize(s->st));
+    if (en_st) {
+        if (st_clc)
+            for (int i = 0; i < 7; i++) en_st[i] = tot[i];
+        else
+            en_st[0] = tot[0];
+    }
+    return MG_OK;
+}
+
+int mg_ff_energy_calc(mg_system* s, double* energy)
+{
+    CHK(check_sys(s));
+    if (!s->initialized) return fail(MG_ERR_STATE, "energy_calc before init");
+    Dev& d = s->d;
+    CHK(timed_begin(s));
+    int rows = 0;
+    if (s->style == STYLE_EAM || s->style == STYLE_FS) {
+        CU(cudaMemsetAsync(d.rho, 0, (size_t)s->natms * sizeof(double), s->st));
+        CU(s->style == STYLE_EAM ? launch_eam_energy(d, &rows, s->st) : launch_fs_energy(d, &rows, s->st));
+    } else {
+        CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
+        CU(launch_dmd_energy(d, &rows, s->st));
+    }
+    double tot[8] = {0};
+    CU(launch_reduce_partials(d, rows, 1, s->red_out, s->st));
+    CHK(timed_end(s, &s->t_energy));
+    CU(cudaMemcpyAsync(tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    if (energy) *energy = tot[0];
+    return MG_OK;
+}
+
+int mg_ff_create_2nd_neigh_lst(mg_system* s)
+{
+    CHK(check_sys(s));
+    if (!s->dmd) return MG_OK;  // empty in EAM / FS (ff_eam.h:61)
+    if (!s->initialized) return fail(MG_ERR_STATE, "create_2nd_neigh_lst before init");
+    Dev& d = s->d;
+    for (int attempt = 0; attempt < 4; attempt++) {
+        CU(cudaMemsetAsync(d.crd, 0, (size_t)d.nall * sizeof(int), s->st));
+        CU(cudaMemsetAsync(d.status, 0, 8 * sizeof(int), s->st));
+        CU(launch_dmd_crd(d, s->st));
+        int st_h[8];
+        CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+        CU(cudaStreamSynchronize(s->st));
+        if (!st_h[2]) break;
+        d.maxcrd = st_h[3] + 8;
+        CHK(dalloc(&d.crdl, (size_t)s->natms * d.maxcrd));
+        if (attempt == 3) return fail(MG_ERR_CAPACITY, "coordination list capacity could not be met");
+    }
+    s->crd_built = 1;
+    return MG_OK;
+}
+
+int mg_ff_c_d_calc(mg_system* s, double* c_d)
+{
+    CHK(check_sys(s));
+    if (!s->dmd) return MG_OK;
+    if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before c_d_calc");
+    Dev& d = s->d;
+    size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
+    CHK(timed_begin(s));
+    CU(cudaMemsetAsync(d.E, 0, bytes, s->st));
+    CU(cudaMemsetAsync(d.c_d, 0, bytes, s->st));
+    CU(launch_dmd_cdot(d, s->st));
+    CHK(timed_end(s, &s->t_cd));
+    CHK(copy_out(s, c_d, d.c_d, bytes));
+    CU(cudaStreamSynchronize(s->st));
+    return MG_OK;
+}
+
+int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g, double* cost)
+{
+    CHK(check_sys(s));
+    if (!s->dmd) {
+        if (cost) *cost = 0.0;  // ff_eam.h:62 returns 0
+        return MG_OK;
+    }
+    if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before calc_g");
+    if (!a) return fail(MG_ERR_ARG, "null a");
+    Dev& d = s->d;
+    size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
+    CU(cudaMemcpyAsync(d.a_in, a, bytes, is_device_ptr(a) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->st));
+    CHK(timed_begin(s));
+    CU(cudaMemsetAsync(d.E, 0, bytes, s->st));
+    int rows = 0;
+    CU(launch_dmd_calc_g(d, chk, alpha, &rows, s->st));
+    CU(launch_reduce_partials(d, rows, 1, s->red_out, s->st));
+    CHK(timed_end(s, &s->t_g));
+    double tot[2] = {0, 0};
+    CU(cudaMemcpyAsync(tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    if (!chk) CHK(copy_out(s, g, d.g, bytes));
+    CU(cudaStreamSynchronize(s->st));
+    if (cost) *cost = tot[0] * 0.25;
+    return MG_OK;
+}
+
+int mg_ff_fin(mg_system* s)
+{
+    CHK(check_sys(s));
+    Dev& d = s->d;
+    cudaStreamSynchronize(s->st);
+    if (d.pr) cudaFree(d.pr);
+    d.pr = nullptr;
+    d.maxp = 0;
+    s->initialized = false;
+    s->crd_built = 0;
+    return MG_OK;
+}
+
+int mg_neighbor_create_list(mg_system* s)
+{
+    CHK(check_sys(s));
+    if (!s->initialized) return fail(MG_ERR_STATE, "init must run first");
+    CU(launch_x2s(s->d, s->st));
+    return rebuild(s);
+}
+
+int mg_neighbor_counts(mg_system* s, int* natms, int* natms_ph, long long* no_pairs)
+{
+    CHK(check_sys(s));
+    if (natms) *natms = s->natms;
+    if (natms_ph) *natms_ph = s->d.nph;
+    if (no_pairs) {
+        std::vector<int> n(s->natms);
+        if (s->natms) CU(cudaMemcpy(n.data(), s->d.nnb, s->natms * sizeof(int), cudaMemcpyDeviceToHost));
+        long long t = 0;
+        for (int v : n) t += v;
+        *no_pairs = t;
+    }
+    return MG_OK;
+}
+
+int mg_neighbor_get_list(mg_system* s, int* sizes, int* pairs)
+{
+    CHK(check_sys(s));
+    int natms = s->natms, maxnb = s->d.maxnb;
+    std::vector<int> n(natms), all((size_t)natms * maxnb);
+    if (natms) {
+        CU(cudaMemcpy(n.data(), s->d.nnb, natms * sizeof(int), cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(all.data(), s->d.nbr, all.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    long long off = 0;
+    for (int i = 0; i < natms; i++) {
+        if (sizes) sizes[i] = n[i];
+        if (pairs) memcpy(pairs + off, all.data() + (size_t)i * maxnb, n[i] * sizeof(int));
+        off += n[i];
+    }
+    return MG_OK;
+}
+
+int mg_get_vector(mg_system* s, const char* name, double* out)
+{
+    CHK(check_sys(s));
+    if (!name || !out) return fail(MG_ERR_ARG, "null argument");
+    Dev& d = s->d;
+    int nall = d.nall, nt = s->nt;
+    const double* src = nullptr;
+    size_t count = 0;
+    if (!strcmp(name, "E")) src = d.E, count = (size_t)s->natms * nt;
+    else if (!strcmp(name, "dE")) src = d.dE, count = (size_t)s->natms * nt;
+    else if (!strcmp(name, "ddE")) src = d.ddE, count = (size_t)s->natms * nt;
+    else if (!strcmp(name, "n")) src = d.n, count = (size_t)s->natms * nt;
+    else if (!strcmp(name, "c_d")) src = d.c_d, count = (size_t)s->natms * nt;
+    else if (!strcmp(name, "rho")) src = d.rho, count = (size_t)s->natms;
+    else return fail(MG_ERR_ARG, "unknown vector %s", name);
+    (void)nall;
+    CHK(copy_out(s, out, src, count * sizeof(double)));
+    CU(cudaStreamSynchronize(s->st));
+    return MG_OK;
+}
+
+int mg_get_int_vector(mg_system* s, const char* name, int* out)
+{
+    CHK(check_sys(s));
+    if (!name || !out) return fail(MG_ERR_ARG, "null argument");
+    if (!strcmp(name, "crd")) {
+        CHK(copy_out(s, out, s->d.crd, (size_t)s->d.nall * sizeof(int)));
+        CU(cudaStreamSynchronize(s->st));
+        return MG_OK;
+    }
+    return fail(MG_ERR_ARG, "unknown vector %s", name);
+}
+
+int mg_last_time(mg_system* s, const char* phase, double* ms)
+{
+    CHK(check_sys(s));
+    if (!phase || !ms) return fail(MG_ERR_ARG, "null argument");
+    if (!strcmp(phase, "list")) *ms = s->t_list;
+    else if (!strcmp(phase, "force")) *ms = s->t_force;
+    else if (!strcmp(phase, "energy")) *ms = s->t_energy;
+    else if (!strcmp(phase, "c_d")) *ms = s->t_cd;
+    else if (!strcmp(phase, "calc_g")) *ms = s->t_g;
+    else return fail(MG_ERR_ARG, "unknown phase %s", phase);
+    return MG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,393 @@
+// Atoms / Neighbor kernels: x<->s conversion, ghost (phantom) build and
+// refresh, binning, half neighbour list, skin check.
+//
+// Every floating-point step that decides list membership uses explicit
+// round-to-nearest intrinsics (no fused multiply-add) in the reference's
+// operation order, so positions, bins and the (i, j) pair set are bit-identical
+// to the reference's: x2s atoms.cpp:1869-1897, s2x atoms.cpp:1924-1941,
+// s2bin neighbor.cpp:507-525, rsq neighbor.cpp:212-215, ghost s shift
+// atoms.cpp:489-495, ghost x refresh atoms.cpp:1340-1348, skin check
+// atoms.cpp:1804-1819.
+#include <cub/device/device_scan.cuh>
+
+#include "mg_internal.h"
+
+namespace mg {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+__device__ __forceinline__ double comp3(const double4& p, int k) { return k == 0 ? p.x : (k == 1 ? p.y : p.z); }
+
+__device__ __forceinline__ void set3(double4& p, int k, double v)
+{
+    if (k == 0) p.x = v;
+    else if (k == 1) p.y = v;
+    else p.z = v;
+}
+
+__global__ void k_split_x(Dev d, const double* __restrict__ x, int frac)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.natms) return;
+    const double* p = x + (size_t)i * d.x_dim;
+    double4 v = make_double4(p[0], p[1], p[2], 0.0);
+    if (frac) d.sfr[i] = v;
+    else d.pos[i] = v;
+    for (int a = 0; a < d.x_dim - 3; a++) d.alpha[(size_t)i * d.nt + a] = p[3 + a];
+}
+
+// Atoms::x2s for owned atoms, including the wrap loops into [0, 1).
+__global__ void k_x2s(Dev d)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.natms) return;
+    double4 p = d.pos[i];
+    for (int j = 0; j < 3; j++) {
+        double v = dmul(comp3(p, j), d.B[j][j]);
+        for (int k = j + 1; k < 3; k++) v = dadd(v, dmul(d.B[k][j], comp3(p, k)));
+        set3(p, j, v);
+    }
+    for (int j = 0; j < 3; j++) {
+        double v = comp3(p, j);
+        // the reference steps by one until inside; bounded here by a generous
+        // iteration limit so an absurd coordinate cannot spin a thread forever
+        for (int it = 0; v < 0.0 && it < (1 << 20); it++) v = dadd(v, 1.0);
+        for (int it = 0; v >= 1.0 && it < (1 << 20); it++) v = dsub(v, 1.0);
+        set3(p, j, v);
+    }
+    p.w = 0.0;
+    d.sfr[i] = p;
+    d.root[i] = i;
+    d.gchain[i] = 0ull;
+}
+
+// One swap pass of Atoms::ph_setup: flag atoms of [lo, hi) whose s in `dim`
+// lies in the low (dir 0) or high (dir 1) phantom shell.
+__global__ void k_ghost_flags(Dev d, int lo, int hi, int dim, int dir, int* __restrict__ flags)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= hi - lo) return;
+    double sv = comp3(d.sfr[lo + k], dim);
+    int take = dir == 0 ? (sv <= d.s_ph_lo[dim]) : (d.s_ph_hi[dim] <= sv);
+    flags[k] = take;
+}
+
+// Stable scatter of the flagged atoms to new ghost slots base + offs[k]:
+// copy the phantom vectors, shift s[dim] by +1 (dir 0) or -1 (dir 1) and
+// append (dim, dir) to the image chain.
+__global__ void k_ghost_scatter(Dev d, int lo, int hi, int dim, int dir, const int* __restrict__ flags,
+                                const int* __restrict__ offs, int base)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= hi - lo || !flags[k]) return;
+    int src = lo + k, g = base + offs[k];
+    double4 s = d.sfr[src];
+    double v = comp3(s, dim);
+    set3(s, dim, dir == 0 ? dadd(v, 1.0) : dsub(v, 1.0));
+    d.sfr[g] = s;
+    for (int a = 0; a < d.x_dim - 3; a++) d.alpha[(size_t)g * d.nt + a] = d.alpha[(size_t)src * d.nt + a];
+    if (d.c)
+        for (int a = 0; a < d.nt; a++) d.c[(size_t)g * d.nt + a] = d.c[(size_t)src * d.nt + a];
+    if (d.type) d.type[g] = d.type[src];
+    d.root[g] = d.root[src];
+    unsigned long long ch = d.gchain[src];
+    int used = __popcll(ch & 0x8888888888888888ull);
+    if (used < kMaxChain) ch |= (unsigned long long)(8 | (dim << 1) | dir) << (4 * used);
+    else atomicExch(&d.status[4], 1);  // chain too deep: reported as a capacity error
+    d.gchain[g] = ch;
+}
+
+// Neighbor::s2bin for every atom, then Atoms::s2x (owned + ghost), counting
+// atoms per bin.
+__global__ void k_bin_s2x(Dev d)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nall) return;
+    double4 s = d.sfr[i];
+    int no = 0;
+    for (int k = 0; k < 3; k++) {
+        double q = __ddiv_rn(dsub(dadd(comp3(s, k), d.cut_ph_s[k]), 0.0), d.cut_ph_s[k]);
+        no += (int)q * d.denom[k];
+    }
+    d.bin[i] = no;
+    atomicAdd(&d.cell_count[no], 1);
+    double4 x = s;
+    for (int j = 0; j < 3; j++) {
+        double v = dmul(comp3(s, j), d.H[j][j]);
+        for (int k = j + 1; k < 3; k++) v = dadd(v, dmul(d.H[k][j], comp3(s, k)));
+        set3(x, j, v);
+    }
+    x.w = 0.0;
+    d.pos[i] = x;
+}
+
+__device__ __forceinline__ double pack_idx(int idx, int type)
+{
+    return __longlong_as_double(((long long)type << 32) | (unsigned int)idx);
+}
+__device__ __forceinline__ int unpack_idx(double w) { return (int)(__double_as_longlong(w) & 0xffffffffll); }
+__device__ __forceinline__ int unpack_type(double w) { return (int)(__double_as_longlong(w) >> 32); }
+
+__global__ void k_cell_fill(Dev d, int* __restrict__ cursor)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nall) return;
+    int b = d.bin[i];
+    int slot = d.cell_start[b] + atomicAdd(&cursor[b], 1);
+    double4 p = d.pos[i];
+    p.w = pack_idx(i, d.type ? d.type[i] : 0);
+    d.cell_pos[slot] = p;
+}
+
+// Neighbor::create_list, one warp per owned atom: the 27-bin stencil is nine
+// contiguous rows of the bin-sorted atom array; each lane tests one candidate,
+// and a ballot compacts the accepted j (> i, rsq < cut_sk_sq) into the list.
+__global__ void __launch_bounds__(kBlock) k_neigh(Dev d)
+{
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    double4 xi = d.pos[i];
+    int ti = d.type ? d.type[i] : 0;
+    int b = d.bin[i];
+    int b2 = b / d.denom[2];
+    int rem = b - b2 * d.denom[2];
+    int b1 = rem / d.denom[1];
+    int b0 = rem - b1 * d.denom[1];
+    int x_lo = max(b0 - 1, 0), x_hi = min(b0 + 1, d.grid[0] - 1);
+    unsigned lt = (1u << lane) - 1u;
+    int cnt = 0;
+    int* out = d.nbr + (size_t)i * d.maxnb;
+    const bool md = d.style <= STYLE_FS;
+    for (int dz = -1; dz <= 1; dz++) {
+        int z = b2 + dz;
+        if (z < 0 || z >= d.grid[2]) continue;
+        for (int dy = -1; dy <= 1; dy++) {
+            int y = b1 + dy;
+            if (y < 0 || y >= d.grid[1]) continue;
+            int row = y * d.denom[1] + z * d.denom[2];
+            int start = d.cell_start[row + x_lo], end = d.cell_start[row + x_hi + 1];
+            for (int k0 = start; k0 < end; k0 += 32) {
+                int k = k0 + lane;
+                bool ok = false;
+                int j = 0;
+                if (k < end) {
+                    double4 e = d.cell_pos[k];
+                    j = unpack_idx(e.w);
+                    if (j > i) {
+                        double d0 = dsub(xi.x, e.x), d1 = dsub(xi.y, e.y), d2 = dsub(xi.z, e.z);
+                        double rsq = dadd(dadd(dmul(d0, d0), dmul(d1, d1)), dmul(d2, d2));
+                        double cut = md ? d.cut_sk_sq[comp_idx(ti, unpack_type(e.w))] : d.cut_sk_sq[0];
+                        ok = rsq < cut;
+                    }
+                }
+                unsigned m = __ballot_sync(0xffffffffu, ok);
+                if (ok) {
+                    int slot = cnt + __popc(m & lt);
+                    if (slot < d.maxnb) out[slot] = j;
+                }
+                cnt += __popc(m);
+            }
+        }
+    }
+    if (lane == 0) {
+        d.nnb[i] = min(cnt, d.maxnb);
+        if (cnt > d.maxnb) {
+            d.status[0] = 1;
+            atomicMax(&d.status[1], cnt);
+        }
+    }
+}
+
+__global__ void k_store_x0(Dev d)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < d.natms) d.pos0[i] = d.pos[i];
+}
+
+__global__ void k_skin_check(Dev d, double sq_skin, int* __restrict__ flag)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.natms) return;
+    double4 p = d.pos[i], q = d.pos0[i];
+    double dx0 = dsub(p.x, q.x), dx1 = dsub(p.y, q.y), dx2 = dsub(p.z, q.z);
+    double sq = dadd(dadd(dmul(dx0, dx0), dmul(dx1, dx1)), dmul(dx2, dx2));
+    if (sq > sq_skin) atomicOr(flag, 1);
+}
+
+// Atoms::update for x: each ghost = its root's x with the chain of +-H[dim][0..dim]
+// additions applied in creation order; alpha (the rest of vector x) is copied.
+__global__ void k_refresh_x(Dev d)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.nph) return;
+    int g = d.natms + k;
+    int r = d.root[g];
+    double4 p = d.pos[r];
+    unsigned long long ch = d.gchain[g];
+    for (int s = 0; s < kMaxChain; s++) {
+        unsigned code = (unsigned)(ch >> (4 * s)) & 15u;
+        if (!(code & 8u)) break;
+        int dim = (code >> 1) & 3, dir = code & 1;
+        for (int j = 0; j <= dim; j++) {
+            double v = comp3(p, j);
+            set3(p, j, dir == 0 ? dadd(v, d.H[dim][j]) : dsub(v, d.H[dim][j]));
+        }
+    }
+    p.w = 0.0;
+    d.pos[g] = p;
+    for (int a = 0; a < d.x_dim - 3; a++) d.alpha[(size_t)g * d.nt + a] = d.alpha[(size_t)r * d.nt + a];
+}
+
+__global__ void k_refresh_c(Dev d)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.nph) return;
+    int g = d.natms + k, r = d.root[g];
+    for (int a = 0; a < d.nt; a++) d.c[(size_t)g * d.nt + a] = d.c[(size_t)r * d.nt + a];
+}
+
+__global__ void k_merge_x(Dev d, double* __restrict__ x, int first, int count)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    int i = first + k;
+    double* p = x + (size_t)k * d.x_dim;
+    double4 v = d.pos[i];
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+    for (int a = 0; a < d.x_dim - 3; a++) p[3 + a] = d.alpha[(size_t)i * d.nt + a];
+}
+
+// Deterministic final reduction of per-block partial sums: one block, each
+// thread strides over blocks for one value column, then a shared-memory tree.
+__global__ void k_reduce_partials(const double* __restrict__ partial, int nblocks, int nvals, double* __restrict__ out)
+{
+    __shared__ double sh[kBlock];
+    for (int v = 0; v < nvals; v++) {
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) acc += partial[(size_t)b * 8 + v];
+        sh[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[v] = sh[0];
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+int num_sms()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+cudaError_t launch_split_x(const Dev& d, const double* x_aos, int frac, cudaStream_t st)
+{
+    if (d.natms) k_split_x<<<div_up(d.natms, kBlock), kBlock, 0, st>>>(d, x_aos, frac);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_x2s(const Dev& d, cudaStream_t st)
+{
+    if (d.natms) k_x2s<<<div_up(d.natms, kBlock), kBlock, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_flags(const Dev& d, int lo, int hi, int dim, int dir, int* flags, cudaStream_t st)
+{
+    if (hi > lo) k_ghost_flags<<<div_up(hi - lo, kBlock), kBlock, 0, st>>>(d, lo, hi, dim, dir, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_scatter(const Dev& d, int lo, int hi, int dim, int dir, const int* flags, const int* offs,
+                                 int base, cudaStream_t st)
+{
+    if (hi > lo) k_ghost_scatter<<<div_up(hi - lo, kBlock), kBlock, 0, st>>>(d, lo, hi, dim, dir, flags, offs, base);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_and_s2x(const Dev& d, cudaStream_t st)
+{
+    if (d.nall) k_bin_s2x<<<div_up(d.nall, kBlock), kBlock, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_fill(const Dev& d, int* cursor, cudaStream_t st)
+{
+    if (d.nall) k_cell_fill<<<div_up(d.nall, kBlock), kBlock, 0, st>>>(d, cursor);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_neigh(const Dev& d, cudaStream_t st)
+{
+    if (d.natms) k_neigh<<<div_up((long long)d.natms * 32, kBlock), kBlock, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_store_x0(const Dev& d, cudaStream_t st)
+{
+    if (d.natms) k_store_x0<<<div_up(d.natms, kBlock), kBlock, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_skin_check(const Dev& d, double sq_skin, int* flag, cudaStream_t st)
+{
+    if (d.natms) k_skin_check<<<div_up(d.natms, kBlock), kBlock, 0, st>>>(d, sq_skin, flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refresh_x(const Dev& d, cudaStream_t st)
+{
+    if (d.nph) k_refresh_x<<<div_up(d.nph, kBlock), kBlock, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refresh_c(const Dev& d, cudaStream_t st)
+{
+    if (d.nph && d.c) k_refresh_c<<<div_up(d.nph, kBlock), kBlock, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_x(const Dev& d, double* x_aos, int first, int count, cudaStream_t st)
+{
+    if (count) k_merge_x<<<div_up(count, kBlock), kBlock, 0, st>>>(d, x_aos, first, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_partials(const Dev& d, int nblocks, int nvals, double* out, cudaStream_t st)
+{
+    k_reduce_partials<<<1, kBlock, 0, st>>>(d.partial, nblocks, nvals, out);
+    return cudaGetLastError();
+}
+
+size_t scan_temp_bytes(int n)
+{
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int*)nullptr, (int*)nullptr, n);
+    return bytes;
+}
+
+cudaError_t launch_exclusive_scan(const int* in, int* out, int n, void* temp, size_t temp_bytes, cudaStream_t st)
+{
+    return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, in, out, n, st);
+}
+
+}  // namespace mg

@@ -1,0 +1,1005 @@
+// Diffusive-MD free energy, forces and chemical potentials
+// (ForceField_DMD_I / DMD_II / DMD: ff_dmd_I.cpp:88-668, 2138-2674;
+// ff_dmd_II.cpp:2151-2630; ff_dmd.cpp:2221-2606), plain FP64 form.
+//
+// Work layout as in mg_eam.cu: one warp per owned site i, lanes over i's half
+// list; i-side sums by warp shuffles, j-side sums by FP64 atomics on owned j.
+// Per-pair results of the force pass live in SoA blocks of the pair scratch
+// `pr` (pair slot i*maxnb+k), in the reference's slot order
+// (rho slot b*nt+a for species pair (a,b) = type2rho[a][b]; phi slot COMP(a,b)):
+//   block 0        rho           [nt*nt]
+//   block nt^2     drho_dr       [nt*nt]
+//   block 2nt^2    drho_dalpha   [nt*nt]
+//   block 3nt^2    phi           [nc]     nc = nt(nt+1)/2
+//   block 3nt^2+nc dphi_dr, then dphi_dalpha
+// Slots the reference would leave untouched (pair beyond the smeared cut,
+// alpha outside (alpha_min, alpha_max), no node inside the table) are written
+// as zero, so results never depend on earlier calls.
+#include "mg_reduce.cuh"
+
+namespace mg {
+
+namespace {
+
+constexpr double kPiInSq = 0.564189583547756286948079451561;  // 1/sqrt(pi)
+
+__device__ __forceinline__ int owner(const Dev& d, int j) { return j < d.natms ? j : d.root[j]; }
+
+// c0..c3 of one spline knot (rows of 8 doubles, 64-byte aligned) as two
+// read-only 16-byte loads
+__device__ __forceinline__ double4 knot4(const double* __restrict__ row)
+{
+    double2 lo = __ldg(reinterpret_cast<const double2*>(row));
+    double2 hi = __ldg(reinterpret_cast<const double2*>(row) + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
+template <int NT>
+struct Slots {
+    static constexpr int NC = NT * (NT + 1) / 2;
+    static constexpr int RHO = 0, DRR = NT * NT, DRA = 2 * NT * NT, PHI = 3 * NT * NT, DPR = 3 * NT * NT + NC,
+                         DPA = 3 * NT * NT + 2 * NC, TOTAL = 3 * NT * NT + 3 * NC;
+};
+
+__device__ __forceinline__ double calc_ent(double x)
+{
+    if (x < 1.0e-8 || 0.99999999 < x) return 0.0;
+    return x * log(x) + (1 - x) * log(1 - x);
+}
+
+// F(E), F'(E) (and F''(E)) from the quartic embedding spline (ff_dmd_I.cpp:322-341,
+// interpolate_m ff_dmd_I.cpp:1794-1836); index clamp nr-2 as in the reference.
+__device__ __forceinline__ void embed_F(const Dev& d, int a, double Ev, double& tmp0, double& tmp1, double* dd)
+{
+    double p = Ev * d.drho_inv;
+    int m = min((int)p, d.nr - 2);
+    p -= m;
+    p = fmin(p, 1.0);
+    double p2 = p * p, p3 = p2 * p, p4 = p3 * p;
+    const double* cf = d.FT + ((size_t)a * (d.nrho + 1) + m) * d.Fw;
+    tmp0 = cf[4] * p4 + cf[3] * p3 + cf[2] * p2 + cf[1] * p + cf[0];
+    tmp1 = cf[8] * p3 + cf[7] * p2 + cf[6] * p + cf[5];
+    if (Ev > d.rho_max) tmp0 += tmp1 * (Ev - d.rho_max);
+    if (dd) *dd = (3.0 * cf[8] * p2 + cf[7] * p + cf[6]) * d.drho_inv;
+}
+
+// One species pair of one site pair: the Gauss-Hermite smearing of r*rho and
+// r*phi (ff_dmd_I.cpp:178-259) or the plain EAM values above alpha_max
+// (ff_dmd_I.cpp:261-310).  Returns false when the reference writes nothing.
+template <bool kPhi, bool kDeriv>
+__device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double r, double r_inv, double rsq,
+                                      double alpha, double& g0, double& g_dr, double& g_da, double& f0, double& f_dr,
+                                      double& f_da)
+{
+    if (d.alpha_min < alpha && alpha < d.alpha_max) {
+        double asq = sqrt(alpha);
+        double inv_asq = 1.0 / asq;
+        double upper = (r + d.rc) * asq, lower = (r - d.rc) * asq;
+        if (!(lower < d.xi[d.nq - 1])) return false;
+        double fa = 0.0, fb = 0.0, fc = 0.0, ga = 0.0, gb = 0.0, gc = 0.0;
+        const double* rt = d.rhoT + (size_t)rslot * d.nr * 8;
+        const double* pt = d.phiT + (size_t)pslot * d.nr * 8;
+        for (int q = 0; q < d.nq; q++) {
+            double xq = d.xi[q];
+            if (xq > lower && xq < upper) {
+                double tmp0 = r - xq * inv_asq;
+                double p = fabs(tmp0) * d.dr_inv;
+                int m = min((int)p, d.nr - 2);
+                p -= m;
+                p = fmin(p, 1.0);
+                double p2 = p * p, p3 = p2 * p;
+                double4 cr = knot4(rt + 8 * m);
+                double tmp2 = (cr.w * p3 + cr.z * p2 + cr.y * p + cr.x) * tmp0;
+                ga += d.w0[q] * tmp2;
+                if (kDeriv) {
+                    gb += d.w1[q] * tmp2;
+                    gc += d.w2[q] * tmp2;
+                }
+                if (kPhi) {
+                    double4 cp = knot4(pt + 8 * m);
+                    double tmp1 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
+                    if (tmp0 < 0.0) tmp1 = -tmp1;
+                    fa += d.w0[q] * tmp1;
+                    if (kDeriv) {
+                        fb += d.w1[q] * tmp1;
+                        fc += d.w2[q] * tmp1;
+                    }
+                }
+            }
+        }
+        double sc = kPiInSq * r_inv;
+        g0 = ga * sc;
+        if (kDeriv) {
+            gb *= sc;
+            gc *= sc;
+            g_dr = -g0 * r_inv - 2.0 * asq * gb;
+            g_da = (0.5 * g0 - gc) / alpha;
+        }
+        if (kPhi) {
+            f0 = fa * sc;
+            if (kDeriv) {
+                fb *= sc;
+                fc *= sc;
+                f_dr = -f0 * r_inv - 2.0 * asq * fb;
+                f_da = (0.5 * f0 - fc) / alpha;
+            }
+        }
+        return true;
+    }
+    if (d.alpha_max <= alpha) {
+        if (!(rsq < d.cut_sq)) return false;
+        double p = r * d.dr_inv;
+        int m = min((int)p, d.nr - 2);
+        p -= m;
+        p = fmin(p, 1.0);
+        double p2 = p * p, p3 = p2 * p;
+        const double* cr = d.rhoT + ((size_t)rslot * d.nr + m) * 8;
+        g0 = cr[3] * p3 + cr[2] * p2 + cr[1] * p + cr[0];
+        if (kDeriv) {
+            g_da = 0.0;
+            g_dr = cr[6] * p2 + cr[5] * p + cr[4];
+        }
+        if (kPhi) {
+            const double* cp = d.phiT + ((size_t)pslot * d.nr + m) * 8;
+            double z2 = cp[3] * p3 + cp[2] * p2 + cp[1] * p + cp[0];
+            f0 = z2 * r_inv;
+            if (kDeriv) {
+                double z2p = cp[6] * p2 + cp[5] * p + cp[4];
+                f_da = 0.0;
+                f_dr = (z2p - z2 * r_inv) * r_inv;
+            }
+        }
+        return true;
+    }
+    return false;
+}
+
+// ---- force_calc pass 1 (ff_dmd_I.cpp:156-320) ----------------------------
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_dmd_pass1(Dev d, int row0)
+{
+    using S = Slots<NT>;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (i < d.natms) {
+        double4 xi = d.pos[i];
+        double ai[NT], ci[NT], Ei[NT];
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            ai[a] = d.alpha[(size_t)i * NT + a];
+            ci[a] = d.c[(size_t)i * NT + a];
+            Ei[a] = 0.0;
+        }
+        int nn = d.nnb[i];
+        for (int k = lane; k < nn; k += 32) {
+            long long slot = (long long)i * d.maxnb + k;
+            int j = d.nbr[slot];
+            double4 xj = d.pos[j];
+            double aj[NT], cj[NT], Ej[NT];
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                aj[b] = d.alpha[(size_t)j * NT + b];
+                cj[b] = d.c[(size_t)j * NT + b];
+                Ej[b] = 0.0;
+            }
+            double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
+            double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
+            double v[S::TOTAL];
+#pragma unroll
+            for (int q = 0; q < S::TOTAL; q++) v[q] = 0.0;
+            bool own_j = j < d.natms;
+            if (rsq < d.cut_sq_mod) {
+                double r = sqrt(rsq);
+                double r_inv = 1.0 / r;
+                double w = own_j ? 0.5 : 0.25;
+#pragma unroll
+                for (int a = 0; a < NT; a++)
+#pragma unroll
+                    for (int b = 0; b < NT; b++) {
+                        const int rs = b * NT + a, ps = comp_idx(a, b);
+                        double alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
+                        double g0 = 0, gdr = 0, gda = 0, f0 = 0, fdr = 0, fda = 0;
+                        bool hit = (a >= b) ? smear<true, true>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr, gda, f0, fdr, fda)
+                                            : smear<false, true>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr, gda, f0, fdr, fda);
+                        if (hit) {
+                            v[S::RHO + rs] = g0;
+                            v[S::DRR + rs] = gdr;
+                            v[S::DRA + rs] = gda;
+                            if (a >= b) {
+                                v[S::PHI + ps] = f0;
+                                v[S::DPR + ps] = fdr;
+                                v[S::DPA + ps] = fda;
+                                acc[0] += w * (cj[b] * ci[a] + cj[a] * ci[b]) * f0;
+                            }
+                            Ei[a] += g0 * cj[b];
+                            Ej[b] += g0 * ci[a];
+                        }
+                    }
+                if (own_j) {
+#pragma unroll
+                    for (int b = 0; b < NT; b++)
+                        if (Ej[b] != 0.0) atomicAdd(&d.E[(size_t)j * NT + b], Ej[b]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < S::TOTAL; q++) d.pr[(size_t)q * d.maxp + slot] = v[q];
+        }
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            double s = warp_sum(Ei[a]);
+            if (lane == 0) atomicAdd(&d.E[(size_t)i * NT + a], s);
+        }
+    }
+    block_partials<7>(acc, d.partial, row0 + blockIdx.x);
+}
+
+// ---- per-site embedding, entropy and alpha terms (ff_dmd_I.cpp:322-351) ---
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_dmd_embed(Dev d, int with_force, int row0)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (i < d.natms) {
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            double tmp0, tmp1;
+            embed_F(d, a, d.E[(size_t)i * NT + a], tmp0, tmp1, nullptr);
+            double ca = d.c[(size_t)i * NT + a], al = d.alpha[(size_t)i * NT + a];
+            d.E[(size_t)i * NT + a] = tmp0;
+            if (with_force) d.dE[(size_t)i * NT + a] = tmp1;
+            acc[0] += ca * tmp0;
+            acc[0] += d.kbT * calc_ent(ca);
+            acc[0] += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
+            if (with_force) d.f[(size_t)i * d.x_dim + 3 + a] -= 1.5 * d.kbT * ca / al;
+        }
+    }
+    block_partials<7>(acc, d.partial, row0 + blockIdx.x);
+}
+
+// ---- force_calc pass 2 (ff_dmd_I.cpp:357-436) ----------------------------
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_dmd_pass2(Dev d, int st_clc, int row0)
+{
+    using S = Slots<NT>;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (i < d.natms) {
+        double4 xi = d.pos[i];
+        double ai[NT], ci[NT], dEi[NT], fi[3 + NT];
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            ai[a] = d.alpha[(size_t)i * NT + a];
+            ci[a] = d.c[(size_t)i * NT + a];
+            dEi[a] = d.dE[(size_t)i * NT + a];
+        }
+#pragma unroll
+        for (int q = 0; q < 3 + NT; q++) fi[q] = 0.0;
+        int nn = d.nnb[i];
+        for (int k = lane; k < nn; k += 32) {
+            long long slot = (long long)i * d.maxnb + k;
+            int j = d.nbr[slot];
+            int oj = owner(d, j);
+            double4 xj = d.pos[j];
+            double aj[NT], cj[NT], dEj[NT], fj[3 + NT];
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                aj[b] = d.alpha[(size_t)j * NT + b];
+                cj[b] = d.c[(size_t)j * NT + b];
+                dEj[b] = d.dE[(size_t)oj * NT + b];
+            }
+#pragma unroll
+            for (int q = 0; q < 3 + NT; q++) fj[q] = 0.0;
+            double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
+            double r_inv = 1.0 / sqrt(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
+            bool own_j = j < d.natms;
+            double wv = own_j ? 1.0 : 0.5;
+            double fsum = 0.0;
+#pragma unroll
+            for (int a = 0; a < NT; a++)
+#pragma unroll
+                for (int b = 0; b < NT; b++) {
+                    const int ab = a * NT + b, ba = b * NT + a, ps = comp_idx(a, b);
+                    double cc = ci[a] * cj[b];
+                    double fpair = -(d.pr[(size_t)(S::DRR + ab) * d.maxp + slot] * dEi[a] +
+                                     d.pr[(size_t)(S::DRR + ba) * d.maxp + slot] * dEj[b] +
+                                     d.pr[(size_t)(S::DPR + ps) * d.maxp + slot]) *
+                                   cc * r_inv;
+                    double sa = ai[a] + aj[b];
+                    double apair = -(d.pr[(size_t)(S::DRA + ab) * d.maxp + slot] * dEi[a] +
+                                     d.pr[(size_t)(S::DRA + ba) * d.maxp + slot] * dEj[b] +
+                                     d.pr[(size_t)(S::DPA + ps) * d.maxp + slot]) *
+                                   cc / (sa * sa);
+                    fsum += fpair;
+                    fi[3 + a] += apair * aj[b] * aj[b];
+                    fj[3 + b] += apair * ai[a] * ai[a];
+                }
+            fi[0] += dx0 * fsum;
+            fi[1] += dx1 * fsum;
+            fi[2] += dx2 * fsum;
+            if (st_clc) {
+                double wf = wv * fsum;
+                acc[1] -= wf * dx0 * dx0;
+                acc[2] -= wf * dx1 * dx1;
+                acc[3] -= wf * dx2 * dx2;
+                acc[4] -= wf * dx1 * dx2;
+                acc[5] -= wf * dx2 * dx0;
+                acc[6] -= wf * dx0 * dx1;
+            }
+            if (own_j) {
+                double* fjp = d.f + (size_t)j * d.x_dim;
+                if (fsum != 0.0) {
+                    atomicAdd(fjp + 0, -dx0 * fsum);
+                    atomicAdd(fjp + 1, -dx1 * fsum);
+                    atomicAdd(fjp + 2, -dx2 * fsum);
+                }
+#pragma unroll
+                for (int b = 0; b < NT; b++)
+                    if (fj[3 + b] != 0.0) atomicAdd(fjp + 3 + b, fj[3 + b]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 3 + NT; q++) {
+            double s = warp_sum(fi[q]);
+            if (lane == 0) atomicAdd(d.f + (size_t)i * d.x_dim + q, s);
+        }
+    }
+    block_partials<7>(acc, d.partial, row0 + blockIdx.x);
+}
+
+// ---- energy_calc pass (ff_dmd_I.cpp:489-633): species pairs b >= a only --
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_dmd_energy_pass(Dev d, int row0)
+{
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (i < d.natms) {
+        double4 xi = d.pos[i];
+        double ai[NT], ci[NT], Ei[NT];
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            ai[a] = d.alpha[(size_t)i * NT + a];
+            ci[a] = d.c[(size_t)i * NT + a];
+            Ei[a] = 0.0;
+        }
+        int nn = d.nnb[i];
+        for (int k = lane; k < nn; k += 32) {
+            long long slot = (long long)i * d.maxnb + k;
+            int j = d.nbr[slot];
+            double4 xj = d.pos[j];
+            double aj[NT], cj[NT], Ej[NT];
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                aj[b] = d.alpha[(size_t)j * NT + b];
+                cj[b] = d.c[(size_t)j * NT + b];
+                Ej[b] = 0.0;
+            }
+            double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
+            double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
+            if (!(rsq < d.cut_sq_mod)) continue;
+            bool own_j = j < d.natms;
+            double r = sqrt(rsq);
+            double r_inv = 1.0 / r;
+            double w = own_j ? 0.5 : 0.25;
+#pragma unroll
+            for (int a = 0; a < NT; a++)
+#pragma unroll
+                for (int b = a; b < NT; b++) {
+                    const int rs = b * NT + a, ps = comp_idx(a, b);
+                    double alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
+                    double g0 = 0, f0 = 0, u0, u1, u2, u3;
+                    bool hit = (a == b) ? smear<true, false>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3)
+                                        : smear<false, false>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3);
+                    if (hit) {
+                        Ei[a] += g0 * cj[b];
+                        Ej[b] += g0 * ci[a];
+                        if (a == b) acc[0] += w * (cj[b] * ci[a] + cj[a] * ci[b]) * f0;
+                    }
+                }
+            if (own_j) {
+#pragma unroll
+                for (int b = 0; b < NT; b++)
+                    if (Ej[b] != 0.0) atomicAdd(&d.E[(size_t)j * NT + b], Ej[b]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            double s = warp_sum(Ei[a]);
+            if (lane == 0) atomicAdd(&d.E[(size_t)i * NT + a], s);
+        }
+    }
+    block_partials<7>(acc, d.partial, row0 + blockIdx.x);
+}
+
+// ---- create_2nd_neigh_lst (ff_dmd_I.cpp:2138-2217) ------------------------
+__global__ void __launch_bounds__(kFFBlock) k_dmd_crd(Dev d)
+{
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    double4 xi = d.pos[i];
+    int nn = d.nnb[i];
+    unsigned lt = (1u << lane) - 1u;
+    int cnt = 0;
+    for (int k0 = 0; k0 < nn; k0 += 32) {
+        int k = k0 + lane;
+        bool ok = false;
+        int j = 0;
+        if (k < nn) {
+            j = d.nbr[(size_t)i * d.maxnb + k];
+            double4 xj = d.pos[j];
+            double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
+            double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
+            ok = rsq < d.rsq_crd;
+        }
+        unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+            int s = cnt + __popc(m & lt);
+            if (s < d.maxcrd) d.crdl[(size_t)i * d.maxcrd + s] = j;
+            if (j < d.natms) atomicAdd(&d.crd[j], 1);
+        }
+        cnt += __popc(m);
+    }
+    if (lane == 0) {
+        d.ncrd[i] = min(cnt, d.maxcrd);
+        atomicAdd(&d.crd[i], cnt);
+        if (cnt > d.maxcrd) {
+            d.status[2] = 1;
+            atomicMax(&d.status[3], cnt);
+        }
+    }
+}
+
+__global__ void k_crd_ghosts(Dev d)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < d.nph) d.crd[d.natms + k] = d.crd[d.root[d.natms + k]];
+}
+
+// ---- c_d_calc / calc_g shared passes -------------------------------------
+// E from the stored per-pair densities (ff_dmd_I.cpp:2273-2292).
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
+{
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    double ci[NT], Ei[NT];
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        ci[a] = d.c[(size_t)i * NT + a];
+        Ei[a] = 0.0;
+    }
+    int nn = d.nnb[i];
+    for (int k = lane; k < nn; k += 32) {
+        long long slot = (long long)i * d.maxnb + k;
+        int j = d.nbr[slot];
+        double cj[NT], Ej[NT];
+#pragma unroll
+        for (int b = 0; b < NT; b++) {
+            cj[b] = d.c[(size_t)j * NT + b];
+            Ej[b] = 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < NT; a++)
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                Ei[a] += cj[b] * d.pr[(size_t)(a * NT + b) * d.maxp + slot];
+                Ej[b] += ci[a] * d.pr[(size_t)(b * NT + a) * d.maxp + slot];
+            }
+        if (j < d.natms) {
+#pragma unroll
+            for (int b = 0; b < NT; b++)
+                if (Ej[b] != 0.0) atomicAdd(&d.E[(size_t)j * NT + b], Ej[b]);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        double s = warp_sum(Ei[a]);
+        if (lane == 0) atomicAdd(&d.E[(size_t)i * NT + a], s);
+    }
+}
+
+// n = E = F(E), dE = F'(E) (and ddE) per owned site (ff_dmd_I.cpp:2294-2314, 2472-2494).
+template <int NT>
+__global__ void k_mu_embed(Dev d, int with_dd)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= d.natms * NT) return;
+    int a = idx % NT;
+    double tmp0, tmp1, dd;
+    embed_F(d, a, d.E[idx], tmp0, tmp1, with_dd ? &dd : nullptr);
+    d.n[idx] = d.E[idx] = tmp0;
+    d.dE[idx] = tmp1;
+    if (with_dd) d.ddE[idx] = dd;
+}
+
+// Value of dE at the reference's flat index q = atom + species (the
+// dE[jatm+jtype] indexing of ff_dmd_I.cpp:2336,2339), ghost entries read from
+// their owner.
+template <int NT>
+__device__ __forceinline__ double dE_flat(const Dev& d, int q)
+{
+    int atom = q / NT, sp = q - atom * NT;
+    return d.dE[(size_t)owner(d, atom) * NT + sp];
+}
+
+// chemical-potential pair sums (ff_dmd_I.cpp:2320-2345).
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
+{
+    using S = Slots<NT>;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    double ci[NT], ni[NT], dEi_q[NT];
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        ci[a] = d.c[(size_t)i * NT + a];
+        ni[a] = 0.0;
+        dEi_q[a] = dE_flat<NT>(d, i + a);
+    }
+    int nn = d.nnb[i];
+    for (int k = lane; k < nn; k += 32) {
+        long long slot = (long long)i * d.maxnb + k;
+        int j = d.nbr[slot];
+        double cj[NT], nj[NT], dEj_q[NT];
+#pragma unroll
+        for (int b = 0; b < NT; b++) {
+            cj[b] = d.c[(size_t)j * NT + b];
+            nj[b] = 0.0;
+            dEj_q[b] = dE_flat<NT>(d, j + b);
+        }
+#pragma unroll
+        for (int a = 0; a < NT; a++)
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                double ph = d.pr[(size_t)(S::PHI + comp_idx(a, b)) * d.maxp + slot];
+                ni[a] += cj[b] * (d.pr[(size_t)(b * NT + a) * d.maxp + slot] * dEj_q[b] + ph);
+                nj[b] += ci[a] * (d.pr[(size_t)(a * NT + b) * d.maxp + slot] * dEi_q[a] + ph);
+            }
+        if (j < d.natms) {
+#pragma unroll
+            for (int b = 0; b < NT; b++)
+                if (nj[b] != 0.0) atomicAdd(&d.n[(size_t)j * NT + b], nj[b]);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        double s = warp_sum(ni[a]);
+        if (lane == 0) atomicAdd(&d.n[(size_t)i * NT + a], s);
+    }
+}
+
+// per-site finalisation of n; mode as in the oracle:
+//   0 c_d_calc DMD_I/DMD, 1 c_d_calc DMD_II, 2 calc_g DMD_I/DMD, 3 calc_g DMD_II
+template <int NT>
+__global__ void k_mu_nfinal(Dev d, int mode)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= d.natms * NT) return;
+    int a = idx % NT;
+    double la = d.alpha[idx];
+    double v = d.n[idx];
+    if (mode == 0) {
+        v += d.c0[a] + 1.5 * d.kbT * log(la);
+        v *= d.beta;
+    } else if (mode == 1) {
+        v += d.c0[a] + 1.5 * d.kbT * log(la);
+    } else if (mode == 2) {
+        v += d.c0[a];
+        v *= d.beta;
+        v += 1.5 * log(la);
+    } else {
+        v += d.c0[a];
+        v += 1.5 * d.kbT * log(la);
+    }
+    d.n[idx] = v;
+}
+
+// jump-rate term of one crd pair and species (ff_dmd_I.cpp:2372-2376,
+// ff_dmd.cpp:2371-2376, ff_dmd_II.cpp:2314-2322)
+__device__ __forceinline__ double rate_sij(const Dev& d, double ni, double nj, double ci, double cj)
+{
+    if (d.style == STYLE_DMD_II) {
+        double mt = (ni > nj ? ni : nj) + 0.5;
+        double exp_fi = exp(d.beta * (ni - mt));
+        double exp_fj = exp(d.beta * (nj - mt));
+        return cj * (1.0 - ci) * exp_fj - ci * (1.0 - cj) * exp_fi;
+    }
+    double Mat = (d.style == STYLE_DMD ? 5.2 : 0.4) * d.beta;
+    double tmp0, tmp1;
+    if (d.style == STYLE_DMD) {
+        tmp0 = exp(ni + Mat);
+        tmp1 = exp(nj + Mat);
+    } else {
+        tmp0 = exp(0.5 * (ni - nj) + Mat);
+        tmp1 = exp(0.5 * (nj - ni) + Mat);
+    }
+    return (1.0 - ci) * cj * tmp1 - (1.0 - cj) * ci * tmp0;
+}
+
+// c_d over the r_crd sub-list (ff_dmd_I.cpp:2361-2382).
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_cd_rates(Dev d)
+{
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    double ni[NT], ci[NT], cdi[NT];
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        ni[a] = d.n[(size_t)i * NT + a];
+        ci[a] = d.c[(size_t)i * NT + a];
+        cdi[a] = 0.0;
+    }
+    int nc = d.ncrd[i];
+    for (int k = lane; k < nc; k += 32) {
+        int j = d.crdl[(size_t)i * d.maxcrd + k];
+        int oj = owner(d, j);
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            double s = rate_sij(d, ni[a], d.n[(size_t)oj * NT + a], ci[a], d.c[(size_t)j * NT + a]);
+            cdi[a] += s;
+            if (j < d.natms) atomicAdd(&d.c_d[(size_t)j * NT + a], -s);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        double s = warp_sum(cdi[a]);
+        if (lane == 0) atomicAdd(&d.c_d[(size_t)i * NT + a], s);
+    }
+}
+
+// calc_g: s = 2(c + a) then the rate terms (ff_dmd_I.cpp:2537-2564,
+// ff_dmd_II.cpp:2471-2511); block partial of sum s^2 computed in k_g_cost.
+template <int NT>
+__global__ void k_g_sinit(Dev d)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= d.natms * NT) return;
+    d.s[idx] = 2.0 * (d.c[idx] + d.a_in[idx]);
+    if (d.style == STYLE_DMD_II) d.c_d[idx] = 0.0;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_g_srates(Dev d, double alpha)
+{
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    double ni[NT], ci[NT], si[NT], cdi[NT];
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        ni[a] = d.n[(size_t)i * NT + a];
+        ci[a] = d.c[(size_t)i * NT + a];
+        si[a] = cdi[a] = 0.0;
+    }
+    bool II = d.style == STYLE_DMD_II;
+    int nc = d.ncrd[i];
+    for (int k = lane; k < nc; k += 32) {
+        int j = d.crdl[(size_t)i * d.maxcrd + k];
+        int oj = owner(d, j);
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            double sij = rate_sij(d, ni[a], d.n[(size_t)oj * NT + a], ci[a], d.c[(size_t)j * NT + a]);
+            // DMD_I / DMD: s_ij = -2 alpha * (rate); DMD_II: s -= 2 alpha s_ij, c_d += s_ij
+            double ds = -2.0 * alpha * sij;
+            si[a] += ds;
+            if (II) cdi[a] += sij;
+            if (j < d.natms) {
+                atomicAdd(&d.s[(size_t)j * NT + a], -ds);
+                if (II) atomicAdd(&d.c_d[(size_t)j * NT + a], -sij);
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        double s = warp_sum(si[a]);
+        if (lane == 0) atomicAdd(&d.s[(size_t)i * NT + a], s);
+        if (II) {
+            double c2 = warp_sum(cdi[a]);
+            if (lane == 0) atomicAdd(&d.c_d[(size_t)i * NT + a], c2);
+        }
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_g_cost(Dev d, int row0)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (idx < d.natms * NT) {
+        double s = d.s[idx];
+        acc[0] = s * s;
+        d.g[idx] = -s;
+        d.t[idx] = 0.0;
+        d.v[idx] = 0.0;
+    }
+    block_partials<7>(acc, d.partial, row0 + blockIdx.x);
+}
+
+// t and the first g terms over the crd sub-list (ff_dmd_I.cpp:2582-2608,
+// ff_dmd.cpp:2582-2605, ff_dmd_II.cpp:2529-2564).
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_g_trates(Dev d, double alpha)
+{
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    double ni[NT], ci[NT], si[NT], ti[NT], gi[NT];
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        ni[a] = d.n[(size_t)i * NT + a];
+        ci[a] = d.c[(size_t)i * NT + a];
+        si[a] = d.s[(size_t)i * NT + a];
+        ti[a] = gi[a] = 0.0;
+    }
+    int nc = d.ncrd[i];
+    for (int k = lane; k < nc; k += 32) {
+        int j = d.crdl[(size_t)i * d.maxcrd + k];
+        int oj = owner(d, j);
+        bool own_j = j < d.natms;
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            double nj = d.n[(size_t)oj * NT + a], cj = d.c[(size_t)j * NT + a], sj = d.s[(size_t)oj * NT + a];
+            double dt_i, dt_j, dg_i, dg_j;
+            double ds = si[a] - sj;
+            if (d.style == STYLE_DMD_II) {
+                double mt = (ni[a] > nj ? ni[a] : nj) + 0.5;
+                double exp_fi = exp(d.beta * (ni[a] - mt)), exp_fj = exp(d.beta * (nj - mt));
+                double tmpi = ci[a] * (1.0 - cj), tmpj = cj * (1.0 - ci[a]);
+                double dmi = ni[a] > nj ? 1.0 : 0.0, dmj = nj > ni[a] ? 1.0 : 0.0;
+                dt_i = (tmpi * exp_fi + dmi * (tmpj * exp_fj - tmpi * exp_fi)) * ds;
+                dt_j = (tmpj * exp_fj + dmj * (tmpi * exp_fi - tmpj * exp_fj)) * ds;
+                dg_i = -alpha * ((1.0 - cj) * exp_fi + cj * exp_fj) * ds;
+                dg_j = alpha * ((1.0 - ci[a]) * exp_fj + ci[a] * exp_fi) * ds;
+            } else if (d.style == STYLE_DMD) {
+                double Mat = 5.2 * d.beta;
+                double tmp0 = ds * exp(Mat + ni[a]), tmp1 = ds * exp(Mat + nj);
+                dt_i = ci[a] * tmp0 * (1.0 - cj);
+                dt_j = cj * tmp1 * (1.0 - ci[a]);
+                dg_i = -alpha * (tmp0 * (1.0 - cj) + tmp1 * cj);
+                dg_j = alpha * (tmp1 * (1.0 - ci[a]) + ci[a] * tmp0);
+            } else {
+                double Mat = 0.4 * d.beta;
+                double tmp0 = exp(0.5 * (ni[a] - nj) + Mat) * ds, tmp1 = exp(0.5 * (nj - ni[a]) + Mat) * ds;
+                double t_ij = 0.5 * (ci[a] * (1.0 - cj) * tmp0 + cj * (1.0 - ci[a]) * tmp1);
+                dt_i = t_ij;
+                dt_j = t_ij;
+                dg_i = -alpha * (tmp0 * (1.0 - cj) + tmp1 * cj);
+                dg_j = alpha * (tmp1 * (1.0 - ci[a]) + ci[a] * tmp0);
+            }
+            ti[a] += dt_i;
+            gi[a] += dg_i;
+            if (own_j) {
+                atomicAdd(&d.t[(size_t)j * NT + a], -dt_j);
+                atomicAdd(&d.g[(size_t)j * NT + a], dg_j);
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        double s = warp_sum(ti[a]), g = warp_sum(gi[a]);
+        if (lane == 0) {
+            atomicAdd(&d.t[(size_t)i * NT + a], s);
+            atomicAdd(&d.g[(size_t)i * NT + a], g);
+        }
+    }
+}
+
+// v and the t-weighted g terms over the full list (ff_dmd_I.cpp:2612-2644).
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
+{
+    using S = Slots<NT>;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    double dEi[NT], ti[NT], vi[NT], gi[NT];
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        dEi[a] = d.dE[(size_t)i * NT + a];
+        ti[a] = d.t[(size_t)i * NT + a];
+        vi[a] = gi[a] = 0.0;
+    }
+    double ba = d.beta * alpha;
+    int nn = d.nnb[i];
+    for (int k = lane; k < nn; k += 32) {
+        long long slot = (long long)i * d.maxnb + k;
+        int j = d.nbr[slot];
+        int oj = owner(d, j);
+        double dEj[NT], tj[NT], vj[NT], gj[NT];
+#pragma unroll
+        for (int b = 0; b < NT; b++) {
+            dEj[b] = d.dE[(size_t)oj * NT + b];
+            tj[b] = d.t[(size_t)oj * NT + b];
+            vj[b] = gj[b] = 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < NT; a++)
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                double r_ab = d.pr[(size_t)(a * NT + b) * d.maxp + slot];  // type2rho[jtype][itype]
+                double r_ba = d.pr[(size_t)(b * NT + a) * d.maxp + slot];  // type2rho[itype][jtype]
+                double tmp0 = d.pr[(size_t)(S::PHI + comp_idx(b, a)) * d.maxp + slot] + r_ab * dEi[a] + r_ba * dEj[b];
+                tmp0 *= ba;
+                vi[a] += r_ab * tj[b];
+                gi[a] += tmp0 * tj[b];
+                vj[b] += r_ba * ti[a];
+                gj[b] += tmp0 * ti[a];
+            }
+        if (j < d.natms) {
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                if (vj[b] != 0.0) atomicAdd(&d.v[(size_t)j * NT + b], vj[b]);
+                if (gj[b] != 0.0) atomicAdd(&d.g[(size_t)j * NT + b], gj[b]);
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        double s = warp_sum(vi[a]), g = warp_sum(gi[a]);
+        if (lane == 0) {
+            atomicAdd(&d.v[(size_t)i * NT + a], s);
+            atomicAdd(&d.g[(size_t)i * NT + a], g);
+        }
+    }
+}
+
+// last g terms with ddE (ff_dmd_I.cpp:2649-2670).
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
+{
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    double wi[NT], gi[NT];
+    double ab = alpha * d.beta;
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        size_t q = (size_t)i * NT + a;
+        wi[a] = d.ddE[q] * d.c[q] * d.v[q];
+        gi[a] = 0.0;
+    }
+    int nn = d.nnb[i];
+    for (int k = lane; k < nn; k += 32) {
+        long long slot = (long long)i * d.maxnb + k;
+        int j = d.nbr[slot];
+        int oj = owner(d, j);
+        double wj[NT], gj[NT];
+#pragma unroll
+        for (int b = 0; b < NT; b++) {
+            size_t q = (size_t)oj * NT + b;
+            wj[b] = d.ddE[q] * d.c[(size_t)j * NT + b] * d.v[q];
+            gj[b] = 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < NT; a++)
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                gi[a] += ab * d.pr[(size_t)(b * NT + a) * d.maxp + slot] * wj[b];
+                gj[b] += ab * d.pr[(size_t)(a * NT + b) * d.maxp + slot] * wi[a];
+            }
+        if (j < d.natms) {
+#pragma unroll
+            for (int b = 0; b < NT; b++)
+                if (gj[b] != 0.0) atomicAdd(&d.g[(size_t)j * NT + b], gj[b]);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        double g = warp_sum(gi[a]);
+        if (lane == 0) atomicAdd(&d.g[(size_t)i * NT + a], g);
+    }
+}
+
+template <int NT>
+cudaError_t dmd_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st)
+{
+    int g1 = div_up((long long)d.natms * 32, kFFBlock), g2 = div_up(d.natms, kFFBlock);
+    k_dmd_pass1<NT><<<g1, kFFBlock, 0, st>>>(d, 0);
+    k_dmd_embed<NT><<<g2, kFFBlock, 0, st>>>(d, 1, g1);
+    k_dmd_pass2<NT><<<g1, kFFBlock, 0, st>>>(d, st_clc, g1 + g2);
+    *nb = 2 * g1 + g2;
+    return cudaGetLastError();
+}
+
+template <int NT>
+cudaError_t dmd_energy_nt(const Dev& d, int* nb, cudaStream_t st)
+{
+    int g1 = div_up((long long)d.natms * 32, kFFBlock), g2 = div_up(d.natms, kFFBlock);
+    k_dmd_energy_pass<NT><<<g1, kFFBlock, 0, st>>>(d, 0);
+    k_dmd_embed<NT><<<g2, kFFBlock, 0, st>>>(d, 0, g1);
+    *nb = g1 + g2;
+    return cudaGetLastError();
+}
+
+template <int NT>
+cudaError_t dmd_cdot_nt(const Dev& d, cudaStream_t st)
+{
+    int gw = div_up((long long)d.natms * 32, kFFBlock), gs = div_up((long long)d.natms * NT, kFFBlock);
+    k_mu_E<NT><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_embed<NT><<<gs, kFFBlock, 0, st>>>(d, 0);
+    k_mu_npairs<NT><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_nfinal<NT><<<gs, kFFBlock, 0, st>>>(d, d.style == STYLE_DMD_II ? 1 : 0);
+    k_cd_rates<NT><<<gw, kFFBlock, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+template <int NT>
+cudaError_t dmd_calc_g_nt(const Dev& d, int chk, double alpha, int* nb, cudaStream_t st)
+{
+    int gw = div_up((long long)d.natms * 32, kFFBlock), gs = div_up((long long)d.natms * NT, kFFBlock);
+    k_mu_E<NT><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_embed<NT><<<gs, kFFBlock, 0, st>>>(d, 1);
+    k_mu_npairs<NT><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_nfinal<NT><<<gs, kFFBlock, 0, st>>>(d, d.style == STYLE_DMD_II ? 3 : 2);
+    k_g_sinit<NT><<<gs, kFFBlock, 0, st>>>(d);
+    k_g_srates<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
+    k_g_cost<NT><<<gs, kFFBlock, 0, st>>>(d, 0);
+    *nb = gs;
+    if (!chk) {
+        k_g_trates<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
+        k_g_vpass<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
+        k_g_last<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_dmd_force(const Dev& d, int st_clc, int* nb, cudaStream_t st)
+{
+    switch (d.nt) {
+    case 1: return dmd_force_nt<1>(d, st_clc, nb, st);
+    case 2: return dmd_force_nt<2>(d, st_clc, nb, st);
+    case 3: return dmd_force_nt<3>(d, st_clc, nb, st);
+    case 4: return dmd_force_nt<4>(d, st_clc, nb, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_dmd_energy(const Dev& d, int* nb, cudaStream_t st)
+{
+    switch (d.nt) {
+    case 1: return dmd_energy_nt<1>(d, nb, st);
+    case 2: return dmd_energy_nt<2>(d, nb, st);
+    case 3: return dmd_energy_nt<3>(d, nb, st);
+    case 4: return dmd_energy_nt<4>(d, nb, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_dmd_crd(const Dev& d, cudaStream_t st)
+{
+    if (d.natms) k_dmd_crd<<<div_up((long long)d.natms * 32, kFFBlock), kFFBlock, 0, st>>>(d);
+    if (d.nph) k_crd_ghosts<<<div_up(d.nph, kFFBlock), kFFBlock, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st)
+{
+    switch (d.nt) {
+    case 1: return dmd_cdot_nt<1>(d, st);
+    case 2: return dmd_cdot_nt<2>(d, st);
+    case 3: return dmd_cdot_nt<3>(d, st);
+    case 4: return dmd_cdot_nt<4>(d, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nb, cudaStream_t st)
+{
+    switch (d.nt) {
+    case 1: return dmd_calc_g_nt<1>(d, chk, alpha, nb, st);
+    case 2: return dmd_calc_g_nt<2>(d, chk, alpha, nb, st);
+    case 3: return dmd_calc_g_nt<3>(d, chk, alpha, nb, st);
+    case 4: return dmd_calc_g_nt<4>(d, chk, alpha, nb, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace mg

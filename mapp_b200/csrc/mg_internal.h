@@ -1,0 +1,144 @@
+// Internal state and kernel launchers of the mapp_b200 library.
+//
+// Device data layout (reference index space: owned atoms [0, natms) first,
+// then ghosts [natms, natms+nph) in the exact order Atoms::ph_setup creates
+// them, atoms.cpp:317-372):
+//   pos[i]    double4  Cartesian x, y, z (w = 0)              owned + ghost
+//   sfr[i]    double4  fractional s during a rebuild          owned + ghost
+//   alpha[i*nt+a], c[i*nt+a]   DMD per-site vectors           owned + ghost
+//   type[i]   int      species (EAM / FS)                     owned + ghost
+//   root[g]   int      owned atom a ghost images (owned: itself)
+//   gchain[g] uint64   the ordered (dim, dir) image shifts that made ghost g
+//                      from root[g]: 4 bits each, low bits first, bit 3 set
+//                      marks a used slot; ghosts refresh as
+//                      x_g = ((x_root (+-) H[d1]) (+-) H[d2]) ... in that order,
+//                      the same sequence of additions as Atoms::update
+//                      (atoms.cpp:1320-1352) performs along the swap chain.
+//   nbr[i*maxnb+k] int half neighbour list (j > i), nnb[i] its length
+//   pair slots (DMD)  SoA over pair index i*maxnb+k, 21 double per pair for
+//                      two species: rho[nt*nt], drho_dr, drho_dalpha,
+//                      phi[nt(nt+1)/2], dphi_dr, dphi_dalpha
+// A ghost refresh of a plain vector v is never materialised: kernels read
+// v[root[j]] for j >= natms.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+namespace mg {
+
+enum Style { STYLE_EAM = 0, STYLE_FS = 1, STYLE_DMD_I = 2, STYLE_DMD_II = 3, STYLE_DMD = 4 };
+
+constexpr int kMaxTypes = 4;
+constexpr int kMaxQuad = 14;
+constexpr int kMaxChain = 15;
+
+// Everything a kernel needs, passed by value.
+struct Dev {
+    // sizes
+    int natms, nph, nall, nt, x_dim, maxnb, maxcrd, style, form;
+    // box
+    double H[3][3], B[3][3];
+    double cut_ph_s[3], s_ph_lo[3], s_ph_hi[3];
+    int grid[3], denom[3], tot_bin;
+    // atoms
+    double4* pos;
+    double4* sfr;
+    double4* pos0;
+    double* alpha;
+    double* c;
+    int* type;
+    int* root;
+    unsigned long long* gchain;
+    // bins / list
+    int* bin;
+    int* cell_start;
+    int* cell_count;
+    double4* cell_pos;  // sorted copy: x,y,z and (index | type<<24) in .w bits
+    int* nbr;
+    int* nnb;
+    int* crdl;
+    int* ncrd;
+    int* crd;
+    // per-atom FF vectors
+    double* f;     // natms * x_dim
+    double* rho;   // EAM/FS rho then F'(rho), nall
+    double* E;     // nall * nt
+    double* dE;
+    double* ddE;
+    double* n;
+    double* s;
+    double* t;
+    double* v;
+    double* c_d;
+    double* a_in;
+    double* g;
+    // per-pair scratch
+    double* pr;    // EAM/FS: drhoi[maxp], drhoj[maxp]; DMD: 21 SoA blocks of maxp
+    long long maxp;
+    // reductions
+    double* partial;   // [nblocks][8]
+    int* status;       // [0] overflow of nbr, [1] needed maxnb, [2] overflow crd, [3] needed maxcrd
+    // tables (device)
+    int nr, nrho;
+    double dr, drho, dr_inv, drho_inv, rho_max, cut_sq, cut_sq_mod, rc;
+    const double* rhoT;  // [nt*nt][nr][8]
+    const double* phiT;  // [ncomp][nr][8]
+    const double* FT;    // [nt][nrho+1][Fw]
+    int Fw;
+    const float* rhoTf;  // FP32 copies [slot][nr][4] (c0..c3)
+    const float* phiTf;
+    double cut_sk_sq[16];
+    // FS analytic
+    double fsA[kMaxTypes], fst1[kMaxTypes][kMaxTypes], fst2[kMaxTypes][kMaxTypes];
+    double fs_cut_rho[16], fs_cut_phi[16], fsk1[16], fsk2[16], fsk3[16], fs_cut_sq[16];
+    int fs_chk[16];
+    // DMD
+    double rsq_crd, alpha_min, alpha_max, kbT, beta, c0[kMaxTypes];
+    int nq;
+    double xi[kMaxQuad], w0[kMaxQuad], w1[kMaxQuad], w2[kMaxQuad];
+};
+
+__host__ __device__ inline int comp_idx(int i, int j)
+{
+    return i < j ? (j + 1) * j / 2 + i : (i + 1) * i / 2 + j;
+}
+
+// ---- launchers (defined in the .cu files) ---------------------------------
+// atoms / neighbour
+cudaError_t launch_x2s(const Dev& d, cudaStream_t st);
+cudaError_t launch_split_x(const Dev& d, const double* x_aos, int frac, cudaStream_t st);
+cudaError_t launch_ghost_flags(const Dev& d, int lo, int hi, int dim, int dir, int* flags, cudaStream_t st);
+cudaError_t launch_ghost_scatter(const Dev& d, int lo, int hi, int dim, int dir, const int* flags,
+                                 const int* offs, int base, cudaStream_t st);
+cudaError_t launch_bin_and_s2x(const Dev& d, cudaStream_t st);
+cudaError_t launch_cell_fill(const Dev& d, int* cursor, cudaStream_t st);
+cudaError_t launch_neigh(const Dev& d, cudaStream_t st);
+cudaError_t launch_store_x0(const Dev& d, cudaStream_t st);
+cudaError_t launch_skin_check(const Dev& d, double sq_skin, int* flag, cudaStream_t st);
+cudaError_t launch_refresh_x(const Dev& d, cudaStream_t st);
+cudaError_t launch_refresh_c(const Dev& d, cudaStream_t st);
+cudaError_t launch_merge_x(const Dev& d, double* x_aos, int first, int count, cudaStream_t st);
+cudaError_t launch_reduce_partials(const Dev& d, int nblocks, int nvals, double* out, cudaStream_t st);
+size_t scan_temp_bytes(int n);
+cudaError_t launch_exclusive_scan(const int* in, int* out, int n, void* temp, size_t temp_bytes, cudaStream_t st);
+// EAM / FS
+cudaError_t launch_eam_force(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_eam_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_fs_force(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_fs_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
+// DMD
+cudaError_t launch_dmd_force(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_dmd_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_dmd_crd(const Dev& d, cudaStream_t st);
+cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st);
+cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nblocks_out, cudaStream_t st);
+
+// grid sizing helpers
+int num_sms();
+inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace mg

@@ -1,0 +1,46 @@
+// Warp / block reduction helpers shared by the force-field kernels.
+#pragma once
+
+#include "mg_internal.h"
+
+namespace mg {
+
+constexpr int kFFBlock = 256;           // threads per force-field block (8 warps)
+constexpr int kFFWarps = kFFBlock / 32;
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_sumf(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sums NV per-thread values over the block and writes them to
+// partial[(row) * 8 + v] (row = blockIdx.x + row_offset).  Every thread of the
+// block must call it.
+template <int NV>
+__device__ __forceinline__ void block_partials(const double (&vals)[NV], double* partial, int row)
+{
+    __shared__ double sh[kFFWarps][8];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        double s = warp_sum(vals[v]);
+        if (lane == 0) sh[w][v] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = 0.0;
+        for (int k = 0; k < kFFWarps; k++) s += sh[k][threadIdx.x];
+        partial[(size_t)row * 8 + threadIdx.x] = s;
+    }
+}
+
+}  // namespace mg

@@ -56,6 +56,10 @@ class Species:
 
 SPECIES_A = Species("A", MASS_A, 0.35, 2.556, 8.0, 4.0, 1.8)
 SPECIES_B = Species("B", MASS_B, 0.40, 2.49, 8.4, 4.2, 2.0)
+# extra synthetic species for multi-component tests (not part of any benchmark workload)
+SPECIES_C = Species("C", 55.845, 0.38, 2.52, 8.2, 4.1, 1.9)
+SPECIES_D = Species("D", 58.933, 0.36, 2.54, 8.1, 4.05, 1.85)
+ALL_SPECIES = (SPECIES_A, SPECIES_B, SPECIES_C, SPECIES_D)
 
 
 def taper(r: np.ndarray) -> np.ndarray:
@@ -298,7 +302,7 @@ def make_dmd_config(n=20, a=3.58, sigma=0.0, seed=4321, nt=2,
         c[:, 1] = 1.0 - cA
         if nt > 2:
             c[:, 1:] = (1.0 - cA)[:, None] / (nt - 1)
-    return Config(L, s, ["A", "B", "C", "D"][:nt], [MASS_A, MASS_B, 55.845, 58.933][:nt],
+    return Config(L, s, [sp.name for sp in ALL_SPECIES[:nt]], [sp.mass for sp in ALL_SPECIES[:nt]],
                   alpha=alpha, c=c)
 
 
@@ -384,7 +388,7 @@ def write_workload(dirpath: str, kind: str, **kw) -> dict:
         coef_kw = {k: kw.pop(k) for k in ("r_crd", "n_quad", "alpha_min", "alpha_max", "T") if k in kw}
         cfg = make_dmd_config(**kw)
         nt = len(cfg.names)
-        tables = make_tables((SPECIES_A, SPECIES_B)[:nt] if nt <= 2 else (SPECIES_A,) * nt)
+        tables = make_tables(ALL_SPECIES[:nt])
         pot = os.path.join(dirpath, "pot.fs")
         write_fs(pot, tables)
         out["coef"] = dmd_coef_args(pot, **coef_kw)

@@ -312,12 +312,17 @@ void do_setx(const std::string& path, const std::string& prefix)
     double* x = vec<double>("x");
     size_t n = (size_t)atoms->natms * H.x_dim;
     memcpy(x, raw.data(), n * sizeof(double));
-    int before = H.mapp->neighbor->no_pairs;
-    (void)before;
-    /* a rebuild reallocates the list; record whether one happened by comparing list pointers */
-    int** old_list = H.mapp->neighbor->neighbor_list;
+    /* update_0 rewrites x_0 (vector 1) only when it rebuilds (atoms.cpp:1842-1853) */
+    double* x0 = nullptr;
+    atoms->vectors[1].ret(x0);
+    int d0 = atoms->vectors[1].dim;
+    std::vector<double> before(x0, x0 + (size_t)atoms->natms * d0);
     atoms->update_0(0, 1, H.vecs);
-    meta(prefix, "rebuilt %d", H.mapp->neighbor->neighbor_list != old_list ? 1 : 0);
+    atoms->vectors[1].ret(x0);
+    int rebuilt = 0;
+    for (size_t k = 0; k < before.size(); k++)
+        if (before[k] != x0[k]) { rebuilt = 1; break; }
+    meta(prefix, "rebuilt %d", rebuilt);
 }
 
 void do_setc(const std::string& path)

@@ -1,0 +1,80 @@
+"""Pins the C restatement oracle (oracle/mapp_oracle.c) to the compiled
+reference (oracle/_ref/mapp_ref_harness): every output must agree bit for bit.
+
+The reference ships no tests or golden vectors, so this is the pin: the
+restatement, built with the reference's arithmetic flags, reproduces the
+reference's own doubles on seeded fixtures, including the reference defects
+the restatement keeps (DMD energy_calc species loop, dE[jatm+jtype] indexing,
+embedding index clamp nr-2)."""
+import numpy as np
+import pytest
+
+from mapp_b200 import fixtures as fx
+from oracle import reference
+from oracle.restated import Oracle
+
+pytestmark = pytest.mark.skipif(not reference.available(), reason="reference harness not built")
+
+CASES = [
+    ("eam", dict(n=4)),
+    ("eam", dict(n=4, nt=2, fmt="FS")),
+    ("fs", dict(n=4, nt=2)),
+    ("dmd", dict(n=4, sigma=0.02, style="DMD_I")),
+    ("dmd", dict(n=4, sigma=0.02, style="DMD_II")),
+    ("dmd", dict(n=4, sigma=0.02, style="DMD")),
+]
+
+
+def _same(a, b):
+    a = np.asarray(a).ravel()
+    b = np.asarray(b).ravel()
+    assert a.shape == b.shape
+    assert np.array_equal(a, b), f"max |diff| = {np.max(np.abs(a - b))}"
+
+
+@pytest.mark.parametrize("kind,kw", CASES, ids=[f"{k}-{v.get('style', v.get('fmt', 'SetFL'))}-{v.get('nt', 1)}" for k, v in CASES])
+def test_restated_oracle_bit_exact(tmp_path, kind, kw):
+    w = fx.write_workload(str(tmp_path / "w"), kind, **kw)
+    N = w["cfg"].natms
+    run = reference.RefRun(w, workdir=str(tmp_path / "ref")) if False else None
+    import os
+    os.makedirs(tmp_path / "ref", exist_ok=True)
+    rr = reference.RefRun(w, workdir=str(tmp_path / "ref")).dump("s0").force("f0").energy("e0")
+    dmd = w["cfg"].dmd
+    a = np.random.default_rng(7).normal(0, 0.01, (N, 2))
+    if dmd:
+        rr.crd("crd").cdot("cd").calcg(a, 0.001, tag="g")
+    # a displacement within the skin (ghost refresh) then one beyond it (rebuild)
+    o = Oracle(w)
+    x0 = o.x_all()[:N].copy()
+    rng = np.random.default_rng(11)
+    x1 = x0.copy()
+    x1[:, :3] += rng.normal(0, 0.05, (N, 3))
+    x2 = x1.copy()
+    x2[:5, :3] += 0.8
+    rr.setx(x1, tag="u1").force("f1").setx(x2, tag="u2").dump("s2").force("f2")
+    r = rr.run()
+
+    _same(o.x_all(), r["s0"]["x"])
+    ns, fl = o.neighbor_list()
+    _same(ns, r["s0"]["nsize"])
+    _same(fl, r["s0"]["nlist"])
+    f, en = o.force()
+    _same(f, r["f0"]["f"])
+    _same(en, r["f0"]["meta"]["en"])
+    _same(o.energy(), r["e0"]["meta"]["energy"])
+    if dmd:
+        _same(o.crd(), r["crd"]["crd"])
+        _same(o.c_d(), r["cd"]["c_d"])
+        cost, g = o.calc_g(a, 0.001)
+        _same(cost, r["g"]["meta"]["cost"])
+        _same(g, r["g"]["g"])
+    assert o.update_x(x1) == r["u1"]["meta"]["rebuilt"] == 0
+    f1, en1 = o.force()
+    _same(f1, r["f1"]["f"])
+    _same(en1, r["f1"]["meta"]["en"])
+    assert o.update_x(x2) == r["u2"]["meta"]["rebuilt"] == 1
+    _same(o.x_all(), r["s2"]["x"])
+    f2, en2 = o.force()
+    _same(f2, r["f2"]["f"])
+    _same(en2, r["f2"]["meta"]["en"])
