@@ -1,0 +1,382 @@
+"""Benchmark of the MAPP force-field hot path on B200.
+
+Metric: DMD site-force evaluations per second (owned sites x force_calc calls
+/ device seconds) for the binary DMD_I system of FCC 20^3 = 32000 sites
+(a = 3.58 A, alpha = 1/w^2 with w ~ U(0.08, 0.15) A, c_A ~ Beta(2,2),
+n = 3 Gauss-Hermite nodes, T = 600 K), synthetic seeded inputs.
+
+One step = one ForceField::force_calc(1, en_st) of the whole system (both
+passes, embedding and the energy/virial reduction), inputs resident in HBM;
+L2 is flushed (256 MiB write) before every timed step.  `e2e` repeats the step
+through the C ABI with host buffers: owned x and c copied in (update_0 +
+update(c)), forces and en_st copied out.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank relaxes its own independent system (replicas, no
+collective on the data path); `value` sums the sites of all ranks over the
+slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DMD site-force evals/s, surrogate & FP32 vs FP64 on 1 B200 at max|dF|<=1e-4 eV/A"
+UNIT = "site-force evals/s"
+WORKLOAD = dict(n=20, a=3.58, sigma=0.0, style="DMD_I")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cells", type=int, default=WORKLOAD["n"], help="FCC cells per edge (default 20 -> 32000 sites)")
+    p.add_argument("--cpu-reps", type=int, default=0, help="reference force_calc calls per CPU process (0: auto)")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU reference timing")
+    return p.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload_config(args, extra=None):
+    c = {"workload": f"DMD_I binary FCC {args.cells}^3 = {4 * args.cells ** 3} sites, a=3.58 A, "
+                     "w~U(0.08,0.15) A (alpha=1/w^2), c_A~Beta(2,2), n_quad=3, T=600 K, "
+                     "r_crd=3.0, alpha_min=20, alpha_max=1000, skin 0.5 A",
+         "sites": 4 * args.cells ** 3, "species": 2, "step": "force_calc(st_clc=1)",
+         "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if args.gpus > 1 else "1 gpu"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (the reference's own force_calc through oracle/_ref)
+# ---------------------------------------------------------------------------
+def cpu_reference(w, natms, reps, procs):
+    from oracle import reference
+
+    if not reference.available():
+        return None
+    cmds = []
+    for p in range(procs):
+        d = tempfile.mkdtemp(prefix=f"mapp_cpu{p}_")
+        # one untimed call first: the reference allocates its per-pair buffers on the first force_calc
+        rr = reference.RefRun(w, workdir=d).time("force", 1, tag="warm").time("force", reps, tag="t")
+        # reuse RefRun's command-file writer without running it
+        cmds.append(rr)
+    t0 = time.time()
+    threads, results = [], [None] * procs
+
+    def run(k):
+        results[k] = cmds[k].run(timeout=1800)
+
+    for k in range(procs):
+        th = threading.Thread(target=run, args=(k,))
+        th.start()
+        threads.append(th)
+    for th in threads:
+        th.join()
+    wall = time.time() - t0
+    per = [r["t"]["meta"]["time_force"][1] for r in results]
+    value = sum(natms * reps / t for t in per)
+    return dict(value=value, per_proc_s=per, wall=wall)
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from mapp_b200 import fixtures as fx
+
+    d = tempfile.mkdtemp(prefix="mapp_bench_ref_")
+    w = fx.write_workload(d, "dmd", n=args.cells, a=WORKLOAD["a"], sigma=WORKLOAD["sigma"], style="DMD_I")
+    natms = w["cfg"].natms
+    procs = os.cpu_count() or 1
+    reps = max(1, args.cpu_reps or 2)
+    values = []
+    # warm-up calls are part of each process's init (first force_calc); time K steps of `reps` calls
+    steps = max(1, min(args.steps, 3))
+    for _ in range(steps):
+        r = cpu_reference(w, natms, reps, procs)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref/mapp_ref_harness not built"}))
+            return 0
+        values.append(r["value"])
+    value = float(np.median(values))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": natms / value * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                         "sample": f"{procs} concurrent single-rank reference processes x {reps} force_calc calls "
+                                   f"of the {natms}-site system each ({cpu_model()})"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.fp = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fp, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fp.close()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fp:
+            return json.load(fp), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def pass1_flops_per_pair(nt, nq):
+    """Algorithmic FP64 operations of one half pair inside the smeared cut in
+    the force pass 1 (sqrt, division and reciprocal counted as one):
+    10 for the pair geometry, then per species pair 9 for alpha / sqrt /
+    bracket, 21 per quadrature node for the density (node offset, table index,
+    cubic, three weighted sums) and 9 to finish value and both derivatives;
+    per unordered species pair 13 per node and 9 more for phi."""
+    nc = nt * (nt + 1) // 2
+    return 10 + nt * nt * (9 + 21 * nq + 9) + nc * (13 * nq + 9)
+
+
+def run_ours(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    import mapp_b200 as mb
+    from mapp_b200 import fixtures as fx
+
+    d = tempfile.mkdtemp(prefix=f"mapp_bench_{rank}_")
+    w = fx.write_workload(d, "dmd", n=args.cells, a=WORKLOAD["a"], sigma=WORKLOAD["sigma"], style="DMD_I",
+                          seed=4321 + rank)
+    s = mb.system_from_workload(w, device=local)
+    natms = s.natms
+    nt = s.nt
+    cnt = s.counts()
+    f_dev = torch.zeros((natms, s.x_dim), dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    # pairs inside the smeared cut (for the algorithmic FLOP count), from the list itself
+    sizes, pairs = s.neighbor_list()
+    xo = s.get_x()
+    gx, _ = s.ghosts()
+    xall = np.concatenate([xo, gx])[:, :3]
+    ii = np.repeat(np.arange(natms), sizes)
+    rsq = np.sum((xall[ii] - xall[pairs]) ** 2, axis=1)
+    mod_rc = 5.0 + 1.224744871391589 / np.sqrt(20.0)
+    in_cut = int(np.count_nonzero(rsq < mod_rc * mod_rc))
+
+    for _ in range(args.warmup):
+        s.force_calc(1, f=f_dev)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    t_dev = 0.0
+    t_p1 = 0.0
+    with Clocks(local) as clk:
+        wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s.force_calc(1, f=f_dev)
+            t_dev += s.last_time("force")
+            t_p1 += s.last_time("force.pass1")
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+    if ws > 1:
+        tt = torch.tensor([t_dev], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        t_dev = float(tt.item())
+    value = ws * natms * args.steps / (t_dev * 1e-3)
+
+    # end to end through the C ABI with host buffers
+    x_host = torch.from_numpy(xo.copy()).pin_memory()
+    c_host = torch.from_numpy(np.ascontiguousarray(w["cfg"].c)).pin_memory()
+    f_host = torch.zeros((natms, s.x_dim), dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        s.update_x(x_host)
+        s.update_c(c_host)
+        s.force_calc(1, f=f_host)
+    torch.cuda.synchronize()
+    e2e_steps = max(10, args.steps // 4)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.update_x(x_host)
+        s.update_c(c_host)
+        s.force_calc(1, f=f_host)
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if ws > 1:
+        tt = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e_value = ws * natms * e2e_steps / t_e2e
+
+    # side measurements (list build, energy_calc, c_d_calc, calc_g)
+    s.rebuild_list()
+    t_list = s.last_time("list")
+    s.energy_calc()
+    t_energy = s.last_time("energy")
+    s.create_2nd_neigh_lst()
+    s.c_d_calc()
+    t_cd = s.last_time("c_d")
+    s.calc_g(np.zeros((natms, nt)), 1e-3)
+    t_g = s.last_time("calc_g")
+
+    if rank != 0:
+        if ws > 1:
+            dist.destroy_process_group()
+        return 0
+
+    peaks, peak_kind = measured_peaks()
+    p1_ms = t_p1 / args.steps
+    flops = pass1_flops_per_pair(nt, 3) * in_cut
+    # algorithmic DRAM bytes of pass 1: list (4 B) and 21 FP64 per-pair results
+    # written per listed pair, plus site arrays read once (pos 32 B, alpha and c
+    # 8 B per species, owned + ghost) and E written (8 B per species)
+    nall = natms + cnt["nph"]
+    bytes_p1 = cnt["npairs"] * (4 + 8 * (3 * nt * nt + 3 * nt * (nt + 1) // 2)) + nall * (32 + 16 * nt) + natms * 8 * nt
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved_gbs = bytes_p1 / (p1_ms * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "dmd_pass1_traffic.json")
+    if os.path.exists(tf):
+        try:
+            t = json.load(open(tf))
+            traffic = t["bytes_per_site"] * natms
+        except (OSError, KeyError, ValueError):
+            traffic = None
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_dev / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded lattice, alpha and c; random tables of the named potentials)",
+        "form": "plain FP64",
+        "config": workload_config(args, {"pairs": cnt["npairs"], "pairs_in_smeared_cut": in_cut, "ghosts": cnt["nph"]}),
+        "roofline": {"bound": "hbm", "kernel": "k_dmd_pass1", "achieved": achieved_gbs, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved_gbs / hbm, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": bytes_p1, "launch_ms": p1_ms,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "fp64_tflops_achieved": flops / (p1_ms * 1e-3) / 1e12,
+                     "fp64_flops_per_launch": flops},
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": natms * (s.x_dim + nt) * 8, "d2h_bytes_per_step": natms * s.x_dim * 8 + 56,
+                "steps": e2e_steps, "path": "mg_atoms_update_x + mg_atoms_update_c + mg_ff_force_calc, pinned host buffers"},
+        "gpu_launches": 4 * args.steps,
+        "phases_ms": {"force": t_dev / args.steps, "force.pass1": p1_ms, "list_rebuild": t_list,
+                      "energy_calc": t_energy, "c_d_calc": t_cd, "calc_g": t_g},
+        "wall_s": wall,
+        "clocks": clocks,
+    }
+    if not args.no_cpu and ws == 1:
+        reps = args.cpu_reps or 3
+        procs = os.cpu_count() or 1
+        r = cpu_reference(w, natms, reps, procs)
+        if r is not None:
+            line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": procs, "kind": "reference",
+                                    "sample": f"{procs} concurrent single-rank reference processes x {reps} "
+                                              f"force_calc calls of the {natms}-site system ({cpu_model()}), "
+                                              f"{r['wall']:.1f} s"}
+    print(json.dumps(line))
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -128,7 +128,9 @@ int mg_get_vector(mg_system* s, const char* name, double* out);
 /* Per-atom int vectors: "crd" (owned + ghost). */
 int mg_get_int_vector(mg_system* s, const char* name, int* out);
 /* Device time in ms of the last call of each phase, measured with CUDA events
-   on the system's stream: "list", "force", "energy", "c_d", "calc_g". */
+   on the system's stream: "list", "force", "energy", "c_d", "calc_g", and for
+   DMD styles the three force kernels "force.pass1", "force.embed",
+   "force.pass2". */
 int mg_last_time(mg_system* s, const char* phase, double* ms);
 
 #ifdef __cplusplus

@@ -226,7 +226,9 @@ struct mg_system {
     int npair_blocks = 2;
     long long npairs = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};
     double t_list = 0, t_force = 0, t_energy = 0, t_cd = 0, t_g = 0;
+    double t_k[3] = {0, 0, 0};  // DMD force: pass 1, embedding, pass 2
     long long partial_rows = 0;
 };
 
@@ -690,6 +692,7 @@ int mg_create(const char* style, int device, mg_system** out)
     s->own_stream = true;
     cudaEventCreate(&s->ev0);
     cudaEventCreate(&s->ev1);
+    for (int k = 0; k < 4; k++) cudaEventCreate(&s->evk[k]);
     memset(&s->d, 0, sizeof(Dev));
     int r = dalloc(&s->d.status, 8);
     if (!r) r = dalloc(&s->red_out, 8);
@@ -715,6 +718,8 @@ int mg_destroy(mg_system* s)
         if (p) cudaFree(p);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
+    for (int k = 0; k < 4; k++)
+        if (s->evk[k]) cudaEventDestroy(s->evk[k]);
     if (s->own_stream && s->st) cudaStreamDestroy(s->st);
     delete s;
     return MG_OK;
@@ -1011,11 +1016,17 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
         CU(s->style == STYLE_EAM ? launch_eam_force(d, st_clc, &rows, s->st) : launch_fs_force(d, st_clc, &rows, s->st));
     } else {
         CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
-        CU(launch_dmd_force(d, st_clc, &rows, s->st));
+        CU(launch_dmd_force(d, st_clc, &rows, s->st, s->evk));
     }
     double tot[8] = {0};
     CU(launch_reduce_partials(d, rows, 7, s->red_out, s->st));
     CHK(timed_end(s, &s->t_force));
+    if (s->dmd)
+        for (int k = 0; k < 3; k++) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, s->evk[k], s->evk[k + 1]);
+            s->t_k[k] = ms;
+        }
     CU(cudaMemcpyAsync(tot, s->red_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CHK(copy_out(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
     CU(cudaStreamSynchronize(s->st));
@@ -1212,6 +1223,9 @@ int mg_last_time(mg_system* s, const char* phase, double* ms)
     else if (!strcmp(phase, "energy")) *ms = s->t_energy;
     else if (!strcmp(phase, "c_d")) *ms = s->t_cd;
     else if (!strcmp(phase, "calc_g")) *ms = s->t_g;
+    else if (!strcmp(phase, "force.pass1")) *ms = s->t_k[0];
+    else if (!strcmp(phase, "force.embed")) *ms = s->t_k[1];
+    else if (!strcmp(phase, "force.pass2")) *ms = s->t_k[2];
     else return fail(MG_ERR_ARG, "unknown phase %s", phase);
     return MG_OK;
 }

@@ -266,22 +266,35 @@ __global__ void k_merge_x(Dev d, double* __restrict__ x, int first, int count)
     for (int a = 0; a < d.x_dim - 3; a++) p[3 + a] = d.alpha[(size_t)i * d.nt + a];
 }
 
-// Deterministic final reduction of per-block partial sums: one block, each
-// thread strides over blocks for one value column, then a shared-memory tree.
-__global__ void k_reduce_partials(const double* __restrict__ partial, int nblocks, int nvals, double* __restrict__ out)
+// Deterministic final reduction of per-block partial sums: one block of 1024
+// threads; each thread sums its strided rows for all columns at once (rows are
+// 64-byte records), then a warp-shuffle and shared-memory tree per column.
+__global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restrict__ partial, int nblocks, int nvals,
+                                                         double* __restrict__ out)
 {
-    __shared__ double sh[kBlock];
-    for (int v = 0; v < nvals; v++) {
-        double acc = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) acc += partial[(size_t)b * 8 + v];
-        sh[threadIdx.x] = acc;
-        __syncthreads();
-        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-            if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-            __syncthreads();
+    __shared__ double sh[32][8];
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        const double2* row = reinterpret_cast<const double2*>(partial + (size_t)b * 8);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            double2 v = row[q];
+            acc[2 * q] += v.x;
+            acc[2 * q + 1] += v.y;
         }
-        if (threadIdx.x == 0) out[v] = sh[0];
-        __syncthreads();
+    }
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        double s = acc[v];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) sh[w][v] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < nvals) {
+        double s = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += sh[k][threadIdx.x];
+        out[threadIdx.x] = s;
     }
 }
 
@@ -374,7 +387,7 @@ cudaError_t launch_merge_x(const Dev& d, double* x_aos, int first, int count, cu
 
 cudaError_t launch_reduce_partials(const Dev& d, int nblocks, int nvals, double* out, cudaStream_t st)
 {
-    k_reduce_partials<<<1, kBlock, 0, st>>>(d.partial, nblocks, nvals, out);
+    k_reduce_partials<<<1, 1024, 0, st>>>(d.partial, nblocks, nvals, out);
     return cudaGetLastError();
 }
 

@@ -66,20 +66,31 @@ __device__ __forceinline__ void embed_F(const Dev& d, int a, double Ev, double& 
 // One species pair of one site pair: the Gauss-Hermite smearing of r*rho and
 // r*phi (ff_dmd_I.cpp:178-259) or the plain EAM values above alpha_max
 // (ff_dmd_I.cpp:261-310).  Returns false when the reference writes nothing.
-template <bool kPhi, bool kDeriv>
+//
+// NQ > 0 fixes the node count at compile time so the node loop unrolls and
+// the table loads of all nodes issue together; NQ = 0 reads it from d.nq.
+// The branch-deciding quantities (alpha against alpha_min / alpha_max, rsq
+// against the cut-offs) are computed exactly as the reference does; powers of
+// alpha and 1/r come from rsqrt, which moves results by ulps only (the node and
+// table-index decisions they feed are continuous in the result).
+template <bool kPhi, bool kDeriv, int NQ>
 __device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double r, double r_inv, double rsq,
                                       double alpha, double& g0, double& g_dr, double& g_da, double& f0, double& f_dr,
                                       double& f_da)
 {
     if (d.alpha_min < alpha && alpha < d.alpha_max) {
-        double asq = sqrt(alpha);
-        double inv_asq = 1.0 / asq;
+        const int nq = NQ > 0 ? NQ : d.nq;
+        double inv_asq = rsqrt(alpha);
+        double asq = alpha * inv_asq;
+        double inv_alpha = inv_asq * inv_asq;
         double upper = (r + d.rc) * asq, lower = (r - d.rc) * asq;
-        if (!(lower < d.xi[d.nq - 1])) return false;
+        if (!(lower < d.xi[nq - 1])) return false;
         double fa = 0.0, fb = 0.0, fc = 0.0, ga = 0.0, gb = 0.0, gc = 0.0;
         const double* rt = d.rhoT + (size_t)rslot * d.nr * 8;
         const double* pt = d.phiT + (size_t)pslot * d.nr * 8;
-        for (int q = 0; q < d.nq; q++) {
+#pragma unroll
+        for (int q = 0; q < (NQ > 0 ? NQ : kMaxQuad); q++) {
+            if (NQ == 0 && q >= nq) break;
             double xq = d.xi[q];
             if (xq > lower && xq < upper) {
                 double tmp0 = r - xq * inv_asq;
@@ -113,7 +124,7 @@ __device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double
             gb *= sc;
             gc *= sc;
             g_dr = -g0 * r_inv - 2.0 * asq * gb;
-            g_da = (0.5 * g0 - gc) / alpha;
+            g_da = (0.5 * g0 - gc) * inv_alpha;
         }
         if (kPhi) {
             f0 = fa * sc;
@@ -121,7 +132,7 @@ __device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double
                 fb *= sc;
                 fc *= sc;
                 f_dr = -f0 * r_inv - 2.0 * asq * fb;
-                f_da = (0.5 * f0 - fc) / alpha;
+                f_da = (0.5 * f0 - fc) * inv_alpha;
             }
         }
         return true;
@@ -155,14 +166,27 @@ __device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double
 }
 
 // ---- force_calc pass 1 (ff_dmd_I.cpp:156-320) ----------------------------
-template <int NT>
-__global__ void __launch_bounds__(kFFBlock) k_dmd_pass1(Dev d, int row0)
+// G lanes per site (a 16-lane group covers the ~40-50 half pairs of a site in
+// three rounds), persistent grid-stride over sites, per-pair results streamed
+// to the pair scratch as soon as each species pair is done.
+#ifndef MG_DMD_GROUP
+#define MG_DMD_GROUP 32
+#endif
+constexpr int kGroup = MG_DMD_GROUP;
+// resident blocks per SM requested from the compiler for the two force passes
+#ifndef MG_DMD_MINB
+#define MG_DMD_MINB 3
+#endif
+
+template <int NT, int NQ>
+__global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int row0)
 {
     using S = Slots<NT>;
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    constexpr int G = kGroup;
+    const int lane = threadIdx.x & (G - 1);
+    const int ngroups = gridDim.x * (blockDim.x / G);
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (i < d.natms) {
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < d.natms; i += ngroups) {
         double4 xi = d.pos[i];
         double ai[NT], ci[NT], Ei[NT];
 #pragma unroll
@@ -172,7 +196,7 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_pass1(Dev d, int row0)
             Ei[a] = 0.0;
         }
         int nn = d.nnb[i];
-        for (int k = lane; k < nn; k += 32) {
+        for (int k = lane; k < nn; k += G) {
             long long slot = (long long)i * d.maxnb + k;
             int j = d.nbr[slot];
             double4 xj = d.pos[j];
@@ -185,49 +209,47 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_pass1(Dev d, int row0)
             }
             double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
             double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
-            double v[S::TOTAL];
-#pragma unroll
-            for (int q = 0; q < S::TOTAL; q++) v[q] = 0.0;
             bool own_j = j < d.natms;
-            if (rsq < d.cut_sq_mod) {
-                double r = sqrt(rsq);
-                double r_inv = 1.0 / r;
-                double w = own_j ? 0.5 : 0.25;
+            bool in_cut = rsq < d.cut_sq_mod;
+            double r_inv = rsqrt(rsq);
+            double r = rsq * r_inv;
+            double w = own_j ? 0.5 : 0.25;
+            double* out = d.pr + slot;
+            const size_t mp = (size_t)d.maxp;
 #pragma unroll
-                for (int a = 0; a < NT; a++)
+            for (int a = 0; a < NT; a++)
 #pragma unroll
-                    for (int b = 0; b < NT; b++) {
-                        const int rs = b * NT + a, ps = comp_idx(a, b);
+                for (int b = 0; b < NT; b++) {
+                    const int rs = b * NT + a, ps = comp_idx(a, b);
+                    double g0 = 0, gdr = 0, gda = 0, f0 = 0, fdr = 0, fda = 0;
+                    bool hit = false;
+                    if (in_cut) {
                         double alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
-                        double g0 = 0, gdr = 0, gda = 0, f0 = 0, fdr = 0, fda = 0;
-                        bool hit = (a >= b) ? smear<true, true>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr, gda, f0, fdr, fda)
-                                            : smear<false, true>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr, gda, f0, fdr, fda);
-                        if (hit) {
-                            v[S::RHO + rs] = g0;
-                            v[S::DRR + rs] = gdr;
-                            v[S::DRA + rs] = gda;
-                            if (a >= b) {
-                                v[S::PHI + ps] = f0;
-                                v[S::DPR + ps] = fdr;
-                                v[S::DPA + ps] = fda;
-                                acc[0] += w * (cj[b] * ci[a] + cj[a] * ci[b]) * f0;
-                            }
-                            Ei[a] += g0 * cj[b];
-                            Ej[b] += g0 * ci[a];
-                        }
+                        hit = (a >= b) ? smear<true, true, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr, gda, f0, fdr, fda)
+                                       : smear<false, true, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr, gda, f0, fdr, fda);
                     }
-                if (own_j) {
-#pragma unroll
-                    for (int b = 0; b < NT; b++)
-                        if (Ej[b] != 0.0) atomicAdd(&d.E[(size_t)j * NT + b], Ej[b]);
+                    if (!hit) g0 = gdr = gda = f0 = fdr = fda = 0.0;
+                    __stcs(out + (S::RHO + rs) * mp, g0);
+                    __stcs(out + (S::DRR + rs) * mp, gdr);
+                    __stcs(out + (S::DRA + rs) * mp, gda);
+                    if (a >= b) {
+                        __stcs(out + (S::PHI + ps) * mp, f0);
+                        __stcs(out + (S::DPR + ps) * mp, fdr);
+                        __stcs(out + (S::DPA + ps) * mp, fda);
+                        acc[0] += w * (cj[b] * ci[a] + cj[a] * ci[b]) * f0;
+                    }
+                    Ei[a] += g0 * cj[b];
+                    Ej[b] += g0 * ci[a];
                 }
-            }
+            if (own_j && in_cut) {
 #pragma unroll
-            for (int q = 0; q < S::TOTAL; q++) d.pr[(size_t)q * d.maxp + slot] = v[q];
+                for (int b = 0; b < NT; b++)
+                    if (Ej[b] != 0.0) atomicAdd(&d.E[(size_t)j * NT + b], Ej[b]);
+            }
         }
 #pragma unroll
         for (int a = 0; a < NT; a++) {
-            double s = warp_sum(Ei[a]);
+            double s = group_sum<G>(Ei[a]);
             if (lane == 0) atomicAdd(&d.E[(size_t)i * NT + a], s);
         }
     }
@@ -259,13 +281,15 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_embed(Dev d, int with_force, i
 
 // ---- force_calc pass 2 (ff_dmd_I.cpp:357-436) ----------------------------
 template <int NT>
-__global__ void __launch_bounds__(kFFBlock) k_dmd_pass2(Dev d, int st_clc, int row0)
+__global__ void __launch_bounds__(kFFBlock, 2) k_dmd_pass2(Dev d, int st_clc, int row0)
 {
     using S = Slots<NT>;
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    constexpr int G = 32;
+    const int lane = threadIdx.x & (G - 1);
+    const int ngroups = gridDim.x * (blockDim.x / G);
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (i < d.natms) {
+    const size_t mp = (size_t)d.maxp;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < d.natms; i += ngroups) {
         double4 xi = d.pos[i];
         double ai[NT], ci[NT], dEi[NT], fi[3 + NT];
 #pragma unroll
@@ -277,24 +301,23 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_pass2(Dev d, int st_clc, int r
 #pragma unroll
         for (int q = 0; q < 3 + NT; q++) fi[q] = 0.0;
         int nn = d.nnb[i];
-        for (int k = lane; k < nn; k += 32) {
+        for (int k = lane; k < nn; k += G) {
             long long slot = (long long)i * d.maxnb + k;
+            const double* in = d.pr + slot;
             int j = d.nbr[slot];
             int oj = owner(d, j);
             double4 xj = d.pos[j];
-            double aj[NT], cj[NT], dEj[NT], fj[3 + NT];
+            double aj[NT], cj[NT], dEj[NT], fj[NT];
 #pragma unroll
             for (int b = 0; b < NT; b++) {
                 aj[b] = d.alpha[(size_t)j * NT + b];
                 cj[b] = d.c[(size_t)j * NT + b];
                 dEj[b] = d.dE[(size_t)oj * NT + b];
+                fj[b] = 0.0;
             }
-#pragma unroll
-            for (int q = 0; q < 3 + NT; q++) fj[q] = 0.0;
             double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
-            double r_inv = 1.0 / sqrt(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
+            double r_inv = rsqrt(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
             bool own_j = j < d.natms;
-            double wv = own_j ? 1.0 : 0.5;
             double fsum = 0.0;
 #pragma unroll
             for (int a = 0; a < NT; a++)
@@ -302,24 +325,22 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_pass2(Dev d, int st_clc, int r
                 for (int b = 0; b < NT; b++) {
                     const int ab = a * NT + b, ba = b * NT + a, ps = comp_idx(a, b);
                     double cc = ci[a] * cj[b];
-                    double fpair = -(d.pr[(size_t)(S::DRR + ab) * d.maxp + slot] * dEi[a] +
-                                     d.pr[(size_t)(S::DRR + ba) * d.maxp + slot] * dEj[b] +
-                                     d.pr[(size_t)(S::DPR + ps) * d.maxp + slot]) *
+                    double fpair = -(__ldcs(in + (S::DRR + ab) * mp) * dEi[a] + __ldcs(in + (S::DRR + ba) * mp) * dEj[b] +
+                                     __ldg(in + (S::DPR + ps) * mp)) *
                                    cc * r_inv;
                     double sa = ai[a] + aj[b];
-                    double apair = -(d.pr[(size_t)(S::DRA + ab) * d.maxp + slot] * dEi[a] +
-                                     d.pr[(size_t)(S::DRA + ba) * d.maxp + slot] * dEj[b] +
-                                     d.pr[(size_t)(S::DPA + ps) * d.maxp + slot]) *
+                    double apair = -(__ldcs(in + (S::DRA + ab) * mp) * dEi[a] + __ldcs(in + (S::DRA + ba) * mp) * dEj[b] +
+                                     __ldg(in + (S::DPA + ps) * mp)) *
                                    cc / (sa * sa);
                     fsum += fpair;
                     fi[3 + a] += apair * aj[b] * aj[b];
-                    fj[3 + b] += apair * ai[a] * ai[a];
+                    fj[b] += apair * ai[a] * ai[a];
                 }
             fi[0] += dx0 * fsum;
             fi[1] += dx1 * fsum;
             fi[2] += dx2 * fsum;
             if (st_clc) {
-                double wf = wv * fsum;
+                double wf = (own_j ? 1.0 : 0.5) * fsum;
                 acc[1] -= wf * dx0 * dx0;
                 acc[2] -= wf * dx1 * dx1;
                 acc[3] -= wf * dx2 * dx2;
@@ -336,12 +357,12 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_pass2(Dev d, int st_clc, int r
                 }
 #pragma unroll
                 for (int b = 0; b < NT; b++)
-                    if (fj[3 + b] != 0.0) atomicAdd(fjp + 3 + b, fj[3 + b]);
+                    if (fj[b] != 0.0) atomicAdd(fjp + 3 + b, fj[b]);
             }
         }
 #pragma unroll
         for (int q = 0; q < 3 + NT; q++) {
-            double s = warp_sum(fi[q]);
+            double s = group_sum<G>(fi[q]);
             if (lane == 0) atomicAdd(d.f + (size_t)i * d.x_dim + q, s);
         }
     }
@@ -349,7 +370,7 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_pass2(Dev d, int st_clc, int r
 }
 
 // ---- energy_calc pass (ff_dmd_I.cpp:489-633): species pairs b >= a only --
-template <int NT>
+template <int NT, int NQ>
 __global__ void __launch_bounds__(kFFBlock) k_dmd_energy_pass(Dev d, int row0)
 {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -390,8 +411,8 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_energy_pass(Dev d, int row0)
                     const int rs = b * NT + a, ps = comp_idx(a, b);
                     double alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
                     double g0 = 0, f0 = 0, u0, u1, u2, u3;
-                    bool hit = (a == b) ? smear<true, false>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3)
-                                        : smear<false, false>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3);
+                    bool hit = (a == b) ? smear<true, false, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3)
+                                        : smear<false, false, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3);
                     if (hit) {
                         Ei[a] += g0 * cj[b];
                         Ej[b] += g0 * ci[a];
@@ -897,13 +918,19 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
 }
 
 template <int NT>
-cudaError_t dmd_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st)
+cudaError_t dmd_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
 {
-    int g1 = div_up((long long)d.natms * 32, kFFBlock), g2 = div_up(d.natms, kFFBlock);
-    k_dmd_pass1<NT><<<g1, kFFBlock, 0, st>>>(d, 0);
+    int g1 = persistent_grid((long long)d.natms * kGroup, MG_DMD_MINB), g2 = div_up(d.natms, kFFBlock);
+    int g3 = persistent_grid((long long)d.natms * 32, 2);
+    if (evs) cudaEventRecord(evs[0], st);
+    if (d.nq == 3) k_dmd_pass1<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
+    else k_dmd_pass1<NT, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
+    if (evs) cudaEventRecord(evs[1], st);
     k_dmd_embed<NT><<<g2, kFFBlock, 0, st>>>(d, 1, g1);
-    k_dmd_pass2<NT><<<g1, kFFBlock, 0, st>>>(d, st_clc, g1 + g2);
-    *nb = 2 * g1 + g2;
+    if (evs) cudaEventRecord(evs[2], st);
+    k_dmd_pass2<NT><<<g3, kFFBlock, 0, st>>>(d, st_clc, g1 + g2);
+    if (evs) cudaEventRecord(evs[3], st);
+    *nb = g1 + g2 + g3;
     return cudaGetLastError();
 }
 
@@ -911,7 +938,8 @@ template <int NT>
 cudaError_t dmd_energy_nt(const Dev& d, int* nb, cudaStream_t st)
 {
     int g1 = div_up((long long)d.natms * 32, kFFBlock), g2 = div_up(d.natms, kFFBlock);
-    k_dmd_energy_pass<NT><<<g1, kFFBlock, 0, st>>>(d, 0);
+    if (d.nq == 3) k_dmd_energy_pass<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
+    else k_dmd_energy_pass<NT, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
     k_dmd_embed<NT><<<g2, kFFBlock, 0, st>>>(d, 0, g1);
     *nb = g1 + g2;
     return cudaGetLastError();
@@ -951,13 +979,13 @@ cudaError_t dmd_calc_g_nt(const Dev& d, int chk, double alpha, int* nb, cudaStre
 
 }  // namespace
 
-cudaError_t launch_dmd_force(const Dev& d, int st_clc, int* nb, cudaStream_t st)
+cudaError_t launch_dmd_force(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
 {
     switch (d.nt) {
-    case 1: return dmd_force_nt<1>(d, st_clc, nb, st);
-    case 2: return dmd_force_nt<2>(d, st_clc, nb, st);
-    case 3: return dmd_force_nt<3>(d, st_clc, nb, st);
-    case 4: return dmd_force_nt<4>(d, st_clc, nb, st);
+    case 1: return dmd_force_nt<1>(d, st_clc, nb, st, evs);
+    case 2: return dmd_force_nt<2>(d, st_clc, nb, st, evs);
+    case 3: return dmd_force_nt<3>(d, st_clc, nb, st, evs);
+    case 4: return dmd_force_nt<4>(d, st_clc, nb, st, evs);
     default: return cudaErrorInvalidValue;
     }
 }

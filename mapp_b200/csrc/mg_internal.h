@@ -131,7 +131,9 @@ cudaError_t launch_eam_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
 cudaError_t launch_fs_force(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st);
 cudaError_t launch_fs_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
 // DMD
-cudaError_t launch_dmd_force(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st);
+// evs (may be null): 4 events recorded before pass 1, before the embedding
+// kernel, before pass 2 and after pass 2, for per-kernel device times
+cudaError_t launch_dmd_force(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st, cudaEvent_t* evs);
 cudaError_t launch_dmd_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
 cudaError_t launch_dmd_crd(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st);

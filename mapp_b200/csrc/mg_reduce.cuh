@@ -22,6 +22,26 @@ __device__ __forceinline__ float warp_sumf(float v)
     return v;
 }
 
+// Sum over an aligned group of G lanes (G = 8, 16 or 32) of one warp; every
+// lane of the group must call it (other groups of the warp may be elsewhere).
+template <int G>
+__device__ __forceinline__ double group_sum(double v)
+{
+    const unsigned mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
+// Persistent grid size for a force kernel: enough blocks to fill every SM at
+// the kernel's resident-block count, never more than the work needs.
+inline int persistent_grid(long long threads_needed, int blocks_per_sm)
+{
+    long long need = (threads_needed + kFFBlock - 1) / kFFBlock;
+    long long cap = (long long)num_sms() * blocks_per_sm;
+    return (int)(need < cap ? (need > 0 ? need : 1) : cap);
+}
+
 // Sums NV per-thread values over the block and writes them to
 // partial[(row) * 8 + v] (row = blockIdx.x + row_offset).  Every thread of the
 // block must call it.
