@@ -133,6 +133,45 @@ int mg_get_int_vector(mg_system* s, const char* name, int* out);
    "force.pass2". */
 int mg_last_time(mg_system* s, const char* phase, double* ms);
 
+/* ---- allocation-free entry point ---------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc:
+   code where another allocator owns all device memory (a framework's caching
+   allocator, a preallocated pool), code that may not allocate once started,
+   or code that must not trigger the implicit synchronisation an allocation
+   can cause.  It computes the Finnis-Sinclair energy of ForceField_fs::
+   energy_calc (ff_fs.cpp:609-684) from caller-owned device buffers and
+   allocates nothing: its scratch (per-atom densities, per-block partial sums)
+   is one fixed array of MG_NOALLOC_SCRATCH_BYTES in the library's device
+   memory, held by every GPU that loads the library until the process exits.
+     x        nall * 3 Cartesian positions, owned atoms first, then ghosts
+     type     nall species indices
+     nbr_off  natms + 1 offsets into nbr (CSR)
+     nbr      half neighbour list: for owned i, the j > i (indices < nall)
+     energy   one double, host or device
+   x, type, nbr_off and nbr must be device memory; natms may not exceed
+   MG_NOALLOC_MAX_ATOMS (MG_ERR_CAPACITY otherwise).  The first call on a
+   device looks up the scratch's device address with that device current, so
+   make it before any stream capture.  Every call shares the scratch and
+   clears the densities it uses: calls that overlap on the GPU race. */
+#define MG_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define MG_NOALLOC_MAX_ATOMS 1000000
+
+typedef struct mg_fs_coeffs {
+    int ntypes;          /* 1..4 */
+    int chk[10];         /* 1 where the pair is defined, COMP order (i <= j: j(j+1)/2 + i) */
+    double A[4];         /* F = -A sqrt(rho) per type */
+    double t1[4][4];     /* rho coefficients [i][j], as in the coefficient file */
+    double t2[4][4];
+    double cut_rho[10];  /* COMP order */
+    double cut_phi[10];
+    double k1[10];
+    double k2[10];
+    double k3[10];
+} mg_fs_coeffs;
+
+int mg_fs_energy_noalloc(const mg_fs_coeffs* coeffs, int natms, int nall, const double* x, const int* type,
+                         const int* nbr_off, const int* nbr, double* energy, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

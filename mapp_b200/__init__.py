@@ -57,7 +57,17 @@ SIGNATURES = {
     "mg_get_vector": (C.c_int, [_P, C.c_char_p, _P]),
     "mg_get_int_vector": (C.c_int, [_P, C.c_char_p, _P]),
     "mg_last_time": (C.c_int, [_P, C.c_char_p, _D]),
+    "mg_fs_energy_noalloc": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
 }
+
+
+class FsCoeffs(C.Structure):
+    """mg_fs_coeffs of include/mapp_b200.h (analytic Finnis-Sinclair coefficients)."""
+
+    _fields_ = [("ntypes", C.c_int), ("chk", C.c_int * 10), ("A", C.c_double * 4),
+                ("t1", (C.c_double * 4) * 4), ("t2", (C.c_double * 4) * 4),
+                ("cut_rho", C.c_double * 10), ("cut_phi", C.c_double * 10),
+                ("k1", C.c_double * 10), ("k2", C.c_double * 10), ("k3", C.c_double * 10)]
 
 
 class MGError(RuntimeError):
@@ -248,6 +258,15 @@ class System:
         ms = C.c_double(0.0)
         _check(load_library().mg_last_time(self.h, phase.encode(), C.byref(ms)))
         return ms.value
+
+
+def fs_energy_noalloc(coeffs: "FsCoeffs", natms: int, nall: int, x, type, nbr_off, nbr, energy, stream: int = 0):
+    """ForceField_fs::energy_calc from caller-owned device buffers without any
+    allocation in the library (mg_fs_energy_noalloc).  x, type, nbr_off and
+    nbr must be device tensors; energy may be a host numpy array or a device
+    tensor of one double."""
+    _check(load_library().mg_fs_energy_noalloc(C.byref(coeffs), natms, nall, _ptr(x), _ptr(type), _ptr(nbr_off),
+                                               _ptr(nbr), _ptr(energy), stream))
 
 
 def system_from_workload(w: dict, device: int = 0, skin: float = 0.5) -> System:

@@ -183,6 +183,8 @@ std::vector<std::string> tokens(const std::string& line)
 
 }  // namespace
 
+int mg::internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
 struct mg_system {
     int style = 0, form = MG_FORM_FP64, device = 0, nt = 0, x_dim = 3, dmd = 0;
     std::vector<std::string> names;

@@ -139,6 +139,9 @@ cudaError_t launch_dmd_crd(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nblocks_out, cudaStream_t st);
 
+// records msg as the calling thread's last error and returns code
+int internal_fail(int code, const char* msg);
+
 // grid sizing helpers
 int num_sms();
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
