@@ -227,6 +227,7 @@ struct mg_system {
     int crd_built = 0;
     int npair_blocks = 2;
     long long npairs = 0;
+    long long pair_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};
     double t_list = 0, t_force = 0, t_energy = 0, t_cd = 0, t_g = 0;
@@ -311,14 +312,33 @@ int ensure_atoms(mg_system* s, size_t need, size_t keep)
     return MG_OK;
 }
 
+// ELL list storage; EAM / FS keep their two per-pair derivatives in ELL slots
 int ensure_pairs(mg_system* s, int maxnb)
 {
     Dev& d = s->d;
     size_t np = (size_t)s->natms * maxnb;
     CHK(dalloc(&d.nbr, np));
-    CHK(dalloc(&d.pr, np * s->npair_blocks));
     d.maxnb = maxnb;
-    d.maxp = (long long)np;
+    if (!s->dmd) {
+        CHK(dalloc(&d.pr, np * s->npair_blocks));
+        d.maxp = (long long)np;
+    }
+    return MG_OK;
+}
+
+// compact pair list and (DMD) per-pair scratch for npairs pairs
+int ensure_compact(mg_system* s, long long npairs)
+{
+    Dev& d = s->d;
+    if (npairs <= s->pair_cap) return MG_OK;
+    long long cap = npairs + npairs / 5 + 1024;
+    CHK(dalloc(&d.pair_i, (size_t)cap));
+    CHK(dalloc(&d.pair_j, (size_t)cap));
+    if (s->dmd) {
+        CHK(dalloc(&d.pr, (size_t)cap * s->npair_blocks));
+        d.maxp = cap;
+    }
+    s->pair_cap = cap;
     return MG_OK;
 }
 
@@ -463,6 +483,15 @@ int rebuild(mg_system* s)
         CHK(ensure_pairs(s, need));
         if (attempt == 3) return fail(MG_ERR_CAPACITY, "neighbour list capacity could not be met");
     }
+    // compact CSR pair list (pairs sorted by i)
+    CU(cudaMemsetAsync(d.nnb + natms, 0, sizeof(int), st));
+    CU(launch_exclusive_scan(d.nnb, d.poff, natms + 1, s->scan_tmp, s->scan_tmp_bytes, st));
+    int np_h = 0;
+    CU(cudaMemcpyAsync(&np_h, d.poff + natms, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    CHK(ensure_compact(s, np_h));
+    d.npairs = np_h;
+    CU(launch_pairs_compact(d, st));
     CU(launch_store_x0(d, st));
     s->crd_built = 0;
     CU(cudaEventRecord(s->ev1, st));
@@ -712,7 +741,7 @@ int mg_destroy(mg_system* s)
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->st);
     Dev& d = s->d;
-    void* ptrs[] = {d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
+    void* ptrs[] = {d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
                     d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status,
                     s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};
@@ -816,7 +845,9 @@ int mg_atoms_set(mg_system* s, int natms, const double* x, const int* type, cons
     s->cap = 0;
     CHK(ensure_atoms(s, cap0, 0));
     CHK(dalloc(&d.pos0, natms));
-    CHK(dalloc(&d.nnb, natms));
+    CHK(dalloc(&d.nnb, (size_t)natms + 1));
+    CHK(dalloc(&d.poff, (size_t)natms + 1));
+    s->pair_cap = 0;
     CHK(dalloc(&d.ncrd, natms));
     CHK(dalloc(&d.f, (size_t)natms * s->x_dim));
     CHK(dalloc(&d.c_d, (size_t)natms * s->nt));
@@ -1137,6 +1168,7 @@ int mg_ff_fin(mg_system* s)
     if (d.pr) cudaFree(d.pr);
     d.pr = nullptr;
     d.maxp = 0;
+    if (s->dmd) s->pair_cap = 0;
     s->initialized = false;
     s->crd_built = 0;
     return MG_OK;

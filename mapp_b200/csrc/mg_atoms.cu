@@ -205,6 +205,19 @@ __global__ void __launch_bounds__(kBlock) k_neigh(Dev d)
     }
 }
 
+// Compact CSR copy of the half list: pair p = poff[i] + k is (i, nbr[i][k]).
+__global__ void __launch_bounds__(kBlock) k_pairs_compact(Dev d)
+{
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= d.natms) return;
+    int nn = d.nnb[i], o = d.poff[i];
+    for (int k = lane; k < nn; k += 32) {
+        d.pair_i[o + k] = i;
+        d.pair_j[o + k] = d.nbr[(size_t)i * d.maxnb + k];
+    }
+}
+
 __global__ void k_store_x0(Dev d)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -352,6 +365,12 @@ cudaError_t launch_cell_fill(const Dev& d, int* cursor, cudaStream_t st)
 cudaError_t launch_neigh(const Dev& d, cudaStream_t st)
 {
     if (d.natms) k_neigh<<<div_up((long long)d.natms * 32, kBlock), kBlock, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pairs_compact(const Dev& d, cudaStream_t st)
+{
+    if (d.natms) k_pairs_compact<<<div_up((long long)d.natms * 32, kBlock), kBlock, 0, st>>>(d);
     return cudaGetLastError();
 }
 

@@ -166,14 +166,10 @@ __device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double
 }
 
 // ---- force_calc pass 1 (ff_dmd_I.cpp:156-320) ----------------------------
-// G lanes per site (a 16-lane group covers the ~40-50 half pairs of a site in
-// three rounds), persistent grid-stride over sites, per-pair results streamed
-// to the pair scratch as soon as each species pair is done.
-#ifndef MG_DMD_GROUP
-#define MG_DMD_GROUP 32
-#endif
-constexpr int kGroup = MG_DMD_GROUP;
-// resident blocks per SM requested from the compiler for the two force passes
+// One thread per half pair of the compact pair list (pairs sorted by i), so
+// every lane carries work however many neighbours a site has; the i-side sums
+// of a warp are segmented shuffles finished by one atomic per site.  Per-pair
+// results are streamed to the pair scratch at the pair's compact index.
 #ifndef MG_DMD_MINB
 #define MG_DMD_MINB 3
 #endif
@@ -182,30 +178,28 @@ template <int NT, int NQ>
 __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int row0)
 {
     using S = Slots<NT>;
-    constexpr int G = kGroup;
-    const int lane = threadIdx.x & (G - 1);
-    const int ngroups = gridDim.x * (blockDim.x / G);
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const size_t mp = (size_t)d.maxp;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < d.natms; i += ngroups) {
-        double4 xi = d.pos[i];
-        double ai[NT], ci[NT], Ei[NT];
+    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < d.npairs; base += stride) {
+        long long p = base + lane;
+        bool valid = p < d.npairs;
+        int i = valid ? d.pair_i[p] : -1;
+        double Ei[NT];
 #pragma unroll
-        for (int a = 0; a < NT; a++) {
-            ai[a] = d.alpha[(size_t)i * NT + a];
-            ci[a] = d.c[(size_t)i * NT + a];
-            Ei[a] = 0.0;
-        }
-        int nn = d.nnb[i];
-        for (int k = lane; k < nn; k += G) {
-            long long slot = (long long)i * d.maxnb + k;
-            int j = d.nbr[slot];
-            double4 xj = d.pos[j];
-            double aj[NT], cj[NT], Ej[NT];
+        for (int a = 0; a < NT; a++) Ei[a] = 0.0;
+        if (valid) {
+            int j = d.pair_j[p];
+            double4 xi = d.pos[i], xj = d.pos[j];
+            double ai[NT], ci[NT], aj[NT], cj[NT], Ej[NT];
 #pragma unroll
-            for (int b = 0; b < NT; b++) {
-                aj[b] = d.alpha[(size_t)j * NT + b];
-                cj[b] = d.c[(size_t)j * NT + b];
-                Ej[b] = 0.0;
+            for (int a = 0; a < NT; a++) {
+                ai[a] = d.alpha[(size_t)i * NT + a];
+                ci[a] = d.c[(size_t)i * NT + a];
+                aj[a] = d.alpha[(size_t)j * NT + a];
+                cj[a] = d.c[(size_t)j * NT + a];
+                Ej[a] = 0.0;
             }
             double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
             double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
@@ -214,8 +208,7 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int 
             double r_inv = rsqrt(rsq);
             double r = rsq * r_inv;
             double w = own_j ? 0.5 : 0.25;
-            double* out = d.pr + slot;
-            const size_t mp = (size_t)d.maxp;
+            double* out = d.pr + p;
 #pragma unroll
             for (int a = 0; a < NT; a++)
 #pragma unroll
@@ -247,10 +240,11 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int 
                     if (Ej[b] != 0.0) atomicAdd(&d.E[(size_t)j * NT + b], Ej[b]);
             }
         }
+        Seg sg = seg_of(i);
 #pragma unroll
         for (int a = 0; a < NT; a++) {
-            double s = group_sum<G>(Ei[a]);
-            if (lane == 0) atomicAdd(&d.E[(size_t)i * NT + a], s);
+            double t = seg_sum(Ei[a], sg);
+            if (valid && lane == sg.first && t != 0.0) atomicAdd(&d.E[(size_t)i * NT + a], t);
         }
     }
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
@@ -280,40 +274,49 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_embed(Dev d, int with_force, i
 }
 
 // ---- force_calc pass 2 (ff_dmd_I.cpp:357-436) ----------------------------
+// One thread per compact pair: the 14 stored derivatives of a pair are read
+// with coalesced streaming loads; i-side forces by segmented shuffles.
 template <int NT>
-__global__ void __launch_bounds__(kFFBlock, 2) k_dmd_pass2(Dev d, int st_clc, int row0)
+__global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass2(Dev d, int st_clc, int row0)
 {
     using S = Slots<NT>;
-    constexpr int G = 32;
-    const int lane = threadIdx.x & (G - 1);
-    const int ngroups = gridDim.x * (blockDim.x / G);
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
     const size_t mp = (size_t)d.maxp;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < d.natms; i += ngroups) {
-        double4 xi = d.pos[i];
-        double ai[NT], ci[NT], dEi[NT], fi[3 + NT];
-#pragma unroll
-        for (int a = 0; a < NT; a++) {
-            ai[a] = d.alpha[(size_t)i * NT + a];
-            ci[a] = d.c[(size_t)i * NT + a];
-            dEi[a] = d.dE[(size_t)i * NT + a];
-        }
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < d.npairs; base += stride) {
+        long long p = base + lane;
+        bool valid = p < d.npairs;
+        int i = valid ? d.pair_i[p] : -1;
+        double fi[3 + NT];
 #pragma unroll
         for (int q = 0; q < 3 + NT; q++) fi[q] = 0.0;
-        int nn = d.nnb[i];
-        for (int k = lane; k < nn; k += G) {
-            long long slot = (long long)i * d.maxnb + k;
-            const double* in = d.pr + slot;
-            int j = d.nbr[slot];
-            int oj = owner(d, j);
-            double4 xj = d.pos[j];
-            double aj[NT], cj[NT], dEj[NT], fj[NT];
+        if (valid) {
+            const double* in = d.pr + p;
+            double drr[NT * NT], dra[NT * NT], dpr[S::NC], dpa[S::NC];
 #pragma unroll
-            for (int b = 0; b < NT; b++) {
-                aj[b] = d.alpha[(size_t)j * NT + b];
-                cj[b] = d.c[(size_t)j * NT + b];
-                dEj[b] = d.dE[(size_t)oj * NT + b];
-                fj[b] = 0.0;
+            for (int q = 0; q < NT * NT; q++) {
+                drr[q] = __ldcs(in + (S::DRR + q) * mp);
+                dra[q] = __ldcs(in + (S::DRA + q) * mp);
+            }
+#pragma unroll
+            for (int q = 0; q < S::NC; q++) {
+                dpr[q] = __ldcs(in + (S::DPR + q) * mp);
+                dpa[q] = __ldcs(in + (S::DPA + q) * mp);
+            }
+            int j = d.pair_j[p];
+            int oj = owner(d, j);
+            double4 xi = d.pos[i], xj = d.pos[j];
+            double ai[NT], ci[NT], dEi[NT], aj[NT], cj[NT], dEj[NT], fj[NT];
+#pragma unroll
+            for (int a = 0; a < NT; a++) {
+                ai[a] = d.alpha[(size_t)i * NT + a];
+                ci[a] = d.c[(size_t)i * NT + a];
+                dEi[a] = d.dE[(size_t)i * NT + a];
+                aj[a] = d.alpha[(size_t)j * NT + a];
+                cj[a] = d.c[(size_t)j * NT + a];
+                dEj[a] = d.dE[(size_t)oj * NT + a];
+                fj[a] = 0.0;
             }
             double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
             double r_inv = rsqrt(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
@@ -325,20 +328,16 @@ __global__ void __launch_bounds__(kFFBlock, 2) k_dmd_pass2(Dev d, int st_clc, in
                 for (int b = 0; b < NT; b++) {
                     const int ab = a * NT + b, ba = b * NT + a, ps = comp_idx(a, b);
                     double cc = ci[a] * cj[b];
-                    double fpair = -(__ldcs(in + (S::DRR + ab) * mp) * dEi[a] + __ldcs(in + (S::DRR + ba) * mp) * dEj[b] +
-                                     __ldg(in + (S::DPR + ps) * mp)) *
-                                   cc * r_inv;
+                    double fpair = -(drr[ab] * dEi[a] + drr[ba] * dEj[b] + dpr[ps]) * cc * r_inv;
                     double sa = ai[a] + aj[b];
-                    double apair = -(__ldcs(in + (S::DRA + ab) * mp) * dEi[a] + __ldcs(in + (S::DRA + ba) * mp) * dEj[b] +
-                                     __ldg(in + (S::DPA + ps) * mp)) *
-                                   cc / (sa * sa);
+                    double apair = -(dra[ab] * dEi[a] + dra[ba] * dEj[b] + dpa[ps]) * cc / (sa * sa);
                     fsum += fpair;
                     fi[3 + a] += apair * aj[b] * aj[b];
                     fj[b] += apair * ai[a] * ai[a];
                 }
-            fi[0] += dx0 * fsum;
-            fi[1] += dx1 * fsum;
-            fi[2] += dx2 * fsum;
+            fi[0] = dx0 * fsum;
+            fi[1] = dx1 * fsum;
+            fi[2] = dx2 * fsum;
             if (st_clc) {
                 double wf = (own_j ? 1.0 : 0.5) * fsum;
                 acc[1] -= wf * dx0 * dx0;
@@ -360,10 +359,11 @@ __global__ void __launch_bounds__(kFFBlock, 2) k_dmd_pass2(Dev d, int st_clc, in
                     if (fj[b] != 0.0) atomicAdd(fjp + 3 + b, fj[b]);
             }
         }
+        Seg sg = seg_of(i);
 #pragma unroll
         for (int q = 0; q < 3 + NT; q++) {
-            double s = group_sum<G>(fi[q]);
-            if (lane == 0) atomicAdd(d.f + (size_t)i * d.x_dim + q, s);
+            double t = seg_sum(fi[q], sg);
+            if (valid && lane == sg.first && t != 0.0) atomicAdd(d.f + (size_t)i * d.x_dim + q, t);
         }
     }
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
@@ -495,8 +495,8 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
     }
     int nn = d.nnb[i];
     for (int k = lane; k < nn; k += 32) {
-        long long slot = (long long)i * d.maxnb + k;
-        int j = d.nbr[slot];
+        long long slot = (long long)d.poff[i] + k;
+        int j = d.nbr[(size_t)i * d.maxnb + k];
         double cj[NT], Ej[NT];
 #pragma unroll
         for (int b = 0; b < NT; b++) {
@@ -564,8 +564,8 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
     }
     int nn = d.nnb[i];
     for (int k = lane; k < nn; k += 32) {
-        long long slot = (long long)i * d.maxnb + k;
-        int j = d.nbr[slot];
+        long long slot = (long long)d.poff[i] + k;
+        int j = d.nbr[(size_t)i * d.maxnb + k];
         double cj[NT], nj[NT], dEj_q[NT];
 #pragma unroll
         for (int b = 0; b < NT; b++) {
@@ -829,8 +829,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
     double ba = d.beta * alpha;
     int nn = d.nnb[i];
     for (int k = lane; k < nn; k += 32) {
-        long long slot = (long long)i * d.maxnb + k;
-        int j = d.nbr[slot];
+        long long slot = (long long)d.poff[i] + k;
+        int j = d.nbr[(size_t)i * d.maxnb + k];
         int oj = owner(d, j);
         double dEj[NT], tj[NT], vj[NT], gj[NT];
 #pragma unroll
@@ -887,8 +887,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
     }
     int nn = d.nnb[i];
     for (int k = lane; k < nn; k += 32) {
-        long long slot = (long long)i * d.maxnb + k;
-        int j = d.nbr[slot];
+        long long slot = (long long)d.poff[i] + k;
+        int j = d.nbr[(size_t)i * d.maxnb + k];
         int oj = owner(d, j);
         double wj[NT], gj[NT];
 #pragma unroll
@@ -920,8 +920,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
 template <int NT>
 cudaError_t dmd_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
 {
-    int g1 = persistent_grid((long long)d.natms * kGroup, MG_DMD_MINB), g2 = div_up(d.natms, kFFBlock);
-    int g3 = persistent_grid((long long)d.natms * 32, 2);
+    int g1 = persistent_grid(d.npairs, MG_DMD_MINB), g2 = div_up(d.natms, kFFBlock);
+    int g3 = g1;
     if (evs) cudaEventRecord(evs[0], st);
     if (d.nq == 3) k_dmd_pass1<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
     else k_dmd_pass1<NT, 0><<<g1, kFFBlock, 0, st>>>(d, 0);

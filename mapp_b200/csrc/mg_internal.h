@@ -59,7 +59,11 @@ struct Dev {
     int* cell_count;
     double4* cell_pos;  // sorted copy: x,y,z and (index | type<<24) in .w bits
     int* nbr;
-    int* nnb;
+    int* nnb;      // natms + 1 (last entry 0, so its exclusive scan ends in the pair count)
+    int* poff;     // natms + 1: first compact pair of each owned atom
+    int* pair_i;   // compact pair list sorted by i (DMD pair scratch is indexed by it)
+    int* pair_j;
+    long long npairs;
     int* crdl;
     int* ncrd;
     int* crd;
@@ -117,6 +121,7 @@ cudaError_t launch_ghost_scatter(const Dev& d, int lo, int hi, int dim, int dir,
 cudaError_t launch_bin_and_s2x(const Dev& d, cudaStream_t st);
 cudaError_t launch_cell_fill(const Dev& d, int* cursor, cudaStream_t st);
 cudaError_t launch_neigh(const Dev& d, cudaStream_t st);
+cudaError_t launch_pairs_compact(const Dev& d, cudaStream_t st);
 cudaError_t launch_store_x0(const Dev& d, cudaStream_t st);
 cudaError_t launch_skin_check(const Dev& d, double sq_skin, int* flag, cudaStream_t st);
 cudaError_t launch_refresh_x(const Dev& d, cudaStream_t st);

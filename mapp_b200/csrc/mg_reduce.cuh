@@ -33,6 +33,34 @@ __device__ __forceinline__ double group_sum(double v)
     return v;
 }
 
+// Lanes of a warp that hold the same key: pairs are sorted by their first
+// site, so equal keys are contiguous lanes [first, last].
+struct Seg {
+    int first, last;
+};
+
+__device__ __forceinline__ Seg seg_of(int key)
+{
+    unsigned m = __match_any_sync(0xffffffffu, key);
+    Seg s;
+    s.first = __ffs(m) - 1;
+    s.last = 31 - __clz(m);
+    return s;
+}
+
+// Sum of v over the lanes of the caller's segment, returned in the segment's
+// first lane (every lane of the warp must call it).
+__device__ __forceinline__ double seg_sum(double v, const Seg& s)
+{
+    int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double t = __shfl_down_sync(0xffffffffu, v, o);
+        if (lane + o <= s.last) v += t;
+    }
+    return v;
+}
+
 // Persistent grid size for a force kernel: enough blocks to fill every SM at
 // the kernel's resident-block count, never more than the work needs.
 inline int persistent_grid(long long threads_needed, int blocks_per_sm)
