@@ -277,6 +277,30 @@ def run_ours(args):
         t_dev = float(tt.item())
     value = ws * natms * args.steps / (t_dev * 1e-3)
 
+    # precision form on the same system: throughput and error against the FP64 form
+    f64_ref = f_dev.clone()
+    s.force_calc(1, f=f64_ref)
+    _, en64 = s.force_calc(1)
+    s.set_form(mb.MG_FORM_FP32)
+    f32 = torch.zeros_like(f_dev)
+    for _ in range(args.warmup):
+        s.force_calc(1, f=f32)
+    t32 = 0.0
+    t32_p1 = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        _, en32 = s.force_calc(1, f=f32)
+        t32 += s.last_time("force")
+        t32_p1 += s.last_time("force.pass1")
+    fp32_form = {"value": natms * args.steps / (t32 * 1e-3), "unit": UNIT, "ms_per_step": t32 / args.steps,
+                 "pass1_ms": t32_p1 / args.steps,
+                 "max_abs_dF_eV_per_A": float((f32 - f64_ref).abs().max().item()),
+                 "abs_dE_per_site_eV": abs(float(en32[0]) - float(en64[0])) / natms,
+                 "speedup_vs_fp64": t_dev / t32,
+                 "error_reference": "plain FP64 GPU form (itself within 1e-10 of the CPU oracle)"}
+    s.set_form(mb.MG_FORM_FP64)
+
     # end to end through the C ABI with host buffers
     x_host = torch.from_numpy(xo.copy()).pin_memory()
     c_host = torch.from_numpy(np.ascontiguousarray(w["cfg"].c)).pin_memory()
@@ -350,6 +374,7 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": natms * (s.x_dim + nt) * 8, "d2h_bytes_per_step": natms * s.x_dim * 8 + 56,
                 "steps": e2e_steps, "path": "mg_atoms_update_x + mg_atoms_update_c + mg_ff_force_calc, pinned host buffers"},
+        "forms": {"fp32": fp32_form},
         "gpu_launches": 4 * args.steps,
         "phases_ms": {"force": t_dev / args.steps, "force.pass1": p1_ms, "list_rebuild": t_list,
                       "energy_calc": t_energy, "c_d_calc": t_cd, "calc_g": t_g},

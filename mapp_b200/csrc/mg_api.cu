@@ -223,6 +223,7 @@ struct mg_system {
     double* d_rhoT = nullptr;
     double* d_phiT = nullptr;
     double* d_FT = nullptr;
+    float* d_pkT = nullptr;
     int* cursor = nullptr;
     int crd_built = 0;
     int npair_blocks = 2;
@@ -336,6 +337,7 @@ int ensure_compact(mg_system* s, long long npairs)
     CHK(dalloc(&d.pair_j, (size_t)cap));
     if (s->dmd) {
         CHK(dalloc(&d.pr, (size_t)cap * s->npair_blocks));
+        CHK(dalloc(&d.prf, (size_t)cap * s->npair_blocks));
         d.maxp = cap;
     }
     s->pair_cap = cap;
@@ -657,6 +659,25 @@ int upload_tables(mg_system* s)
     d.rhoT = s->d_rhoT;
     d.phiT = s->d_phiT;
     d.FT = s->d_FT;
+    if (s->dmd) {
+        // precision form: {rho c0..c3 of slot b*nt+a, phi c0..c3 of COMP(a,b)} per (a,b) and knot
+        int nt = s->nt, nr = s->nr;
+        std::vector<float> pk((size_t)nt * nt * nr * 8, 0.0f);
+        for (int a = 0; a < nt; a++)
+            for (int b = 0; b < nt; b++)
+                for (int m = 0; m < nr; m++) {
+                    float* dst = pk.data() + (((size_t)(a * nt + b) * nr + m) * 8);
+                    const double* rr = s->rhoT.data() + ((size_t)(b * nt + a) * nr + m) * 8;
+                    for (int k = 0; k < 4; k++) dst[k] = (float)rr[k];
+                    if (a >= b) {
+                        const double* pp = s->phiT.data() + ((size_t)comp_idx(a, b) * nr + m) * 8;
+                        for (int k = 0; k < 4; k++) dst[4 + k] = (float)pp[k];
+                    }
+                }
+        CHK(dalloc(&s->d_pkT, pk.size()));
+        CU(cudaMemcpy(s->d_pkT, pk.data(), pk.size() * sizeof(float), cudaMemcpyHostToDevice));
+        d.pkT = reinterpret_cast<const float4*>(s->d_pkT);
+    }
     d.Fw = s->Fw;
     d.nr = s->nr;
     d.nrho = s->nrho;
@@ -741,7 +762,7 @@ int mg_destroy(mg_system* s)
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->st);
     Dev& d = s->d;
-    void* ptrs[] = {d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
+    void* ptrs[] = {d.prf, s->d_pkT, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
                     d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status,
                     s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};
@@ -769,8 +790,12 @@ int mg_set_stream(mg_system* s, void* stream)
 int mg_set_form(mg_system* s, int form)
 {
     CHK(check_sys(s));
-    if (form != MG_FORM_FP64) return fail(MG_ERR_UNSUPPORTED, "form %d is not available in this build", form);
+    if (form == MG_FORM_FP32 && !s->dmd)
+        return fail(MG_ERR_UNSUPPORTED, "the FP32 precision form is implemented for the DMD styles");
+    if (form != MG_FORM_FP64 && form != MG_FORM_FP32)
+        return fail(MG_ERR_UNSUPPORTED, "form %d is not available in this build", form);
     s->form = form;
+    s->d.form = form;
     return MG_OK;
 }
 
@@ -1049,7 +1074,8 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
         CU(s->style == STYLE_EAM ? launch_eam_force(d, st_clc, &rows, s->st) : launch_fs_force(d, st_clc, &rows, s->st));
     } else {
         CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
-        CU(launch_dmd_force(d, st_clc, &rows, s->st, s->evk));
+        if (s->form == MG_FORM_FP32) CU(launch_dmd_force_f32(d, st_clc, &rows, s->st, s->evk));
+        else CU(launch_dmd_force(d, st_clc, &rows, s->st, s->evk));
     }
     double tot[8] = {0};
     CU(launch_reduce_partials(d, rows, 7, s->red_out, s->st));

@@ -16,52 +16,11 @@
 // alpha outside (alpha_min, alpha_max), no node inside the table) are written
 // as zero, so results never depend on earlier calls.
 #include "mg_reduce.cuh"
+#include "mg_dmd_common.cuh"
 
 namespace mg {
 
 namespace {
-
-constexpr double kPiInSq = 0.564189583547756286948079451561;  // 1/sqrt(pi)
-
-__device__ __forceinline__ int owner(const Dev& d, int j) { return j < d.natms ? j : d.root[j]; }
-
-// c0..c3 of one spline knot (rows of 8 doubles, 64-byte aligned) as two
-// read-only 16-byte loads
-__device__ __forceinline__ double4 knot4(const double* __restrict__ row)
-{
-    double2 lo = __ldg(reinterpret_cast<const double2*>(row));
-    double2 hi = __ldg(reinterpret_cast<const double2*>(row) + 1);
-    return make_double4(lo.x, lo.y, hi.x, hi.y);
-}
-
-template <int NT>
-struct Slots {
-    static constexpr int NC = NT * (NT + 1) / 2;
-    static constexpr int RHO = 0, DRR = NT * NT, DRA = 2 * NT * NT, PHI = 3 * NT * NT, DPR = 3 * NT * NT + NC,
-                         DPA = 3 * NT * NT + 2 * NC, TOTAL = 3 * NT * NT + 3 * NC;
-};
-
-__device__ __forceinline__ double calc_ent(double x)
-{
-    if (x < 1.0e-8 || 0.99999999 < x) return 0.0;
-    return x * log(x) + (1 - x) * log(1 - x);
-}
-
-// F(E), F'(E) (and F''(E)) from the quartic embedding spline (ff_dmd_I.cpp:322-341,
-// interpolate_m ff_dmd_I.cpp:1794-1836); index clamp nr-2 as in the reference.
-__device__ __forceinline__ void embed_F(const Dev& d, int a, double Ev, double& tmp0, double& tmp1, double* dd)
-{
-    double p = Ev * d.drho_inv;
-    int m = min((int)p, d.nr - 2);
-    p -= m;
-    p = fmin(p, 1.0);
-    double p2 = p * p, p3 = p2 * p, p4 = p3 * p;
-    const double* cf = d.FT + ((size_t)a * (d.nrho + 1) + m) * d.Fw;
-    tmp0 = cf[4] * p4 + cf[3] * p3 + cf[2] * p2 + cf[1] * p + cf[0];
-    tmp1 = cf[8] * p3 + cf[7] * p2 + cf[6] * p + cf[5];
-    if (Ev > d.rho_max) tmp0 += tmp1 * (Ev - d.rho_max);
-    if (dd) *dd = (3.0 * cf[8] * p2 + cf[7] * p + cf[6]) * d.drho_inv;
-}
 
 // One species pair of one site pair: the Gauss-Hermite smearing of r*rho and
 // r*phi (ff_dmd_I.cpp:178-259) or the plain EAM values above alpha_max
@@ -481,7 +440,7 @@ __global__ void k_crd_ghosts(Dev d)
 
 // ---- c_d_calc / calc_g shared passes -------------------------------------
 // E from the stored per-pair densities (ff_dmd_I.cpp:2273-2292).
-template <int NT>
+template <int NT, typename P>
 __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
 {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -507,8 +466,8 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
         for (int a = 0; a < NT; a++)
 #pragma unroll
             for (int b = 0; b < NT; b++) {
-                Ei[a] += cj[b] * d.pr[(size_t)(a * NT + b) * d.maxp + slot];
-                Ej[b] += ci[a] * d.pr[(size_t)(b * NT + a) * d.maxp + slot];
+                Ei[a] += cj[b] * (double)pr_ptr<P>(d)[(size_t)(a * NT + b) * d.maxp + slot];
+                Ej[b] += ci[a] * (double)pr_ptr<P>(d)[(size_t)(b * NT + a) * d.maxp + slot];
             }
         if (j < d.natms) {
 #pragma unroll
@@ -548,7 +507,7 @@ __device__ __forceinline__ double dE_flat(const Dev& d, int q)
 }
 
 // chemical-potential pair sums (ff_dmd_I.cpp:2320-2345).
-template <int NT>
+template <int NT, typename P>
 __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
 {
     using S = Slots<NT>;
@@ -577,9 +536,10 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
         for (int a = 0; a < NT; a++)
 #pragma unroll
             for (int b = 0; b < NT; b++) {
-                double ph = d.pr[(size_t)(S::PHI + comp_idx(a, b)) * d.maxp + slot];
-                ni[a] += cj[b] * (d.pr[(size_t)(b * NT + a) * d.maxp + slot] * dEj_q[b] + ph);
-                nj[b] += ci[a] * (d.pr[(size_t)(a * NT + b) * d.maxp + slot] * dEi_q[a] + ph);
+                const P* pr = pr_ptr<P>(d);
+                double ph = pr[(size_t)(S::PHI + comp_idx(a, b)) * d.maxp + slot];
+                ni[a] += cj[b] * ((double)pr[(size_t)(b * NT + a) * d.maxp + slot] * dEj_q[b] + ph);
+                nj[b] += ci[a] * ((double)pr[(size_t)(a * NT + b) * d.maxp + slot] * dEi_q[a] + ph);
             }
         if (j < d.natms) {
 #pragma unroll
@@ -812,7 +772,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_trates(Dev d, double alpha)
 }
 
 // v and the t-weighted g terms over the full list (ff_dmd_I.cpp:2612-2644).
-template <int NT>
+template <int NT, typename P>
 __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
 {
     using S = Slots<NT>;
@@ -843,9 +803,10 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
         for (int a = 0; a < NT; a++)
 #pragma unroll
             for (int b = 0; b < NT; b++) {
-                double r_ab = d.pr[(size_t)(a * NT + b) * d.maxp + slot];  // type2rho[jtype][itype]
-                double r_ba = d.pr[(size_t)(b * NT + a) * d.maxp + slot];  // type2rho[itype][jtype]
-                double tmp0 = d.pr[(size_t)(S::PHI + comp_idx(b, a)) * d.maxp + slot] + r_ab * dEi[a] + r_ba * dEj[b];
+                const P* pr = pr_ptr<P>(d);
+                double r_ab = pr[(size_t)(a * NT + b) * d.maxp + slot];  // type2rho[jtype][itype]
+                double r_ba = pr[(size_t)(b * NT + a) * d.maxp + slot];  // type2rho[itype][jtype]
+                double tmp0 = (double)pr[(size_t)(S::PHI + comp_idx(b, a)) * d.maxp + slot] + r_ab * dEi[a] + r_ba * dEj[b];
                 tmp0 *= ba;
                 vi[a] += r_ab * tj[b];
                 gi[a] += tmp0 * tj[b];
@@ -871,7 +832,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
 }
 
 // last g terms with ddE (ff_dmd_I.cpp:2649-2670).
-template <int NT>
+template <int NT, typename P>
 __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
 {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -901,8 +862,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
         for (int a = 0; a < NT; a++)
 #pragma unroll
             for (int b = 0; b < NT; b++) {
-                gi[a] += ab * d.pr[(size_t)(b * NT + a) * d.maxp + slot] * wj[b];
-                gj[b] += ab * d.pr[(size_t)(a * NT + b) * d.maxp + slot] * wi[a];
+                gi[a] += ab * (double)pr_ptr<P>(d)[(size_t)(b * NT + a) * d.maxp + slot] * wj[b];
+                gj[b] += ab * (double)pr_ptr<P>(d)[(size_t)(a * NT + b) * d.maxp + slot] * wi[a];
             }
         if (j < d.natms) {
 #pragma unroll
@@ -945,25 +906,31 @@ cudaError_t dmd_energy_nt(const Dev& d, int* nb, cudaStream_t st)
     return cudaGetLastError();
 }
 
-template <int NT>
-cudaError_t dmd_cdot_nt(const Dev& d, cudaStream_t st)
+template <int NT, typename P>
+cudaError_t dmd_cdot_ntp(const Dev& d, cudaStream_t st)
 {
     int gw = div_up((long long)d.natms * 32, kFFBlock), gs = div_up((long long)d.natms * NT, kFFBlock);
-    k_mu_E<NT><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_E<NT, P><<<gw, kFFBlock, 0, st>>>(d);
     k_mu_embed<NT><<<gs, kFFBlock, 0, st>>>(d, 0);
-    k_mu_npairs<NT><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_npairs<NT, P><<<gw, kFFBlock, 0, st>>>(d);
     k_mu_nfinal<NT><<<gs, kFFBlock, 0, st>>>(d, d.style == STYLE_DMD_II ? 1 : 0);
     k_cd_rates<NT><<<gw, kFFBlock, 0, st>>>(d);
     return cudaGetLastError();
 }
 
 template <int NT>
-cudaError_t dmd_calc_g_nt(const Dev& d, int chk, double alpha, int* nb, cudaStream_t st)
+cudaError_t dmd_cdot_nt(const Dev& d, cudaStream_t st)
+{
+    return d.form == 1 ? dmd_cdot_ntp<NT, float>(d, st) : dmd_cdot_ntp<NT, double>(d, st);
+}
+
+template <int NT, typename P>
+cudaError_t dmd_calc_g_ntp(const Dev& d, int chk, double alpha, int* nb, cudaStream_t st)
 {
     int gw = div_up((long long)d.natms * 32, kFFBlock), gs = div_up((long long)d.natms * NT, kFFBlock);
-    k_mu_E<NT><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_E<NT, P><<<gw, kFFBlock, 0, st>>>(d);
     k_mu_embed<NT><<<gs, kFFBlock, 0, st>>>(d, 1);
-    k_mu_npairs<NT><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_npairs<NT, P><<<gw, kFFBlock, 0, st>>>(d);
     k_mu_nfinal<NT><<<gs, kFFBlock, 0, st>>>(d, d.style == STYLE_DMD_II ? 3 : 2);
     k_g_sinit<NT><<<gs, kFFBlock, 0, st>>>(d);
     k_g_srates<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
@@ -971,10 +938,17 @@ cudaError_t dmd_calc_g_nt(const Dev& d, int chk, double alpha, int* nb, cudaStre
     *nb = gs;
     if (!chk) {
         k_g_trates<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
-        k_g_vpass<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
-        k_g_last<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
+        k_g_vpass<NT, P><<<gw, kFFBlock, 0, st>>>(d, alpha);
+        k_g_last<NT, P><<<gw, kFFBlock, 0, st>>>(d, alpha);
     }
     return cudaGetLastError();
+}
+
+template <int NT>
+cudaError_t dmd_calc_g_nt(const Dev& d, int chk, double alpha, int* nb, cudaStream_t st)
+{
+    return d.form == 1 ? dmd_calc_g_ntp<NT, float>(d, chk, alpha, nb, st)
+                       : dmd_calc_g_ntp<NT, double>(d, chk, alpha, nb, st);
 }
 
 }  // namespace

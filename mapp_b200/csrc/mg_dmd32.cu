@@ -1,0 +1,381 @@
+// Precision form (MG_FORM_FP32) of ForceField_DMD_I/II/DMD::force_calc
+// (ff_dmd_I.cpp:88-450): the per-pair work -- pair geometry after the cut
+// test, the Gauss-Hermite smearing, the spline lookups and the force
+// projections -- runs in FP32; per-site density and force sums are
+// compensated; the cut test on rsq, the per-site embedding F(E) and the energy
+// and virial totals stay FP64.
+//
+// Tables: one 32-byte sector per ordered species pair (a,b) and knot,
+// {rho c0..c3 of density slot b*nt+a, phi c0..c3 of slot COMP(a,b)}, so a
+// quadrature node costs one sector where the FP64 form needs two.
+//
+// Per-site sums: a site's i-side pairs are summed inside the warp with TwoSum
+// (error-free addition) steps, and every contribution is accumulated into the
+// site's FP64 density / force with a fire-and-forget atomic add.  A Kahan
+// (sum, compensation) float pair would need a compare-and-swap round trip per
+// update, which measured 1.5x slower for the whole force call; the FP64
+// accumulator is at least as accurate.
+#include "mg_reduce.cuh"
+#include "mg_dmd_common.cuh"
+
+namespace mg {
+namespace {
+
+#ifndef MG_DMD32_MINB
+#define MG_DMD32_MINB 4
+#endif
+
+constexpr float kPiInSqF = 0.564189583547756286948079451561f;
+
+// Accumulate a compensated (hi, lo) FP32 value into an FP64 per-site sum.
+__device__ __forceinline__ void acc_add(double* dst, float hi, float lo)
+{
+    double v = (double)hi + (double)lo;
+    if (v != 0.0) atomicAdd(dst, v);
+}
+
+// TwoSum-compensated sum over the caller's segment of lanes; the first lane of
+// the segment receives (hi, lo) with value hi + lo.
+__device__ __forceinline__ float2 seg_sum2(float v, const Seg& s)
+{
+    int lane = threadIdx.x & 31;
+    float hi = v, lo = 0.0f;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        float h2 = __shfl_down_sync(0xffffffffu, hi, o);
+        float l2 = __shfl_down_sync(0xffffffffu, lo, o);
+        if (lane + o <= s.last) {
+            float t = hi + h2;
+            float bp = t - hi;
+            float err = (hi - (t - bp)) + (h2 - bp);
+            hi = t;
+            lo = lo + l2 + err;
+        }
+    }
+    return make_float2(hi, lo);
+}
+
+struct F32Consts {
+    float rc, dr_inv, alpha_min, alpha_max;
+    int nr;
+};
+
+__device__ __forceinline__ F32Consts f32_consts(const Dev& d)
+{
+    F32Consts c;
+    c.rc = (float)d.rc;
+    c.dr_inv = (float)d.dr_inv;
+    c.alpha_min = (float)d.alpha_min;
+    c.alpha_max = (float)d.alpha_max;
+    c.nr = d.nr;
+    return c;
+}
+
+// FP32 counterpart of smear() in mg_dmd.cu: one species pair of one site pair.
+template <bool kPhi, int NQ>
+__device__ __forceinline__ bool smear_f(const Dev& d, const F32Consts& k, const float4* __restrict__ pk, float r,
+                                        float r_inv, bool below_rc, float alpha, float& g0, float& g_dr, float& g_da,
+                                        float& f0, float& f_dr, float& f_da)
+{
+    if (k.alpha_min < alpha && alpha < k.alpha_max) {
+        const int nq = NQ > 0 ? NQ : d.nq;
+        float inv_asq = rsqrtf(alpha);
+        float asq = alpha * inv_asq;
+        float inv_alpha = inv_asq * inv_asq;
+        float upper = (r + k.rc) * asq, lower = (r - k.rc) * asq;
+        if (!(lower < (float)d.xi[nq - 1])) return false;
+        float fa = 0.f, fb = 0.f, fc = 0.f, ga = 0.f, gb = 0.f, gc = 0.f;
+#pragma unroll
+        for (int q = 0; q < (NQ > 0 ? NQ : kMaxQuad); q++) {
+            if (NQ == 0 && q >= nq) break;
+            float xq = (float)d.xi[q];
+            if (xq > lower && xq < upper) {
+                float tmp0 = r - xq * inv_asq;
+                float p = fabsf(tmp0) * k.dr_inv;
+                int m = min((int)p, k.nr - 2);
+                p -= (float)m;
+                p = fminf(p, 1.0f);
+                float p2 = p * p, p3 = p2 * p;
+                float4 cr = __ldg(pk + 2 * m);
+                float tmp2 = (cr.w * p3 + cr.z * p2 + cr.y * p + cr.x) * tmp0;
+                float w0 = (float)d.w0[q], w1 = (float)d.w1[q], w2 = (float)d.w2[q];
+                ga += w0 * tmp2;
+                gb += w1 * tmp2;
+                gc += w2 * tmp2;
+                if (kPhi) {
+                    float4 cp = __ldg(pk + 2 * m + 1);
+                    float tmp1 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
+                    if (tmp0 < 0.0f) tmp1 = -tmp1;
+                    fa += w0 * tmp1;
+                    fb += w1 * tmp1;
+                    fc += w2 * tmp1;
+                }
+            }
+        }
+        float sc = kPiInSqF * r_inv;
+        g0 = ga * sc;
+        gb *= sc;
+        gc *= sc;
+        g_dr = -g0 * r_inv - 2.0f * asq * gb;
+        g_da = (0.5f * g0 - gc) * inv_alpha;
+        if (kPhi) {
+            f0 = fa * sc;
+            fb *= sc;
+            fc *= sc;
+            f_dr = -f0 * r_inv - 2.0f * asq * fb;
+            f_da = (0.5f * f0 - fc) * inv_alpha;
+        }
+        return true;
+    }
+    if (k.alpha_max <= alpha) {
+        if (!below_rc) return false;
+        float p = r * k.dr_inv;
+        int m = min((int)p, k.nr - 2);
+        p -= (float)m;
+        p = fminf(p, 1.0f);
+        float p2 = p * p, p3 = p2 * p;
+        float4 cr = __ldg(pk + 2 * m);
+        g0 = cr.w * p3 + cr.z * p2 + cr.y * p + cr.x;
+        g_da = 0.0f;
+        g_dr = (cr.y + 2.0f * cr.z * p + 3.0f * cr.w * p2) * k.dr_inv;
+        if (kPhi) {
+            float4 cp = __ldg(pk + 2 * m + 1);
+            float z2 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
+            float z2p = (cp.y + 2.0f * cp.z * p + 3.0f * cp.w * p2) * k.dr_inv;
+            f0 = z2 * r_inv;
+            f_da = 0.0f;
+            f_dr = (z2p - z2 * r_inv) * r_inv;
+        }
+        return true;
+    }
+    return false;
+}
+
+// ---- pass 1: FP32 smearing, compensated densities -------------------------
+template <int NT, int NQ>
+__global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass1(Dev d, int row0)
+{
+    using S = Slots<NT>;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const size_t mp = (size_t)d.maxp;
+    const F32Consts kc = f32_consts(d);
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < d.npairs; base += stride) {
+        long long p = base + lane;
+        bool valid = p < d.npairs;
+        int i = valid ? d.pair_i[p] : -1;
+        float Ei[NT];
+#pragma unroll
+        for (int a = 0; a < NT; a++) Ei[a] = 0.0f;
+        if (valid) {
+            int j = d.pair_j[p];
+            double4 xi = d.pos[i], xj = d.pos[j];
+            float ai[NT], ci[NT], aj[NT], cj[NT], Ej[NT];
+#pragma unroll
+            for (int a = 0; a < NT; a++) {
+                ai[a] = (float)d.alpha[(size_t)i * NT + a];
+                ci[a] = (float)d.c[(size_t)i * NT + a];
+                aj[a] = (float)d.alpha[(size_t)j * NT + a];
+                cj[a] = (float)d.c[(size_t)j * NT + a];
+                Ej[a] = 0.0f;
+            }
+            double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
+            double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
+            bool own_j = j < d.natms;
+            bool in_cut = rsq < d.cut_sq_mod;
+            bool below_rc = rsq < d.cut_sq;
+            float rsqf = (float)rsq;
+            float r_inv = rsqrtf(rsqf);
+            float r = rsqf * r_inv;
+            double w = own_j ? 0.5 : 0.25;
+            float* out = d.prf + p;
+#pragma unroll
+            for (int a = 0; a < NT; a++)
+#pragma unroll
+                for (int b = 0; b < NT; b++) {
+                    const int rs = b * NT + a, ps = comp_idx(a, b);
+                    const float4* pk = d.pkT + (size_t)(a * NT + b) * d.nr * 2;
+                    float g0 = 0, gdr = 0, gda = 0, f0 = 0, fdr = 0, fda = 0;
+                    bool hit = false;
+                    if (in_cut) {
+                        float alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
+                        hit = (a >= b) ? smear_f<true, NQ>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr, gda, f0, fdr, fda)
+                                       : smear_f<false, NQ>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr, gda, f0, fdr, fda);
+                    }
+                    if (!hit) g0 = gdr = gda = f0 = fdr = fda = 0.0f;
+                    __stcs(out + (S::RHO + rs) * mp, g0);
+                    __stcs(out + (S::DRR + rs) * mp, gdr);
+                    __stcs(out + (S::DRA + rs) * mp, gda);
+                    if (a >= b) {
+                        __stcs(out + (S::PHI + ps) * mp, f0);
+                        __stcs(out + (S::DPR + ps) * mp, fdr);
+                        __stcs(out + (S::DPA + ps) * mp, fda);
+                        acc[0] += w * (double)((cj[b] * ci[a] + cj[a] * ci[b]) * f0);
+                    }
+                    Ei[a] += g0 * cj[b];
+                    Ej[b] += g0 * ci[a];
+                }
+            if (own_j && in_cut) {
+#pragma unroll
+                for (int b = 0; b < NT; b++) acc_add(&d.E[(size_t)j * NT + b], Ej[b], 0.0f);
+            }
+        }
+        Seg sg = seg_of(i);
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            float2 t = seg_sum2(Ei[a], sg);
+            if (valid && lane == sg.first) acc_add(&d.E[(size_t)i * NT + a], t.x, t.y);
+        }
+    }
+    block_partials<7>(acc, d.partial, row0 + blockIdx.x);
+}
+
+// ---- per-site embedding (FP64, as in the plain form) ----------------------
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_dmd32_embed(Dev d, int row0)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (i < d.natms) {
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            size_t q = (size_t)i * NT + a;
+            double Ev = d.E[q];
+            double tmp0, tmp1;
+            embed_F(d, a, Ev, tmp0, tmp1, nullptr);
+            double ca = d.c[q], al = d.alpha[q];
+            d.E[q] = tmp0;
+            d.dE[q] = tmp1;
+            acc[0] += ca * tmp0;
+            acc[0] += d.kbT * calc_ent(ca);
+            acc[0] += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
+            d.f[(size_t)i * d.x_dim + 3 + a] -= 1.5 * d.kbT * ca / al;
+        }
+    }
+    block_partials<7>(acc, d.partial, row0 + blockIdx.x);
+}
+
+// ---- pass 2: FP32 force projections, compensated force sums ----------------
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass2(Dev d, int st_clc, int row0)
+{
+    using S = Slots<NT>;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const size_t mp = (size_t)d.maxp;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < d.npairs; base += stride) {
+        long long p = base + lane;
+        bool valid = p < d.npairs;
+        int i = valid ? d.pair_i[p] : -1;
+        float fi[3 + NT];
+#pragma unroll
+        for (int q = 0; q < 3 + NT; q++) fi[q] = 0.0f;
+        if (valid) {
+            const float* in = d.prf + p;
+            float drr[NT * NT], dra[NT * NT], dpr[S::NC], dpa[S::NC];
+#pragma unroll
+            for (int q = 0; q < NT * NT; q++) {
+                drr[q] = __ldcs(in + (S::DRR + q) * mp);
+                dra[q] = __ldcs(in + (S::DRA + q) * mp);
+            }
+#pragma unroll
+            for (int q = 0; q < S::NC; q++) {
+                dpr[q] = __ldcs(in + (S::DPR + q) * mp);
+                dpa[q] = __ldcs(in + (S::DPA + q) * mp);
+            }
+            int j = d.pair_j[p];
+            int oj = owner(d, j);
+            double4 xi = d.pos[i], xj = d.pos[j];
+            float ai[NT], ci[NT], dEi[NT], aj[NT], cj[NT], dEj[NT], fj[NT];
+#pragma unroll
+            for (int a = 0; a < NT; a++) {
+                ai[a] = (float)d.alpha[(size_t)i * NT + a];
+                ci[a] = (float)d.c[(size_t)i * NT + a];
+                dEi[a] = (float)d.dE[(size_t)i * NT + a];
+                aj[a] = (float)d.alpha[(size_t)j * NT + a];
+                cj[a] = (float)d.c[(size_t)j * NT + a];
+                dEj[a] = (float)d.dE[(size_t)oj * NT + a];
+                fj[a] = 0.0f;
+            }
+            float dx0 = (float)(xi.x - xj.x), dx1 = (float)(xi.y - xj.y), dx2 = (float)(xi.z - xj.z);
+            float r_inv = rsqrtf(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
+            bool own_j = j < d.natms;
+            float fsum = 0.0f;
+#pragma unroll
+            for (int a = 0; a < NT; a++)
+#pragma unroll
+                for (int b = 0; b < NT; b++) {
+                    const int ab = a * NT + b, ba = b * NT + a, ps = comp_idx(a, b);
+                    float cc = ci[a] * cj[b];
+                    float fpair = -(drr[ab] * dEi[a] + drr[ba] * dEj[b] + dpr[ps]) * cc * r_inv;
+                    float sa = ai[a] + aj[b];
+                    float apair = -(dra[ab] * dEi[a] + dra[ba] * dEj[b] + dpa[ps]) * cc * __frcp_rn(sa * sa);
+                    fsum += fpair;
+                    fi[3 + a] += apair * aj[b] * aj[b];
+                    fj[b] += apair * ai[a] * ai[a];
+                }
+            fi[0] = dx0 * fsum;
+            fi[1] = dx1 * fsum;
+            fi[2] = dx2 * fsum;
+            if (st_clc) {
+                double wf = (own_j ? 1.0 : 0.5) * (double)fsum;
+                acc[1] -= wf * dx0 * dx0;
+                acc[2] -= wf * dx1 * dx1;
+                acc[3] -= wf * dx2 * dx2;
+                acc[4] -= wf * dx1 * dx2;
+                acc[5] -= wf * dx2 * dx0;
+                acc[6] -= wf * dx0 * dx1;
+            }
+            if (own_j) {
+                double* fj_out = d.f + (size_t)j * d.x_dim;
+                if (fsum != 0.0f) {
+                    acc_add(fj_out + 0, -dx0 * fsum, 0.0f);
+                    acc_add(fj_out + 1, -dx1 * fsum, 0.0f);
+                    acc_add(fj_out + 2, -dx2 * fsum, 0.0f);
+                }
+#pragma unroll
+                for (int b = 0; b < NT; b++) acc_add(fj_out + 3 + b, fj[b], 0.0f);
+            }
+        }
+        Seg sg = seg_of(i);
+#pragma unroll
+        for (int q = 0; q < 3 + NT; q++) {
+            float2 t = seg_sum2(fi[q], sg);
+            if (valid && lane == sg.first) acc_add(d.f + (size_t)i * d.x_dim + q, t.x, t.y);
+        }
+    }
+    block_partials<7>(acc, d.partial, row0 + blockIdx.x);
+}
+
+template <int NT>
+cudaError_t dmd32_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
+{
+    int g1 = persistent_grid(d.npairs, MG_DMD32_MINB), g2 = div_up(d.natms, kFFBlock);
+    if (evs) cudaEventRecord(evs[0], st);
+    if (d.nq == 3) k_dmd32_pass1<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
+    else k_dmd32_pass1<NT, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
+    if (evs) cudaEventRecord(evs[1], st);
+    k_dmd32_embed<NT><<<g2, kFFBlock, 0, st>>>(d, g1);
+    if (evs) cudaEventRecord(evs[2], st);
+    k_dmd32_pass2<NT><<<g1, kFFBlock, 0, st>>>(d, st_clc, g1 + g2);
+    if (evs) cudaEventRecord(evs[3], st);
+    *nb = 2 * g1 + g2;
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_dmd_force_f32(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
+{
+    switch (d.nt) {
+    case 1: return dmd32_force_nt<1>(d, st_clc, nb, st, evs);
+    case 2: return dmd32_force_nt<2>(d, st_clc, nb, st, evs);
+    case 3: return dmd32_force_nt<3>(d, st_clc, nb, st, evs);
+    case 4: return dmd32_force_nt<4>(d, st_clc, nb, st, evs);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace mg

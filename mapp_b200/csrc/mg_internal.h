@@ -93,8 +93,10 @@ struct Dev {
     const double* phiT;  // [ncomp][nr][8]
     const double* FT;    // [nt][nrho+1][Fw]
     int Fw;
-    const float* rhoTf;  // FP32 copies [slot][nr][4] (c0..c3)
-    const float* phiTf;
+    // precision form: per ordered species pair (a,b) and knot, one 32-byte
+    // sector {rho c0..c3 of slot b*nt+a, phi c0..c3 of slot COMP(a,b) (zero when a < b)}
+    const float4* pkT;
+    float* prf;          // FP32 pair scratch, same SoA layout as pr
     double cut_sk_sq[16];
     // FS analytic
     double fsA[kMaxTypes], fst1[kMaxTypes][kMaxTypes], fst2[kMaxTypes][kMaxTypes];
@@ -140,6 +142,8 @@ cudaError_t launch_fs_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
 // kernel, before pass 2 and after pass 2, for per-kernel device times
 cudaError_t launch_dmd_force(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st, cudaEvent_t* evs);
 cudaError_t launch_dmd_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
+// precision form (MG_FORM_FP32) force_calc; evs as for launch_dmd_force
+cudaError_t launch_dmd_force_f32(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st, cudaEvent_t* evs);
 cudaError_t launch_dmd_crd(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nblocks_out, cudaStream_t st);

@@ -1,0 +1,50 @@
+"""Precision form (MG_FORM_FP32) against the FP64 oracle.
+
+Accuracy gates of the precision form: max|dF| <= 1e-4 eV/A over all force
+components (positions and alphas), |dE|/site <= 1e-6 eV for the total free
+energy.  The chemical-potential rates computed after an FP32 force call read
+FP32 per-pair densities; they are checked at 1e-5 relative to max|c_d|."""
+import numpy as np
+import pytest
+
+from mapp_b200 import fixtures as fx
+
+pytestmark = pytest.mark.gpu
+
+
+def _mb():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import mapp_b200
+
+    return mapp_b200
+
+
+@pytest.mark.parametrize("style,n,nt", [("DMD_I", 6, 2), ("DMD_II", 5, 2), ("DMD", 5, 2), ("DMD_I", 5, 1), ("DMD_I", 10, 2)])
+def test_fp32_form_accuracy(tmp_path, style, n, nt):
+    mb = _mb()
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=n, sigma=0.03, style=style, nt=nt)
+    s = mb.system_from_workload(w)
+    s.set_form(mb.MG_FORM_FP32)
+    o = Oracle(w)
+    f, en = s.force_calc(1)
+    fo, eno = o.force(1)
+    N = w["cfg"].natms
+    assert np.max(np.abs(f - fo)) <= 1e-4
+    assert abs(en[0] - eno[0]) / N <= 1e-6
+    s.create_2nd_neigh_lst()
+    o.crd()
+    cd, cdo = s.c_d_calc(), o.c_d()
+    assert np.max(np.abs(cd - cdo)) <= 1e-5 * np.max(np.abs(cdo))
+
+
+def test_fp32_form_rejected_for_eam(tmp_path):
+    mb = _mb()
+    w = fx.write_workload(str(tmp_path / "w"), "eam", n=3)
+    s = mb.system_from_workload(w)
+    with pytest.raises(mb.MGError) as e:
+        s.set_form(mb.MG_FORM_FP32)
+    assert e.value.code == 7
