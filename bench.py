@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--cells", type=int, default=WORKLOAD["n"], help="FCC cells per edge (default 20 -> 32000 sites)")
     p.add_argument("--cpu-reps", type=int, default=0, help="reference force_calc calls per CPU process (0: auto)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU reference timing")
+    p.add_argument("--skip-forms", action="store_true", help="skip the FP32 and learned forms (profiling runs)")
     return p.parse_args()
 
 
@@ -219,6 +220,73 @@ def pass1_flops_per_pair(nt, nq):
     return 10 + nt * nt * (9 + 21 * nq + 9) + nc * (13 * nq + 9)
 
 
+def run_forms(args, s, mb, natms, f_dev, flush, t_dev):
+    """Precision and learned forms on the same system: throughput, and errors
+    against the plain FP64 form."""
+    import torch
+
+    f64_ref = f_dev.clone()
+    s.force_calc(1, f=f64_ref)
+    _, en64 = s.force_calc(1)
+    s.set_form(mb.MG_FORM_FP32)
+    f32 = torch.zeros_like(f_dev)
+    for _ in range(args.warmup):
+        s.force_calc(1, f=f32)
+    t32 = 0.0
+    t32_p1 = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        _, en32 = s.force_calc(1, f=f32)
+        t32 += s.last_time("force")
+        t32_p1 += s.last_time("force.pass1")
+    fp32_form = {"value": natms * args.steps / (t32 * 1e-3), "unit": UNIT, "ms_per_step": t32 / args.steps,
+                 "pass1_ms": t32_p1 / args.steps,
+                 "max_abs_dF_eV_per_A": float((f32 - f64_ref).abs().max().item()),
+                 "abs_dE_per_site_eV": abs(float(en32[0]) - float(en64[0])) / natms,
+                 "speedup_vs_fp64": t_dev / t32,
+                 "error_reference": "plain FP64 GPU form (itself within 1e-10 of the CPU oracle)"}
+    s.set_form(mb.MG_FORM_FP64)
+
+    # learned form: train on the GPU (2M quadrature-labelled samples, 20k Adam
+    # steps of 4096, lr 1e-3 cosine), then force_calc with the network, the
+    # quadrature fallback outside the training box and the 1% audit
+    s.mlp_init(1.8, 5.0, 0.05, 0.20, seed=5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mlp_loss = s.mlp_train(nsamples=2_000_000, steps=20_000, batch=4096, lr=1e-3, seed=11)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    s.set_form(mb.MG_FORM_MLP)
+    fm = torch.zeros_like(f_dev)
+    for _ in range(args.warmup):
+        s.force_calc(1, f=fm)
+    mlp_steps = max(10, min(args.steps, 400))
+    tm = 0.0
+    tm_p1 = 0.0
+    for _ in range(mlp_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        _, enm = s.force_calc(1, f=fm)
+        tm += s.last_time("force")
+        tm_p1 += s.last_time("force.pass1")
+    audit, audit_counts = s.mlp_audit()
+    mlp_form = {"value": natms * mlp_steps / (tm * 1e-3), "unit": UNIT, "ms_per_step": tm / mlp_steps,
+                "steps": mlp_steps, "pass1_ms": tm_p1 / mlp_steps,
+                "max_abs_dF_eV_per_A": float((fm - f64_ref).abs().max().item()),
+                "abs_dE_per_site_eV": abs(float(enm[0]) - float(en64[0])) / natms,
+                "speedup_vs_fp64": (t_dev / args.steps) / (tm / mlp_steps),
+                "train_s": t_train, "train_final_loss": mlp_loss,
+                "training": "2M samples, 20000 steps x 4096, Adam lr 1e-3 cosine, box r [1.8,5.0] w [0.05,0.20]",
+                "audit_max_abs_err": {k: float(v) for k, v in zip(
+                    ("phi", "rho", "dphi_dr", "drho_dr", "dphi_dalpha", "drho_dalpha"), audit)},
+                "audited_rows": int(audit_counts[0]), "fallback_rows": int(audit_counts[1]),
+                "error_reference": "plain FP64 GPU form (itself within 1e-10 of the CPU oracle)"}
+    s.set_form(mb.MG_FORM_FP64)
+
+    return {"fp32": fp32_form, "mlp": mlp_form}
+
+
 def run_ours(args):
     import torch
 
@@ -277,28 +345,7 @@ def run_ours(args):
         t_dev = float(tt.item())
     value = ws * natms * args.steps / (t_dev * 1e-3)
 
-    # precision form on the same system: throughput and error against the FP64 form
-    f64_ref = f_dev.clone()
-    s.force_calc(1, f=f64_ref)
-    _, en64 = s.force_calc(1)
-    s.set_form(mb.MG_FORM_FP32)
-    f32 = torch.zeros_like(f_dev)
-    for _ in range(args.warmup):
-        s.force_calc(1, f=f32)
-    t32 = 0.0
-    t32_p1 = 0.0
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        _, en32 = s.force_calc(1, f=f32)
-        t32 += s.last_time("force")
-        t32_p1 += s.last_time("force.pass1")
-    fp32_form = {"value": natms * args.steps / (t32 * 1e-3), "unit": UNIT, "ms_per_step": t32 / args.steps,
-                 "pass1_ms": t32_p1 / args.steps,
-                 "max_abs_dF_eV_per_A": float((f32 - f64_ref).abs().max().item()),
-                 "abs_dE_per_site_eV": abs(float(en32[0]) - float(en64[0])) / natms,
-                 "speedup_vs_fp64": t_dev / t32,
-                 "error_reference": "plain FP64 GPU form (itself within 1e-10 of the CPU oracle)"}
+    forms = {} if args.skip_forms else run_forms(args, s, mb, natms, f_dev, flush, t_dev)
     s.set_form(mb.MG_FORM_FP64)
 
     # end to end through the C ABI with host buffers
@@ -374,7 +421,7 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": natms * (s.x_dim + nt) * 8, "d2h_bytes_per_step": natms * s.x_dim * 8 + 56,
                 "steps": e2e_steps, "path": "mg_atoms_update_x + mg_atoms_update_c + mg_ff_force_calc, pinned host buffers"},
-        "forms": {"fp32": fp32_form},
+        "forms": forms,
         "gpu_launches": 4 * args.steps,
         "phases_ms": {"force": t_dev / args.steps, "force.pass1": p1_ms, "list_rebuild": t_list,
                       "energy_calc": t_energy, "c_d_calc": t_cd, "calc_g": t_g},

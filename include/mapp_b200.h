@@ -133,6 +133,37 @@ int mg_get_int_vector(mg_system* s, const char* name, int* out);
    "force.pass2". */
 int mg_last_time(mg_system* s, const char* phase, double* ms);
 
+/* ---- learned form (MG_FORM_MLP) ------------------------------------------ */
+/* A 4 -> 64 -> 64 -> 64 -> 6 SiLU network replaces the Gauss-Hermite smearing
+   of phi, rho and their r and alpha derivatives (ff_dmd_I.cpp:178-259) for
+   pairs inside its training box; other pairs keep the quadrature, and a
+   hashed 1% of network pairs is re-evaluated by the quadrature every
+   force_calc (mg_mlp_audit).  Inputs (r, w_i, w_j, species pair) with
+   w = alpha^-1/2 per site; outputs (phi, rho, dphi/dr, drho/dr, dphi/dalpha,
+   drho/dalpha).  DMD styles with one or two species. */
+int mg_mlp_nparam(void);
+/* allocate the network for the training box r in [r_lo, r_hi] A and
+   w_i, w_j in [w_lo, w_hi] A; random initial weights from `seed` */
+int mg_mlp_init(mg_system* s, double r_lo, double r_hi, double w_lo, double w_hi, unsigned long long seed);
+/* label nsamples seeded samples with the FP64 quadrature of the loaded tables
+   and train `steps` Adam steps of `batch` rows (multiple of 64), cosine
+   learning rate from lr; *final_loss = last batch loss (standardised MSE) */
+int mg_mlp_train(mg_system* s, long long nsamples, int steps, int batch, double lr, unsigned long long seed,
+                 double* final_loss);
+int mg_mlp_loss_history(mg_system* s, int n, float* loss);
+/* read and/or write the FP32 parameters (mg_mlp_nparam floats) and the output
+   standardisation (6 means then 6 scales); any pointer may be NULL */
+int mg_mlp_state(mg_system* s, float* params_out, const float* params_in, float* scaling_out,
+                 const float* scaling_in);
+/* physical outputs y (n * 6) of raw inputs x (n * 4: r, w_i, w_j, code) */
+int mg_mlp_eval(mg_system* s, int n, const float* x, float* y);
+/* gradient (mg_mlp_nparam floats) of the standardised MSE over n rows
+   (multiple of 64) and the loss, without updating the weights */
+int mg_mlp_grad(mg_system* s, int n, const float* x, const float* y, float* grad, double* loss);
+/* audit of the last learned-form force_calc: max |network - quadrature| per
+   output (6 doubles); counts[0] audited rows, counts[1] rows that fell back */
+int mg_mlp_audit(mg_system* s, double* max_err, long long* counts);
+
 /* ---- allocation-free entry point ---------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc:
    code where another allocator owns all device memory (a framework's caching

@@ -58,6 +58,14 @@ SIGNATURES = {
     "mg_get_int_vector": (C.c_int, [_P, C.c_char_p, _P]),
     "mg_last_time": (C.c_int, [_P, C.c_char_p, _D]),
     "mg_fs_energy_noalloc": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
+    "mg_mlp_nparam": (C.c_int, []),
+    "mg_mlp_init": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_ulonglong]),
+    "mg_mlp_train": (C.c_int, [_P, C.c_longlong, C.c_int, C.c_int, C.c_double, C.c_ulonglong, _D]),
+    "mg_mlp_loss_history": (C.c_int, [_P, C.c_int, _P]),
+    "mg_mlp_state": (C.c_int, [_P, _P, _P, _P, _P]),
+    "mg_mlp_eval": (C.c_int, [_P, C.c_int, _P, _P]),
+    "mg_mlp_grad": (C.c_int, [_P, C.c_int, _P, _P, _P, _D]),
+    "mg_mlp_audit": (C.c_int, [_P, _D, C.POINTER(C.c_longlong)]),
 }
 
 
@@ -253,6 +261,51 @@ class System:
         out = np.zeros(c["natms"] + c["nph"], dtype=np.int32)
         _check(load_library().mg_get_int_vector(self.h, b"crd", out.ctypes.data))
         return out
+
+    # ---- learned form ------------------------------------------------------
+    def mlp_init(self, r_lo=1.8, r_hi=5.0, w_lo=0.05, w_hi=0.20, seed=1):
+        _check(load_library().mg_mlp_init(self.h, r_lo, r_hi, w_lo, w_hi, seed))
+
+    def mlp_train(self, nsamples=2_000_000, steps=20_000, batch=4096, lr=1e-3, seed=7):
+        loss = C.c_double(0.0)
+        _check(load_library().mg_mlp_train(self.h, nsamples, steps, batch, lr, seed, C.byref(loss)))
+        return loss.value
+
+    def mlp_loss_history(self, n):
+        out = np.zeros(n, dtype=np.float32)
+        _check(load_library().mg_mlp_loss_history(self.h, n, out.ctypes.data))
+        return out
+
+    def mlp_state(self, params=None, scaling=None):
+        L = load_library()
+        npar = L.mg_mlp_nparam()
+        pout = np.zeros(npar, dtype=np.float32)
+        sout = np.zeros(12, dtype=np.float32)
+        pin = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        sin = None if scaling is None else np.ascontiguousarray(scaling, dtype=np.float32)
+        _check(L.mg_mlp_state(self.h, pout.ctypes.data, _ptr(pin), sout.ctypes.data, _ptr(sin)))
+        return pout, sout
+
+    def mlp_eval(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], 6), dtype=np.float32)
+        _check(load_library().mg_mlp_eval(self.h, x.shape[0], x.ctypes.data, y.ctypes.data))
+        return y
+
+    def mlp_grad(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        g = np.zeros(load_library().mg_mlp_nparam(), dtype=np.float32)
+        loss = C.c_double(0.0)
+        _check(load_library().mg_mlp_grad(self.h, x.shape[0], x.ctypes.data, y.ctypes.data, g.ctypes.data,
+                                          C.byref(loss)))
+        return g, loss.value
+
+    def mlp_audit(self):
+        err = np.zeros(6)
+        cnt = np.zeros(2, dtype=np.int64)
+        _check(load_library().mg_mlp_audit(self.h, err.ctypes.data_as(_D), cnt.ctypes.data_as(C.POINTER(C.c_longlong))))
+        return err, cnt
 
     def last_time(self, phase):
         ms = C.c_double(0.0)

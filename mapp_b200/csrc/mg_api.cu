@@ -231,6 +231,12 @@ struct mg_system {
     long long pair_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};
+    // learned form
+    MlpState mlp{};
+    bool mlp_ready = false;
+    float* mlp_loss = nullptr;
+    int mlp_loss_n = 0;
+    unsigned long long mlp_calls = 0;
     double t_list = 0, t_force = 0, t_energy = 0, t_cd = 0, t_g = 0;
     double t_k[3] = {0, 0, 0};  // DMD force: pass 1, embedding, pass 2
     long long partial_rows = 0;
@@ -492,6 +498,10 @@ int rebuild(mg_system* s)
     CU(cudaMemcpyAsync(&np_h, d.poff + natms, sizeof(int), cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
     CHK(ensure_compact(s, np_h));
+    // partial rows: every launcher's grid is at most one block per 256 pairs (or
+    // 4 * SMs for the persistent learned-form pass) plus per-atom grids
+    CHK(ensure_partials(s, 2LL * div_up((long long)np_h, kFFBlock) + 2LL * div_up((long long)natms * 32, kFFBlock) +
+                               div_up((long long)natms * s->nt, kFFBlock) + 4LL * num_sms() + 64));
     d.npairs = np_h;
     CU(launch_pairs_compact(d, st));
     CU(launch_store_x0(d, st));
@@ -768,6 +778,9 @@ int mg_destroy(mg_system* s)
                     s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    void* mptrs[] = {s->mlp.par, s->mlp.wbf, s->mlp.m, s->mlp.v, s->mlp.gpart, s->mlp.audit, s->mlp_loss};
+    for (void* p : mptrs)
+        if (p) cudaFree(p);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     for (int k = 0; k < 4; k++)
@@ -792,7 +805,11 @@ int mg_set_form(mg_system* s, int form)
     CHK(check_sys(s));
     if (form == MG_FORM_FP32 && !s->dmd)
         return fail(MG_ERR_UNSUPPORTED, "the FP32 precision form is implemented for the DMD styles");
-    if (form != MG_FORM_FP64 && form != MG_FORM_FP32)
+    if (form == MG_FORM_MLP && (!s->dmd || s->nt > 2))
+        return fail(MG_ERR_UNSUPPORTED, "the learned form is implemented for the DMD styles with one or two species");
+    if (form == MG_FORM_MLP && !s->mlp_ready)
+        return fail(MG_ERR_STATE, "the learned form needs mg_mlp_init (and normally mg_mlp_train) first");
+    if (form != MG_FORM_FP64 && form != MG_FORM_FP32 && form != MG_FORM_MLP)
         return fail(MG_ERR_UNSUPPORTED, "form %d is not available in this build", form);
     s->form = form;
     s->d.form = form;
@@ -1075,7 +1092,12 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     } else {
         CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
         if (s->form == MG_FORM_FP32) CU(launch_dmd_force_f32(d, st_clc, &rows, s->st, s->evk));
-        else CU(launch_dmd_force(d, st_clc, &rows, s->st, s->evk));
+        else if (s->form == MG_FORM_MLP) {
+            CU(cudaMemsetAsync(s->mlp.audit, 0, 16 * sizeof(float), s->st));
+            CU(launch_dmd_force_mlp(d, s->mlp, 0x51ed270b3a5d4e1ull + 0x9e37ull * (++s->mlp_calls), st_clc, &rows,
+                                    s->st, s->evk));
+        } else
+            CU(launch_dmd_force(d, st_clc, &rows, s->st, s->evk));
     }
     double tot[8] = {0};
     CU(launch_reduce_partials(d, rows, 7, s->red_out, s->st));
@@ -1287,6 +1309,217 @@ int mg_last_time(mg_system* s, const char* phase, double* ms)
     else if (!strcmp(phase, "force.embed")) *ms = s->t_k[1];
     else if (!strcmp(phase, "force.pass2")) *ms = s->t_k[2];
     else return fail(MG_ERR_ARG, "unknown phase %s", phase);
+    return MG_OK;
+}
+
+// ---- learned form ------------------------------------------------------------
+static unsigned short f2bf(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    uint32_t r = 0x7fffu + ((u >> 16) & 1u);
+    return (unsigned short)((u + r) >> 16);
+}
+
+static int mlp_upload_params(mg_system* s, const std::vector<float>& par)
+{
+    std::vector<unsigned short> bf(par.size());
+    for (size_t k = 0; k < par.size(); k++) bf[k] = f2bf(par[k]);
+    CU(cudaMemcpy(s->mlp.par, par.data(), par.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->mlp.wbf, bf.data(), bf.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+    return MG_OK;
+}
+
+int mg_mlp_nparam(void) { return mlp_nparam(); }
+
+int mg_mlp_init(mg_system* s, double r_lo, double r_hi, double w_lo, double w_hi, unsigned long long seed)
+{
+    CHK(check_sys(s));
+    if (!s->dmd || !s->coef_set) return fail(MG_ERR_STATE, "the learned form needs a DMD style with ff_coef done");
+    if (s->nt > 2) return fail(MG_ERR_UNSUPPORTED, "the learned form is implemented for one or two species");
+    if (!(r_hi > r_lo) || !(w_hi > w_lo) || w_lo <= 0.0) return fail(MG_ERR_ARG, "bad training box");
+    if (!s->d_rhoT) CHK(upload_tables(s));
+    int np = mlp_nparam(), npart = mlp_npart();
+    MlpState& M = s->mlp;
+    CHK(dalloc(&M.par, np));
+    CHK(dalloc((unsigned short**)&M.wbf, np));
+    CHK(dalloc(&M.m, np));
+    CHK(dalloc(&M.v, np));
+    CHK(dalloc(&M.gpart, (size_t)npart * 4096));  // up to 4096 tiles of 64 rows per step
+    CHK(dalloc(&M.audit, 16));
+    CU(cudaMemset(M.m, 0, np * sizeof(float)));
+    CU(cudaMemset(M.v, 0, np * sizeof(float)));
+    M.box.r_lo = (float)r_lo;
+    M.box.r_hi = (float)r_hi;
+    M.box.w_lo = (float)w_lo;
+    M.box.w_hi = (float)w_hi;
+    for (int q = 0; q < 6; q++) {
+        M.out_mean[q] = 0.f;
+        M.out_scale[q] = 1.f;
+    }
+    // weights U(-1/sqrt(fan_in), 1/sqrt(fan_in)) from a splitmix64 stream; biases
+    // and the padding rows / columns zero
+    std::vector<float> par(np, 0.0f);
+    unsigned long long st = seed;
+    auto next = [&]() {
+        st += 0x9e3779b97f4a7c15ull;
+        unsigned long long z = st;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    const int H = 64;
+    auto fill = [&](int off, int rows, int cols, int real_rows, int real_cols, int fan_in) {
+        double bnd = 1.0 / sqrt((double)fan_in);
+        for (int r = 0; r < rows; r++)
+            for (int c = 0; c < cols; c++) {
+                double u = next();
+                par[off + r * cols + c] = (r < real_rows && c < real_cols) ? (float)((2.0 * u - 1.0) * bnd) : 0.0f;
+            }
+    };
+    fill(0, 16, H, 4, H, 4);
+    fill(16 * H + H, H, H, H, H, H);
+    fill(16 * H + H + H * H + H, H, H, H, H, H);
+    fill(16 * H + H + 2 * (H * H + H), H, 8, H, 6, H);
+    CHK(mlp_upload_params(s, par));
+    s->mlp_ready = true;
+    return MG_OK;
+}
+
+int mg_mlp_state(mg_system* s, float* par_out, const float* par_in, float* scaling_out, const float* scaling_in)
+{
+    CHK(check_sys(s));
+    if (!s->mlp_ready) return fail(MG_ERR_STATE, "mg_mlp_init first");
+    int np = mlp_nparam();
+    if (par_in) {
+        std::vector<float> par(par_in, par_in + np);
+        CHK(mlp_upload_params(s, par));
+    }
+    if (scaling_in)
+        for (int q = 0; q < 6; q++) {
+            s->mlp.out_mean[q] = scaling_in[q];
+            s->mlp.out_scale[q] = scaling_in[6 + q];
+        }
+    if (par_out) CU(cudaMemcpy(par_out, s->mlp.par, np * sizeof(float), cudaMemcpyDeviceToHost));
+    if (scaling_out)
+        for (int q = 0; q < 6; q++) {
+            scaling_out[q] = s->mlp.out_mean[q];
+            scaling_out[6 + q] = s->mlp.out_scale[q];
+        }
+    return MG_OK;
+}
+
+int mg_mlp_train(mg_system* s, long long nsamples, int steps, int batch, double lr, unsigned long long seed,
+                 double* final_loss)
+{
+    CHK(check_sys(s));
+    if (!s->mlp_ready) return fail(MG_ERR_STATE, "mg_mlp_init first");
+    if (nsamples < 64 || steps < 1 || batch < 64 || batch % 64 || batch / 64 > 4096)
+        return fail(MG_ERR_ARG, "need nsamples >= 64, steps >= 1, batch a multiple of 64 up to 262144");
+    if (nsamples > (1LL << 31) - 1) return fail(MG_ERR_ARG, "too many samples");
+    int n = (int)nsamples;
+    float *X = nullptr, *Y = nullptr;
+    CHK(dalloc(&X, (size_t)n * 4));
+    CHK(dalloc(&Y, (size_t)n * 6));
+    fill_dev_scalars(s);
+    CU(launch_mlp_labels(s->d, s->mlp.box, seed, n, X, Y, s->st));
+    // output standardisation from the labels
+    std::vector<float> yh((size_t)n * 6);
+    CU(cudaMemcpyAsync(yh.data(), Y, yh.size() * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    for (int q = 0; q < 6; q++) {
+        double m = 0, m2 = 0;
+        for (int k = 0; k < n; k++) {
+            double v = yh[(size_t)k * 6 + q];
+            m += v;
+            m2 += v * v;
+        }
+        m /= n;
+        double var = m2 / n - m * m;
+        s->mlp.out_mean[q] = (float)m;
+        s->mlp.out_scale[q] = (float)(var > 1e-30 ? sqrt(var) : 1.0);
+    }
+    if (s->mlp_loss_n < steps) {
+        CHK(dalloc(&s->mlp_loss, steps));
+        s->mlp_loss_n = steps;
+    }
+    for (int t = 0; t < steps; t++)
+        CU(launch_mlp_train_step(s->mlp, X, Y, n, batch, seed, t, steps, (float)lr, 0, nullptr, s->mlp_loss, s->st));
+    float last = 0.f;
+    CU(cudaMemcpyAsync(&last, s->mlp_loss + steps - 1, sizeof(float), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    cudaFree(X);
+    cudaFree(Y);
+    if (final_loss) *final_loss = last;
+    return MG_OK;
+}
+
+int mg_mlp_loss_history(mg_system* s, int n, float* out)
+{
+    CHK(check_sys(s));
+    if (n > s->mlp_loss_n) return fail(MG_ERR_ARG, "history holds %d steps", s->mlp_loss_n);
+    if (n > 0) CU(cudaMemcpy(out, s->mlp_loss, n * sizeof(float), cudaMemcpyDeviceToHost));
+    return MG_OK;
+}
+
+int mg_mlp_eval(mg_system* s, int n, const float* x, float* y)
+{
+    CHK(check_sys(s));
+    if (!s->mlp_ready) return fail(MG_ERR_STATE, "mg_mlp_init first");
+    if (n < 1 || !x || !y) return fail(MG_ERR_ARG, "need n >= 1 and non-null x, y");
+    float *X = nullptr, *Y = nullptr;
+    CHK(dalloc(&X, (size_t)n * 4));
+    CHK(dalloc(&Y, (size_t)n * 6));
+    CU(cudaMemcpy(X, x, (size_t)n * 4 * sizeof(float), cudaMemcpyDefault));
+    CU(launch_mlp_eval(s->mlp, X, n, Y, s->st));
+    CU(cudaMemcpyAsync(y, Y, (size_t)n * 6 * sizeof(float), cudaMemcpyDefault, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    cudaFree(X);
+    cudaFree(Y);
+    return MG_OK;
+}
+
+int mg_mlp_grad(mg_system* s, int n, const float* x, const float* y, float* grad, double* loss)
+{
+    CHK(check_sys(s));
+    if (!s->mlp_ready) return fail(MG_ERR_STATE, "mg_mlp_init first");
+    if (n < 64 || n % 64 || n / 64 > 4096) return fail(MG_ERR_ARG, "n must be a multiple of 64");
+    float *X = nullptr, *Y = nullptr, *G = nullptr, *L = nullptr;
+    CHK(dalloc(&X, (size_t)n * 4));
+    CHK(dalloc(&Y, (size_t)n * 6));
+    CHK(dalloc(&G, (size_t)mlp_nparam()));
+    CHK(dalloc(&L, 1));
+    CU(cudaMemcpy(X, x, (size_t)n * 4 * sizeof(float), cudaMemcpyDefault));
+    CU(cudaMemcpy(Y, y, (size_t)n * 6 * sizeof(float), cudaMemcpyDefault));
+    CU(launch_mlp_train_step(s->mlp, X, Y, n, n, 0, 0, 1, 0.0f, 1, G, L, s->st));
+    CU(cudaMemcpyAsync(grad, G, mlp_nparam() * sizeof(float), cudaMemcpyDefault, s->st));
+    float l = 0;
+    CU(cudaMemcpyAsync(&l, L, sizeof(float), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    if (loss) *loss = l;
+    cudaFree(X);
+    cudaFree(Y);
+    cudaFree(G);
+    cudaFree(L);
+    return MG_OK;
+}
+
+int mg_mlp_audit(mg_system* s, double* max_err, long long* counts)
+{
+    CHK(check_sys(s));
+    if (!s->mlp_ready) return fail(MG_ERR_STATE, "mg_mlp_init first");
+    float a[16];
+    CU(cudaMemcpy(a, s->mlp.audit, sizeof(a), cudaMemcpyDeviceToHost));
+    if (max_err)
+        for (int q = 0; q < 6; q++) max_err[q] = a[q];
+    if (counts) {
+        unsigned long long c[2];
+        memcpy(&c[0], a + 6, 8);
+        memcpy(&c[1], a + 8, 8);
+        counts[0] = (long long)c[0];
+        counts[1] = (long long)c[1];
+    }
     return MG_OK;
 }
 

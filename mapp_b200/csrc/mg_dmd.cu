@@ -22,108 +22,6 @@ namespace mg {
 
 namespace {
 
-// One species pair of one site pair: the Gauss-Hermite smearing of r*rho and
-// r*phi (ff_dmd_I.cpp:178-259) or the plain EAM values above alpha_max
-// (ff_dmd_I.cpp:261-310).  Returns false when the reference writes nothing.
-//
-// NQ > 0 fixes the node count at compile time so the node loop unrolls and
-// the table loads of all nodes issue together; NQ = 0 reads it from d.nq.
-// The branch-deciding quantities (alpha against alpha_min / alpha_max, rsq
-// against the cut-offs) are computed exactly as the reference does; powers of
-// alpha and 1/r come from rsqrt, which moves results by ulps only (the node and
-// table-index decisions they feed are continuous in the result).
-template <bool kPhi, bool kDeriv, int NQ>
-__device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double r, double r_inv, double rsq,
-                                      double alpha, double& g0, double& g_dr, double& g_da, double& f0, double& f_dr,
-                                      double& f_da)
-{
-    if (d.alpha_min < alpha && alpha < d.alpha_max) {
-        const int nq = NQ > 0 ? NQ : d.nq;
-        double inv_asq = rsqrt(alpha);
-        double asq = alpha * inv_asq;
-        double inv_alpha = inv_asq * inv_asq;
-        double upper = (r + d.rc) * asq, lower = (r - d.rc) * asq;
-        if (!(lower < d.xi[nq - 1])) return false;
-        double fa = 0.0, fb = 0.0, fc = 0.0, ga = 0.0, gb = 0.0, gc = 0.0;
-        const double* rt = d.rhoT + (size_t)rslot * d.nr * 8;
-        const double* pt = d.phiT + (size_t)pslot * d.nr * 8;
-#pragma unroll
-        for (int q = 0; q < (NQ > 0 ? NQ : kMaxQuad); q++) {
-            if (NQ == 0 && q >= nq) break;
-            double xq = d.xi[q];
-            if (xq > lower && xq < upper) {
-                double tmp0 = r - xq * inv_asq;
-                double p = fabs(tmp0) * d.dr_inv;
-                int m = min((int)p, d.nr - 2);
-                p -= m;
-                p = fmin(p, 1.0);
-                double p2 = p * p, p3 = p2 * p;
-                double4 cr = knot4(rt + 8 * m);
-                double tmp2 = (cr.w * p3 + cr.z * p2 + cr.y * p + cr.x) * tmp0;
-                ga += d.w0[q] * tmp2;
-                if (kDeriv) {
-                    gb += d.w1[q] * tmp2;
-                    gc += d.w2[q] * tmp2;
-                }
-                if (kPhi) {
-                    double4 cp = knot4(pt + 8 * m);
-                    double tmp1 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
-                    if (tmp0 < 0.0) tmp1 = -tmp1;
-                    fa += d.w0[q] * tmp1;
-                    if (kDeriv) {
-                        fb += d.w1[q] * tmp1;
-                        fc += d.w2[q] * tmp1;
-                    }
-                }
-            }
-        }
-        double sc = kPiInSq * r_inv;
-        g0 = ga * sc;
-        if (kDeriv) {
-            gb *= sc;
-            gc *= sc;
-            g_dr = -g0 * r_inv - 2.0 * asq * gb;
-            g_da = (0.5 * g0 - gc) * inv_alpha;
-        }
-        if (kPhi) {
-            f0 = fa * sc;
-            if (kDeriv) {
-                fb *= sc;
-                fc *= sc;
-                f_dr = -f0 * r_inv - 2.0 * asq * fb;
-                f_da = (0.5 * f0 - fc) * inv_alpha;
-            }
-        }
-        return true;
-    }
-    if (d.alpha_max <= alpha) {
-        if (!(rsq < d.cut_sq)) return false;
-        double p = r * d.dr_inv;
-        int m = min((int)p, d.nr - 2);
-        p -= m;
-        p = fmin(p, 1.0);
-        double p2 = p * p, p3 = p2 * p;
-        const double* cr = d.rhoT + ((size_t)rslot * d.nr + m) * 8;
-        g0 = cr[3] * p3 + cr[2] * p2 + cr[1] * p + cr[0];
-        if (kDeriv) {
-            g_da = 0.0;
-            g_dr = cr[6] * p2 + cr[5] * p + cr[4];
-        }
-        if (kPhi) {
-            const double* cp = d.phiT + ((size_t)pslot * d.nr + m) * 8;
-            double z2 = cp[3] * p3 + cp[2] * p2 + cp[1] * p + cp[0];
-            f0 = z2 * r_inv;
-            if (kDeriv) {
-                double z2p = cp[6] * p2 + cp[5] * p + cp[4];
-                f_da = 0.0;
-                f_dr = (z2p - z2 * r_inv) * r_inv;
-            }
-        }
-        return true;
-    }
-    return false;
-}
-
 // ---- force_calc pass 1 (ff_dmd_I.cpp:156-320) ----------------------------
 // One thread per half pair of the compact pair list (pairs sorted by i), so
 // every lane carries work however many neighbours a site has; the i-side sums
@@ -921,7 +819,7 @@ cudaError_t dmd_cdot_ntp(const Dev& d, cudaStream_t st)
 template <int NT>
 cudaError_t dmd_cdot_nt(const Dev& d, cudaStream_t st)
 {
-    return d.form == 1 ? dmd_cdot_ntp<NT, float>(d, st) : dmd_cdot_ntp<NT, double>(d, st);
+    return d.form != 0 ? dmd_cdot_ntp<NT, float>(d, st) : dmd_cdot_ntp<NT, double>(d, st);
 }
 
 template <int NT, typename P>
@@ -947,7 +845,7 @@ cudaError_t dmd_calc_g_ntp(const Dev& d, int chk, double alpha, int* nb, cudaStr
 template <int NT>
 cudaError_t dmd_calc_g_nt(const Dev& d, int chk, double alpha, int* nb, cudaStream_t st)
 {
-    return d.form == 1 ? dmd_calc_g_ntp<NT, float>(d, chk, alpha, nb, st)
+    return d.form != 0 ? dmd_calc_g_ntp<NT, float>(d, chk, alpha, nb, st)
                        : dmd_calc_g_ntp<NT, double>(d, chk, alpha, nb, st);
 }
 

@@ -25,8 +25,6 @@ namespace {
 #define MG_DMD32_MINB 4
 #endif
 
-constexpr float kPiInSqF = 0.564189583547756286948079451561f;
-
 // Accumulate a compensated (hi, lo) FP32 value into an FP64 per-site sum.
 __device__ __forceinline__ void acc_add(double* dst, float hi, float lo)
 {
@@ -53,102 +51,6 @@ __device__ __forceinline__ float2 seg_sum2(float v, const Seg& s)
         }
     }
     return make_float2(hi, lo);
-}
-
-struct F32Consts {
-    float rc, dr_inv, alpha_min, alpha_max;
-    int nr;
-};
-
-__device__ __forceinline__ F32Consts f32_consts(const Dev& d)
-{
-    F32Consts c;
-    c.rc = (float)d.rc;
-    c.dr_inv = (float)d.dr_inv;
-    c.alpha_min = (float)d.alpha_min;
-    c.alpha_max = (float)d.alpha_max;
-    c.nr = d.nr;
-    return c;
-}
-
-// FP32 counterpart of smear() in mg_dmd.cu: one species pair of one site pair.
-template <bool kPhi, int NQ>
-__device__ __forceinline__ bool smear_f(const Dev& d, const F32Consts& k, const float4* __restrict__ pk, float r,
-                                        float r_inv, bool below_rc, float alpha, float& g0, float& g_dr, float& g_da,
-                                        float& f0, float& f_dr, float& f_da)
-{
-    if (k.alpha_min < alpha && alpha < k.alpha_max) {
-        const int nq = NQ > 0 ? NQ : d.nq;
-        float inv_asq = rsqrtf(alpha);
-        float asq = alpha * inv_asq;
-        float inv_alpha = inv_asq * inv_asq;
-        float upper = (r + k.rc) * asq, lower = (r - k.rc) * asq;
-        if (!(lower < (float)d.xi[nq - 1])) return false;
-        float fa = 0.f, fb = 0.f, fc = 0.f, ga = 0.f, gb = 0.f, gc = 0.f;
-#pragma unroll
-        for (int q = 0; q < (NQ > 0 ? NQ : kMaxQuad); q++) {
-            if (NQ == 0 && q >= nq) break;
-            float xq = (float)d.xi[q];
-            if (xq > lower && xq < upper) {
-                float tmp0 = r - xq * inv_asq;
-                float p = fabsf(tmp0) * k.dr_inv;
-                int m = min((int)p, k.nr - 2);
-                p -= (float)m;
-                p = fminf(p, 1.0f);
-                float p2 = p * p, p3 = p2 * p;
-                float4 cr = __ldg(pk + 2 * m);
-                float tmp2 = (cr.w * p3 + cr.z * p2 + cr.y * p + cr.x) * tmp0;
-                float w0 = (float)d.w0[q], w1 = (float)d.w1[q], w2 = (float)d.w2[q];
-                ga += w0 * tmp2;
-                gb += w1 * tmp2;
-                gc += w2 * tmp2;
-                if (kPhi) {
-                    float4 cp = __ldg(pk + 2 * m + 1);
-                    float tmp1 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
-                    if (tmp0 < 0.0f) tmp1 = -tmp1;
-                    fa += w0 * tmp1;
-                    fb += w1 * tmp1;
-                    fc += w2 * tmp1;
-                }
-            }
-        }
-        float sc = kPiInSqF * r_inv;
-        g0 = ga * sc;
-        gb *= sc;
-        gc *= sc;
-        g_dr = -g0 * r_inv - 2.0f * asq * gb;
-        g_da = (0.5f * g0 - gc) * inv_alpha;
-        if (kPhi) {
-            f0 = fa * sc;
-            fb *= sc;
-            fc *= sc;
-            f_dr = -f0 * r_inv - 2.0f * asq * fb;
-            f_da = (0.5f * f0 - fc) * inv_alpha;
-        }
-        return true;
-    }
-    if (k.alpha_max <= alpha) {
-        if (!below_rc) return false;
-        float p = r * k.dr_inv;
-        int m = min((int)p, k.nr - 2);
-        p -= (float)m;
-        p = fminf(p, 1.0f);
-        float p2 = p * p, p3 = p2 * p;
-        float4 cr = __ldg(pk + 2 * m);
-        g0 = cr.w * p3 + cr.z * p2 + cr.y * p + cr.x;
-        g_da = 0.0f;
-        g_dr = (cr.y + 2.0f * cr.z * p + 3.0f * cr.w * p2) * k.dr_inv;
-        if (kPhi) {
-            float4 cp = __ldg(pk + 2 * m + 1);
-            float z2 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
-            float z2p = (cp.y + 2.0f * cp.z * p + 3.0f * cp.w * p2) * k.dr_inv;
-            f0 = z2 * r_inv;
-            f_da = 0.0f;
-            f_dr = (z2p - z2 * r_inv) * r_inv;
-        }
-        return true;
-    }
-    return false;
 }
 
 // ---- pass 1: FP32 smearing, compensated densities -------------------------
@@ -365,7 +267,31 @@ cudaError_t dmd32_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, c
     return cudaGetLastError();
 }
 
+template <int NT>
+cudaError_t dmd32_tail_nt(const Dev& d, int st_clc, int row0, int* nb, cudaStream_t st, cudaEvent_t* evs)
+{
+    int g1 = persistent_grid(d.npairs, MG_DMD32_MINB), g2 = div_up(d.natms, kFFBlock);
+    k_dmd32_embed<NT><<<g2, kFFBlock, 0, st>>>(d, row0);
+    if (evs) cudaEventRecord(evs[2], st);
+    k_dmd32_pass2<NT><<<g1, kFFBlock, 0, st>>>(d, st_clc, row0 + g2);
+    if (evs) cudaEventRecord(evs[3], st);
+    *nb = g1 + g2;
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t launch_dmd_force_f32_after_pass1(const Dev& d, int st_clc, int row0, int* nb, cudaStream_t st,
+                                             cudaEvent_t* evs)
+{
+    switch (d.nt) {
+    case 1: return dmd32_tail_nt<1>(d, st_clc, row0, nb, st, evs);
+    case 2: return dmd32_tail_nt<2>(d, st_clc, row0, nb, st, evs);
+    case 3: return dmd32_tail_nt<3>(d, st_clc, row0, nb, st, evs);
+    case 4: return dmd32_tail_nt<4>(d, st_clc, row0, nb, st, evs);
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 cudaError_t launch_dmd_force_f32(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
 {

@@ -1,4 +1,5 @@
-// Device helpers shared by the FP64 (mg_dmd.cu) and FP32 (mg_dmd32.cu) DMD kernels.
+// Device helpers shared by the FP64 (mg_dmd.cu), FP32 (mg_dmd32.cu) and learned
+// (mg_mlp.cu) DMD kernels.
 #pragma once
 
 #include "mg_internal.h"
@@ -46,6 +47,207 @@ __device__ __forceinline__ void embed_F(const Dev& d, int a, double Ev, double& 
     tmp1 = cf[8] * p3 + cf[7] * p2 + cf[6] * p + cf[5];
     if (Ev > d.rho_max) tmp0 += tmp1 * (Ev - d.rho_max);
     if (dd) *dd = (3.0 * cf[8] * p2 + cf[7] * p + cf[6]) * d.drho_inv;
+}
+
+// One species pair of one site pair: the Gauss-Hermite smearing of r*rho and
+// r*phi (ff_dmd_I.cpp:178-259) or the plain EAM values above alpha_max
+// (ff_dmd_I.cpp:261-310).  Returns false when the reference writes nothing.
+//
+// NQ > 0 fixes the node count at compile time so the node loop unrolls and
+// the table loads of all nodes issue together; NQ = 0 reads it from d.nq.
+// The branch-deciding quantities (alpha against alpha_min / alpha_max, rsq
+// against the cut-offs) are computed exactly as the reference does; powers of
+// alpha and 1/r come from rsqrt, which moves results by ulps only (the node and
+// table-index decisions they feed are continuous in the result).
+template <bool kPhi, bool kDeriv, int NQ>
+__device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double r, double r_inv, double rsq,
+                                      double alpha, double& g0, double& g_dr, double& g_da, double& f0, double& f_dr,
+                                      double& f_da)
+{
+    if (d.alpha_min < alpha && alpha < d.alpha_max) {
+        const int nq = NQ > 0 ? NQ : d.nq;
+        double inv_asq = rsqrt(alpha);
+        double asq = alpha * inv_asq;
+        double inv_alpha = inv_asq * inv_asq;
+        double upper = (r + d.rc) * asq, lower = (r - d.rc) * asq;
+        if (!(lower < d.xi[nq - 1])) return false;
+        double fa = 0.0, fb = 0.0, fc = 0.0, ga = 0.0, gb = 0.0, gc = 0.0;
+        const double* rt = d.rhoT + (size_t)rslot * d.nr * 8;
+        const double* pt = d.phiT + (size_t)pslot * d.nr * 8;
+#pragma unroll
+        for (int q = 0; q < (NQ > 0 ? NQ : kMaxQuad); q++) {
+            if (NQ == 0 && q >= nq) break;
+            double xq = d.xi[q];
+            if (xq > lower && xq < upper) {
+                double tmp0 = r - xq * inv_asq;
+                double p = fabs(tmp0) * d.dr_inv;
+                int m = min((int)p, d.nr - 2);
+                p -= m;
+                p = fmin(p, 1.0);
+                double p2 = p * p, p3 = p2 * p;
+                double4 cr = knot4(rt + 8 * m);
+                double tmp2 = (cr.w * p3 + cr.z * p2 + cr.y * p + cr.x) * tmp0;
+                ga += d.w0[q] * tmp2;
+                if (kDeriv) {
+                    gb += d.w1[q] * tmp2;
+                    gc += d.w2[q] * tmp2;
+                }
+                if (kPhi) {
+                    double4 cp = knot4(pt + 8 * m);
+                    double tmp1 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
+                    if (tmp0 < 0.0) tmp1 = -tmp1;
+                    fa += d.w0[q] * tmp1;
+                    if (kDeriv) {
+                        fb += d.w1[q] * tmp1;
+                        fc += d.w2[q] * tmp1;
+                    }
+                }
+            }
+        }
+        double sc = kPiInSq * r_inv;
+        g0 = ga * sc;
+        if (kDeriv) {
+            gb *= sc;
+            gc *= sc;
+            g_dr = -g0 * r_inv - 2.0 * asq * gb;
+            g_da = (0.5 * g0 - gc) * inv_alpha;
+        }
+        if (kPhi) {
+            f0 = fa * sc;
+            if (kDeriv) {
+                fb *= sc;
+                fc *= sc;
+                f_dr = -f0 * r_inv - 2.0 * asq * fb;
+                f_da = (0.5 * f0 - fc) * inv_alpha;
+            }
+        }
+        return true;
+    }
+    if (d.alpha_max <= alpha) {
+        if (!(rsq < d.cut_sq)) return false;
+        double p = r * d.dr_inv;
+        int m = min((int)p, d.nr - 2);
+        p -= m;
+        p = fmin(p, 1.0);
+        double p2 = p * p, p3 = p2 * p;
+        const double* cr = d.rhoT + ((size_t)rslot * d.nr + m) * 8;
+        g0 = cr[3] * p3 + cr[2] * p2 + cr[1] * p + cr[0];
+        if (kDeriv) {
+            g_da = 0.0;
+            g_dr = cr[6] * p2 + cr[5] * p + cr[4];
+        }
+        if (kPhi) {
+            const double* cp = d.phiT + ((size_t)pslot * d.nr + m) * 8;
+            double z2 = cp[3] * p3 + cp[2] * p2 + cp[1] * p + cp[0];
+            f0 = z2 * r_inv;
+            if (kDeriv) {
+                double z2p = cp[6] * p2 + cp[5] * p + cp[4];
+                f_da = 0.0;
+                f_dr = (z2p - z2 * r_inv) * r_inv;
+            }
+        }
+        return true;
+    }
+    return false;
+}
+
+constexpr float kPiInSqF = 0.564189583547756286948079451561f;
+
+struct F32Consts {
+    float rc, dr_inv, alpha_min, alpha_max;
+    int nr;
+};
+
+__device__ __forceinline__ F32Consts f32_consts(const Dev& d)
+{
+    F32Consts c;
+    c.rc = (float)d.rc;
+    c.dr_inv = (float)d.dr_inv;
+    c.alpha_min = (float)d.alpha_min;
+    c.alpha_max = (float)d.alpha_max;
+    c.nr = d.nr;
+    return c;
+}
+
+// FP32 counterpart of smear(): one species pair of one site pair, tables
+// packed one 32-byte sector per knot {rho c0..c3, phi c0..c3} (pk).
+template <bool kPhi, int NQ>
+__device__ __forceinline__ bool smear_f(const Dev& d, const F32Consts& k, const float4* __restrict__ pk, float r,
+                                        float r_inv, bool below_rc, float alpha, float& g0, float& g_dr, float& g_da,
+                                        float& f0, float& f_dr, float& f_da)
+{
+    if (k.alpha_min < alpha && alpha < k.alpha_max) {
+        const int nq = NQ > 0 ? NQ : d.nq;
+        float inv_asq = rsqrtf(alpha);
+        float asq = alpha * inv_asq;
+        float inv_alpha = inv_asq * inv_asq;
+        float upper = (r + k.rc) * asq, lower = (r - k.rc) * asq;
+        if (!(lower < (float)d.xi[nq - 1])) return false;
+        float fa = 0.f, fb = 0.f, fc = 0.f, ga = 0.f, gb = 0.f, gc = 0.f;
+#pragma unroll
+        for (int q = 0; q < (NQ > 0 ? NQ : kMaxQuad); q++) {
+            if (NQ == 0 && q >= nq) break;
+            float xq = (float)d.xi[q];
+            if (xq > lower && xq < upper) {
+                float tmp0 = r - xq * inv_asq;
+                float p = fabsf(tmp0) * k.dr_inv;
+                int m = min((int)p, k.nr - 2);
+                p -= (float)m;
+                p = fminf(p, 1.0f);
+                float p2 = p * p, p3 = p2 * p;
+                float4 cr = __ldg(pk + 2 * m);
+                float tmp2 = (cr.w * p3 + cr.z * p2 + cr.y * p + cr.x) * tmp0;
+                float w0 = (float)d.w0[q], w1 = (float)d.w1[q], w2 = (float)d.w2[q];
+                ga += w0 * tmp2;
+                gb += w1 * tmp2;
+                gc += w2 * tmp2;
+                if (kPhi) {
+                    float4 cp = __ldg(pk + 2 * m + 1);
+                    float tmp1 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
+                    if (tmp0 < 0.0f) tmp1 = -tmp1;
+                    fa += w0 * tmp1;
+                    fb += w1 * tmp1;
+                    fc += w2 * tmp1;
+                }
+            }
+        }
+        float sc = kPiInSqF * r_inv;
+        g0 = ga * sc;
+        gb *= sc;
+        gc *= sc;
+        g_dr = -g0 * r_inv - 2.0f * asq * gb;
+        g_da = (0.5f * g0 - gc) * inv_alpha;
+        if (kPhi) {
+            f0 = fa * sc;
+            fb *= sc;
+            fc *= sc;
+            f_dr = -f0 * r_inv - 2.0f * asq * fb;
+            f_da = (0.5f * f0 - fc) * inv_alpha;
+        }
+        return true;
+    }
+    if (k.alpha_max <= alpha) {
+        if (!below_rc) return false;
+        float p = r * k.dr_inv;
+        int m = min((int)p, k.nr - 2);
+        p -= (float)m;
+        p = fminf(p, 1.0f);
+        float p2 = p * p, p3 = p2 * p;
+        float4 cr = __ldg(pk + 2 * m);
+        g0 = cr.w * p3 + cr.z * p2 + cr.y * p + cr.x;
+        g_da = 0.0f;
+        g_dr = (cr.y + 2.0f * cr.z * p + 3.0f * cr.w * p2) * k.dr_inv;
+        if (kPhi) {
+            float4 cp = __ldg(pk + 2 * m + 1);
+            float z2 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
+            float z2p = (cp.y + 2.0f * cp.z * p + 3.0f * cp.w * p2) * k.dr_inv;
+            f0 = z2 * r_inv;
+            f_da = 0.0f;
+            f_dr = (z2p - z2 * r_inv) * r_inv;
+        }
+        return true;
+    }
+    return false;
 }
 
 // pair scratch of the running form: FP64 (plain) or FP32 (precision form)

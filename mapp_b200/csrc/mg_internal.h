@@ -27,6 +27,7 @@
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 
 namespace mg {
 
@@ -113,6 +114,23 @@ __host__ __device__ inline int comp_idx(int i, int j)
     return i < j ? (j + 1) * j / 2 + i : (i + 1) * i / 2 + j;
 }
 
+// training box of the learned form (inputs outside it fall back to quadrature)
+struct MlpBox {
+    float r_lo, r_hi, w_lo, w_hi;
+};
+
+// network parameters, optimiser state and deployment bookkeeping
+struct MlpState {
+    float* par;             // FP32 master parameters
+    __nv_bfloat16* wbf;     // BF16 copy used by the tensor-core kernels
+    float* m;               // Adam moments
+    float* v;
+    float* gpart;           // per-CTA partial gradients
+    float* audit;           // [0..5] max |network - quadrature| per output, [6..7] audited rows (u64), [8..9] fallback rows (u64)
+    MlpBox box;
+    float out_mean[6], out_scale[6];
+};
+
 // ---- launchers (defined in the .cu files) ---------------------------------
 // atoms / neighbour
 cudaError_t launch_x2s(const Dev& d, cudaStream_t st);
@@ -144,6 +162,21 @@ cudaError_t launch_dmd_force(const Dev& d, int st_clc, int* nblocks_out, cudaStr
 cudaError_t launch_dmd_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
 // precision form (MG_FORM_FP32) force_calc; evs as for launch_dmd_force
 cudaError_t launch_dmd_force_f32(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st, cudaEvent_t* evs);
+// the precision form's embedding and pass 2 after a pass 1 that filled the FP32 pair scratch
+cudaError_t launch_dmd_force_f32_after_pass1(const Dev& d, int st_clc, int row0, int* nblocks_out, cudaStream_t st,
+                                             cudaEvent_t* evs);
+// learned form
+size_t mlp_smem_bytes();
+int mlp_nparam();
+int mlp_npart();
+cudaError_t launch_mlp_labels(const Dev& d, const MlpBox& box, unsigned long long seed, int n, float* X, float* Y,
+                              cudaStream_t st);
+cudaError_t launch_mlp_train_step(const MlpState& S, const float* X, const float* Y, int n, int batch,
+                                  unsigned long long seed, int step, int total, float lr, int fixed, float* grad_out,
+                                  float* loss_hist, cudaStream_t st);
+cudaError_t launch_mlp_eval(const MlpState& S, const float* X, int n, float* Y, cudaStream_t st);
+cudaError_t launch_dmd_force_mlp(const Dev& d, const MlpState& S, unsigned long long audit_seed, int st_clc, int* nb,
+                                 cudaStream_t st, cudaEvent_t* evs);
 cudaError_t launch_dmd_crd(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nblocks_out, cudaStream_t st);

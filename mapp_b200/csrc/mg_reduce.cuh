@@ -70,7 +70,7 @@ inline int persistent_grid(long long threads_needed, int blocks_per_sm)
     return (int)(need < cap ? (need > 0 ? need : 1) : cap);
 }
 
-// Sums NV per-thread values over the block and writes them to
+// Sums NV per-thread values over the block (up to kFFBlock threads) and writes them to
 // partial[(row) * 8 + v] (row = blockIdx.x + row_offset).  Every thread of the
 // block must call it.
 template <int NV>
@@ -86,7 +86,7 @@ __device__ __forceinline__ void block_partials(const double (&vals)[NV], double*
     __syncthreads();
     if (threadIdx.x < NV) {
         double s = 0.0;
-        for (int k = 0; k < kFFWarps; k++) s += sh[k][threadIdx.x];
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += sh[k][threadIdx.x];
         partial[(size_t)row * 8 + threadIdx.x] = s;
     }
 }
