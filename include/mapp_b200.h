@@ -203,6 +203,68 @@ typedef struct mg_fs_coeffs {
 int mg_fs_energy_noalloc(const mg_fs_coeffs* coeffs, int natms, int nall, const double* x, const int* type,
                          const int* nbr_off, const int* nbr, double* energy, void* cuda_stream);
 
+/* ---- batched form: many independent DMD cells relaxed together ----------- */
+/* No counterpart in the reference, which relaxes one system per process with
+   Min_LBFGS::run (min_l-bfgs.cpp:616-773) and LineSearch_BackTrack::line_min
+   (line_search.cpp:223-342).  Every cell of a batch runs that algorithm on the
+   GPU -- m-entry two-loop recursion, Armijo backtracking with c = 0.4,
+   rho = 0.5 and first step min(1, max|h|) after |h| = 1, the reference's
+   stopping codes -- with all cells advancing together: one force evaluation
+   per active cell per iteration, inside one CUDA-graph launch whose
+   device-side while loop runs until every cell has stopped.  Cells may
+   differ in size and box.  Line-search energies are those of the force pass
+   (see the oracle's orc_lbfgs), the L-BFGS dot products, Armijo tests and
+   energies are FP64, and the force passes are FP64 or the FP32 precision
+   form (mg_batch_set_form).
+
+   The batch builds each cell's ghosts and neighbour list with `builder`, a
+   DMD system with types, skin and ff_coef set: its own atoms are replaced. */
+typedef struct mg_batch mg_batch;
+
+typedef struct mg_batch_stats {
+    double relax_ms;        /* device-loop wall time, list rebuilds included */
+    double build_ms;        /* ghosts + lists of every cell, gathered into the batch */
+    double tune_ms;         /* autotuning (0 when the choice came from the cache) */
+    long long iterations;   /* while-loop iterations (force evaluations of the longest cell) */
+    long long evaluations;  /* force evaluations summed over cells */
+    int rebuild_rounds;     /* list rebuilds triggered by the skin rule */
+    int converged;          /* cells stopped by max|f| < fmax_tol */
+    int bps1, bps2;         /* blocks per SM of force pass 1 and pass 2 */
+    int lbfgs_threads;      /* threads per cell of the L-BFGS step */
+    int from_cache;         /* launch shapes read from the tuning cache */
+} mg_batch_stats;
+
+typedef struct mg_cell_result {
+    double energy;          /* free energy at the final point */
+    double max_f;           /* max |f| over the cell's degrees of freedom at the last accepted point */
+    double t_ms;            /* time from the start of the relaxation to this cell's stop */
+    int code;               /* line_search.h codes: 0 running, 1 not downhill, 2 zero gradient,
+                               3 minimum step, 4 max iterations, 5 tolerance (energy or max|f|) */
+    int iterations;         /* line searches */
+    int evaluations;        /* force evaluations */
+    int natms;
+} mg_cell_result;
+
+int mg_batch_create(mg_system* builder, mg_batch** out);
+int mg_batch_destroy(mg_batch* b);
+/* one periodic cell: box H (3x3, lower triangular as Atoms::H), natms sites
+   with x_frac = natms * (3 + nt) (fractional position, then alpha per
+   species) and c = natms * nt */
+int mg_batch_add_cell(mg_batch* b, int natms, const double* H, const double* x_frac, const double* c, int* index);
+/* history m (1..8), iteration limit, stop when max|f| < fmax_tol (0: off),
+   reference energy tolerance, backtracking limit (halvings per line search) */
+int mg_batch_set_params(mg_batch* b, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings);
+/* MG_FORM_FP64 or MG_FORM_FP32 force passes */
+int mg_batch_set_form(mg_batch* b, int form);
+/* autotune = 1: time candidate launch shapes on the batch (or read them from
+   cache_path, a text file of earlier choices, which is then extended);
+   0: built-in shapes.  cache_path may be NULL. */
+int mg_batch_set_tuning(mg_batch* b, int autotune, const char* cache_path);
+int mg_batch_relax(mg_batch* b, mg_batch_stats* stats);
+/* final state of one cell: x = natms * (3 + nt) Cartesian positions and
+   alpha, f the same shape; either may be NULL */
+int mg_batch_cell_result(mg_batch* b, int cell, double* x, double* f, mg_cell_result* r);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,7 +66,31 @@ SIGNATURES = {
     "mg_mlp_eval": (C.c_int, [_P, C.c_int, _P, _P]),
     "mg_mlp_grad": (C.c_int, [_P, C.c_int, _P, _P, _P, _D]),
     "mg_mlp_audit": (C.c_int, [_P, _D, C.POINTER(C.c_longlong)]),
+    "mg_batch_create": (C.c_int, [_P, C.POINTER(C.c_void_p)]),
+    "mg_batch_destroy": (C.c_int, [_P]),
+    "mg_batch_add_cell": (C.c_int, [_P, C.c_int, _P, _P, _P, _I]),
+    "mg_batch_set_params": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]),
+    "mg_batch_set_form": (C.c_int, [_P, C.c_int]),
+    "mg_batch_set_tuning": (C.c_int, [_P, C.c_int, C.c_char_p]),
+    "mg_batch_relax": (C.c_int, [_P, _P]),
+    "mg_batch_cell_result": (C.c_int, [_P, C.c_int, _P, _P, _P]),
 }
+
+
+class BatchStats(C.Structure):
+    """mg_batch_stats (include/mapp_b200.h)."""
+
+    _fields_ = [("relax_ms", C.c_double), ("build_ms", C.c_double), ("tune_ms", C.c_double),
+                ("iterations", C.c_longlong), ("evaluations", C.c_longlong), ("rebuild_rounds", C.c_int),
+                ("converged", C.c_int), ("bps1", C.c_int), ("bps2", C.c_int), ("lbfgs_threads", C.c_int),
+                ("from_cache", C.c_int)]
+
+
+class CellResult(C.Structure):
+    """mg_cell_result (include/mapp_b200.h)."""
+
+    _fields_ = [("energy", C.c_double), ("max_f", C.c_double), ("t_ms", C.c_double), ("code", C.c_int),
+                ("iterations", C.c_int), ("evaluations", C.c_int), ("natms", C.c_int)]
 
 
 class FsCoeffs(C.Structure):
@@ -320,6 +344,68 @@ def fs_energy_noalloc(coeffs: "FsCoeffs", natms: int, nall: int, x, type, nbr_of
     tensor of one double."""
     _check(load_library().mg_fs_energy_noalloc(C.byref(coeffs), natms, nall, _ptr(x), _ptr(type), _ptr(nbr_off),
                                                _ptr(nbr), _ptr(energy), stream))
+
+
+class Batch:
+    """Batched form: independent DMD cells relaxed by L-BFGS together on one GPU
+    (mg_batch_*).  `builder` is a DMD System with types, skin and ff_coef set;
+    its atoms are replaced while the batch builds each cell's lists."""
+
+    def __init__(self, builder: "System"):
+        L = load_library()
+        self.builder = builder
+        self.nt = builder.nt
+        h = C.c_void_p()
+        _check(L.mg_batch_create(builder.h, C.byref(h)))
+        self.h = h.value
+        self.natms = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().mg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_cell(self, cfg) -> int:
+        """Add a fixtures.Config cell (its box, s + alpha, c)."""
+        H = np.ascontiguousarray(cfg.H(), dtype=np.float64)
+        x = np.ascontiguousarray(cfg.x_dmd(), dtype=np.float64)
+        c = np.ascontiguousarray(cfg.c, dtype=np.float64)
+        idx = C.c_int(-1)
+        _check(load_library().mg_batch_add_cell(self.h, cfg.natms, H.ctypes.data, x.ctypes.data, c.ctypes.data,
+                                                C.byref(idx)))
+        self.natms.append(cfg.natms)
+        return idx.value
+
+    def set_params(self, m=5, max_iter=10000, fmax_tol=1e-5, energy_tol=1e-8, max_halvings=60):
+        _check(load_library().mg_batch_set_params(self.h, m, max_iter, fmax_tol, energy_tol, max_halvings))
+
+    def set_form(self, form):
+        _check(load_library().mg_batch_set_form(self.h, form))
+
+    def set_tuning(self, autotune=True, cache_path=None):
+        _check(load_library().mg_batch_set_tuning(self.h, int(autotune),
+                                                  None if cache_path is None else str(cache_path).encode()))
+
+    def relax(self) -> dict:
+        st = BatchStats()
+        _check(load_library().mg_batch_relax(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in BatchStats._fields_}
+
+    def cell_result(self, cell: int):
+        """(x, f, info): final Cartesian x + alpha and forces (natms x (3 + nt)), result fields."""
+        n = self.natms[cell]
+        xd = 3 + self.nt
+        x = np.zeros((n, xd))
+        f = np.zeros((n, xd))
+        r = CellResult()
+        _check(load_library().mg_batch_cell_result(self.h, cell, x.ctypes.data, f.ctypes.data, C.byref(r)))
+        return x, f, {k: getattr(r, k) for k, _ in CellResult._fields_}
 
 
 def system_from_workload(w: dict, device: int = 0, skin: float = 0.5) -> System:

@@ -184,6 +184,7 @@ std::vector<std::string> tokens(const std::string& line)
 }  // namespace
 
 int mg::internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+const char* mg::internal_last_error() { return g_err.c_str(); }
 
 struct mg_system {
     int style = 0, form = MG_FORM_FP64, device = 0, nt = 0, x_dim = 3, dmd = 0;
@@ -240,6 +241,7 @@ struct mg_system {
     double t_list = 0, t_force = 0, t_energy = 0, t_cd = 0, t_g = 0;
     double t_k[3] = {0, 0, 0};  // DMD force: pass 1, embedding, pass 2
     long long partial_rows = 0;
+    bool tables_uploaded = false;  // device tables match the last ff_coef
 };
 
 namespace {
@@ -514,14 +516,6 @@ int rebuild(mg_system* s)
     return MG_OK;
 }
 
-int reduce_to_host(mg_system* s, int rows, int nvals, double* out)
-{
-    CU(launch_reduce_partials(s->d, rows, nvals, s->red_out, s->st));
-    CU(cudaMemcpyAsync(out, s->red_out, nvals * sizeof(double), cudaMemcpyDeviceToHost, s->st));
-    CU(cudaStreamSynchronize(s->st));
-    return MG_OK;
-}
-
 // ---- potential readers -----------------------------------------------------
 
 int read_all(const char* path, std::vector<std::string>& lines)
@@ -617,7 +611,7 @@ int read_fs_coeffs(mg_system* s, const char* path)
         std::vector<std::string> t = tokens(l);
         if (!t.empty()) rows.push_back(t);
     }
-    int nt = s->nt, ncomp = nt * (nt + 1) / 2;
+    int nt = s->nt;
     size_t r = 0;
     if (rows.empty() || (int)rows[0].size() != nt)
         return fail(MG_ERR_FORMAT, "number of types represented and forcefield do not match");
@@ -652,14 +646,13 @@ int read_fs_coeffs(mg_system* s, const char* path)
             d.fsk3[c] = atof(rows[r][4].c_str());
             d.fs_chk[c] = 1;
         }
-    (void)ncomp;
     return MG_OK;
 }
 
 int upload_tables(mg_system* s)
 {
     Dev& d = s->d;
-    if (s->style == STYLE_FS) return MG_OK;
+    if (s->style == STYLE_FS || s->tables_uploaded) return MG_OK;
     CHK(dalloc(&s->d_rhoT, s->rhoT.size()));
     CHK(dalloc(&s->d_phiT, s->phiT.size()));
     CHK(dalloc(&s->d_FT, s->FT.size()));
@@ -695,6 +688,7 @@ int upload_tables(mg_system* s)
     d.drho = s->drho;
     d.dr_inv = 1.0 / s->dr;
     d.drho_inv = 1.0 / s->drho;
+    s->tables_uploaded = true;
     return MG_OK;
 }
 
@@ -980,6 +974,7 @@ int mg_ff_coef(mg_system* s, int narg, const char* const* arg)
         d.cut_sq_mod = mod_rc * mod_rc;
     }
     s->coef_set = true;
+    s->tables_uploaded = false;
     s->initialized = false;
     return MG_OK;
 }
@@ -1268,7 +1263,7 @@ int mg_get_vector(mg_system* s, const char* name, double* out)
     CHK(check_sys(s));
     if (!name || !out) return fail(MG_ERR_ARG, "null argument");
     Dev& d = s->d;
-    int nall = d.nall, nt = s->nt;
+    int nt = s->nt;
     const double* src = nullptr;
     size_t count = 0;
     if (!strcmp(name, "E")) src = d.E, count = (size_t)s->natms * nt;
@@ -1278,7 +1273,6 @@ int mg_get_vector(mg_system* s, const char* name, double* out)
     else if (!strcmp(name, "c_d")) src = d.c_d, count = (size_t)s->natms * nt;
     else if (!strcmp(name, "rho")) src = d.rho, count = (size_t)s->natms;
     else return fail(MG_ERR_ARG, "unknown vector %s", name);
-    (void)nall;
     CHK(copy_out(s, out, src, count * sizeof(double)));
     CU(cudaStreamSynchronize(s->st));
     return MG_OK;
@@ -1524,3 +1518,19 @@ int mg_mlp_audit(mg_system* s, double* max_err, long long* counts)
 }
 
 }  // extern "C"
+
+// ---- accessors for the batched form ---------------------------------------
+Dev& mg::system_dev(mg_system* s) { return s->d; }
+cudaStream_t mg::system_stream(mg_system* s) { return s->st; }
+int mg::system_device(mg_system* s) { return s->device; }
+void mg::system_shape(mg_system* s, int* style, int* nt, int* x_dim, int* form, double* B_out)
+{
+    if (style) *style = s->coef_set ? s->style : -1;
+    if (nt) *nt = s->nt;
+    if (x_dim) *x_dim = s->x_dim;
+    if (form) *form = s->form;
+    if (B_out)
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) B_out[3 * i + j] = s->B[i][j];
+}
+double mg::system_skin(mg_system* s) { return s->skin; }

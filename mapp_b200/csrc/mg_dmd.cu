@@ -46,7 +46,9 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int 
         double Ei[NT];
 #pragma unroll
         for (int a = 0; a < NT; a++) Ei[a] = 0.0;
-        if (valid) {
+        const bool act = valid && site_active(d, i);
+        double epair = 0.0;
+        if (act) {
             int j = d.pair_j[p];
             double4 xi = d.pos[i], xj = d.pos[j];
             double ai[NT], ci[NT], aj[NT], cj[NT], Ej[NT];
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int 
                         __stcs(out + (S::PHI + ps) * mp, f0);
                         __stcs(out + (S::DPR + ps) * mp, fdr);
                         __stcs(out + (S::DPA + ps) * mp, fda);
-                        acc[0] += w * (cj[b] * ci[a] + cj[a] * ci[b]) * f0;
+                        epair += w * (cj[b] * ci[a] + cj[a] * ci[b]) * f0;
                     }
                     Ei[a] += g0 * cj[b];
                     Ej[b] += g0 * ci[a];
@@ -103,6 +105,8 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int 
             double t = seg_sum(Ei[a], sg);
             if (valid && lane == sg.first && t != 0.0) atomicAdd(&d.E[(size_t)i * NT + a], t);
         }
+        if (d.site_cell) cell_energy_add(d, valid ? i : -1, epair);
+        else acc[0] += epair;
     }
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
 }
@@ -113,7 +117,8 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_embed(Dev d, int with_force, i
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (i < d.natms) {
+    double e = 0.0;
+    if (i < d.natms && site_active(d, i)) {
 #pragma unroll
         for (int a = 0; a < NT; a++) {
             double tmp0, tmp1;
@@ -121,12 +126,14 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_embed(Dev d, int with_force, i
             double ca = d.c[(size_t)i * NT + a], al = d.alpha[(size_t)i * NT + a];
             d.E[(size_t)i * NT + a] = tmp0;
             if (with_force) d.dE[(size_t)i * NT + a] = tmp1;
-            acc[0] += ca * tmp0;
-            acc[0] += d.kbT * calc_ent(ca);
-            acc[0] += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
+            e += ca * tmp0;
+            e += d.kbT * calc_ent(ca);
+            e += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
             if (with_force) d.f[(size_t)i * d.x_dim + 3 + a] -= 1.5 * d.kbT * ca / al;
         }
     }
+    if (d.site_cell) cell_energy_add(d, i < d.natms ? i : -1, e);
+    else acc[0] += e;
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
 }
 
@@ -148,7 +155,8 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass2(Dev d, int 
         double fi[3 + NT];
 #pragma unroll
         for (int q = 0; q < 3 + NT; q++) fi[q] = 0.0;
-        if (valid) {
+        const bool act = valid && site_active(d, i);
+        if (act) {
             const double* in = d.pr + p;
             double drr[NT * NT], dra[NT * NT], dpr[S::NC], dpa[S::NC];
 #pragma unroll
@@ -779,8 +787,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
 template <int NT>
 cudaError_t dmd_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
 {
-    int g1 = persistent_grid(d.npairs, MG_DMD_MINB), g2 = div_up(d.natms, kFFBlock);
-    int g3 = g1;
+    int g1 = persistent_grid(d.npairs, d.tune_bps > 0 ? d.tune_bps : MG_DMD_MINB), g2 = div_up(d.natms, kFFBlock);
+    int g3 = persistent_grid(d.npairs, d.tune_bps2 > 0 ? d.tune_bps2 : MG_DMD_MINB);
     if (evs) cudaEventRecord(evs[0], st);
     if (d.nq == 3) k_dmd_pass1<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
     else k_dmd_pass1<NT, 0><<<g1, kFFBlock, 0, st>>>(d, 0);

@@ -70,7 +70,9 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass1(Dev d, 
         float Ei[NT];
 #pragma unroll
         for (int a = 0; a < NT; a++) Ei[a] = 0.0f;
-        if (valid) {
+        const bool act = valid && site_active(d, i);
+        double epair = 0.0;
+        if (act) {
             int j = d.pair_j[p];
             double4 xi = d.pos[i], xj = d.pos[j];
             float ai[NT], ci[NT], aj[NT], cj[NT], Ej[NT];
@@ -113,7 +115,7 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass1(Dev d, 
                         __stcs(out + (S::PHI + ps) * mp, f0);
                         __stcs(out + (S::DPR + ps) * mp, fdr);
                         __stcs(out + (S::DPA + ps) * mp, fda);
-                        acc[0] += w * (double)((cj[b] * ci[a] + cj[a] * ci[b]) * f0);
+                        epair += w * (double)((cj[b] * ci[a] + cj[a] * ci[b]) * f0);
                     }
                     Ei[a] += g0 * cj[b];
                     Ej[b] += g0 * ci[a];
@@ -129,6 +131,8 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass1(Dev d, 
             float2 t = seg_sum2(Ei[a], sg);
             if (valid && lane == sg.first) acc_add(&d.E[(size_t)i * NT + a], t.x, t.y);
         }
+        if (d.site_cell) cell_energy_add(d, valid ? i : -1, epair);
+        else acc[0] += epair;
     }
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
 }
@@ -139,7 +143,8 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd32_embed(Dev d, int row0)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (i < d.natms) {
+    double e = 0.0;
+    if (i < d.natms && site_active(d, i)) {
 #pragma unroll
         for (int a = 0; a < NT; a++) {
             size_t q = (size_t)i * NT + a;
@@ -149,12 +154,14 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd32_embed(Dev d, int row0)
             double ca = d.c[q], al = d.alpha[q];
             d.E[q] = tmp0;
             d.dE[q] = tmp1;
-            acc[0] += ca * tmp0;
-            acc[0] += d.kbT * calc_ent(ca);
-            acc[0] += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
+            e += ca * tmp0;
+            e += d.kbT * calc_ent(ca);
+            e += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
             d.f[(size_t)i * d.x_dim + 3 + a] -= 1.5 * d.kbT * ca / al;
         }
     }
+    if (d.site_cell) cell_energy_add(d, i < d.natms ? i : -1, e);
+    else acc[0] += e;
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
 }
 
@@ -174,7 +181,8 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass2(Dev d, 
         float fi[3 + NT];
 #pragma unroll
         for (int q = 0; q < 3 + NT; q++) fi[q] = 0.0f;
-        if (valid) {
+        const bool act = valid && site_active(d, i);
+        if (act) {
             const float* in = d.prf + p;
             float drr[NT * NT], dra[NT * NT], dpr[S::NC], dpa[S::NC];
 #pragma unroll
@@ -254,23 +262,24 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass2(Dev d, 
 template <int NT>
 cudaError_t dmd32_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
 {
-    int g1 = persistent_grid(d.npairs, MG_DMD32_MINB), g2 = div_up(d.natms, kFFBlock);
+    int g1 = persistent_grid(d.npairs, d.tune_bps > 0 ? d.tune_bps : MG_DMD32_MINB), g2 = div_up(d.natms, kFFBlock);
+    int g3 = persistent_grid(d.npairs, d.tune_bps2 > 0 ? d.tune_bps2 : MG_DMD32_MINB);
     if (evs) cudaEventRecord(evs[0], st);
     if (d.nq == 3) k_dmd32_pass1<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
     else k_dmd32_pass1<NT, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
     if (evs) cudaEventRecord(evs[1], st);
     k_dmd32_embed<NT><<<g2, kFFBlock, 0, st>>>(d, g1);
     if (evs) cudaEventRecord(evs[2], st);
-    k_dmd32_pass2<NT><<<g1, kFFBlock, 0, st>>>(d, st_clc, g1 + g2);
+    k_dmd32_pass2<NT><<<g3, kFFBlock, 0, st>>>(d, st_clc, g1 + g2);
     if (evs) cudaEventRecord(evs[3], st);
-    *nb = 2 * g1 + g2;
+    *nb = g1 + g2 + g3;
     return cudaGetLastError();
 }
 
 template <int NT>
 cudaError_t dmd32_tail_nt(const Dev& d, int st_clc, int row0, int* nb, cudaStream_t st, cudaEvent_t* evs)
 {
-    int g1 = persistent_grid(d.npairs, MG_DMD32_MINB), g2 = div_up(d.natms, kFFBlock);
+    int g1 = persistent_grid(d.npairs, d.tune_bps2 > 0 ? d.tune_bps2 : MG_DMD32_MINB), g2 = div_up(d.natms, kFFBlock);
     k_dmd32_embed<NT><<<g2, kFFBlock, 0, st>>>(d, row0);
     if (evs) cudaEventRecord(evs[2], st);
     k_dmd32_pass2<NT><<<g1, kFFBlock, 0, st>>>(d, st_clc, row0 + g2);

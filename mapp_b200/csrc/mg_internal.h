@@ -29,6 +29,8 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 
+struct mg_system;
+
 namespace mg {
 
 enum Style { STYLE_EAM = 0, STYLE_FS = 1, STYLE_DMD_I = 2, STYLE_DMD_II = 3, STYLE_DMD = 4 };
@@ -107,6 +109,12 @@ struct Dev {
     double rsq_crd, alpha_min, alpha_max, kbT, beta, c0[kMaxTypes];
     int nq;
     double xi[kMaxQuad], w0[kMaxQuad], w1[kMaxQuad], w2[kMaxQuad];
+    // batched form (many independent cells in one site / pair numbering);
+    // all null for a single system
+    const int* site_cell;              // owned site -> cell
+    const unsigned char* cell_active;  // cells whose pairs / sites are evaluated
+    double* cell_E;                    // per-cell energy accumulators
+    int tune_bps, tune_bps2;           // blocks per SM of pair pass 1 / pass 2 (0: built-in)
 };
 
 __host__ __device__ inline int comp_idx(int i, int j)
@@ -183,9 +191,17 @@ cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nblocks_
 
 // records msg as the calling thread's last error and returns code
 int internal_fail(int code, const char* msg);
+const char* internal_last_error();
 
 // grid sizing helpers
 int num_sms();
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// accessors of a single system for the batched form (mg_api.cu)
+Dev& system_dev(mg_system* s);
+cudaStream_t system_stream(mg_system* s);
+int system_device(mg_system* s);
+void system_shape(mg_system* s, int* style, int* nt, int* x_dim, int* form, double* B_out);
+double system_skin(mg_system* s);
 
 }  // namespace mg

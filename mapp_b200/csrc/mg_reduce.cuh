@@ -61,6 +61,24 @@ __device__ __forceinline__ double seg_sum(double v, const Seg& s)
     return v;
 }
 
+// Batched form: is the cell of owned site i still being evaluated?
+__device__ __forceinline__ bool site_active(const Dev& d, int i)
+{
+    return d.cell_active == nullptr || d.cell_active[d.site_cell[i]] != 0;
+}
+
+// Batched form: adds e (this lane's energy term of owned site i; i < 0 for a
+// lane without one) to the energy of i's cell, one atomic per run of equal
+// cells in the warp (sites and pairs are numbered cell by cell).  Every lane
+// of the warp must call it.
+__device__ __forceinline__ void cell_energy_add(const Dev& d, int i, double e)
+{
+    const int cell = i >= 0 ? d.site_cell[i] : -1;
+    const Seg s = seg_of(cell);
+    const double t = seg_sum(e, s);
+    if (cell >= 0 && (int)(threadIdx.x & 31) == s.first && t != 0.0) atomicAdd(&d.cell_E[cell], t);
+}
+
 // Persistent grid size for a force kernel: enough blocks to fill every SM at
 // the kernel's resident-block count, never more than the work needs.
 inline int persistent_grid(long long threads_needed, int blocks_per_sm)

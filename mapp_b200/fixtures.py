@@ -246,6 +246,8 @@ class Config:
         return self.alpha is not None
 
     def H(self) -> np.ndarray:
+        if "H" in self.extra:
+            return np.array(self.extra["H"], dtype=np.float64)
         return np.diag([self.L, self.L, self.L]).astype(np.float64)
 
     def x_dmd(self) -> np.ndarray:
@@ -257,6 +259,13 @@ def fcc_sites(n: int, a: float) -> np.ndarray:
     base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]], dtype=np.float64)
     g = np.arange(n, dtype=np.float64)
     cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+    return ((cells[:, None, :] + base[None, :, :]).reshape(-1, 3)) * a
+
+
+def fcc_box(nx: int, ny: int, nz: int, a: float) -> np.ndarray:
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]], dtype=np.float64)
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), axis=-1)
+    cells = g.reshape(-1, 3).astype(np.float64)
     return ((cells[:, None, :] + base[None, :, :]).reshape(-1, 3)) * a
 
 
@@ -306,6 +315,57 @@ def make_dmd_config(n=20, a=3.58, sigma=0.0, seed=4321, nt=2,
                   alpha=alpha, c=c)
 
 
+def make_dmd_cell(nx, ny, nz, a=3.58, sigma=0.0, seed=0, nt=2, w_lo=0.08, w_hi=0.15, mean_cA=None) -> Config:
+    """One periodic DMD cell of nx x ny x nz FCC unit cells (box diag(nx, ny, nz) a):
+    alpha = 1/w^2 with w ~ U(w_lo, w_hi) A per site and species, c_A ~ Beta(2,2)
+    shifted to mean_cA (clipped to [0.01, 0.99]) when given, c_B = 1 - c_A."""
+    rng = np.random.default_rng(seed)
+    x = fcc_box(nx, ny, nz, a)
+    if sigma > 0:
+        x = x + rng.normal(0.0, sigma, size=x.shape)
+    edges = np.array([nx, ny, nz], dtype=np.float64) * a
+    s = _wrap(x / edges)
+    N = len(s)
+    w = rng.uniform(w_lo, w_hi, size=(N, nt))
+    alpha = 1.0 / (w * w)
+    if nt == 1:
+        c = np.ones((N, 1))
+    else:
+        cA = rng.beta(2.0, 2.0, size=N)
+        if mean_cA is not None:
+            cA = np.clip(cA + (mean_cA - 0.5), 0.01, 0.99)
+        c = np.zeros((N, nt))
+        c[:, 0] = cA
+        c[:, 1:] = (1.0 - cA)[:, None] / (nt - 1)
+    return Config(float(edges[0]), s, [sp.name for sp in ALL_SPECIES[:nt]], [sp.mass for sp in ALL_SPECIES[:nt]],
+                  alpha=alpha, c=c, extra={"H": np.diag(edges)})
+
+
+def make_batch_cells(ncells=512, seed=2024, lo=500, hi=8000, a=3.58, sigma=0.0, nt=2):
+    """Cells of the batched form: site counts log-uniform in [lo, hi], rounded
+    to whole FCC unit cells (4 nx ny nz sites), cubic or slab (nx = ny != nz)
+    with equal odds; per cell a mean c_A ~ U(0.1, 0.9), per site w ~ U(0.08, 0.15) A."""
+    rng = np.random.default_rng(seed)
+    cells = []
+    for k in range(ncells):
+        target = float(np.exp(rng.uniform(np.log(lo), np.log(hi)))) / 4.0
+        if rng.uniform() < 0.5:
+            n = max(2, int(round(target ** (1.0 / 3.0))))
+            shape = (n, n, n)
+        else:
+            nz = max(2, int(round(target ** (1.0 / 3.0) / 2.0)))
+            nxy = max(2, int(round(np.sqrt(target / nz))))
+            shape = (nxy, nxy, nz)
+        shape = list(shape)
+        while 4 * np.prod(shape) > hi:
+            shape[int(np.argmax(shape))] -= 1
+        while 4 * np.prod(shape) < lo:
+            shape[int(np.argmin(shape))] += 1
+        cells.append(make_dmd_cell(*shape, a=a, sigma=sigma, seed=int(rng.integers(1 << 31)), nt=nt,
+                                   mean_cA=float(rng.uniform(0.1, 0.9))))
+    return cells
+
+
 def write_cfg(path: str, cfg: Config):
     """Extended CFG with .NO_VELOCITY.; DMD lines are s alpha c (read_cfg.cpp:562-627).
 
@@ -318,9 +378,10 @@ def write_cfg(path: str, cfg: Config):
     with open(path, "w") as fp:
         fp.write("Number of particles = %d\n" % cfg.natms)
         fp.write("A = 1.0 Angstrom (basic length-scale)\n")
+        Hm = cfg.H()
         for i in range(3):
             for j in range(3):
-                fp.write("H0(%d,%d) = %.17g A\n" % (i + 1, j + 1, cfg.L if i == j else 0.0))
+                fp.write("H0(%d,%d) = %.17g A\n" % (i + 1, j + 1, Hm[i][j]))
         fp.write(".NO_VELOCITY.\n")
         fp.write("entry_count = %d\n" % (3 + 2 * nt if cfg.dmd else 3))
         if cfg.dmd:
@@ -365,7 +426,8 @@ def write_workload(dirpath: str, kind: str, **kw) -> dict:
     kind: "eam" (configs[0]-style FCC EAM), "fs" (analytic FS), "dmd" (binary DMD).
     """
     os.makedirs(dirpath, exist_ok=True)
-    out = {"kind": kind, "dir": dirpath}
+    skin = kw.pop("skin", 0.5)
+    out = {"kind": kind, "dir": dirpath, "skin": skin}
     if kind == "eam":
         nt = kw.pop("nt", 1)
         fmt = kw.pop("fmt", "SetFL")
@@ -386,7 +448,7 @@ def write_workload(dirpath: str, kind: str, **kw) -> dict:
     elif kind == "dmd":
         style = kw.pop("style", "DMD_I")
         coef_kw = {k: kw.pop(k) for k in ("r_crd", "n_quad", "alpha_min", "alpha_max", "T") if k in kw}
-        cfg = make_dmd_config(**kw)
+        cfg = kw.pop("cfg", None) or make_dmd_config(**kw)
         nt = len(cfg.names)
         tables = make_tables(ALL_SPECIES[:nt])
         pot = os.path.join(dirpath, "pot.fs")
@@ -398,6 +460,6 @@ def write_workload(dirpath: str, kind: str, **kw) -> dict:
     cfg_path = os.path.join(dirpath, "conf.cfg")
     write_cfg(cfg_path, cfg)
     script = os.path.join(dirpath, "in.mapp")
-    write_script(script, cfg_path, cfg.dmd, kw.get("skin", 0.5))
+    write_script(script, cfg_path, cfg.dmd, skin)
     out.update(cfg=cfg, cfg_path=cfg_path, script=script, pot=pot)
     return out

@@ -1706,3 +1706,195 @@ void orc_get_pairs(orc_t* o, double* out)
     memcpy(out + 3 * n0 + n1, o->p_dphi_dr, n1 * 8);
     memcpy(out + 3 * n0 + 2 * n1, o->p_dphi_da, n1 * 8);
 }
+
+/* ------------------------------------------------------------------ */
+/* L-BFGS relaxation                                                   */
+/* ------------------------------------------------------------------ */
+/* Codes of line_search.h:7. */
+enum { ORC_LS_S, ORC_LS_F_DOWNHILL, ORC_LS_F_GRAD0, ORC_LS_F_ALPHAMIN, ORC_MIN_F_MAX_ITER, ORC_MIN_F_TOLERANCE };
+
+/* LineSearch::energy (line_search.cpp:180-195), fixed box: x = x_prev + a h, update_0, energy_calc */
+static double ls_energy(orc_t* o, const double* x_prev, const double* h, double a, double* xw, int* nevals,
+                        double* fw)
+{
+    size_t n = (size_t)o->natms * o->x_dim;
+    for (size_t i = 0; i < n; i++) xw[i] = x_prev[i] + a * h[i];
+    orc_update_x(o, xw, NULL);
+    (*nevals)++;
+    if (fw) {
+        double en[7];
+        orc_force(o, 0, fw, en);
+        return en[0];
+    }
+    return orc_energy(o);
+}
+
+/*
+ * Min_LBFGS::init tail and Min_LBFGS::run, fixed-box branch
+ * (min_l-bfgs.cpp:277-286, 616-773), with LineSearch_BackTrack::line_min, DMD
+ * branch (line_search.cpp:223-342; c = 0.4, rho = 0.5, alpha_max = 1,
+ * d_max = 1, line_search.cpp:203-208).  Same operation order as the
+ * reference: serial dot products, the two-loop recursion of
+ * min_l-bfgs.cpp:632-670, the history rotation of :716-728.
+ *
+ * Stopping: the reference's own codes (line-search failure, energy tolerance,
+ * max_iter), plus -- when fmax_tol > 0 -- ORC_MIN_F_TOLERANCE as soon as an
+ * accepted step leaves max|f| < fmax_tol.  max_halvings > 0 bounds the
+ * backtracking (the reference halves until alpha_m <= alpha_min, and its
+ * alpha_min stays 0, line_search.cpp:234-237, so only underflow ends it).
+ *
+ * ls_force_energy = 1 takes the line-search energies from the force pass
+ * instead of energy_calc.  For two-species DMD the reference's energy_calc
+ * sums only same-species phi (ff_dmd_I.cpp:508), so it is not the energy whose
+ * gradient the forces are and the reference's first line search cannot pass
+ * its Armijo test; the batched GPU form uses the force-pass energy, and this
+ * mode is its checker.
+ *
+ * e_hist (max_iter + 2 doubles, may be NULL) receives curr_energy after init
+ * and after every iteration.  Returns the number of line searches.
+ */
+int orc_lbfgs(orc_t* o, int m, int max_iter, double energy_tol, double fmax_tol, int max_halvings,
+              int ls_force_energy, double* e_hist, int* err_out, int* nevals_out)
+{
+    const int xd = o->x_dim, nt = o->nt;
+    const size_t n = (size_t)o->natms * xd;
+    double* f = calloc(n, sizeof(double));
+    double* h = calloc(n, sizeof(double));
+    double* x0 = calloc(n, sizeof(double));
+    double* f0 = calloc(n, sizeof(double));
+    double* xw = calloc(n, sizeof(double));
+    double* fw = ls_force_energy ? calloc(n, sizeof(double)) : NULL;
+    double* sv = calloc((size_t)(m > 0 ? m : 1) * n, sizeof(double));
+    double* yv = calloc((size_t)(m > 0 ? m : 1) * n, sizeof(double));
+    int* s_list = calloc(m > 0 ? m : 1, sizeof(int));
+    double* rho = calloc(m > 0 ? m : 1, sizeof(double));
+    double* alpha = calloc(m > 0 ? m : 1, sizeof(double));
+    for (int i = 0; i < m; i++) s_list[i] = i;
+    int nevals = 0, nls = 0;
+    double en[7];
+    /* init: f = 0; force_calc(1, energy_stress); curr_energy = energy_stress[0] */
+    orc_force(o, 1, f, en);
+    nevals++;
+    double curr_energy = en[0];
+    if (e_hist) e_hist[0] = curr_energy;
+    double ratio = 1.0, ls_alpha_min = 0.0;
+    int k_it = 0, istp = 0, err = ORC_LS_S;
+    while (err == ORC_LS_S) {
+        for (int i = 0; i < o->natms; i++)
+            for (int k = 0; k < xd; k++) x0[(size_t)i * xd + k] = o->x[(size_t)i * xd + k];
+        memcpy(h, f, n * sizeof(double));
+        memcpy(f0, f, n * sizeof(double));
+        double inner, tot_inner;
+        for (int i = k_it - 1; i > -1; i--) {
+            const double* s = sv + (size_t)s_list[i] * n;
+            const double* y = yv + (size_t)s_list[i] * n;
+            inner = 0.0;
+            for (size_t j = 0; j < n; j++) inner += h[j] * s[j];
+            alpha[i] = inner;
+            alpha[i] *= rho[i];
+            for (size_t j = 0; j < n; j++) h[j] -= alpha[i] * y[j];
+        }
+        for (size_t j = 0; j < n; j++) h[j] *= ratio;
+        for (int i = 0; i < k_it; i++) {
+            const double* s = sv + (size_t)s_list[i] * n;
+            const double* y = yv + (size_t)s_list[i] * n;
+            inner = 0.0;
+            for (size_t j = 0; j < n; j++) inner += h[j] * y[j];
+            tot_inner = inner;
+            tot_inner *= rho[i];
+            for (size_t j = 0; j < n; j++) h[j] -= (tot_inner + alpha[i]) * s[j];
+        }
+        double prev_energy = curr_energy;
+        /* line_min(curr_energy, alpha_m) */
+        double alpha_m = 0.0;
+        {
+            double min_h = INFINITY;
+            for (int i = 0; i < o->natms; i++)
+                for (int j = 0; j < nt; j++) min_h = MINV(min_h, o->x[(size_t)i * (3 + nt) + 3 + j]);
+            min_h *= 0.99;
+            ls_alpha_min = MINV(ls_alpha_min, min_h);
+            double hh = 0.0;
+            for (size_t j = 0; j < n; j++) hh += h[j] * h[j];
+            hh = 1.0 / sqrt(hh);
+            for (size_t j = 0; j < n; j++) h[j] *= hh;
+            double fh = 0.0;
+            for (size_t j = 0; j < n; j++) fh += f[j] * h[j];
+            nls++;
+            if (fh <= 0) err = ORC_LS_F_DOWNHILL;
+            double max_h = 0.0;
+            if (err == ORC_LS_S) {
+                for (size_t j = 0; j < n; j++) max_h = MAXV(max_h, fabs(h[j]));
+                if (max_h == 0) err = ORC_LS_F_GRAD0;
+            }
+            double a = 0.0;
+            if (err == ORC_LS_S) {
+                a = MINV(1.0, max_h);
+                if (a <= ls_alpha_min) err = ORC_LS_F_ALPHAMIN;
+            }
+            int halvings = 0;
+            while (err == ORC_LS_S) {
+                double ideal_energy = curr_energy - a * 0.4 * fh;
+                double cur = ls_energy(o, x0, h, a, xw, &nevals, fw);
+                if (cur <= ideal_energy) {
+                    curr_energy = cur;
+                    alpha_m = a;
+                    break;
+                }
+                a *= 0.5;
+                halvings++;
+                if (a <= ls_alpha_min || (max_halvings > 0 && halvings >= max_halvings)) {
+                    curr_energy = ls_energy(o, x0, h, 0.0, xw, &nevals, fw);
+                    err = ORC_LS_F_ALPHAMIN;
+                }
+            }
+        }
+        if (err == ORC_LS_S && prev_energy - curr_energy < energy_tol) err = ORC_MIN_F_TOLERANCE;
+        if (err == ORC_LS_S && istp == max_iter) err = ORC_MIN_F_MAX_ITER;
+        orc_force(o, 1, f, en);
+        nevals++;
+        curr_energy = en[0];
+        if (e_hist) e_hist[istp + 1] = curr_energy;
+        if (err == ORC_LS_S && fmax_tol > 0.0) {
+            double fm = 0.0;
+            for (size_t j = 0; j < n; j++) fm = MAXV(fm, fabs(f[j]));
+            if (fm < fmax_tol) err = ORC_MIN_F_TOLERANCE;
+        }
+        if (err) break;
+        if (m) {
+            if (k_it == m) {
+                int tmp = s_list[0];
+                for (int i = 0; i < m - 1; i++) {
+                    s_list[i] = s_list[i + 1];
+                    rho[i] = rho[i + 1];
+                }
+                s_list[m - 1] = tmp;
+            } else
+                k_it++;
+            double* s = sv + (size_t)s_list[k_it - 1] * n;
+            double* y = yv + (size_t)s_list[k_it - 1] * n;
+            inner = 0.0;
+            double inner_tmp = 0.0;
+            for (size_t i = 0; i < n; i++) {
+                s[i] = alpha_m * h[i];
+                y[i] = f[i] - f0[i];
+                inner += s[i] * y[i];
+                inner_tmp += y[i] * y[i];
+            }
+            ratio = -inner / inner_tmp;
+            rho[k_it - 1] = 1.0 / inner;
+        } else {
+            inner = 0.0;
+            double inner_tmp = 0.0;
+            for (size_t i = 0; i < n; i++) {
+                inner += (alpha_m * h[i]) * (f[i] - f0[i]);
+                inner_tmp += (f[i] - f0[i]) * (f[i] - f0[i]);
+            }
+            ratio = -inner / inner_tmp;
+        }
+        istp++;
+    }
+    if (err_out) *err_out = err;
+    if (nevals_out) *nevals_out = nevals;
+    free(f); free(h); free(x0); free(f0); free(xw); free(fw); free(sv); free(yv); free(s_list); free(rho); free(alpha);
+    return nls;
+}

@@ -13,6 +13,8 @@
  *   setx    = LineSearch::energy (line_search.cpp:180-195): write x, then
  *             atoms->update_0(0,1,..) (skin check, ghost refresh or rebuild)
  *   force / energy / crd / cdot / calcg call the ForceField virtuals.
+ *   lbfgs   = Min_LBFGS (min_l-bfgs.cpp) constructed, init, run, fin, with
+ *             the energy of every force_calc logged by the oracle subclass.
  *
  * Two harness-side measures (no change to reference arithmetic):
  *   - OracleDMD<Base>::coef restates ff_dmd_I.cpp:735-796 but routes "FS" to
@@ -47,6 +49,7 @@
 #include "ff_dmd_I.h"
 #include "ff_dmd_II.h"
 #include "ff_dmd.h"
+#include "min_l-bfgs.h"
 
 using namespace MAPP_NS;
 
@@ -108,10 +111,27 @@ public:
             memset(this->dphi_dalpha, 0, n1 * sizeof(double));
         }
         Base::force_calc(st_clc, en_st);
+        if (force_log) force_log->push_back(en_st[0]);
     }
+
+    double energy_calc() override
+    {
+        n_energy++;
+        return Base::energy_calc();
+    }
+
+    std::vector<double>* force_log = nullptr;  // en_st[0] of every force_calc while set
+    long n_energy = 0;
 
 private:
     bool route_fs_;
+};
+
+/* the reference minimiser with its protected result fields exposed */
+struct LbfgsRun : public Min_LBFGS {
+    LbfgsRun(MAPP* m, int narg, char** arg) : Min_LBFGS(m, narg, arg) {}
+    int code() const { return err; }
+    double energy() const { return curr_energy; }
 };
 
 struct Harness {
@@ -189,6 +209,56 @@ void do_oracle_ff(const std::string& style)
     else { fprintf(stderr, "harness: unknown oracle style %s\n", style.c_str()); exit(2); }
     if (H.mapp->forcefield) delete H.mapp->forcefield;
     H.mapp->forcefield = ff;
+}
+
+/* logging hooks of whichever OracleDMD<Base> is installed */
+template <class Base>
+bool set_log(ForceField* ff, std::vector<double>* log, long* n_energy_out)
+{
+    OracleDMD<Base>* o = dynamic_cast<OracleDMD<Base>*>(ff);
+    if (!o) return false;
+    if (n_energy_out) *n_energy_out = o->n_energy;
+    o->force_log = log;
+    if (log) o->n_energy = 0;
+    return true;
+}
+
+bool ff_log(std::vector<double>* log, long* n_energy_out)
+{
+    ForceField* ff = H.mapp->forcefield;
+    return set_log<ForceField_DMD_I>(ff, log, n_energy_out) || set_log<ForceField_DMD>(ff, log, n_energy_out) ||
+           set_log<ForceField_DMD_II>(ff, log, n_energy_out);
+}
+
+/* Min_LBFGS (min_l-bfgs.cpp) run on the scripted system: init, run, fin.
+   Writes the final owned x, the energy of every force_calc (init first, then
+   one per iteration) and the result code. */
+void do_lbfgs(int m, int max_iter, double etol, const std::string& prefix)
+{
+    char buf[64];
+    snprintf(buf, sizeof(buf), "%.17g", etol);
+    std::vector<std::string> a = {"min", "l-bfgs", "m", std::to_string(m), "max_iteration", std::to_string(max_iter),
+                                  "energy_tol", buf};
+    std::vector<char*> argv;
+    for (auto& t : a) argv.push_back(strdup(t.c_str()));
+    std::vector<double> log;
+    if (!ff_log(&log, nullptr)) { fprintf(stderr, "harness: lbfgs needs an oracle DMD force field\n"); exit(2); }
+    LbfgsRun* mn = new LbfgsRun(H.mapp, (int)argv.size(), argv.data());
+    mn->init();
+    mn->run();
+    long n_energy = 0;
+    ff_log(nullptr, &n_energy);
+    Atoms* atoms = H.mapp->atoms;
+    double* x = vec<double>("x");
+    write_raw(prefix + ".x.bin", x, sizeof(double) * (size_t)atoms->natms * H.x_dim);
+    write_raw(prefix + ".ehist.bin", log.data(), sizeof(double) * log.size());
+    meta(prefix, "code %d", mn->code());
+    meta(prefix, "energy %.17g", mn->energy());
+    meta(prefix, "n_force %d", (int)log.size());
+    meta(prefix, "n_energy %ld", n_energy);
+    mn->fin();
+    delete mn;
+    for (char* t : argv) free(t);
 }
 
 void do_ffcoef(const std::string& rest)
@@ -375,6 +445,7 @@ void run_command(const std::string& line)
     else if (cmd == "calcg") { int chk; double a; std::string ap, p; rs >> chk >> a >> ap >> p; do_calcg(chk, a, ap, p); }
     else if (cmd == "setx") { std::string xp, p; rs >> xp >> p; do_setx(xp, p); }
     else if (cmd == "setc") { std::string cp; rs >> cp; do_setc(cp); }
+    else if (cmd == "lbfgs") { int m, k; double tol; std::string p; rs >> m >> k >> tol >> p; do_lbfgs(m, k, tol, p); }
     else if (cmd == "time") { std::string w, p; int n; rs >> w >> n >> p; do_time(w, n, p); }
     else { fprintf(stderr, "harness: unknown command %s\n", cmd.c_str()); exit(2); }
 }

@@ -43,7 +43,7 @@ def _meta(path):
 class RefRun:
     """Builds a command file, runs the harness once and loads every output."""
 
-    def __init__(self, workload: dict, workdir: str | None = None):
+    def __init__(self, workload: dict, workdir: str | None = None, init: bool = True):
         self.w = workload
         self.dir = workdir or tempfile.mkdtemp(prefix="mapp_ref_")
         self.lines = [f"script {workload['script']}"]
@@ -53,7 +53,8 @@ class RefRun:
         else:
             self.lines.append(f"ffcoef_style {style}")
         self.lines.append("ffcoef " + " ".join(workload["coef"]))
-        self.lines.append("init")
+        if init:  # Min_LBFGS::init does its own set-up (lbfgs runs pass init=False)
+            self.lines.append("init")
         self.steps = []
 
     def _p(self, tag):
@@ -99,6 +100,11 @@ class RefRun:
         cp = self._p(tag + ".c_in.bin")
         np.ascontiguousarray(c, dtype=np.float64).tofile(cp)
         return self.add(f"setc {cp}")
+
+    def lbfgs(self, m: int, max_iter: int, energy_tol: float, tag="lb"):
+        """The reference Min_LBFGS: init, run, fin (construct with init=False)."""
+        self.steps.append(("lbfgs", tag))
+        return self.add(f"lbfgs {m} {max_iter} {energy_tol!r} {self._p(tag)}")
 
     def time(self, what: str, reps: int, tag="t"):
         self.steps.append(("time", tag))

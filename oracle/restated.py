@@ -68,6 +68,9 @@ def lib():
         L.orc_get_dmd_consts.argtypes = [P, dp]
         L.orc_spline7.argtypes = [C.c_int, C.c_double, dp]
         L.orc_spline9.argtypes = [C.c_int, C.c_double, dp]
+        L.orc_lbfgs.argtypes = [P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, dp,
+                                C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.orc_lbfgs.restype = C.c_int
         _lib = L
     return _lib
 
@@ -254,3 +257,16 @@ class Oracle:
         out = np.zeros(3 * n0 + 3 * n1)
         lib().orc_get_pairs(self.h, out)
         return out
+
+    def lbfgs(self, m=5, max_iter=10000, energy_tol=1e-8, fmax_tol=0.0, max_halvings=0, ls_force_energy=False):
+        """Min_LBFGS run (orc_lbfgs): returns dict(code, line_searches, evals,
+        energies = force_calc energy after init and after every iteration, x).
+        ls_force_energy: line-search energies from the force pass (the batched
+        form's rule) instead of energy_calc (the reference's)."""
+        e = np.zeros(max_iter + 2)
+        err = C.c_int(0)
+        nev = C.c_int(0)
+        nls = lib().orc_lbfgs(self.h, m, max_iter, energy_tol, fmax_tol, max_halvings, int(ls_force_energy), e,
+                              C.byref(err), C.byref(nev))
+        x = self.x_all()[: self.counts()["natms"]]
+        return {"code": err.value, "line_searches": nls, "evals": nev.value, "energies": e[: nls + 1], "x": x}
