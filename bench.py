@@ -47,7 +47,9 @@ def parse():
     p.add_argument("--cells", type=int, default=WORKLOAD["n"], help="FCC cells per edge (default 20 -> 32000 sites)")
     p.add_argument("--cpu-reps", type=int, default=0, help="reference force_calc calls per CPU process (0: auto)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU reference timing")
-    p.add_argument("--skip-forms", action="store_true", help="skip the FP32 and learned forms (profiling runs)")
+    p.add_argument("--skip-forms", action="store_true", help="skip the FP32, learned and batched forms (profiling runs)")
+    p.add_argument("--form", default="fp64", choices=["fp64", "fp32", "mlp"],
+                   help="form of the timed force_calc steps (fp32 / mlp imply --skip-forms; for profiling)")
     return p.parse_args()
 
 
@@ -210,14 +212,21 @@ def measured_peaks():
 # our arm
 # ---------------------------------------------------------------------------
 def pass1_flops_per_pair(nt, nq):
-    """Algorithmic FP64 operations of one half pair inside the smeared cut in
-    the force pass 1 (sqrt, division and reciprocal counted as one):
-    10 for the pair geometry, then per species pair 9 for alpha / sqrt /
-    bracket, 21 per quadrature node for the density (node offset, table index,
-    cubic, three weighted sums) and 9 to finish value and both derivatives;
-    per unordered species pair 13 per node and 9 more for phi."""
-    nc = nt * (nt + 1) // 2
-    return 10 + nt * nt * (9 + 21 * nq + 9) + nc * (13 * nq + 9)
+    """Algorithmic FP64 work of force pass 1 per half pair inside the smeared
+    cut, as counted for this workload's measurement: per ordered species pair
+    about 10 flops of geometry and alpha combination plus about 22 per
+    quadrature node (node offset, table index, two cubic evaluations, weighted
+    sums), sqrt and division counted as one: nt^2 (10 + 22 nq), 304 for the
+    binary n = 3 system."""
+    return nt * nt * (10 + 22 * nq)
+
+
+# Algorithmic bytes of force pass 1 per owned site: its share of the minimum
+# traffic of one force evaluation (read x and alpha 40 B and c 16 B, write the
+# densities E 16 B; the whole evaluation also writes f 40 B and dE 16 B, about
+# 130 B per site).  Everything else pass 1 moves (the per-pair scratch, gathers
+# of neighbour sites) is this implementation's traffic, seen in `traffic`.
+PASS1_ALG_BYTES_PER_SITE = 72
 
 
 def run_forms(args, s, mb, natms, f_dev, flush, t_dev):
@@ -369,6 +378,13 @@ def run_ours(args):
     mod_rc = 5.0 + 1.224744871391589 / np.sqrt(20.0)
     in_cut = int(np.count_nonzero(rsq < mod_rc * mod_rc))
 
+    form_id = {"fp64": mb.MG_FORM_FP64, "fp32": mb.MG_FORM_FP32, "mlp": mb.MG_FORM_MLP}[args.form]
+    if args.form != "fp64":
+        args.skip_forms = True
+    if args.form == "mlp":
+        s.mlp_init(1.8, 5.0, 0.05, 0.20, seed=5)
+        s.mlp_train(nsamples=2_000_000, steps=20_000, batch=4096, lr=1e-3, seed=11)
+    s.set_form(form_id)
     for _ in range(args.warmup):
         s.force_calc(1, f=f_dev)
     torch.cuda.synchronize()
@@ -396,7 +412,7 @@ def run_ours(args):
     forms = {} if args.skip_forms else run_forms(args, s, mb, natms, f_dev, flush, t_dev)
     if not args.skip_forms:
         forms["batched"] = run_batched(mb, fx, local)
-    s.set_form(mb.MG_FORM_FP64)
+    s.set_form(form_id)
 
     # end to end through the C ABI with host buffers
     x_host = torch.from_numpy(xo.copy()).pin_memory()
@@ -440,34 +456,38 @@ def run_ours(args):
     peaks, peak_kind = measured_peaks()
     p1_ms = t_p1 / args.steps
     flops = pass1_flops_per_pair(nt, 3) * in_cut
-    # algorithmic DRAM bytes of pass 1: list (4 B) and 21 FP64 per-pair results
-    # written per listed pair, plus site arrays read once (pos 32 B, alpha and c
-    # 8 B per species, owned + ghost) and E written (8 B per species)
-    nall = natms + cnt["nph"]
-    bytes_p1 = cnt["npairs"] * (4 + 8 * (3 * nt * nt + 3 * nt * (nt + 1) // 2)) + nall * (32 + 16 * nt) + natms * 8 * nt
+    bytes_p1 = PASS1_ALG_BYTES_PER_SITE * natms
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved_gbs = bytes_p1 / (p1_ms * 1e-3) / 1e9
+    # DRAM bytes (read + write) of one k_dmd_pass1 launch from the committed ncu
+    # capture, per owned site, scaled to this system
     traffic = None
     tf = os.path.join(ROOT, "profiles", "dmd_pass1_traffic.json")
-    if os.path.exists(tf):
+    if os.path.exists(tf) and args.form == "fp64":
         try:
-            t = json.load(open(tf))
-            traffic = t["bytes_per_site"] * natms
+            with open(tf) as fp:
+                traffic = json.load(fp)["bytes_per_site"] * natms
         except (OSError, KeyError, ValueError):
             traffic = None
     clocks = clk.summary()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_dev / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded lattice, alpha and c; random tables of the named potentials)",
-        "form": "plain FP64",
+        "dtype": {"fp64": "f64", "fp32": "f32", "mlp": "bf16"}[args.form],
+        "data": "synthetic (seeded lattice, alpha and c; random tables of the named potentials)",
+        "form": {"fp64": "plain FP64", "fp32": "precision (FP32)", "mlp": "learned (BF16 MLP)"}[args.form],
         "config": workload_config(args, {"pairs": cnt["npairs"], "pairs_in_smeared_cut": in_cut, "ghosts": cnt["nph"]}),
-        "roofline": {"bound": "hbm", "kernel": "k_dmd_pass1", "achieved": achieved_gbs, "peak": hbm,
+        "roofline": {"bound": "hbm", "kernel": "k_dmd_pass1" if args.form == "fp64" else
+                     {"fp32": "k_dmd32_pass1", "mlp": "k_dmd_pass1_mlp"}[args.form],
+                     "achieved": achieved_gbs, "peak": hbm,
                      "unit": "GB/s", "frac": achieved_gbs / hbm, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": bytes_p1, "launch_ms": p1_ms,
+                     "algorithmic_bytes_per_launch": bytes_p1,
+                     "algorithmic_bytes_rule": f"{PASS1_ALG_BYTES_PER_SITE} B per owned site (x, alpha, c read; E written)",
+                     "launch_ms": p1_ms,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "fp64_tflops_achieved": flops / (p1_ms * 1e-3) / 1e12,
-                     "fp64_flops_per_launch": flops},
+                     "fp64_flops_per_launch": flops,
+                     "fp64_flops_rule": "nt^2 (10 + 22 nq) per half pair inside the smeared cut",
+                     "fp64_tflops_achieved": flops / (p1_ms * 1e-3) / 1e12},
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": natms * (s.x_dim + nt) * 8, "d2h_bytes_per_step": natms * s.x_dim * 8 + 56,
                 "steps": e2e_steps, "path": "mg_atoms_update_x + mg_atoms_update_c + mg_ff_force_calc, pinned host buffers"},
