@@ -200,6 +200,23 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def job_max(value, device="cpu"):
+    """Max over the ranks of a per-rank time; the value itself on one rank."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, steps, t_max_s, world):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return world * units_per_rank * steps / t_max_s
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fp:
@@ -402,40 +419,39 @@ def run_ours(args):
             t_p1 += s.last_time("force.pass1")
         torch.cuda.synchronize()
         wall = time.perf_counter() - wall0
+    t_dev = job_max(t_dev, "cuda")
     if ws > 1:
-        tt = torch.tensor([t_dev], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         dist.barrier()
-        t_dev = float(tt.item())
-    value = ws * natms * args.steps / (t_dev * 1e-3)
+    value = job_rate(natms, args.steps, t_dev * 1e-3, ws)
 
     forms = {} if args.skip_forms else run_forms(args, s, mb, natms, f_dev, flush, t_dev)
     if not args.skip_forms:
         forms["batched"] = run_batched(mb, fx, local)
     s.set_form(form_id)
 
-    # end to end through the C ABI with host buffers
+    # end to end through the C ABI with host buffers, timed with CUDA events on
+    # the stream the library runs on (host gaps between the calls included)
     x_host = torch.from_numpy(xo.copy()).pin_memory()
     c_host = torch.from_numpy(np.ascontiguousarray(w["cfg"].c)).pin_memory()
     f_host = torch.zeros((natms, s.x_dim), dtype=torch.float64).pin_memory()
+    e2e_stream = torch.cuda.Stream()
+    s.set_stream(e2e_stream.cuda_stream)
     for _ in range(2):
         s.update_x(x_host)
         s.update_c(c_host)
         s.force_calc(1, f=f_host)
     torch.cuda.synchronize()
     e2e_steps = max(10, args.steps // 4)
-    t0 = time.perf_counter()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(e2e_stream)
     for _ in range(e2e_steps):
         s.update_x(x_host)
         s.update_c(c_host)
         s.force_calc(1, f=f_host)
+    ev1.record(e2e_stream)
     torch.cuda.synchronize()
-    t_e2e = time.perf_counter() - t0
-    if ws > 1:
-        tt = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e_value = ws * natms * e2e_steps / t_e2e
+    t_e2e = job_max(ev0.elapsed_time(ev1) * 1e-3, "cuda")
+    e2e_value = job_rate(natms, e2e_steps, t_e2e, ws)
 
     # side measurements (list build, energy_calc, c_d_calc, calc_g)
     s.rebuild_list()
