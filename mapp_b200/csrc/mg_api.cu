@@ -3,6 +3,7 @@
 // entry points.  Numbers that decide list membership (B, cut_ph_s, cut_sk_sq,
 // table coefficients) are computed here in plain IEEE double in the
 // reference's operation order, so they equal the reference's bit for bit.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -242,6 +243,7 @@ struct mg_system {
     double t_k[3] = {0, 0, 0};  // DMD force: pass 1, embedding, pass 2
     long long partial_rows = 0;
     bool tables_uploaded = false;  // device tables match the last ff_coef
+    size_t owned_cap = 0, nbr_cap = 0, crdl_cap = 0;  // element capacities of the per-owned-site, ELL and crd buffers
 };
 
 namespace {
@@ -326,12 +328,14 @@ int ensure_pairs(mg_system* s, int maxnb)
 {
     Dev& d = s->d;
     size_t np = (size_t)s->natms * maxnb;
-    CHK(dalloc(&d.nbr, np));
-    d.maxnb = maxnb;
-    if (!s->dmd) {
-        CHK(dalloc(&d.pr, np * s->npair_blocks));
-        d.maxp = (long long)np;
+    if (np > s->nbr_cap) {
+        size_t cap = np + np / 4 + 1024;
+        CHK(dalloc(&d.nbr, cap));
+        if (!s->dmd) CHK(dalloc(&d.pr, cap * s->npair_blocks));
+        s->nbr_cap = cap;
     }
+    d.maxnb = maxnb;
+    if (!s->dmd) d.maxp = (long long)np;
     return MG_OK;
 }
 
@@ -877,22 +881,30 @@ int mg_atoms_set(mg_system* s, int natms, const double* x, const int* type, cons
     s->natms = natms;
     Dev& d = s->d;
     fill_dev_scalars(s);
+    // Buffers keep their capacity from one call to the next, so a system that
+    // is loaded with many configurations of different sizes (the batched form's
+    // builder) allocates for the largest once.
     size_t cap0 = (size_t)natms * 4 + 1024;
-    s->cap = 0;
     CHK(ensure_atoms(s, cap0, 0));
-    CHK(dalloc(&d.pos0, natms));
-    CHK(dalloc(&d.nnb, (size_t)natms + 1));
-    CHK(dalloc(&d.poff, (size_t)natms + 1));
-    s->pair_cap = 0;
-    CHK(dalloc(&d.ncrd, natms));
-    CHK(dalloc(&d.f, (size_t)natms * s->x_dim));
-    CHK(dalloc(&d.c_d, (size_t)natms * s->nt));
-    CHK(dalloc(&d.a_in, (size_t)natms * s->nt));
-    CHK(dalloc(&d.g, (size_t)natms * s->nt));
+    if ((size_t)natms + 1 > s->owned_cap) {
+        size_t oc = (size_t)natms + natms / 4 + 64;
+        CHK(dalloc(&d.pos0, oc));
+        CHK(dalloc(&d.nnb, oc + 1));
+        CHK(dalloc(&d.poff, oc + 1));
+        CHK(dalloc(&d.ncrd, oc));
+        CHK(dalloc(&d.f, oc * s->x_dim));
+        CHK(dalloc(&d.c_d, oc * s->nt));
+        CHK(dalloc(&d.a_in, oc * s->nt));
+        CHK(dalloc(&d.g, oc * s->nt));
+        s->owned_cap = oc;
+    }
     s->npair_blocks = s->dmd ? 3 * s->nt * s->nt + 3 * (s->nt * (s->nt + 1) / 2) : 2;
-    CHK(ensure_pairs(s, s->dmd ? 96 : 64));
-    d.maxcrd = 32;
-    CHK(dalloc(&d.crdl, (size_t)natms * d.maxcrd));
+    CHK(ensure_pairs(s, std::max(d.maxnb, s->dmd ? 96 : 64)));
+    d.maxcrd = std::max(d.maxcrd, 32);
+    if ((size_t)natms * d.maxcrd > s->crdl_cap) {
+        s->crdl_cap = (size_t)natms * d.maxcrd + 1024;
+        CHK(dalloc(&d.crdl, s->crdl_cap));
+    }
     if (natms) {
         const void* dx = nullptr;
         CHK(stage_in(s, x, (size_t)natms * s->x_dim * sizeof(double), &dx));
@@ -1153,7 +1165,10 @@ int mg_ff_create_2nd_neigh_lst(mg_system* s)
         CU(cudaStreamSynchronize(s->st));
         if (!st_h[2]) break;
         d.maxcrd = st_h[3] + 8;
-        CHK(dalloc(&d.crdl, (size_t)s->natms * d.maxcrd));
+        if ((size_t)s->natms * d.maxcrd > s->crdl_cap) {
+            s->crdl_cap = (size_t)s->natms * d.maxcrd + 1024;
+            CHK(dalloc(&d.crdl, s->crdl_cap));
+        }
         if (attempt == 3) return fail(MG_ERR_CAPACITY, "coordination list capacity could not be met");
     }
     s->crd_built = 1;
