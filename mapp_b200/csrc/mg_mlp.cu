@@ -12,7 +12,8 @@
 //     gradients written as per-CTA partials;
 //   * k_mlp_adam    -- sums the partials, Adam with a cosine learning rate,
 //     refreshes the BF16 weight copy;
-//   * k_dmd_pass1_mlp -- force pass 1 with the MLP, quadrature fallback
+//   * k_dmd_pass1_mlp -- force pass 1 with the MLP (only on rows inside the
+//     training box, gathered per warp), quadrature fallback
 //     outside the training box and a 1% audit of MLP pairs against the
 //     quadrature.
 // Species pairs: code 0 = (0,0), 1 = the unordered cross pair, 2 = (1,1); the
@@ -373,9 +374,13 @@ struct MlpFrag {
     float b1[H], b2[H], b3[H], b4[8];
 };
 
+// per-warp queue of rows that go through the network
+constexpr int kQueue = 64;
 struct MlpWarpBuf {
-    float xin[32][4];  // normalised inputs of the warp's rows
-    float y[32][8];    // network outputs (standardised)
+    float xin[kQueue][4];  // normalised inputs of the queued rows
+    float y[32][8];        // network outputs (standardised) of the first 32
+    int pair[kQueue];      // compact pair index of each queued row
+    unsigned char ab[kQueue];  // a * 2 + b
 };
 
 // B fragment of W (row-major [K][N] BF16 at w) for k-chunk kc, n-tile nt, lane
@@ -441,11 +446,12 @@ __device__ __forceinline__ void act64(const float (&c)[8][4], uint32_t (&a)[4][4
     }
 }
 
-// the network on the warp's 32 rows (B.xin -> B.y)
+// the network on rows 0..31 of the queue (B.xin -> B.y), one 16-row m-tile
+// at a time (one unrolled tile keeps the body inside the instruction cache)
 __device__ __forceinline__ void warp_mlp(const MlpFrag& F, MlpWarpBuf& B, int lane)
 {
     const int g = lane >> 2, t = lane & 3;
-#pragma unroll
+#pragma unroll 1
     for (int mt = 0; mt < 2; mt++) {
         const int r0 = mt * 16 + g, r1 = r0 + 8;
         uint32_t ax[4] = {0u, 0u, 0u, 0u};
@@ -481,13 +487,67 @@ __device__ __forceinline__ void warp_mlp(const MlpFrag& F, MlpWarpBuf& B, int la
     }
 }
 
+// the six outputs of one row into the pair scratch (precision form layout)
 template <int NT>
-__global__ void __launch_bounds__(kInfThreads, 2) k_dmd_pass1_mlp(Dev d, MlpState S, unsigned long long audit_seed,
-                                                                 int row0)
+__device__ __forceinline__ void store_row(const Dev& d, long long p, int a, int b, const float (&o)[6])
 {
     using SL = Slots<NT>;
-    constexpr int RP = NT * NT;     // rows per pair
-    constexpr int PPW = 32 / RP;    // pairs per warp step
+    const size_t mp = (size_t)d.maxp;
+    float* out = d.prf + p;
+    const int rs = b * NT + a, ps = comp_idx(a, b);
+    out[(SL::RHO + rs) * mp] = o[1];
+    out[(SL::DRR + rs) * mp] = o[3];
+    out[(SL::DRA + rs) * mp] = o[5];
+    if (a >= b) {
+        out[(SL::PHI + ps) * mp] = o[0];
+        out[(SL::DPR + ps) * mp] = o[2];
+        out[(SL::DPA + ps) * mp] = o[4];
+    }
+}
+
+// Geometry of row (pair p, species a, b): in-cut test, r, pair exponent.
+struct RowGeo {
+    int mode;  // 0 beyond the smeared cut, 1 network, 2 quadrature
+    float r, alpha;
+    bool below_rc;
+};
+
+template <int NT>
+__device__ __forceinline__ RowGeo row_geo(const Dev& d, const MlpState& S, const F32Consts& kc, long long p, int a,
+                                          int b, float (&in)[4])
+{
+    RowGeo g{0, 1.f, 0.f, false};
+    const int i = d.pair_i[p], j = d.pair_j[p];
+    const double4 xi = d.pos[i], xj = d.pos[j];
+    const double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
+    const double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
+    if (!(rsq < d.cut_sq_mod)) return g;
+    const float ai = (float)d.alpha[(size_t)i * NT + a], aj = (float)d.alpha[(size_t)j * NT + b];
+    g.alpha = (ai * aj) / (ai + aj);
+    g.r = sqrtf((float)rsq);
+    g.below_rc = rsq < d.cut_sq;
+    const float wi = rsqrtf(ai), wj = rsqrtf(aj);
+    const int code = NT == 1 ? 0 : (a == b ? 2 * a : 1);
+    const bool inbox = g.r >= S.box.r_lo && g.r <= S.box.r_hi && wi >= S.box.w_lo && wi <= S.box.w_hi &&
+                       wj >= S.box.w_lo && wj <= S.box.w_hi && g.alpha > kc.alpha_min && g.alpha < kc.alpha_max;
+    g.mode = inbox ? 1 : 2;
+    if (inbox) net_inputs(S.box, g.r, wi, wj, code, in);
+    return g;
+}
+
+// Force pass 1 of the learned form: the six smeared quantities of every row
+// into the pair scratch.  A warp walks its rows 32 at a time (32 / NT^2 pairs);
+// rows beyond the smeared cut write zeros, rows outside the training box take
+// the FP32 quadrature at once, and rows inside it join the warp's queue, which
+// runs through the network whenever it holds 32 rows, so the network never
+// evaluates a row it does not use.  A hashed 1% of network rows is re-evaluated
+// by the FP64 quadrature (audit).  Densities and pair energy follow in
+// k_mlp_densities.
+template <int NT>
+__global__ void __launch_bounds__(kInfThreads, 2) k_dmd_pass1_mlp(Dev d, MlpState S, unsigned long long audit_seed)
+{
+    constexpr int RP = NT * NT;   // rows per pair
+    constexpr int PPW = 32 / RP;  // pairs per warp step
     __shared__ MlpFrag F;
     __shared__ MlpWarpBuf WB[kInfWarps];
     build_frags(F, S.wbf, S.par);
@@ -495,117 +555,112 @@ __global__ void __launch_bounds__(kInfThreads, 2) k_dmd_pass1_mlp(Dev d, MlpStat
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     MlpWarpBuf& B = WB[warp];
     const F32Consts kc = f32_consts(d);
-    const size_t mp = (size_t)d.maxp;
-    const int a = (lane % RP) / NT, b = lane % NT;
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     unsigned long long n_audit = 0, n_fallback = 0;
     float audit_err[6] = {0, 0, 0, 0, 0, 0};
-    const long long ngroups = (d.npairs + PPW - 1) / PPW;
-    for (long long grp = (long long)blockIdx.x * kInfWarps + warp; grp < ngroups;
-         grp += (long long)gridDim.x * kInfWarps) {
-        const long long p = grp * PPW + lane / RP;
-        const bool valid = p < d.npairs;
-        int i = -1, j = 0, mode = 0;
-        float rf = 1.f, alpha = 0.f;
-        bool below_rc = false;
-        float in[4] = {0.f, 0.f, 0.f, 0.f};
-        if (valid) {
-            i = d.pair_i[p];
-            j = d.pair_j[p];
-            double4 xi = d.pos[i], xj = d.pos[j];
-            double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
-            double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
-            if (rsq < d.cut_sq_mod) {
-                float ai = (float)d.alpha[(size_t)i * NT + a], aj = (float)d.alpha[(size_t)j * NT + b];
-                alpha = (ai * aj) / (ai + aj);
-                float rsqf = (float)rsq;
-                rf = sqrtf(rsqf);
-                below_rc = rsq < d.cut_sq;
-                float wi = rsqrtf(ai), wj = rsqrtf(aj);
-                int code = NT == 1 ? 0 : (a == b ? 2 * a : 1);
-                bool inbox = rf >= S.box.r_lo && rf <= S.box.r_hi && wi >= S.box.w_lo && wi <= S.box.w_hi &&
-                             wj >= S.box.w_lo && wj <= S.box.w_hi && alpha > kc.alpha_min && alpha < kc.alpha_max;
-                mode = inbox ? 1 : 2;
-                if (inbox) net_inputs(S.box, rf, wi, wj, code, in);
-            }
-        }
-        B.xin[lane][0] = in[0];
-        B.xin[lane][1] = in[1];
-        B.xin[lane][2] = in[2];
-        B.xin[lane][3] = in[3];
+    int qn = 0;  // queued rows (warp-uniform)
+
+    // the network on queue rows 0..31; rows >= nvalid are stale and ignored
+    auto drain = [&](int nvalid) {
         __syncwarp();
         warp_mlp(F, B, lane);
         __syncwarp();
-        float o[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // phi, rho, dphi_dr, drho_dr, dphi_da, drho_da
-        if (mode == 1) {
+        if (lane < nvalid) {
+            const long long p = B.pair[lane];
+            const int a = B.ab[lane] >> 1, b = B.ab[lane] & 1;
+            float o[6];
 #pragma unroll
             for (int q = 0; q < 6; q++) o[q] = B.y[lane][q] * S.out_scale[q] + S.out_mean[q];
-            unsigned long long h = mix64(audit_seed ^ ((unsigned long long)p * RP + lane % RP));
+            store_row<NT>(d, p, a, b, o);
+            const unsigned long long h = mix64(audit_seed ^ ((unsigned long long)p * RP + a * NT + b));
             if ((h >> 40) % 100 == 0) {
+                float in[4];
+                const RowGeo g = row_geo<NT>(d, S, kc, p, a, b, in);
                 double g0, gdr, gda, f0 = 0, fdr = 0, fda = 0;
-                int aa = (a == b) ? a : 1, bb = (a == b) ? b : 0;  // the ordering the network was trained on
-                double rr = rf;
+                const int aa = (a == b) ? a : 1, bb = (a == b) ? b : 0;  // the ordering the network was trained on
+                const double rr = g.r;
                 bool hit = smear<true, true, 0>(d, bb * NT + aa, comp_idx(aa, bb), rr, 1.0 / rr, rr * rr,
-                                                (double)alpha, g0, gdr, gda, f0, fdr, fda);
+                                                (double)g.alpha, g0, gdr, gda, f0, fdr, fda);
                 if (!hit) g0 = gdr = gda = f0 = fdr = fda = 0.0;
                 const double qv[6] = {f0, g0, fdr, gdr, fda, gda};
 #pragma unroll
                 for (int q = 0; q < 6; q++) audit_err[q] = fmaxf(audit_err[q], fabsf((float)(qv[q] - o[q])));
                 n_audit++;
             }
-        } else if (mode == 2) {
-            const float4* pk = d.pkT + (size_t)(a * NT + b) * d.nr * 2;
-            float r_inv = 1.0f / rf;
-            float g0 = 0, gdr = 0, gda = 0, f0 = 0, fdr = 0, fda = 0;
-            bool hit = (a >= b) ? smear_f<true, 0>(d, kc, pk, rf, r_inv, below_rc, alpha, g0, gdr, gda, f0, fdr, fda)
-                                : smear_f<false, 0>(d, kc, pk, rf, r_inv, below_rc, alpha, g0, gdr, gda, f0, fdr, fda);
-            if (hit) {
-                o[0] = f0;
-                o[1] = g0;
-                o[2] = fdr;
-                o[3] = gdr;
-                o[4] = fda;
-                o[5] = gda;
+        }
+        __syncwarp();
+    };
+
+    const long long ngroups = (d.npairs + PPW - 1) / PPW;
+    for (long long grp = (long long)blockIdx.x * kInfWarps + warp; grp < ngroups;
+         grp += (long long)gridDim.x * kInfWarps) {
+        const long long p = grp * PPW + lane / RP;
+        const int a = (lane % RP) / NT, b = lane % NT;
+        float in[4] = {0.f, 0.f, 0.f, 0.f};
+        RowGeo g{0, 1.f, 0.f, false};
+        if (p < d.npairs) g = row_geo<NT>(d, S, kc, p, a, b, in);
+        // network rows join the queue
+        const unsigned net = __ballot_sync(0xffffffffu, p < d.npairs && g.mode == 1);
+        if (p < d.npairs && g.mode == 1) {
+            const int slot = qn + __popc(net & ((1u << lane) - 1u));
+            B.xin[slot][0] = in[0];
+            B.xin[slot][1] = in[1];
+            B.xin[slot][2] = in[2];
+            B.xin[slot][3] = in[3];
+            B.pair[slot] = (int)p;
+            B.ab[slot] = (unsigned char)(a * 2 + b);
+        }
+        qn += __popc(net);
+        // the others now: zeros beyond the cut, FP32 quadrature outside the box
+        if (p < d.npairs && g.mode != 1) {
+            float o[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (g.mode == 2) {
+                const float4* pk = d.pkT + (size_t)(a * NT + b) * d.nr * 2;
+                const float r_inv = 1.0f / g.r;
+                float g0 = 0, gdr = 0, gda = 0, f0 = 0, fdr = 0, fda = 0;
+                const bool hit =
+                    (a >= b) ? smear_f<true, 0>(d, kc, pk, g.r, r_inv, g.below_rc, g.alpha, g0, gdr, gda, f0, fdr, fda)
+                             : smear_f<false, 0>(d, kc, pk, g.r, r_inv, g.below_rc, g.alpha, g0, gdr, gda, f0, fdr, fda);
+                if (hit) {
+                    o[0] = f0;
+                    o[1] = g0;
+                    o[2] = fdr;
+                    o[3] = gdr;
+                    o[4] = fda;
+                    o[5] = gda;
+                }
+                n_fallback++;
             }
-            n_fallback++;
+            store_row<NT>(d, p, a, b, o);
         }
-        // pair scratch (precision form layout) and densities
-        float ei = 0.f, ej = 0.f;
-        if (valid) {
-            float* out = d.prf + p;
-            const int rs = b * NT + a, ps = comp_idx(a, b);
-            out[(SL::RHO + rs) * mp] = o[1];
-            out[(SL::DRR + rs) * mp] = o[3];
-            out[(SL::DRA + rs) * mp] = o[5];
-            double cia = d.c[(size_t)i * NT + a], cjb = d.c[(size_t)j * NT + b];
-            if (a >= b) {
-                out[(SL::PHI + ps) * mp] = o[0];
-                out[(SL::DPR + ps) * mp] = o[2];
-                out[(SL::DPA + ps) * mp] = o[4];
-                double cib = d.c[(size_t)i * NT + b], cja = d.c[(size_t)j * NT + a];
-                double w = j < d.natms ? 0.5 : 0.25;
-                acc[0] += w * (cjb * cia + cja * cib) * (double)o[0];
+        if (qn >= 32) {
+            drain(32);
+            // move the rows queued after the first 32 to the front
+            const int rest = qn - 32;
+            float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
+            int pr = 0;
+            unsigned char ab = 0;
+            if (lane < rest) {
+                x0 = B.xin[32 + lane][0];
+                x1 = B.xin[32 + lane][1];
+                x2 = B.xin[32 + lane][2];
+                x3 = B.xin[32 + lane][3];
+                pr = B.pair[32 + lane];
+                ab = B.ab[32 + lane];
             }
-            ei = o[1] * (float)cjb;  // into E[i][a]
-            ej = o[1] * (float)cia;  // into E[j][b]
+            __syncwarp();
+            if (lane < rest) {
+                B.xin[lane][0] = x0;
+                B.xin[lane][1] = x1;
+                B.xin[lane][2] = x2;
+                B.xin[lane][3] = x3;
+                B.pair[lane] = pr;
+                B.ab[lane] = ab;
+            }
+            __syncwarp();
+            qn = rest;
         }
-        // E[j][b]: sum over a inside the pair, one atomic per (pair, b)
-        if (NT == 2) ej += __shfl_xor_sync(0xffffffffu, ej, 2);
-        if (valid && a == 0 && j < d.natms && ej != 0.f) atomicAdd(&d.E[(size_t)j * NT + b], (double)ej);
-        // E[i][a]: sum over b inside the pair, then over the warp's pairs of the same i
-        if (NT == 2) ei += __shfl_xor_sync(0xffffffffu, ei, 1);
-        const bool lead = valid && b == 0;
-        const int key = lead ? i * NT + a : -1 - lane;
-        const unsigned mm = __match_any_sync(0xffffffffu, key);
-        const int last = 31 - __clz(mm);
-        float v = lead ? ei : 0.f;
-#pragma unroll
-        for (int off = RP; off < 32; off <<= 1) {  // leaders of one (i, a) are RP lanes apart
-            float v2 = __shfl_down_sync(0xffffffffu, v, off);
-            if (lane + off <= last) v += v2;
-        }
-        if (lead && lane == __ffs(mm) - 1 && v != 0.f) atomicAdd(&d.E[(size_t)i * NT + a], (double)v);
     }
+    if (qn > 0) drain(qn);
     // audit and fallback counters: one atomic per warp
 #pragma unroll
     for (int q = 0; q < 6; q++) {
@@ -620,6 +675,59 @@ __global__ void __launch_bounds__(kInfThreads, 2) k_dmd_pass1_mlp(Dev d, MlpStat
     if (lane == 0) {
         if (n_audit) atomicAdd(reinterpret_cast<unsigned long long*>(S.audit + 6), n_audit);
         if (n_fallback) atomicAdd(reinterpret_cast<unsigned long long*>(S.audit + 8), n_fallback);
+    }
+}
+
+// Densities E and pair energy from the pair scratch the learned pass wrote
+// (ff_dmd_I.cpp:196-259 sums): one thread per compact pair, i-side sums by
+// segmented shuffles, one FP64 atomic per site run and per owned j.
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock, 4) k_mlp_densities(Dev d, int row0)
+{
+    using SL = Slots<NT>;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const size_t mp = (size_t)d.maxp;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < d.npairs; base += stride) {
+        const long long p = base + lane;
+        const bool valid = p < d.npairs;
+        const int i = valid ? d.pair_i[p] : -1;
+        double Ei[NT];
+#pragma unroll
+        for (int a = 0; a < NT; a++) Ei[a] = 0.0;
+        if (valid) {
+            const int j = d.pair_j[p];
+            const bool own_j = j < d.natms;
+            const double w = own_j ? 0.5 : 0.25;
+            double ci[NT], cj[NT], Ej[NT];
+#pragma unroll
+            for (int a = 0; a < NT; a++) {
+                ci[a] = d.c[(size_t)i * NT + a];
+                cj[a] = d.c[(size_t)j * NT + a];
+                Ej[a] = 0.0;
+            }
+            const float* in = d.prf + p;
+#pragma unroll
+            for (int a = 0; a < NT; a++)
+#pragma unroll
+                for (int b = 0; b < NT; b++) {
+                    const double g0 = (double)__ldg(in + (SL::RHO + b * NT + a) * mp);
+                    Ei[a] += g0 * cj[b];
+                    Ej[b] += g0 * ci[a];
+                    if (a >= b) acc[0] += w * (cj[b] * ci[a] + cj[a] * ci[b]) * (double)__ldg(in + (SL::PHI + comp_idx(a, b)) * mp);
+                }
+            if (own_j)
+#pragma unroll
+                for (int b = 0; b < NT; b++)
+                    if (Ej[b] != 0.0) atomicAdd(&d.E[(size_t)j * NT + b], Ej[b]);
+        }
+        const Seg sg = seg_of(i);
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            const double t = seg_sum(Ei[a], sg);
+            if (valid && lane == sg.first && t != 0.0) atomicAdd(&d.E[(size_t)i * NT + a], t);
+        }
     }
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
 }
@@ -667,18 +775,25 @@ cudaError_t launch_mlp_eval(const MlpState& S, const float* X, int n, float* Y, 
 cudaError_t launch_dmd_force_mlp(const Dev& d, const MlpState& S, unsigned long long audit_seed, int st_clc, int* nb,
                                  cudaStream_t st, cudaEvent_t* evs)
 {
+    if (d.npairs > 2147483647LL) return cudaErrorInvalidValue;  // queued rows keep the pair index in an int
     const int ppw = 32 / (d.nt * d.nt);
     long long groups = (d.npairs + ppw - 1) / ppw;
     long long need = (groups + kInfWarps - 1) / kInfWarps;
     long long cap = (long long)num_sms() * 2;
     int g1 = (int)(need < cap ? (need > 0 ? need : 1) : cap);
+    int gd = persistent_grid(d.npairs, 4);
     if (evs) cudaEventRecord(evs[0], st);
-    if (d.nt == 1) k_dmd_pass1_mlp<1><<<g1, kInfThreads, 0, st>>>(d, S, audit_seed, 0);
-    else k_dmd_pass1_mlp<2><<<g1, kInfThreads, 0, st>>>(d, S, audit_seed, 0);
+    if (d.nt == 1) {
+        k_dmd_pass1_mlp<1><<<g1, kInfThreads, 0, st>>>(d, S, audit_seed);
+        k_mlp_densities<1><<<gd, kFFBlock, 0, st>>>(d, 0);
+    } else {
+        k_dmd_pass1_mlp<2><<<g1, kInfThreads, 0, st>>>(d, S, audit_seed);
+        k_mlp_densities<2><<<gd, kFFBlock, 0, st>>>(d, 0);
+    }
     if (evs) cudaEventRecord(evs[1], st);
     int rows = 0;
-    cudaError_t e = launch_dmd_force_f32_after_pass1(d, st_clc, g1, &rows, st, evs);
-    *nb = g1 + rows;
+    cudaError_t e = launch_dmd_force_f32_after_pass1(d, st_clc, gd, &rows, st, evs);
+    *nb = gd + rows;
     return e;
 }
 
