@@ -427,6 +427,7 @@ def write_workload(dirpath: str, kind: str, **kw) -> dict:
     """
     os.makedirs(dirpath, exist_ok=True)
     skin = kw.pop("skin", 0.5)
+    box = kw.pop("box", None)  # optional 3x3 lower-triangular H (rows = box vectors); s is kept
     out = {"kind": kind, "dir": dirpath, "skin": skin}
     if kind == "eam":
         nt = kw.pop("nt", 1)
@@ -457,6 +458,8 @@ def write_workload(dirpath: str, kind: str, **kw) -> dict:
         out["style"] = style
     else:
         raise ValueError(kind)
+    if box is not None:
+        cfg.extra["H"] = np.array(box, dtype=np.float64)
     cfg_path = os.path.join(dirpath, "conf.cfg")
     write_cfg(cfg_path, cfg)
     script = os.path.join(dirpath, "in.mapp")

@@ -46,6 +46,7 @@ class RefRun:
     def __init__(self, workload: dict, workdir: str | None = None, init: bool = True):
         self.w = workload
         self.dir = workdir or tempfile.mkdtemp(prefix="mapp_ref_")
+        os.makedirs(self.dir, exist_ok=True)
         self.lines = [f"script {workload['script']}"]
         style = workload["style"]
         if style.startswith("DMD"):

@@ -149,6 +149,41 @@ def test_gpu_matches_oracle(tmp_path, kind, kw):
         assert rel(s.c_d_calc(), o.c_d()) <= TOL
 
 
+BOXES = [
+    ("eam", dict(n=4, sigma=0.05), 4 * 3.615, (1.3, -0.9, 0.7)),
+    ("dmd", dict(n=4, sigma=0.02, style="DMD_I"), 4 * 3.58, (0.8, 0.0, -0.6)),
+    ("eam", dict(n=1, sigma=0.05), 3.615, (0.0, 0.0, 0.0)),
+    ("dmd", dict(n=1, sigma=0.02, style="DMD_I"), 3.58, (0.0, 0.0, 0.0)),
+    ("dmd", dict(n=2, sigma=0.02, style="DMD_II"), 2 * 3.58, (0.4, 0.0, 0.3)),
+]
+
+
+@pytest.mark.parametrize("kind,kw,L,tilt", BOXES,
+                         ids=["eam-sheared", "dmd-sheared", "eam-1cell", "dmd-1cell", "dmd-2cell-sheared"])
+def test_gpu_matches_oracle_sheared_and_small_boxes(tmp_path, kind, kw, L, tilt):
+    """Triclinic boxes and boxes smaller than the cut-off (several ghost passes
+    per direction), the cases the oracle is pinned on in
+    tests/test_oracle_vs_reference.py."""
+    mb = _lib_or_skip()
+    from oracle.restated import Oracle
+
+    H = np.array([[L, 0.0, 0.0], [tilt[0], L, 0.0], [tilt[1], tilt[2], L]])
+    w = fx.write_workload(str(tmp_path / "w"), kind, box=H, **kw)
+    s = mb.system_from_workload(w)
+    o = Oracle(w)
+    check_state(s, o)
+    check_forces(s, o, w["cfg"].dmd)
+    if w["cfg"].dmd:
+        s.create_2nd_neigh_lst()
+        assert np.array_equal(s.crd(), o.crd())
+        assert rel(s.c_d_calc(), o.c_d()) <= TOL
+    N = w["cfg"].natms
+    x1 = s.get_x()
+    x1[:, :3] += np.random.default_rng(9).normal(0, 0.05, (N, 3))
+    assert s.update_x(x1) == o.update_x(x1) == 0
+    check_forces(s, o, w["cfg"].dmd)
+
+
 def test_gpu_dmd_full_size_32000(tmp_path):
     """The binary DMD_I system at its benchmark size (FCC 20^3 = 32000 sites)."""
     mb = _lib_or_skip()

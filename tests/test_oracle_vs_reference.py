@@ -36,9 +36,6 @@ def _same(a, b):
 def test_restated_oracle_bit_exact(tmp_path, kind, kw):
     w = fx.write_workload(str(tmp_path / "w"), kind, **kw)
     N = w["cfg"].natms
-    run = reference.RefRun(w, workdir=str(tmp_path / "ref")) if False else None
-    import os
-    os.makedirs(tmp_path / "ref", exist_ok=True)
     rr = reference.RefRun(w, workdir=str(tmp_path / "ref")).dump("s0").force("f0").energy("e0")
     dmd = w["cfg"].dmd
     a = np.random.default_rng(7).normal(0, 0.01, (N, 2))
@@ -78,3 +75,46 @@ def test_restated_oracle_bit_exact(tmp_path, kind, kw):
     f2, en2 = o.force()
     _same(f2, r["f2"]["f"])
     _same(en2, r["f2"]["meta"]["en"])
+
+
+def _ref_box(meta):
+    return np.array([[float(v) for v in meta[f"H{i}"]] for i in range(3)])
+
+
+BOXES = [
+    # sheared (triclinic) cells: the reference turns the CFG box into its own
+    # lower-triangular H, which is read back and given to the restatement
+    ("eam", dict(n=4, sigma=0.05), 4 * 3.615, (1.3, -0.9, 0.7)),
+    # (a DMD box tilted in H[2][0] stops the reference in create_bin_list,
+    # neighbor.cpp:320, with an allocation failure, so the DMD cases tilt
+    # H[1][0] and H[2][1] only)
+    ("dmd", dict(n=4, sigma=0.02, style="DMD_I"), 4 * 3.58, (0.8, 0.0, -0.6)),
+    # boxes smaller than the cut-off: several ghost passes per direction
+    ("eam", dict(n=1, sigma=0.05), 3.615, (0.0, 0.0, 0.0)),
+    ("dmd", dict(n=1, sigma=0.02, style="DMD_I"), 3.58, (0.0, 0.0, 0.0)),
+    ("dmd", dict(n=2, sigma=0.02, style="DMD_II"), 2 * 3.58, (0.4, 0.0, 0.3)),
+]
+
+
+@pytest.mark.parametrize("kind,kw,L,tilt", BOXES,
+                         ids=["eam-sheared", "dmd-sheared", "eam-1cell", "dmd-1cell", "dmd-2cell-sheared"])
+def test_restated_oracle_bit_exact_sheared_and_small_boxes(tmp_path, kind, kw, L, tilt):
+    H = np.array([[L, 0.0, 0.0], [tilt[0], L, 0.0], [tilt[1], tilt[2], L]])
+    w = fx.write_workload(str(tmp_path / "w"), kind, box=H, **kw)
+    rr = reference.RefRun(w, workdir=str(tmp_path / "ref")).dump("s0").force("f0").energy("e0")
+    if w["cfg"].dmd:
+        rr.crd("crd").cdot("cd")
+    r = rr.run()
+    w["cfg"].extra["H"] = _ref_box(r["s0"]["meta"])
+    o = Oracle(w)
+    _same(o.x_all(), r["s0"]["x"])
+    ns, fl = o.neighbor_list()
+    _same(ns, r["s0"]["nsize"])
+    _same(fl, r["s0"]["nlist"])
+    f, en = o.force()
+    _same(f, r["f0"]["f"])
+    _same(en, r["f0"]["meta"]["en"])
+    _same(o.energy(), r["e0"]["meta"]["energy"])
+    if w["cfg"].dmd:
+        _same(o.crd(), r["crd"]["crd"])
+        _same(o.c_d(), r["cd"]["c_d"])
