@@ -999,6 +999,14 @@ int mg_ff_init(mg_system* s)
     CHK(upload_tables(s));
     fill_dev_scalars(s);
     compute_cutoffs(s);
+    if (s->natms == 0) {  // an empty system: no ghosts, no pairs, zero energy and forces
+        s->d.nph = 0;
+        s->d.nall = 0;
+        s->d.npairs = 0;
+        s->npairs = 0;
+        s->initialized = true;
+        return MG_OK;
+    }
     // owned atoms: root / chain identity, s already in d.sfr
     {
         std::vector<int> root(s->natms);
@@ -1019,6 +1027,10 @@ int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
 {
     CHK(check_sys(s));
     if (!s->initialized) return fail(MG_ERR_STATE, "init must run before update_0");
+    if (s->natms == 0) {
+        if (rebuilt) *rebuilt = 0;
+        return MG_OK;
+    }
     Dev& d = s->d;
     if (s->natms) {
         const void* dx = nullptr;
@@ -1045,6 +1057,7 @@ int mg_atoms_update_c(mg_system* s, const double* c)
     CHK(check_sys(s));
     if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "c exists only in DMD mode");
     if (!s->initialized) return fail(MG_ERR_STATE, "init must run first");
+    if (s->natms == 0) return MG_OK;
     size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
     CU(cudaMemcpyAsync(s->d.c, c, bytes, is_device_ptr(c) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->st));
     CU(launch_refresh_c(s->d, s->st));
@@ -1055,6 +1068,7 @@ int mg_atoms_get_x(mg_system* s, double* x)
 {
     CHK(check_sys(s));
     if (!x) return fail(MG_ERR_ARG, "null x");
+    if (s->natms == 0) return MG_OK;
     size_t bytes = (size_t)s->natms * s->x_dim * sizeof(double);
     if (bytes > s->stage_cap) {
         CHK(dalloc((char**)&s->stage, bytes));
@@ -1088,6 +1102,11 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
 {
     CHK(check_sys(s));
     if (!s->initialized) return fail(MG_ERR_STATE, "force_calc before init");
+    if (s->natms == 0) {
+        if (en_st)
+            for (int i = 0; i < (st_clc ? 7 : 1); i++) en_st[i] = 0.0;
+        return MG_OK;
+    }
     Dev& d = s->d;
     fill_dev_scalars(s);
     CHK(timed_begin(s));
@@ -1131,6 +1150,10 @@ int mg_ff_energy_calc(mg_system* s, double* energy)
 {
     CHK(check_sys(s));
     if (!s->initialized) return fail(MG_ERR_STATE, "energy_calc before init");
+    if (s->natms == 0) {
+        if (energy) *energy = 0.0;
+        return MG_OK;
+    }
     Dev& d = s->d;
     CHK(timed_begin(s));
     int rows = 0;
@@ -1155,6 +1178,10 @@ int mg_ff_create_2nd_neigh_lst(mg_system* s)
     CHK(check_sys(s));
     if (!s->dmd) return MG_OK;  // empty in EAM / FS (ff_eam.h:61)
     if (!s->initialized) return fail(MG_ERR_STATE, "create_2nd_neigh_lst before init");
+    if (s->natms == 0) {
+        s->crd_built = 1;
+        return MG_OK;
+    }
     Dev& d = s->d;
     for (int attempt = 0; attempt < 4; attempt++) {
         CU(cudaMemsetAsync(d.crd, 0, (size_t)d.nall * sizeof(int), s->st));
@@ -1180,6 +1207,7 @@ int mg_ff_c_d_calc(mg_system* s, double* c_d)
     CHK(check_sys(s));
     if (!s->dmd) return MG_OK;
     if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before c_d_calc");
+    if (s->natms == 0) return MG_OK;
     Dev& d = s->d;
     size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
     CHK(timed_begin(s));
@@ -1200,7 +1228,11 @@ int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g
         return MG_OK;
     }
     if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before calc_g");
-    if (!a) return fail(MG_ERR_ARG, "null a");
+    if (!a && s->natms) return fail(MG_ERR_ARG, "null a");
+    if (s->natms == 0) {
+        if (cost) *cost = 0.0;
+        return MG_OK;
+    }
     Dev& d = s->d;
     size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
     CU(cudaMemcpyAsync(d.a_in, a, bytes, is_device_ptr(a) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->st));
@@ -1227,6 +1259,7 @@ int mg_ff_fin(mg_system* s)
     d.pr = nullptr;
     d.maxp = 0;
     if (s->dmd) s->pair_cap = 0;
+    else s->nbr_cap = 0;  // EAM / FS keep their pair derivatives beside the ELL list
     s->initialized = false;
     s->crd_built = 0;
     return MG_OK;
@@ -1236,6 +1269,7 @@ int mg_neighbor_create_list(mg_system* s)
 {
     CHK(check_sys(s));
     if (!s->initialized) return fail(MG_ERR_STATE, "init must run first");
+    if (s->natms == 0) return MG_OK;
     CU(launch_x2s(s->d, s->st));
     return rebuild(s);
 }
