@@ -226,6 +226,7 @@ struct mg_system {
     double* d_phiT = nullptr;
     double* d_FT = nullptr;
     float* d_pkT = nullptr;
+    float* d_pkC = nullptr;
     int* cursor = nullptr;
     int crd_built = 0;
     int npair_blocks = 2;
@@ -684,6 +685,46 @@ int upload_tables(mg_system* s)
         CHK(dalloc(&s->d_pkT, pk.size()));
         CU(cudaMemcpy(s->d_pkT, pk.data(), pk.size() * sizeof(float), cudaMemcpyHostToDevice));
         d.pkT = reinterpret_cast<const float4*>(s->d_pkT);
+        // Coarse copy for the precision form's pass 1: kCoarseKnots knots over
+        // [0, rc], each interval the cubic Hermite piece through the fine
+        // spline's value and slope at its ends (fine interpolant evaluated as in
+        // the force kernels, index clamp nr-2 and p <= 1).  With rho and r*phi
+        // decaying over 0.3-0.6 A the two interpolants differ by ~1e-10 relative,
+        // far below FP32 rounding.
+        const int K = kCoarseKnots;
+        const double rc = (nr - 1) * s->dr, hc = rc / (K - 1);
+        auto fine = [&](const double* slot, double r, double& v, double& dv) {
+            double pp = r * (1.0 / s->dr);
+            int m = std::min((int)pp, nr - 2);
+            double p = std::min(pp - m, 1.0);
+            const double* c = slot + (size_t)m * 8;
+            v = ((c[3] * p + c[2]) * p + c[1]) * p + c[0];
+            dv = ((3.0 * c[3] * p + 2.0 * c[2]) * p + c[1]) * (1.0 / s->dr);
+        };
+        auto hermite = [&](const double* slot, int k, float* dst) {
+            double v0, d0, v1, d1;
+            fine(slot, k * hc, v0, d0);
+            fine(slot, std::min((k + 1) * hc, rc), v1, d1);
+            d0 *= hc;
+            d1 *= hc;
+            dst[0] = (float)v0;
+            dst[1] = (float)d0;
+            dst[2] = (float)(3.0 * (v1 - v0) - 2.0 * d0 - d1);
+            dst[3] = (float)(2.0 * (v0 - v1) + d0 + d1);
+        };
+        std::vector<float> pc((size_t)nt * nt * K * 8, 0.0f);
+        for (int a = 0; a < nt; a++)
+            for (int b = 0; b < nt; b++)
+                for (int k = 0; k < K - 1; k++) {
+                    float* dst = pc.data() + (((size_t)(a * nt + b) * K + k) * 8);
+                    hermite(s->rhoT.data() + (size_t)(b * nt + a) * nr * 8, k, dst);
+                    if (a >= b) hermite(s->phiT.data() + (size_t)comp_idx(a, b) * nr * 8, k, dst + 4);
+                }
+        CHK(dalloc(&s->d_pkC, pc.size()));
+        CU(cudaMemcpy(s->d_pkC, pc.data(), pc.size() * sizeof(float), cudaMemcpyHostToDevice));
+        d.pkC = reinterpret_cast<const float4*>(s->d_pkC);
+        d.nrC = K;
+        d.drC_inv = (float)(1.0 / hc);
     }
     d.Fw = s->Fw;
     d.nr = s->nr;
@@ -770,7 +811,7 @@ int mg_destroy(mg_system* s)
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->st);
     Dev& d = s->d;
-    void* ptrs[] = {d.prf, s->d_pkT, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
+    void* ptrs[] = {d.prf, s->d_pkT, s->d_pkC, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
                     d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status,
                     s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};

@@ -156,7 +156,19 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass2(Dev d, int 
 #pragma unroll
         for (int q = 0; q < 3 + NT; q++) fi[q] = 0.0;
         const bool act = valid && site_active(d, i);
+        // pairs beyond the smeared cut contribute nothing and pass 1 stored no
+        // derivatives for them: the same exact rsq test as pass 1 skips them
+        bool in_cut = false;
+        int j = 0;
+        double4 xi = make_double4(0, 0, 0, 0), xj = xi;
         if (act) {
+            j = d.pair_j[p];
+            xi = d.pos[i];
+            xj = d.pos[j];
+            const double ex0 = xi.x - xj.x, ex1 = xi.y - xj.y, ex2 = xi.z - xj.z;
+            in_cut = __dadd_rn(__dadd_rn(__dmul_rn(ex0, ex0), __dmul_rn(ex1, ex1)), __dmul_rn(ex2, ex2)) < d.cut_sq_mod;
+        }
+        if (in_cut) {
             const double* in = d.pr + p;
             double drr[NT * NT], dra[NT * NT], dpr[S::NC], dpa[S::NC];
 #pragma unroll
@@ -169,9 +181,7 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass2(Dev d, int 
                 dpr[q] = __ldcs(in + (S::DPR + q) * mp);
                 dpa[q] = __ldcs(in + (S::DPA + q) * mp);
             }
-            int j = d.pair_j[p];
             int oj = owner(d, j);
-            double4 xi = d.pos[i], xj = d.pos[j];
             double ai[NT], ci[NT], dEi[NT], aj[NT], cj[NT], dEj[NT], fj[NT];
 #pragma unroll
             for (int a = 0; a < NT; a++) {

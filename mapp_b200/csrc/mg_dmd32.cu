@@ -54,14 +54,27 @@ __device__ __forceinline__ float2 seg_sum2(float v, const Seg& s)
 }
 
 // ---- pass 1: FP32 smearing, compensated densities -------------------------
-template <int NT, int NQ>
-__global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass1(Dev d, int row0)
+// kSmem = 1: the coarse table (d.pkC) is copied into shared memory first and
+// every knot of the quadrature is read from there, one 1024-thread block per
+// SM; kSmem = 0: the fine packed table through L1 / L2.
+template <int NT, int NQ, int kSmem>
+__global__ void __launch_bounds__(kSmem ? 1024 : kFFBlock, kSmem ? 1 : MG_DMD32_MINB) k_dmd32_pass1(Dev d, int row0)
 {
     using S = Slots<NT>;
+    extern __shared__ float4 tab_sh[];
     const int lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x;
     const size_t mp = (size_t)d.maxp;
-    const F32Consts kc = f32_consts(d);
+    F32Consts kc = f32_consts(d);
+    const float4* tab = d.pkT;
+    if (kSmem) {
+        const int n4 = NT * NT * d.nrC * 2;
+        for (int k = threadIdx.x; k < n4; k += blockDim.x) tab_sh[k] = __ldg(d.pkC + k);
+        __syncthreads();
+        tab = tab_sh;
+        kc.nr = d.nrC;
+        kc.dr_inv = d.drC_inv;
+    }
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < d.npairs; base += stride) {
         long long p = base + lane;
@@ -99,13 +112,15 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass1(Dev d, 
 #pragma unroll
                 for (int b = 0; b < NT; b++) {
                     const int rs = b * NT + a, ps = comp_idx(a, b);
-                    const float4* pk = d.pkT + (size_t)(a * NT + b) * d.nr * 2;
+                    const float4* pk = tab + (size_t)(a * NT + b) * kc.nr * 2;
                     float g0 = 0, gdr = 0, gda = 0, f0 = 0, fdr = 0, fda = 0;
                     bool hit = false;
                     if (in_cut) {
                         float alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
-                        hit = (a >= b) ? smear_f<true, NQ>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr, gda, f0, fdr, fda)
-                                       : smear_f<false, NQ>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr, gda, f0, fdr, fda);
+                        hit = (a >= b) ? smear_f<true, NQ, kSmem != 0>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr,
+                                                                      gda, f0, fdr, fda)
+                                       : smear_f<false, NQ, kSmem != 0>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr,
+                                                                       gda, f0, fdr, fda);
                     }
                     if (!hit) g0 = gdr = gda = f0 = fdr = fda = 0.0f;
                     __stcs(out + (S::RHO + rs) * mp, g0);
@@ -182,7 +197,19 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass2(Dev d, 
 #pragma unroll
         for (int q = 0; q < 3 + NT; q++) fi[q] = 0.0f;
         const bool act = valid && site_active(d, i);
+        // pairs beyond the smeared cut contribute nothing and pass 1 stored no
+        // derivatives for them: the same exact rsq test as pass 1 skips them
+        bool in_cut = false;
+        int j = 0;
+        double4 xi = make_double4(0, 0, 0, 0), xj = xi;
         if (act) {
+            j = d.pair_j[p];
+            xi = d.pos[i];
+            xj = d.pos[j];
+            const double ex0 = xi.x - xj.x, ex1 = xi.y - xj.y, ex2 = xi.z - xj.z;
+            in_cut = __dadd_rn(__dadd_rn(__dmul_rn(ex0, ex0), __dmul_rn(ex1, ex1)), __dmul_rn(ex2, ex2)) < d.cut_sq_mod;
+        }
+        if (in_cut) {
             const float* in = d.prf + p;
             float drr[NT * NT], dra[NT * NT], dpr[S::NC], dpa[S::NC];
 #pragma unroll
@@ -195,9 +222,7 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass2(Dev d, 
                 dpr[q] = __ldcs(in + (S::DPR + q) * mp);
                 dpa[q] = __ldcs(in + (S::DPA + q) * mp);
             }
-            int j = d.pair_j[p];
             int oj = owner(d, j);
-            double4 xi = d.pos[i], xj = d.pos[j];
             float ai[NT], ci[NT], dEi[NT], aj[NT], cj[NT], dEj[NT], fj[NT];
 #pragma unroll
             for (int a = 0; a < NT; a++) {
@@ -264,9 +289,26 @@ cudaError_t dmd32_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, c
 {
     int g1 = persistent_grid(d.npairs, d.tune_bps > 0 ? d.tune_bps : MG_DMD32_MINB), g2 = div_up(d.natms, kFFBlock);
     int g3 = persistent_grid(d.npairs, d.tune_bps2 > 0 ? d.tune_bps2 : MG_DMD32_MINB);
+    const size_t tab_bytes = (size_t)NT * NT * d.nrC * 2 * sizeof(float4);
+    const bool smem = d.pkC != nullptr && tab_bytes <= 200 * 1024;
+    if (smem) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_dmd32_pass1<NT, 3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(k_dmd32_pass1<NT, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            attr = true;
+        }
+        long long need = div_up(d.npairs, 1024LL);
+        g1 = (int)(need < num_sms() ? (need > 0 ? need : 1) : num_sms());
+    }
     if (evs) cudaEventRecord(evs[0], st);
-    if (d.nq == 3) k_dmd32_pass1<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
-    else k_dmd32_pass1<NT, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
+    if (smem) {
+        if (d.nq == 3) k_dmd32_pass1<NT, 3, 1><<<g1, 1024, tab_bytes, st>>>(d, 0);
+        else k_dmd32_pass1<NT, 0, 1><<<g1, 1024, tab_bytes, st>>>(d, 0);
+    } else {
+        if (d.nq == 3) k_dmd32_pass1<NT, 3, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
+        else k_dmd32_pass1<NT, 0, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
+    }
     if (evs) cudaEventRecord(evs[1], st);
     k_dmd32_embed<NT><<<g2, kFFBlock, 0, st>>>(d, g1);
     if (evs) cudaEventRecord(evs[2], st);

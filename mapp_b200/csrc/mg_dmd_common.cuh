@@ -171,7 +171,17 @@ __device__ __forceinline__ F32Consts f32_consts(const Dev& d)
 
 // FP32 counterpart of smear(): one species pair of one site pair, tables
 // packed one 32-byte sector per knot {rho c0..c3, phi c0..c3} (pk).
-template <bool kPhi, int NQ>
+// one knot row of the packed table: read-only cache load from global memory,
+// or a plain load when the table is a shared-memory copy (ld.global.nc must
+// not be given a shared-memory address)
+template <bool kShared>
+__device__ __forceinline__ float4 knot_f(const float4* p)
+{
+    if (kShared) return *p;
+    return __ldg(p);
+}
+
+template <bool kPhi, int NQ, bool kShared = false>
 __device__ __forceinline__ bool smear_f(const Dev& d, const F32Consts& k, const float4* __restrict__ pk, float r,
                                         float r_inv, bool below_rc, float alpha, float& g0, float& g_dr, float& g_da,
                                         float& f0, float& f_dr, float& f_da)
@@ -195,14 +205,14 @@ __device__ __forceinline__ bool smear_f(const Dev& d, const F32Consts& k, const 
                 p -= (float)m;
                 p = fminf(p, 1.0f);
                 float p2 = p * p, p3 = p2 * p;
-                float4 cr = __ldg(pk + 2 * m);
+                float4 cr = knot_f<kShared>(pk + 2 * m);
                 float tmp2 = (cr.w * p3 + cr.z * p2 + cr.y * p + cr.x) * tmp0;
                 float w0 = (float)d.w0[q], w1 = (float)d.w1[q], w2 = (float)d.w2[q];
                 ga += w0 * tmp2;
                 gb += w1 * tmp2;
                 gc += w2 * tmp2;
                 if (kPhi) {
-                    float4 cp = __ldg(pk + 2 * m + 1);
+                    float4 cp = knot_f<kShared>(pk + 2 * m + 1);
                     float tmp1 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
                     if (tmp0 < 0.0f) tmp1 = -tmp1;
                     fa += w0 * tmp1;
@@ -233,12 +243,12 @@ __device__ __forceinline__ bool smear_f(const Dev& d, const F32Consts& k, const 
         p -= (float)m;
         p = fminf(p, 1.0f);
         float p2 = p * p, p3 = p2 * p;
-        float4 cr = __ldg(pk + 2 * m);
+        float4 cr = knot_f<kShared>(pk + 2 * m);
         g0 = cr.w * p3 + cr.z * p2 + cr.y * p + cr.x;
         g_da = 0.0f;
         g_dr = (cr.y + 2.0f * cr.z * p + 3.0f * cr.w * p2) * k.dr_inv;
         if (kPhi) {
-            float4 cp = __ldg(pk + 2 * m + 1);
+            float4 cp = knot_f<kShared>(pk + 2 * m + 1);
             float z2 = cp.w * p3 + cp.z * p2 + cp.y * p + cp.x;
             float z2p = (cp.y + 2.0f * cp.z * p + 3.0f * cp.w * p2) * k.dr_inv;
             f0 = z2 * r_inv;

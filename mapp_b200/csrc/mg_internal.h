@@ -37,6 +37,7 @@ enum Style { STYLE_EAM = 0, STYLE_FS = 1, STYLE_DMD_I = 2, STYLE_DMD_II = 3, STY
 
 constexpr int kMaxTypes = 4;
 constexpr int kMaxQuad = 14;
+constexpr int kCoarseKnots = 1024;
 constexpr int kMaxChain = 15;
 
 // Everything a kernel needs, passed by value.
@@ -99,6 +100,11 @@ struct Dev {
     // precision form: per ordered species pair (a,b) and knot, one 32-byte
     // sector {rho c0..c3 of slot b*nt+a, phi c0..c3 of slot COMP(a,b) (zero when a < b)}
     const float4* pkT;
+    // the same splines resampled onto kCoarseKnots knots over [0, rc] (FP32,
+    // packed the same way), small enough for a shared-memory copy in pass 1
+    const float4* pkC;
+    int nrC;
+    float drC_inv;
     float* prf;          // FP32 pair scratch, same SoA layout as pr
     double cut_sk_sq[16];
     // FS analytic

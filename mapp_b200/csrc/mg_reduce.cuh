@@ -88,13 +88,13 @@ inline int persistent_grid(long long threads_needed, int blocks_per_sm)
     return (int)(need < cap ? (need > 0 ? need : 1) : cap);
 }
 
-// Sums NV per-thread values over the block (up to kFFBlock threads) and writes them to
+// Sums NV per-thread values over the block (up to 1024 threads) and writes them to
 // partial[(row) * 8 + v] (row = blockIdx.x + row_offset).  Every thread of the
 // block must call it.
 template <int NV>
 __device__ __forceinline__ void block_partials(const double (&vals)[NV], double* partial, int row)
 {
-    __shared__ double sh[kFFWarps][8];
+    __shared__ double sh[32][8];  // up to 1024 threads
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int v = 0; v < NV; v++) {
