@@ -1000,6 +1000,10 @@ int mg_ff_coef(mg_system* s, int narg, const char* const* arg)
         for (int i = 0; i < n; i++) {
             d.w1[i] = d.w0[i] * d.xi[i];
             d.w2[i] = d.w0[i] * d.xi[i] * d.xi[i];
+            d.xi_f[i] = (float)d.xi[i];
+            d.w0_f[i] = (float)d.w0[i];
+            d.w1_f[i] = (float)d.w1[i];
+            d.w2_f[i] = (float)d.w2[i];
         }
         d.alpha_min = atof(arg[3]);
         d.alpha_max = atof(arg[4]);

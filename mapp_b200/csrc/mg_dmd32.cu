@@ -74,6 +74,8 @@ __global__ void __launch_bounds__(kSmem ? 1024 : kFFBlock, kSmem ? 1 : MG_DMD32_
         tab = tab_sh;
         kc.nr = d.nrC;
         kc.dr_inv = d.drC_inv;
+        kc.top = (float)(d.nrC - 1);
+        kc.top_m = (float)(d.nrC - 2);
     }
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < d.npairs; base += stride) {
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(kSmem ? 1024 : kFFBlock, kSmem ? 1 : MG_DMD32_
                     float g0 = 0, gdr = 0, gda = 0, f0 = 0, fdr = 0, fda = 0;
                     bool hit = false;
                     if (in_cut) {
-                        float alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
+                        float alpha = __fdividef(ai[a] * aj[b], ai[a] + aj[b]);
                         hit = (a >= b) ? smear_f<true, NQ, kSmem != 0>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr,
                                                                       gda, f0, fdr, fda)
                                        : smear_f<false, NQ, kSmem != 0>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr,

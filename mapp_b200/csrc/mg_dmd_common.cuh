@@ -156,6 +156,7 @@ constexpr float kPiInSqF = 0.564189583547756286948079451561f;
 struct F32Consts {
     float rc, dr_inv, alpha_min, alpha_max;
     int nr;
+    float top, top_m;  // nr - 1 and nr - 2 as floats
 };
 
 __device__ __forceinline__ F32Consts f32_consts(const Dev& d)
@@ -166,6 +167,8 @@ __device__ __forceinline__ F32Consts f32_consts(const Dev& d)
     c.alpha_min = (float)d.alpha_min;
     c.alpha_max = (float)d.alpha_max;
     c.nr = d.nr;
+    c.top = (float)(d.nr - 1);
+    c.top_m = (float)(d.nr - 2);
     return c;
 }
 
@@ -181,6 +184,17 @@ __device__ __forceinline__ float4 knot_f(const float4* p)
     return __ldg(p);
 }
 
+// floor of 0 <= p < 2^22 as an int and as a float by the round-to-nearest of
+// p - 1/2 against 1.5 * 2^23, on the FP32 / integer pipes instead of the
+// conversion unit; at an exact integer p it may give p - 1 (then p - m = 1,
+// the end of the previous interval, where the spline takes the same value)
+__device__ __forceinline__ int floor_idx(float p, float& fm)
+{
+    const float t = __fadd_rn(__fadd_rn(p, -0.5f), 12582912.0f);
+    fm = __fadd_rn(t, -12582912.0f);
+    return __float_as_int(t) - 0x4B400000;
+}
+
 template <bool kPhi, int NQ, bool kShared = false>
 __device__ __forceinline__ bool smear_f(const Dev& d, const F32Consts& k, const float4* __restrict__ pk, float r,
                                         float r_inv, bool below_rc, float alpha, float& g0, float& g_dr, float& g_da,
@@ -192,22 +206,27 @@ __device__ __forceinline__ bool smear_f(const Dev& d, const F32Consts& k, const 
         float asq = alpha * inv_asq;
         float inv_alpha = inv_asq * inv_asq;
         float upper = (r + k.rc) * asq, lower = (r - k.rc) * asq;
-        if (!(lower < (float)d.xi[nq - 1])) return false;
+        if (!(lower < d.xi_f[nq - 1])) return false;
         float fa = 0.f, fb = 0.f, fc = 0.f, ga = 0.f, gb = 0.f, gc = 0.f;
 #pragma unroll
         for (int q = 0; q < (NQ > 0 ? NQ : kMaxQuad); q++) {
             if (NQ == 0 && q >= nq) break;
-            float xq = (float)d.xi[q];
+            float xq = d.xi_f[q];
             if (xq > lower && xq < upper) {
                 float tmp0 = r - xq * inv_asq;
-                float p = fabsf(tmp0) * k.dr_inv;
-                int m = min((int)p, k.nr - 2);
-                p -= (float)m;
+                float p = fminf(fabsf(tmp0) * k.dr_inv, k.top);
+                float fm;
+                int m = floor_idx(p, fm);
+                if (m > k.nr - 2) {
+                    m = k.nr - 2;
+                    fm = k.top_m;
+                }
+                p -= fm;
                 p = fminf(p, 1.0f);
                 float p2 = p * p, p3 = p2 * p;
                 float4 cr = knot_f<kShared>(pk + 2 * m);
                 float tmp2 = (cr.w * p3 + cr.z * p2 + cr.y * p + cr.x) * tmp0;
-                float w0 = (float)d.w0[q], w1 = (float)d.w1[q], w2 = (float)d.w2[q];
+                float w0 = d.w0_f[q], w1 = d.w1_f[q], w2 = d.w2_f[q];
                 ga += w0 * tmp2;
                 gb += w1 * tmp2;
                 gc += w2 * tmp2;
@@ -238,9 +257,14 @@ __device__ __forceinline__ bool smear_f(const Dev& d, const F32Consts& k, const 
     }
     if (k.alpha_max <= alpha) {
         if (!below_rc) return false;
-        float p = r * k.dr_inv;
-        int m = min((int)p, k.nr - 2);
-        p -= (float)m;
+        float p = fminf(r * k.dr_inv, k.top);
+        float fm;
+        int m = floor_idx(p, fm);
+        if (m > k.nr - 2) {
+            m = k.nr - 2;
+            fm = k.top_m;
+        }
+        p -= fm;
         p = fminf(p, 1.0f);
         float p2 = p * p, p3 = p2 * p;
         float4 cr = knot_f<kShared>(pk + 2 * m);

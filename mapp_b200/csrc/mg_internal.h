@@ -115,6 +115,7 @@ struct Dev {
     double rsq_crd, alpha_min, alpha_max, kbT, beta, c0[kMaxTypes];
     int nq;
     double xi[kMaxQuad], w0[kMaxQuad], w1[kMaxQuad], w2[kMaxQuad];
+    float xi_f[kMaxQuad], w0_f[kMaxQuad], w1_f[kMaxQuad], w2_f[kMaxQuad];  // FP32 copies (precision form)
     // batched form (many independent cells in one site / pair numbering);
     // all null for a single system
     const int* site_cell;              // owned site -> cell
