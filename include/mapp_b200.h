@@ -230,8 +230,9 @@ typedef struct mg_batch_stats {
     int rebuild_rounds;     /* list rebuilds triggered by the skin rule */
     int converged;          /* cells stopped by max|f| < fmax_tol */
     int bps1, bps2;         /* blocks per SM of force pass 1 and pass 2 */
-    int lbfgs_threads;      /* threads per cell of the L-BFGS step */
+    int lbfgs_threads;      /* threads per CTA of the L-BFGS step */
     int from_cache;         /* launch shapes read from the tuning cache */
+    int lbfgs_cluster;      /* CTAs per cell of the L-BFGS step (a thread-block cluster) */
 } mg_batch_stats;
 
 typedef struct mg_cell_result {
@@ -258,12 +259,33 @@ int mg_batch_set_params(mg_batch* b, int m, int max_iter, double fmax_tol, doubl
 int mg_batch_set_form(mg_batch* b, int form);
 /* autotune = 1: time candidate launch shapes on the batch (or read them from
    cache_path, a text file of earlier choices, which is then extended);
-   0: built-in shapes.  cache_path may be NULL. */
+   0: built-in shapes.  The search covers the blocks per SM of the two pair
+   passes and the threads and cluster size of the L-BFGS step.  cache_path
+   may be NULL. */
 int mg_batch_set_tuning(mg_batch* b, int autotune, const char* cache_path);
+/* fixed launch shapes instead of autotuning: blocks per SM of force pass 1
+   and pass 2 (0: built-in), threads per CTA (32..1024) and CTAs per cell
+   (1, 2, 4, 8 or 16: a thread-block cluster whose CTAs share the cell's
+   vectors) of the L-BFGS step */
+int mg_batch_set_launch(mg_batch* b, int bps1, int bps2, int lbfgs_threads, int lbfgs_cluster);
 int mg_batch_relax(mg_batch* b, mg_batch_stats* stats);
 /* final state of one cell: x = natms * (3 + nt) Cartesian positions and
    alpha, f the same shape; either may be NULL */
 int mg_batch_cell_result(mg_batch* b, int cell, double* x, double* f, mg_cell_result* r);
+
+/* ---- device-resident minimiser for one system ---------------------------- */
+/* Min_LBFGS::run with LineSearch_BackTrack::line_min (min_l-bfgs.cpp:616-773,
+   line_search.cpp:223-342) for the system itself, on the GPU: the same
+   algorithm, stop codes and line-search energies as the batched form (one
+   cell), with the L-BFGS vector work of each step spread over a
+   thread-block cluster of lbfgs_cluster CTAs (1, 2, 4, 8 or 16; 0 = autotune).
+   It replaces the reference's host loop, which copies x and f through the
+   boundary on every force evaluation.  The system (DMD style, initialised,
+   FP64 or FP32 form) starts from its current state and holds the final state
+   on return, ghosts and lists rebuilt; r receives the energy, max|f|, stop code
+   and counts, stats the launch statistics (either may be NULL). */
+int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings,
+                 int lbfgs_cluster, mg_cell_result* r, mg_batch_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -72,8 +72,10 @@ SIGNATURES = {
     "mg_batch_set_params": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]),
     "mg_batch_set_form": (C.c_int, [_P, C.c_int]),
     "mg_batch_set_tuning": (C.c_int, [_P, C.c_int, C.c_char_p]),
+    "mg_batch_set_launch": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     "mg_batch_relax": (C.c_int, [_P, _P]),
     "mg_batch_cell_result": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "mg_min_lbfgs": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _P, _P]),
 }
 
 
@@ -83,7 +85,7 @@ class BatchStats(C.Structure):
     _fields_ = [("relax_ms", C.c_double), ("build_ms", C.c_double), ("tune_ms", C.c_double),
                 ("iterations", C.c_longlong), ("evaluations", C.c_longlong), ("rebuild_rounds", C.c_int),
                 ("converged", C.c_int), ("bps1", C.c_int), ("bps2", C.c_int), ("lbfgs_threads", C.c_int),
-                ("from_cache", C.c_int)]
+                ("from_cache", C.c_int), ("lbfgs_cluster", C.c_int)]
 
 
 class CellResult(C.Structure):
@@ -331,6 +333,15 @@ class System:
         _check(load_library().mg_mlp_audit(self.h, err.ctypes.data_as(_D), cnt.ctypes.data_as(C.POINTER(C.c_longlong))))
         return err, cnt
 
+    def min_lbfgs(self, m=5, max_iter=10000, fmax_tol=1e-5, energy_tol=1e-8, max_halvings=60, cluster=0):
+        """Device-resident L-BFGS relaxation of this system (mg_min_lbfgs);
+        returns (result, stats) dicts.  cluster: CTAs per L-BFGS step, 0 = autotune."""
+        r = CellResult()
+        st = BatchStats()
+        _check(load_library().mg_min_lbfgs(self.h, m, max_iter, fmax_tol, energy_tol, max_halvings, cluster,
+                                           C.byref(r), C.byref(st)))
+        return ({k: getattr(r, k) for k, _ in CellResult._fields_}, {k: getattr(st, k) for k, _ in BatchStats._fields_})
+
     def last_time(self, phase):
         ms = C.c_double(0.0)
         _check(load_library().mg_last_time(self.h, phase.encode(), C.byref(ms)))
@@ -391,6 +402,9 @@ class Batch:
     def set_tuning(self, autotune=True, cache_path=None):
         _check(load_library().mg_batch_set_tuning(self.h, int(autotune),
                                                   None if cache_path is None else str(cache_path).encode()))
+
+    def set_launch(self, bps1=0, bps2=0, lbfgs_threads=256, lbfgs_cluster=1):
+        _check(load_library().mg_batch_set_launch(self.h, bps1, bps2, lbfgs_threads, lbfgs_cluster))
 
     def relax(self) -> dict:
         st = BatchStats()

@@ -1628,3 +1628,9 @@ void mg::system_shape(mg_system* s, int* style, int* nt, int* x_dim, int* form, 
             for (int j = 0; j < 3; j++) B_out[3 * i + j] = s->B[i][j];
 }
 double mg::system_skin(mg_system* s) { return s->skin; }
+void mg::system_box(mg_system* s, double* H_out)
+{
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) H_out[3 * i + j] = s->H[i][j];
+}
+int mg::system_natms(mg_system* s) { return s->natms; }

@@ -43,6 +43,8 @@
 #include <string>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "../../include/mapp_b200.h"
 #include "mg_reduce.cuh"
 
@@ -119,37 +121,69 @@ __device__ __forceinline__ double block_red(double v, double* sh)
     for (int k = 1; k < nw; k++) r = OP == 0 ? r + sh[k] : (OP == 1 ? fmax(r, sh[k]) : fmin(r, sh[k]));
     return r;
 }
-__device__ __forceinline__ double bsum(double v, double* sh) { return block_red<0>(v, sh); }
-__device__ __forceinline__ double bmax(double v, double* sh) { return block_red<1>(v, sh); }
-__device__ __forceinline__ double bmin(double v, double* sh) { return block_red<2>(v, sh); }
+
+// A cell's L-BFGS step runs on a thread-block cluster of CS CTAs (one CTA when
+// CS = 1).  Element e of the cell's vectors belongs to thread e mod (CS * T) of
+// the cluster in every loop; reductions combine the CTAs' block results through
+// distributed shared memory in rank order, so every thread of the cluster gets
+// the same value.
+template <int CS>
+__device__ __forceinline__ void phase_sync()
+{
+    if (CS == 1) __syncthreads();
+    else cooperative_groups::this_cluster().sync();
+}
+
+template <int CS, int OP>
+__device__ __forceinline__ double cred(double v, double* sh, double* slot)
+{
+    double b = block_red<OP>(v, sh);
+    if (CS == 1) return b;
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    if (threadIdx.x == 0) *slot = b;
+    cl.sync();
+    double r = *cl.map_shared_rank(slot, 0);
+#pragma unroll
+    for (int k = 1; k < CS; k++) {
+        const double t = *cl.map_shared_rank(slot, k);
+        r = OP == 0 ? r + t : (OP == 1 ? fmax(r, t) : fmin(r, t));
+    }
+    cl.sync();  // no CTA overwrites its slot before every CTA has read it
+    return r;
+}
 
 // x = x0 + a h over the cell; returns the largest squared displacement of a
 // site from its position at the last list build
-__device__ double set_trial(const Dev& d, const BatchView& B, int base, int nat, double a, double* sh)
+template <int CS>
+__device__ double set_trial(const Dev& d, const BatchView& B, int base, int nat, double a, double* sh, double* slot,
+                           int t0, int ts)
 {
     const int xd = d.x_dim;
     const double* x0 = B.x0 + (size_t)base * xd;
     const double* h = B.h + (size_t)base * xd;
     double dmax = 0.0;
-    __syncthreads();
-    for (int k = threadIdx.x; k < nat; k += blockDim.x) {
+    phase_sync<CS>();
+    for (int k = t0; k < nat; k += ts) {
         const int i = base + k;
         for (int q = 0; q < xd; q++) xset(d, i, q, x0[(size_t)k * xd + q] + a * h[(size_t)k * xd + q]);
         const double4 p = d.pos[i], p0 = B.pos0[i];
         const double dx = p.x - p0.x, dy = p.y - p0.y, dz = p.z - p0.z;
         dmax = fmax(dmax, dx * dx + dy * dy + dz * dz);
     }
-    return bmax(dmax, sh);
+    return cred<CS, 1>(dmax, sh, slot);
 }
 
 // One L-BFGS step of every running cell, after the force evaluation of its
 // current point (d.f, d.cell_E).  Min_LBFGS::run non-box branch
 // (min_l-bfgs.cpp:616-773) with LineSearch_BackTrack::line_min, DMD branch
 // (line_search.cpp:223-342), unrolled into phases.
-__global__ void k_lbfgs_step(Dev d, BatchView B, BatchParams P)
+template <int CS>
+__global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchParams P)
 {
     __shared__ double sh[32];
-    const int c = blockIdx.x;
+    __shared__ double slot_sh;
+    const int c = blockIdx.x / CS, rank = blockIdx.x % CS;
+    const int t0 = rank * blockDim.x + threadIdx.x, ts = CS * blockDim.x;
     CellState* S = B.st + c;
     const int phase = S->phase;
     if (phase == PH_DONE || phase == PH_PAUSED) return;
@@ -185,8 +219,8 @@ __global__ void k_lbfgs_step(Dev d, BatchView B, BatchParams P)
             const double E_prev = E_curr;
             E_curr = E_new;
             double fm = 0.0;
-            for (int e = threadIdx.x; e < n; e += blockDim.x) fm = fmax(fm, fabs(f[e]));
-            max_f = bmax(fm, sh);
+            for (int e = t0; e < n; e += ts) fm = fmax(fm, fabs(f[e]));
+            max_f = cred<CS, 1>(fm, sh, &slot_sh);
             if (E_prev - E_curr < P.energy_tol) code = kTolerance;
             else if (iter == P.max_iter) code = kMaxIter;
             else if (P.fmax_tol > 0.0 && max_f < P.fmax_tol) code = kTolerance;
@@ -202,15 +236,15 @@ __global__ void k_lbfgs_step(Dev d, BatchView B, BatchParams P)
                 double* sv = B.s + (size_t)slot * B.vstride + vb;
                 double* yv = B.y + (size_t)slot * B.vstride + vb;
                 double in1 = 0.0, in2 = 0.0;
-                for (int e = threadIdx.x; e < n; e += blockDim.x) {
+                for (int e = t0; e < n; e += ts) {
                     const double sv_e = alpha_m * h[e], yv_e = f[e] - f0[e];
                     sv[e] = sv_e;
                     yv[e] = yv_e;
                     in1 += sv_e * yv_e;
                     in2 += yv_e * yv_e;
                 }
-                in1 = bsum(in1, sh);
-                in2 = bsum(in2, sh);
+                in1 = cred<CS, 0>(in1, sh, &slot_sh);
+                in2 = cred<CS, 0>(in2, sh, &slot_sh);
                 ratio = -in1 / in2;
                 rho[slot] = 1.0 / in1;
                 iter++;
@@ -221,12 +255,12 @@ __global__ void k_lbfgs_step(Dev d, BatchView B, BatchParams P)
             halvings++;
             if (alpha_m <= ls_alpha_min || (P.max_halvings > 0 && halvings >= P.max_halvings)) {
                 // energy(0): back to x0, whose forces and energy are f0 and E_curr
-                __syncthreads();
-                for (int k = threadIdx.x; k < nat; k += blockDim.x)
+                phase_sync<CS>();
+                for (int k = t0; k < nat; k += ts)
                     for (int q = 0; q < xd; q++) xset(d, base + k, q, x0[(size_t)k * xd + q]);
-                for (int e = threadIdx.x; e < n; e += blockDim.x) f[e] = f0[e];
+                for (int e = t0; e < n; e += ts) f[e] = f0[e];
                 code = kAlphaMin;
-            } else if (set_trial(d, B, base, nat, alpha_m, sh) > P.skin_sq) {
+            } else if (set_trial<CS>(d, B, base, nat, alpha_m, sh, &slot_sh, t0, ts) > P.skin_sq) {
                 next = PH_PAUSED;
             }
         }
@@ -234,10 +268,10 @@ __global__ void k_lbfgs_step(Dev d, BatchView B, BatchParams P)
 
     if (new_dir) {
         // h = f, x_prev = x, f_prev = f, then the two-loop recursion
-        __syncthreads();
-        for (int k = threadIdx.x; k < nat; k += blockDim.x)
+        phase_sync<CS>();
+        for (int k = t0; k < nat; k += ts)
             for (int q = 0; q < xd; q++) x0[(size_t)k * xd + q] = xget(d, base + k, q);
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        for (int e = t0; e < n; e += ts) {
             h[e] = f[e];
             f0[e] = f[e];
         }
@@ -247,50 +281,50 @@ __global__ void k_lbfgs_step(Dev d, BatchView B, BatchParams P)
             const double* sv = B.s + (size_t)slot * B.vstride + vb;
             const double* yv = B.y + (size_t)slot * B.vstride + vb;
             double in = 0.0;
-            for (int e = threadIdx.x; e < n; e += blockDim.x) in += h[e] * sv[e];
-            al[i] = bsum(in, sh) * rho[slot];
-            for (int e = threadIdx.x; e < n; e += blockDim.x) h[e] -= al[i] * yv[e];
+            for (int e = t0; e < n; e += ts) in += h[e] * sv[e];
+            al[i] = cred<CS, 0>(in, sh, &slot_sh) * rho[slot];
+            for (int e = t0; e < n; e += ts) h[e] -= al[i] * yv[e];
         }
-        for (int e = threadIdx.x; e < n; e += blockDim.x) h[e] *= ratio;
+        for (int e = t0; e < n; e += ts) h[e] *= ratio;
         for (int i = 0; i < k_it; i++) {
             const int slot = (head + i) % P.m;
             const double* sv = B.s + (size_t)slot * B.vstride + vb;
             const double* yv = B.y + (size_t)slot * B.vstride + vb;
             double in = 0.0;
-            for (int e = threadIdx.x; e < n; e += blockDim.x) in += h[e] * yv[e];
-            const double be = bsum(in, sh) * rho[slot];
-            for (int e = threadIdx.x; e < n; e += blockDim.x) h[e] -= (be + al[i]) * sv[e];
+            for (int e = t0; e < n; e += ts) in += h[e] * yv[e];
+            const double be = cred<CS, 0>(in, sh, &slot_sh) * rho[slot];
+            for (int e = t0; e < n; e += ts) h[e] -= (be + al[i]) * sv[e];
         }
         // line_min: alpha_min from the smallest alpha coordinate, |h| = 1,
         // downhill test, first step min(1, max|h|)
         double mn = INFINITY;
-        for (int k = threadIdx.x; k < nat; k += blockDim.x)
+        for (int k = t0; k < nat; k += ts)
             for (int t = 0; t < nt; t++) mn = fmin(mn, d.alpha[(size_t)(base + k) * nt + t]);
-        mn = bmin(mn, sh) * 0.99;
+        mn = cred<CS, 2>(mn, sh, &slot_sh) * 0.99;
         ls_alpha_min = fmin(ls_alpha_min, mn);
         double hh = 0.0;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) hh += h[e] * h[e];
-        hh = 1.0 / sqrt(bsum(hh, sh));
+        for (int e = t0; e < n; e += ts) hh += h[e] * h[e];
+        hh = 1.0 / sqrt(cred<CS, 0>(hh, sh, &slot_sh));
         double fhl = 0.0, mh = 0.0;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        for (int e = t0; e < n; e += ts) {
             h[e] *= hh;
             fhl += f[e] * h[e];
             mh = fmax(mh, fabs(h[e]));
         }
-        fh = bsum(fhl, sh);
-        mh = bmax(mh, sh);
+        fh = cred<CS, 0>(fhl, sh, &slot_sh);
+        mh = cred<CS, 1>(mh, sh, &slot_sh);
         if (fh <= 0) code = kDownhill;
         else if (mh == 0) code = kGrad0;
         else {
             alpha_m = fmin(1.0, mh);
             halvings = 0;
             if (alpha_m <= ls_alpha_min) code = kAlphaMin;
-            else if (set_trial(d, B, base, nat, alpha_m, sh) > P.skin_sq) next = PH_PAUSED;
+            else if (set_trial<CS>(d, B, base, nat, alpha_m, sh, &slot_sh, t0, ts) > P.skin_sq) next = PH_PAUSED;
         }
     }
     if (code != kRunning) next = PH_DONE;
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    phase_sync<CS>();  // every CTA of the cluster has read the state before it changes
+    if (rank == 0 && threadIdx.x == 0) {
         S->phase = next;
         S->code = code;
         S->k_it = k_it;
@@ -405,21 +439,74 @@ __global__ void k_gather_cell(Dev s, GatherDst D, int cell, int obase, int gbase
 }
 
 // Probe for the autotuner: the reductions of a full two-loop step
-// (2m + 4 block dot products over the cell's vectors), nothing written but
+// (2m + 4 cluster dot products over the cell's vectors), nothing written but
 // one value per cell.
-__global__ void k_lbfgs_probe(Dev d, BatchView B, int m, double* out)
+template <int CS>
+__global__ void __launch_bounds__(1024) k_lbfgs_probe(Dev d, BatchView B, int m, double* out)
 {
     __shared__ double sh[32];
-    const int c = blockIdx.x, xd = d.x_dim, n = B.nat[c] * xd;
+    __shared__ double slot_sh;
+    const int c = blockIdx.x / CS, rank = blockIdx.x % CS;
+    const int t0 = rank * blockDim.x + threadIdx.x, ts = CS * blockDim.x;
+    const int xd = d.x_dim, n = B.nat[c] * xd;
     const size_t vb = (size_t)B.base[c] * xd;
     double acc = 0.0;
     for (int r = 0; r < 2 * m + 4; r++) {
         const double* a = (r < 2 * m ? (r & 1 ? B.y : B.s) + (size_t)(r >> 1) * B.vstride : B.h) + vb;
         double in = 0.0;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) in += a[e] * d.f[vb + e];
-        acc += bsum(in, sh);
+        for (int e = t0; e < n; e += ts) in += a[e] * d.f[vb + e];
+        acc += cred<CS, 0>(in, sh, &slot_sh);
     }
-    if (threadIdx.x == 0) out[c] = acc;
+    if (rank == 0 && threadIdx.x == 0) out[c] = acc;
+}
+
+// launch of a per-cell kernel on clusters of cs CTAs (cs = 1: plain launch)
+template <class... A>
+cudaError_t launch_cells(void (*kern)(A...), int cs, int ncells, int threads, cudaStream_t st, A... args)
+{
+    if (cs == 1) {
+        kern<<<ncells, threads, 0, st>>>(args...);
+        return cudaGetLastError();
+    }
+    if (cs > 8) cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(ncells * cs), 1, 1);
+    cfg.blockDim = dim3((unsigned)threads, 1, 1);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
+cudaError_t launch_step(int cs, int ncells, int threads, cudaStream_t st, const Dev& d, const BatchView& B,
+                        const BatchParams& P)
+{
+    switch (cs) {
+    case 1: return launch_cells(k_lbfgs_step<1>, 1, ncells, threads, st, d, B, P);
+    case 2: return launch_cells(k_lbfgs_step<2>, 2, ncells, threads, st, d, B, P);
+    case 4: return launch_cells(k_lbfgs_step<4>, 4, ncells, threads, st, d, B, P);
+    case 8: return launch_cells(k_lbfgs_step<8>, 8, ncells, threads, st, d, B, P);
+    case 16: return launch_cells(k_lbfgs_step<16>, 16, ncells, threads, st, d, B, P);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_probe(int cs, int ncells, int threads, cudaStream_t st, const Dev& d, const BatchView& B, int m,
+                         double* out)
+{
+    switch (cs) {
+    case 1: return launch_cells(k_lbfgs_probe<1>, 1, ncells, threads, st, d, B, m, out);
+    case 2: return launch_cells(k_lbfgs_probe<2>, 2, ncells, threads, st, d, B, m, out);
+    case 4: return launch_cells(k_lbfgs_probe<4>, 4, ncells, threads, st, d, B, m, out);
+    case 8: return launch_cells(k_lbfgs_probe<8>, 8, ncells, threads, st, d, B, m, out);
+    case 16: return launch_cells(k_lbfgs_probe<16>, 16, ncells, threads, st, d, B, m, out);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 // ---- host ------------------------------------------------------------------
@@ -528,7 +615,7 @@ struct mg_batch {
     DArr<int> budget;
     DArr<long long> iters;
     // launch shapes
-    int bps1 = 0, bps2 = 0, lbt = 256;
+    int bps1 = 0, bps2 = 0, lbt = 256, lcs = 1;  // pass grids, L-BFGS threads per CTA and CTAs per cell
     bool tuned = false, from_cache = false;
     double tune_ms = 0, build_ms = 0;
     // graph
@@ -726,8 +813,7 @@ int enqueue_iteration(mg_batch* b, cudaGraphConditionalHandle handle, bool with_
         else BCU(launch_dmd_force(d, 0, &rows, st, nullptr));
     }
     if (with_step) {
-        k_lbfgs_step<<<(unsigned)b->cells.size(), b->lbt, 0, st>>>(d, view(b), params(b));
-        BCU(cudaGetLastError());
+        BCU(launch_step(b->lcs, (int)b->cells.size(), b->lbt, st, d, view(b), params(b)));
         k_loop_test<<<1, 256, 0, st>>>(view(b), handle);
         BCU(cudaGetLastError());
     }
@@ -793,8 +879,9 @@ bool cache_lookup(mg_batch* b, const std::string& key, std::vector<int>& v)
         size_t tab = line.find('\t');
         if (tab == std::string::npos || line.compare(0, tab, key) != 0 || tab != key.size()) continue;
         std::istringstream is(line.substr(tab + 1));
-        std::vector<int> w(3);
+        std::vector<int> w(4, 1);
         if (is >> w[0] >> w[1] >> w[2]) {
+            if (!(is >> w[3])) w[3] = 1;
             v = w;
             g_tune_mem[key] = w;
             return true;
@@ -809,7 +896,7 @@ void cache_store(mg_batch* b, const std::string& key, const std::vector<int>& v)
     g_tune_mem[key] = v;
     if (b->cache_path.empty()) return;
     std::ofstream out(b->cache_path, std::ios::app);
-    out << key << '\t' << v[0] << ' ' << v[1] << ' ' << v[2] << '\n';
+    out << key << '\t' << v[0] << ' ' << v[1] << ' ' << v[2] << ' ' << v[3] << '\n';
 }
 
 // time `reps` force evaluations (all cells active) with the current shapes
@@ -831,15 +918,21 @@ int time_force(mg_batch* b, int reps, float* ms)
     return MG_OK;
 }
 
-int time_probe(mg_batch* b, int threads, int reps, float* ms)
+// time the probe at (threads, cs); a shape the device cannot launch (cluster
+// too large for a GPC) reports an infinite time
+int time_probe(mg_batch* b, int threads, int cs, int reps, float* ms)
 {
+    const int nc = (int)b->cells.size();
+    if (launch_probe(cs, nc, threads, b->st, b->bd, view(b), b->m, b->probe_out.p) != cudaSuccess) {
+        cudaGetLastError();
+        *ms = 1e30f;
+        return MG_OK;
+    }
     cudaEvent_t e0, e1;
     BCU(cudaEventCreate(&e0));
     BCU(cudaEventCreate(&e1));
-    const int nc = (int)b->cells.size();
-    k_lbfgs_probe<<<nc, threads, 0, b->st>>>(b->bd, view(b), b->m, b->probe_out.p);
     BCU(cudaEventRecord(e0, b->st));
-    for (int r = 0; r < reps; r++) k_lbfgs_probe<<<nc, threads, 0, b->st>>>(b->bd, view(b), b->m, b->probe_out.p);
+    for (int r = 0; r < reps; r++) BCU(launch_probe(cs, nc, threads, b->st, b->bd, view(b), b->m, b->probe_out.p));
     BCU(cudaEventRecord(e1, b->st));
     BCU(cudaEventSynchronize(e1));
     BCU(cudaEventElapsedTime(ms, e0, e1));
@@ -859,6 +952,7 @@ int autotune(mg_batch* b)
         b->bps1 = v[0];
         b->bps2 = v[1];
         b->lbt = v[2];
+        b->lcs = v[3];
         b->from_cache = true;
         b->tune_ms = 0;
         return MG_OK;
@@ -888,19 +982,22 @@ int autotune(mg_batch* b)
         }
     }
     b->bps2 = best2;
-    const int tc[] = {128, 256, 512, 1024};
+    // threads per CTA x CTAs per cell (a thread-block cluster)
+    const int tc[][2] = {{128, 1}, {256, 1}, {512, 1}, {1024, 1}, {512, 2}, {1024, 2}, {1024, 4}, {1024, 8}, {1024, 16}};
     best = 1e30f;
-    int bestt = 256;
-    for (int t : tc) {
-        BCHK(time_probe(b, t, 5, &ms));
+    int bestt = 256, bestc = 1;
+    for (const auto& t : tc) {
+        BCHK(time_probe(b, t[0], t[1], 5, &ms));
         if (ms < best) {
             best = ms;
-            bestt = t;
+            bestt = t[0];
+            bestc = t[1];
         }
     }
     b->lbt = bestt;
+    b->lcs = bestc;
     b->tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
-    cache_store(b, key, {b->bps1, b->bps2, b->lbt});
+    cache_store(b, key, {b->bps1, b->bps2, b->lbt, b->lcs});
     return MG_OK;
 }
 
@@ -1027,7 +1124,26 @@ int mg_batch_set_tuning(mg_batch* b, int autotune_on, const char* cache_path)
     if (!autotune_on) {
         b->bps1 = b->bps2 = 0;
         b->lbt = 256;
+        b->lcs = 1;
     }
+    destroy_graph(b);
+    return MG_OK;
+}
+
+int mg_batch_set_launch(mg_batch* b, int bps1, int bps2, int lbfgs_threads, int lbfgs_cluster)
+{
+    BCHK(check_batch(b));
+    const bool ok_t = lbfgs_threads >= 32 && lbfgs_threads <= 1024 && lbfgs_threads % 32 == 0;
+    const bool ok_c = lbfgs_cluster == 1 || lbfgs_cluster == 2 || lbfgs_cluster == 4 || lbfgs_cluster == 8 ||
+                      lbfgs_cluster == 16;
+    if (bps1 < 0 || bps2 < 0 || !ok_t || !ok_c)
+        return bfail(MG_ERR_ARG, "need bps >= 0, 32..1024 threads (multiple of 32), cluster 1, 2, 4, 8 or 16");
+    b->autotune = 0;
+    b->tuned = false;
+    b->bps1 = bps1;
+    b->bps2 = bps2;
+    b->lbt = lbfgs_threads;
+    b->lcs = lbfgs_cluster;
     destroy_graph(b);
     return MG_OK;
 }
@@ -1129,6 +1245,7 @@ int mg_batch_relax(mg_batch* b, mg_batch_stats* stats)
         stats->bps1 = b->bps1;
         stats->bps2 = b->bps2;
         stats->lbfgs_threads = b->lbt;
+        stats->lbfgs_cluster = b->lcs;
         stats->from_cache = b->from_cache ? 1 : 0;
     }
     return MG_OK;
@@ -1164,6 +1281,51 @@ int mg_batch_cell_result(mg_batch* b, int cell, double* x, double* f, mg_cell_re
         r->evaluations = s.nevals;
         r->natms = nat;
     }
+    return MG_OK;
+}
+
+int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings,
+                 int lbfgs_cluster, mg_cell_result* r, mg_batch_stats* stats)
+{
+    if (!s) return bfail(MG_ERR_ARG, "null mg_system");
+    int style = -1, nt = 0, xd = 0, form = 0;
+    double B[9], H[9];
+    system_shape(s, &style, &nt, &xd, &form, B);
+    system_box(s, H);
+    const int natms = system_natms(s);
+    if (natms < 1) return bfail(MG_ERR_STATE, "mg_min_lbfgs needs an initialised system with sites");
+    if (form != MG_FORM_FP64 && form != MG_FORM_FP32)
+        return bfail(MG_ERR_UNSUPPORTED, "mg_min_lbfgs runs the FP64 or FP32 force passes");
+    // the current state as one cell: fractional positions (x2s) and alpha, c
+    std::vector<double> x((size_t)natms * xd), xs((size_t)natms * xd), c((size_t)natms * nt);
+    BCHK(mg_atoms_get_x(s, x.data()));
+    BCU(cudaMemcpy(c.data(), system_dev(s).c, c.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < natms; k++) {
+        x2s_host(B, x.data() + (size_t)k * xd, xs.data() + (size_t)k * xd);
+        for (int t = 0; t < nt; t++) xs[(size_t)k * xd + 3 + t] = x[(size_t)k * xd + 3 + t];
+    }
+    mg_batch* b = nullptr;
+    BCHK(mg_batch_create(s, &b));
+    struct Guard {
+        mg_batch* b;
+        ~Guard() { mg_batch_destroy(b); }
+    } guard{b};
+    BCHK(mg_batch_add_cell(b, natms, H, xs.data(), c.data(), nullptr));
+    BCHK(mg_batch_set_params(b, m, max_iter, fmax_tol, energy_tol, max_halvings));
+    BCHK(mg_batch_set_form(b, form));
+    if (lbfgs_cluster > 0) BCHK(mg_batch_set_launch(b, 0, 0, 1024, lbfgs_cluster));
+    else BCHK(mg_batch_set_tuning(b, 1, nullptr));
+    BCHK(mg_batch_relax(b, stats));
+    mg_cell_result res;
+    BCHK(mg_batch_cell_result(b, 0, x.data(), nullptr, &res));
+    if (r) *r = res;
+    // the system takes the final state (ghosts and lists rebuilt from it)
+    for (int k = 0; k < natms; k++) {
+        x2s_host(B, x.data() + (size_t)k * xd, xs.data() + (size_t)k * xd);
+        for (int t = 0; t < nt; t++) xs[(size_t)k * xd + 3 + t] = x[(size_t)k * xd + 3 + t];
+    }
+    BCHK(mg_atoms_set(s, natms, xs.data(), nullptr, c.data()));
+    BCHK(mg_ff_init(s));
     return MG_OK;
 }
 

@@ -210,5 +210,7 @@ cudaStream_t system_stream(mg_system* s);
 int system_device(mg_system* s);
 void system_shape(mg_system* s, int* style, int* nt, int* x_dim, int* form, double* B_out);
 double system_skin(mg_system* s);
+void system_box(mg_system* s, double* H_out);
+int system_natms(mg_system* s);
 
 }  // namespace mg

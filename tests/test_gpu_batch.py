@@ -131,3 +131,66 @@ def test_batch_fp32_form_and_tuning_cache(tmp_path):
     # agree with the FP64 ones to a few meV per cell
     assert np.all(np.abs(e32 - e64) / n < 1e-3)
     assert all(r["code"] in (1, 3, 4, 5) for r in results[mb.MG_FORM_FP32])
+
+
+@pytest.mark.parametrize("threads,cluster", [(128, 2), (128, 4), (64, 16)])
+def test_batch_cluster_steps_match_oracle(threads, cluster):
+    """The L-BFGS step of a cell spread over a thread-block cluster (CTAs
+    share the cell's vectors, reductions through distributed shared memory)
+    follows the same trajectories."""
+    mb = _mb()
+    b0 = _builder(mb)
+    cells = _cells()
+    B = mb.Batch(b0)
+    for c in cells:
+        B.add_cell(c)
+    B.set_params(5, 200, 1e-5, 1e-8, 60)
+    B.set_launch(0, 0, threads, cluster)
+    st = B.relax()
+    assert st["lbfgs_cluster"] == cluster and st["lbfgs_threads"] == threads
+    for k, c in enumerate(cells):
+        x, f, r = B.cell_result(k)
+        ro, fo = _oracle_run(c, 200, 1e-5, 1e-8, 60)
+        e_ref = ro["energies"][-1]
+        assert r["code"] == ro["code"] or {r["code"], ro["code"]} <= {3, 5}, (k, r, ro["code"])
+        assert r["iterations"] == ro["line_searches"] - 1
+        assert abs(r["energy"] - e_ref) <= 1e-12 * abs(e_ref)
+        assert np.max(np.abs(x - ro["x"])) <= 1e-9
+
+
+def test_min_lbfgs_single_system_matches_oracle(tmp_path):
+    """mg_min_lbfgs: the system relaxes itself on the device (one cell, its
+    step on a 16-CTA cluster) and holds the final state afterwards."""
+    mb = _mb()
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=6, sigma=0.03, style="DMD_I")
+    s = mb.system_from_workload(w)
+    r, st = s.min_lbfgs(5, 60, 1e-5, 1e-8, 60, cluster=16)
+    assert st["lbfgs_cluster"] == 16
+    o = Oracle(w)
+    ro = o.lbfgs(5, 60, 1e-8, fmax_tol=1e-5, max_halvings=60, ls_force_energy=True)
+    e_ref = ro["energies"][-1]
+    assert r["code"] == ro["code"] or {r["code"], ro["code"]} <= {3, 5}
+    assert r["iterations"] == ro["line_searches"] - 1
+    assert abs(r["energy"] - e_ref) <= 1e-12 * abs(e_ref)
+    # the system now holds the relaxed state (positions wrapped into the box,
+    # as a list rebuild does): equal up to box vectors
+    L = w["cfg"].L
+    x = s.get_x()
+    dx = x - ro["x"]
+    dx[:, :3] -= L * np.round(dx[:, :3] / L)
+    assert np.max(np.abs(dx)) <= 1e-9
+    # Its own force call agrees with the oracle rebuilt at that state.  (Not
+    # with the oracle's last step: for two species the reference's pair energy
+    # takes the cross-species phi with alpha_i[a], alpha_j[b] for the order the
+    # half list names the pair in, so re-wrapping sites changes the energy.)
+    o2 = Oracle(w)
+    far = x.copy()
+    far[:, :3] += 0.9  # beyond the skin: update_0 rebuilds, then the state itself
+    o2.update_x(far)
+    o2.update_x(x)
+    f, en = s.force_calc(1)
+    fo, eno = o2.force(1)
+    assert abs(en[0] - eno[0]) <= 1e-10 * abs(eno[0])
+    assert np.max(np.abs(f - fo)) <= 1e-9 * np.max(np.abs(fo))
