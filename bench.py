@@ -362,6 +362,67 @@ def run_batched(mb, fx, device, ncells=512):
     return out
 
 
+def run_large_forms(mb, fx, device, mlp_source):
+    """The precision form on FCC 40^3 = 256000 sites and the learned form on
+    FCC 50^3 = 500000 sites (same distributions as the 32000-site system),
+    each against the plain FP64 form on the same system: time per force call
+    (L2 flushed before each), max|dF|, |dE|/site and, for the precision form,
+    max|d mu| of the chemical potentials after c_d_calc.  The learned form
+    reuses the network trained on the 32000-site system (same tables)."""
+    import torch
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    out = {}
+
+    def timed(s, steps, f):
+        t = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            _, en = s.force_calc(1, f=f)
+            t += s.last_time("force")
+        return t / steps, en
+
+    for n, forms in ((40, ("fp32",)), (50, ("mlp",))):
+        d = tempfile.mkdtemp(prefix=f"mapp_bench_{n}_")
+        w = fx.write_workload(d, "dmd", n=n, a=WORKLOAD["a"], sigma=WORKLOAD["sigma"], style="DMD_I")
+        s = mb.system_from_workload(w, device=device)
+        natms = s.natms
+        f64 = torch.zeros((natms, s.x_dim), dtype=torch.float64, device="cuda")
+        s.force_calc(1, f=f64)
+        t64, en64 = timed(s, 10, f64)
+        s.create_2nd_neigh_lst()
+        s.c_d_calc()
+        mu64 = s.vector("n")
+        for form in forms:
+            if form == "mlp":
+                s.mlp_init(1.8, 5.0, 0.05, 0.20, seed=5)
+                par, scal = mlp_source.mlp_state()
+                s.mlp_state(params=par, scaling=scal)
+                s.set_form(mb.MG_FORM_MLP)
+            else:
+                s.set_form(mb.MG_FORM_FP32)
+            fx_ = torch.zeros_like(f64)
+            s.force_calc(1, f=fx_)
+            tf, enf = timed(s, 10, fx_)
+            rec = {"sites": natms, "ms_per_force_call": tf, "fp64_ms_per_force_call": t64,
+                   "site_force_evals_per_s": natms / (tf * 1e-3), "speedup_vs_fp64": t64 / tf,
+                   "max_abs_dF_eV_per_A": float((fx_ - f64).abs().max().item()),
+                   "abs_dE_per_site_eV": abs(float(enf[0]) - float(en64[0])) / natms}
+            if form == "fp32":
+                s.create_2nd_neigh_lst()
+                s.c_d_calc()
+                rec["max_abs_dmu"] = float(np.max(np.abs(s.vector("n") - mu64)))
+            else:
+                audit, counts = s.mlp_audit()
+                rec["audited_rows"] = int(counts[0])
+                rec["fallback_rows"] = int(counts[1])
+            out[f"{form}_{natms}_sites"] = rec
+            s.set_form(mb.MG_FORM_FP64)
+        s.close()
+    return out
+
+
 def run_single_lbfgs(mb, w, device):
     """Device-resident L-BFGS of the 32000-site system itself (mg_min_lbfgs;
     m = 5, max|f| < 1e-5, energy tolerance 1e-8, 60 halvings, at most 200
@@ -447,6 +508,7 @@ def run_ours(args):
     if not args.skip_forms:
         forms["batched"] = run_batched(mb, fx, local)
         forms["single_lbfgs"] = run_single_lbfgs(mb, w, local)
+        forms["large"] = run_large_forms(mb, fx, local, s)
     s.set_form(form_id)
 
     # end to end through the C ABI with host buffers, timed with CUDA events on
