@@ -11,13 +11,13 @@ constexpr double kPiInSq = 0.564189583547756286948079451561;  // 1/sqrt(pi)
 
 __device__ __forceinline__ int owner(const Dev& d, int j) { return j < d.natms ? j : d.root[j]; }
 
-// c0..c3 of one spline knot (rows of 8 doubles, 64-byte aligned) as two
-// read-only 16-byte loads
+// c0..c3 of one spline knot (rows of 8 doubles, 64-byte aligned) as one
+// read-only 32-byte load (one sector, one request per lane)
 __device__ __forceinline__ double4 knot4(const double* __restrict__ row)
 {
-    double2 lo = __ldg(reinterpret_cast<const double2*>(row));
-    double2 hi = __ldg(reinterpret_cast<const double2*>(row) + 1);
-    return make_double4(lo.x, lo.y, hi.x, hi.y);
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(row));
+    return r;
 }
 
 template <int NT>
