@@ -245,65 +245,69 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass2(Dev d, int 
 }
 
 // ---- energy_calc pass (ff_dmd_I.cpp:489-633): species pairs b >= a only --
+// One thread per compact pair like force pass 1, values only (no derivatives,
+// nothing stored per pair); the arithmetic of a pair is the reference's
+// (r = sqrt(rsq), r_inv = 1 / r).
 template <int NT, int NQ>
-__global__ void __launch_bounds__(kFFBlock) k_dmd_energy_pass(Dev d, int row0)
+__global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_energy_pass(Dev d, int row0)
 {
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (i < d.natms) {
-        double4 xi = d.pos[i];
-        double ai[NT], ci[NT], Ei[NT];
+    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < d.npairs; base += stride) {
+        const long long p = base + lane;
+        const bool valid = p < d.npairs;
+        const int i = valid ? d.pair_i[p] : -1;
+        double Ei[NT];
 #pragma unroll
-        for (int a = 0; a < NT; a++) {
-            ai[a] = d.alpha[(size_t)i * NT + a];
-            ci[a] = d.c[(size_t)i * NT + a];
-            Ei[a] = 0.0;
-        }
-        int nn = d.nnb[i];
-        for (int k = lane; k < nn; k += 32) {
-            long long slot = (long long)i * d.maxnb + k;
-            int j = d.nbr[slot];
-            double4 xj = d.pos[j];
-            double aj[NT], cj[NT], Ej[NT];
+        for (int a = 0; a < NT; a++) Ei[a] = 0.0;
+        if (valid) {
+            const int j = d.pair_j[p];
+            const double4 xi = d.pos[i], xj = d.pos[j];
+            const double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
+            const double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
+            if (rsq < d.cut_sq_mod) {
+                double ai[NT], ci[NT], aj[NT], cj[NT], Ej[NT];
 #pragma unroll
-            for (int b = 0; b < NT; b++) {
-                aj[b] = d.alpha[(size_t)j * NT + b];
-                cj[b] = d.c[(size_t)j * NT + b];
-                Ej[b] = 0.0;
-            }
-            double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
-            double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
-            if (!(rsq < d.cut_sq_mod)) continue;
-            bool own_j = j < d.natms;
-            double r = sqrt(rsq);
-            double r_inv = 1.0 / r;
-            double w = own_j ? 0.5 : 0.25;
-#pragma unroll
-            for (int a = 0; a < NT; a++)
-#pragma unroll
-                for (int b = a; b < NT; b++) {
-                    const int rs = b * NT + a, ps = comp_idx(a, b);
-                    double alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
-                    double g0 = 0, f0 = 0, u0, u1, u2, u3;
-                    bool hit = (a == b) ? smear<true, false, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3)
-                                        : smear<false, false, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3);
-                    if (hit) {
-                        Ei[a] += g0 * cj[b];
-                        Ej[b] += g0 * ci[a];
-                        if (a == b) acc[0] += w * (cj[b] * ci[a] + cj[a] * ci[b]) * f0;
-                    }
+                for (int a = 0; a < NT; a++) {
+                    ai[a] = d.alpha[(size_t)i * NT + a];
+                    ci[a] = d.c[(size_t)i * NT + a];
+                    aj[a] = d.alpha[(size_t)j * NT + a];
+                    cj[a] = d.c[(size_t)j * NT + a];
+                    Ej[a] = 0.0;
                 }
-            if (own_j) {
+                const bool own_j = j < d.natms;
+                const double r = sqrt(rsq);
+                const double r_inv = 1.0 / r;
+                const double w = own_j ? 0.5 : 0.25;
 #pragma unroll
-                for (int b = 0; b < NT; b++)
-                    if (Ej[b] != 0.0) atomicAdd(&d.E[(size_t)j * NT + b], Ej[b]);
+                for (int a = 0; a < NT; a++)
+#pragma unroll
+                    for (int b = a; b < NT; b++) {
+                        const int rs = b * NT + a, ps = comp_idx(a, b);
+                        const double alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
+                        double g0 = 0, f0 = 0, u0, u1, u2, u3;
+                        const bool hit =
+                            (a == b) ? smear<true, false, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3)
+                                     : smear<false, false, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, u0, u1, f0, u2, u3);
+                        if (hit) {
+                            Ei[a] += g0 * cj[b];
+                            Ej[b] += g0 * ci[a];
+                            if (a == b) acc[0] += w * (cj[b] * ci[a] + cj[a] * ci[b]) * f0;
+                        }
+                    }
+                if (own_j) {
+#pragma unroll
+                    for (int b = 0; b < NT; b++)
+                        if (Ej[b] != 0.0) atomicAdd(&d.E[(size_t)j * NT + b], Ej[b]);
+                }
             }
         }
+        const Seg sg = seg_of(i);
 #pragma unroll
         for (int a = 0; a < NT; a++) {
-            double s = warp_sum(Ei[a]);
-            if (lane == 0) atomicAdd(&d.E[(size_t)i * NT + a], s);
+            const double t = seg_sum(Ei[a], sg);
+            if (valid && lane == sg.first && t != 0.0) atomicAdd(&d.E[(size_t)i * NT + a], t);
         }
     }
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
@@ -814,7 +818,7 @@ cudaError_t dmd_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, cud
 template <int NT>
 cudaError_t dmd_energy_nt(const Dev& d, int* nb, cudaStream_t st)
 {
-    int g1 = div_up((long long)d.natms * 32, kFFBlock), g2 = div_up(d.natms, kFFBlock);
+    int g1 = persistent_grid(d.npairs, MG_DMD_MINB), g2 = div_up(d.natms, kFFBlock);
     if (d.nq == 3) k_dmd_energy_pass<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
     else k_dmd_energy_pass<NT, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
     k_dmd_embed<NT><<<g2, kFFBlock, 0, st>>>(d, 0, g1);
