@@ -273,6 +273,25 @@ int mg_batch_relax(mg_batch* b, mg_batch_stats* stats);
    alpha, f the same shape; either may be NULL */
 int mg_batch_cell_result(mg_batch* b, int cell, double* x, double* f, mg_cell_result* r);
 
+/* ---- configuration files ------------------------------------------------ */
+/* ReadCFG (read_cfg.cpp:225-700): standard or extended CFG files as the
+   reference reads them -- header keys, H0 x Transform x basic length turned
+   into the lower-triangular H of Atoms::H, fractional positions wrapped into
+   [0, 1), species in the order of their mass / name lines, MD velocities (each
+   times R twice and in the frame of the file's box, as the reference converts
+   them), DMD rows (s, alpha per species, c per species; dmd != 0, extended
+   format only).  eta(i,j) strains are rejected (MG_ERR_UNSUPPORTED).  Host
+   code; pass the results to mg_atoms_set_types / _set_box / _set. */
+typedef struct mg_cfg mg_cfg;
+int mg_cfg_read(const char* path, int dmd, mg_cfg** out);
+int mg_cfg_info(const mg_cfg* c, int* natms, int* ntypes, double* H, int* has_velocity);
+/* names: ntypes slots of name_len chars each; masses: ntypes doubles */
+int mg_cfg_types(const mg_cfg* c, char* names, int name_len, double* masses);
+/* x_frac natms * 3 (MD) or natms * (3 + nt) (DMD), type natms (MD), conc
+   natms * nt (DMD), velocity natms * 3 (MD); any may be NULL */
+int mg_cfg_atoms(const mg_cfg* c, double* x_frac, int* type, double* conc, double* velocity);
+int mg_cfg_free(mg_cfg* c);
+
 /* ---- device-resident minimiser for one system ---------------------------- */
 /* Min_LBFGS::run with LineSearch_BackTrack::line_min (min_l-bfgs.cpp:616-773,
    line_search.cpp:223-342) for the system itself, on the GPU: the same

@@ -76,6 +76,11 @@ SIGNATURES = {
     "mg_batch_relax": (C.c_int, [_P, _P]),
     "mg_batch_cell_result": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mg_min_lbfgs": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _P, _P]),
+    "mg_cfg_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "mg_cfg_info": (C.c_int, [_P, _I, _I, _P, _I]),
+    "mg_cfg_types": (C.c_int, [_P, _P, C.c_int, _P]),
+    "mg_cfg_atoms": (C.c_int, [_P, _P, _P, _P, _P]),
+    "mg_cfg_free": (C.c_int, [_P]),
 }
 
 
@@ -420,6 +425,40 @@ class Batch:
         r = CellResult()
         _check(load_library().mg_batch_cell_result(self.h, cell, x.ctypes.data, f.ctypes.data, C.byref(r)))
         return x, f, {k: getattr(r, k) for k, _ in CellResult._fields_}
+
+
+def read_cfg(path: str, dmd: bool = False) -> dict:
+    """A CFG file as the reference reads it (mg_cfg_*): dict(names, masses, H
+    (lower triangular), s (natms x 3, wrapped), and type + v (MD) or alpha + c
+    (DMD))."""
+    L = load_library()
+    h = C.c_void_p()
+    _check(L.mg_cfg_read(str(path).encode(), int(dmd), C.byref(h)))
+    try:
+        n, nty, hv = C.c_int(), C.c_int(), C.c_int()
+        H = np.zeros(9)
+        _check(L.mg_cfg_info(h, C.byref(n), C.byref(nty), H.ctypes.data, C.byref(hv)))
+        names = C.create_string_buffer(64 * max(nty.value, 1))
+        masses = np.zeros(max(nty.value, 1))
+        _check(L.mg_cfg_types(h, names, 64, masses.ctypes.data))
+        N = n.value
+        out = {"names": [names.raw[64 * k:64 * (k + 1)].split(b"\0")[0].decode() for k in range(nty.value)],
+               "masses": masses[: nty.value].tolist(), "H": H.reshape(3, 3), "has_velocity": bool(hv.value)}
+        if dmd:
+            nt = nty.value
+            x = np.zeros((N, 3 + nt))
+            c = np.zeros((N, nt))
+            _check(L.mg_cfg_atoms(h, x.ctypes.data, None, c.ctypes.data, None))
+            out.update(s=x[:, :3].copy(), alpha=x[:, 3:].copy(), c=c)
+        else:
+            x = np.zeros((N, 3))
+            t = np.zeros(N, dtype=np.int32)
+            v = np.zeros((N, 3))
+            _check(L.mg_cfg_atoms(h, x.ctypes.data, t.ctypes.data, None, v.ctypes.data))
+            out.update(s=x, type=t, v=v)
+        return out
+    finally:
+        L.mg_cfg_free(h)
 
 
 def system_from_workload(w: dict, device: int = 0, skin: float = 0.5) -> System:

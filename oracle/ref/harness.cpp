@@ -293,6 +293,10 @@ void dump_state(const std::string& prefix)
     int natms = atoms->natms, nph = atoms->natms_ph;
     double* x = vec<double>("x");
     write_raw(prefix + ".x.bin", x, sizeof(double) * (size_t)(natms + nph) * H.x_dim);
+    if (atoms->find_exist("x_d") >= 0) {  // MD velocities as read from the CFG
+        double* xd = vec<double>("x_d");
+        write_raw(prefix + ".xd.bin", xd, sizeof(double) * (size_t)natms * 3);
+    }
     if (!H.dmd) {
         int* type = vec<int>("type");
         write_raw(prefix + ".type.bin", type, sizeof(int) * (size_t)(natms + nph));
