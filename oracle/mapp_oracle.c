@@ -13,6 +13,8 @@
  *   DMD_I / DMD_II / DMD  force_calc / energy_calc / create_2nd_neigh_lst /
  *           c_d_calc / calc_g / interpolate_m (ff_dmd_I.cpp:88-668,1760-2674;
  *           ff_dmd_II.cpp:2151-2630; ff_dmd.cpp:2221-2606)
+ *   callers Min_LBFGS + LineSearch_BackTrack (min_l-bfgs.cpp, line_search.cpp)
+ *           and MD_NH without a barostat (md_nh.cpp, rand_engine.cpp)
  *
  * so that, compiled with -ffp-contract=off like the reference, it reproduces
  * the reference's doubles bit for bit (pinned by tests against the compiled
@@ -45,6 +47,7 @@
 #define COMP(i, j) ((i) < (j) ? ((j) + 1) * (j) / 2 + (i) : ((i) + 1) * (i) / 2 + (j))
 #define MINV(a, b) ((a) < (b) ? (a) : (b))
 #define MAXV(a, b) ((a) > (b) ? (a) : (b))
+#define ORC_MAX_CHAIN 16
 #define PI_IN_SQ 0.564189583547756286948079451561
 
 typedef struct {
@@ -667,11 +670,10 @@ int orc_init(orc_t* o)
     return 0;
 }
 
-/* Atoms::update_0(0,1,list), atoms.cpp:1780-1865, with owned x replaced first */
-int orc_update_x(orc_t* o, const double* x, int* rebuilt)
+/* Atoms::update_0(0,1,list), atoms.cpp:1780-1865, on the owned x in place */
+static int update_0(orc_t* o)
 {
     int xd = o->x_dim;
-    memcpy(o->x, x, sizeof(double) * o->natms * xd);
     double sq_skin = o->skin * o->skin;
     int check = 0;
     for (int i = 0; i < o->natms && check == 0; i++) {
@@ -691,6 +693,14 @@ int orc_update_x(orc_t* o, const double* x, int* rebuilt)
     } else {
         refresh_x(o);
     }
+    return check;
+}
+
+/* owned x replaced, then update_0 */
+int orc_update_x(orc_t* o, const double* x, int* rebuilt)
+{
+    memcpy(o->x, x, sizeof(double) * o->natms * o->x_dim);
+    int check = update_0(o);
     if (rebuilt) *rebuilt = check;
     return 0;
 }
@@ -1897,4 +1907,219 @@ int orc_lbfgs(orc_t* o, int m, int max_iter, double energy_tol, double fmax_tol,
     if (nevals_out) *nevals_out = nevals;
     free(f); free(h); free(x0); free(f0); free(xw); free(fw); free(sv); free(yv); free(s_list); free(rho); free(alpha);
     return nls;
+}
+
+/* ---------------------------------------------------------------------------
+ * Nose-Hoover NVT molecular dynamics, MD_NH without a barostat (chk_stress 0)
+ * and without a "dof" vector (md_nh.cpp).
+ * ------------------------------------------------------------------------- */
+
+/* Random (rand_engine.cpp:35-74): Park-Miller minimal standard generator by
+   Schrage's factorisation, and the polar Gaussian that caches its second value */
+typedef struct {
+    int seed, gauss_chk;
+    double reserved;
+} orc_rng_t;
+
+static double rng_uniform(orc_rng_t* r)
+{
+    int first = r->seed / 127773, second = r->seed % 127773;
+    int rnd = 16807 * second - 2836 * first;
+    r->seed = rnd > 0 ? rnd : rnd + 2147483647;
+    return r->seed * 1.0 / 2147483647;
+}
+
+static double rng_gaussian(orc_rng_t* r)
+{
+    if (r->gauss_chk == 0) {
+        double u = 0.0, v = 0.0, s = 1.0;
+        while (s >= 1.0) {
+            u = 2.0 * rng_uniform(r) - 1.0;
+            v = 2.0 * rng_uniform(r) - 1.0;
+            s = u * u + v * v;
+        }
+        double q = sqrt(-2.0 * log(s) / s);
+        r->gauss_chk = 1;
+        r->reserved = v * q;
+        return u * q;
+    }
+    r->gauss_chk = 0;
+    return r->reserved;
+}
+
+typedef struct {
+    int no_dof, no_it, no_ch;
+    double boltz, t_tar, t_freq, ke_tar, ke_cur, t_cur, ke_curr[6];
+    double eta_m[ORC_MAX_CHAIN], eta_d[ORC_MAX_CHAIN], eta_dd[ORC_MAX_CHAIN];
+} orc_nh_t;
+
+/* the kinetic-energy tensor sums of update_x_d / init_vel / create_vel
+   (md_nh.cpp:939-960, 1246-1265, 1315-1328) */
+static void nh_ke(orc_t* o, orc_nh_t* nh, const double* mass, const double* xd)
+{
+    double t[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < o->natms; i++) {
+        double m = mass[o->type[i]];
+        const double* v = xd + 3 * i;
+        t[0] += m * v[0] * v[0];
+        t[1] += m * v[1] * v[1];
+        t[2] += m * v[2] * v[2];
+        t[3] += m * v[1] * v[2];
+        t[4] += m * v[0] * v[2];
+        t[5] += m * v[0] * v[1];
+    }
+    for (int k = 0; k < 6; k++) nh->ke_curr[k] = t[k];
+    nh->ke_cur = nh->ke_curr[0] + nh->ke_curr[1] + nh->ke_curr[2];
+    nh->t_cur = nh->ke_cur / (nh->boltz * nh->no_dof);
+}
+
+/* MD_NH::update_x_d (md_nh.cpp:903-961), no dof vector */
+static void nh_update_x_d(orc_t* o, orc_nh_t* nh, const double* mass, double* xd, const double* f, double dlt)
+{
+    for (int i = 0; i < o->natms; i++) {
+        double m = mass[o->type[i]];
+        for (int k = 0; k < 3; k++) xd[3 * i + k] += f[3 * i + k] * dlt / m;
+    }
+    nh_ke(o, nh, mass, xd);
+}
+
+/* MD_NH::update_NH_T (md_nh.cpp:965-1035) */
+static void nh_update_T(orc_t* o, orc_nh_t* nh, double* xd, double dlt)
+{
+    int nc = nh->no_ch;
+    double* em = nh->eta_m;
+    double* ed = nh->eta_d;
+    double* edd = nh->eta_dd;
+    for (int i = 0; i < nc; i++) em[i] = nh->boltz * nh->t_tar / (nh->t_freq * nh->t_freq);
+    em[0] *= nh->no_dof;
+    double dltm = dlt * (1.0 / nh->no_it), dltm2 = 0.5 * dltm, dltm4 = 0.25 * dltm, velfac = 1.0, exfac;
+    edd[0] = (nh->ke_cur - nh->ke_tar) / em[0];
+    for (int it = 0; it < nh->no_it; it++) {
+        exfac = 1.0;
+        for (int ich = nc - 1; ich > -1; ich--) {
+            ed[ich] *= exfac;
+            ed[ich] += edd[ich] * dltm2;
+            ed[ich] *= exfac;
+            exfac = exp(-dltm4 * ed[ich]);
+        }
+        exfac = exp(-dltm * ed[0]);
+        velfac *= exfac;
+        nh->t_cur *= exfac * exfac;
+        nh->ke_cur *= exfac * exfac;
+        for (int k = 0; k < 6; k++) nh->ke_curr[k] *= exfac * exfac;
+        exfac = exp(-dltm4 * ed[1]);
+        ed[0] *= exfac;
+        edd[0] = (nh->ke_cur - nh->ke_tar) / em[0];
+        ed[0] += edd[0] * dltm2;
+        ed[0] *= exfac;
+        for (int ich = 1; ich < nc; ich++) {
+            exfac = ich == nc - 1 ? 1.0 : exp(-dltm4 * ed[ich + 1]);
+            ed[ich] *= exfac;
+            edd[ich] = (em[ich - 1] * ed[ich - 1] * ed[ich - 1] - nh->boltz * nh->t_tar) / em[ich];
+            ed[ich] += edd[ich] * dltm2;
+            ed[ich] *= exfac;
+        }
+    }
+    for (int i = 0; i < o->natms; i++)
+        for (int k = 0; k < 3; k++) xd[3 * i + k] *= velfac;
+}
+
+/* MD_NH::update_x without a barostat (md_nh.cpp:865-898): drift, then remove
+   the mean displacement of the step */
+static void nh_update_x(orc_t* o, const double* xd, double dlt)
+{
+    double ave[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < o->natms; i++)
+        for (int k = 0; k < 3; k++) {
+            o->x[(size_t)i * 3 + k] += xd[3 * i + k] * dlt;
+            ave[k] += xd[3 * i + k] * dlt;
+        }
+    for (int k = 0; k < 3; k++) ave[k] *= 1.0 / (o->natms);
+    for (int i = 0; i < o->natms; i++)
+        for (int k = 0; k < 3; k++) o->x[(size_t)i * 3 + k] -= ave[k];
+}
+
+/*
+ * MD_NH "md nh nvt temp t_tar t_period eta_iteration no_it eta_chains no_ch
+ * [create_vel seed]" with time_step dt and boltzmann boltz, then run nsteps:
+ * MD_NH::init (md_nh.cpp:385-567) after the set-up of orc_init, and
+ * MD_NH::run's non-barostat loop (md_nh.cpp:636-677).
+ *
+ * xd [natms][3]: in, the initial velocities (seed <= 0: rescaled to t_tar as
+ * init_vel does, md_nh.cpp:1296-1341); ignored with seed > 0 (create_vel,
+ * md_nh.cpp:1211-1280); out, the velocities after the run.
+ * MD_NH::init never stores x_0 (only the minimisers and clocks call
+ * Atoms::store_0), so the first skin check of the run compares against the
+ * x_0 the reader left; it is taken as zero here, which makes the first step
+ * rebuild the ghosts and the list.
+ * thermo (9 + no_ch doubles): energy and the six virial components of the
+ * last step's force_calc(1), ke_cur and t_cur after the last update_NH_T,
+ * then the chain velocities eta_d.
+ * Returns 0, or -1 when the initial velocities are all zero (the reference
+ * aborts) or no_ch / no_it are out of range.
+ */
+int orc_md_nh(orc_t* o, const double* mass, double t_tar, double t_period, int no_it, int no_ch, double dt,
+              double boltz, int seed, double* xd, int nsteps, double* thermo)
+{
+    if (o->dmd || no_ch < 3 || no_ch > ORC_MAX_CHAIN || no_it < 1) return -1;
+    orc_nh_t nh;
+    memset(&nh, 0, sizeof(nh));
+    nh.no_it = no_it;
+    nh.no_ch = no_ch;
+    nh.boltz = boltz;
+    nh.t_tar = t_tar;
+    nh.t_freq = 1.0 / t_period;
+    nh.no_dof = o->natms * 3 - 3;
+    nh.ke_tar = t_tar * boltz * nh.no_dof;
+    double dt2 = 0.5 * dt;
+    int natms = o->natms;
+    if (seed > 0) {
+        orc_rng_t r = {seed, 0, 0.0};
+        for (int i = 0; i < natms; i++)
+            for (int k = 0; k < 3; k++) xd[3 * i + k] = rng_gaussian(&r) / (sqrt(mass[o->type[i]]));
+        nh_ke(o, &nh, mass, xd);
+        double ke_des = (boltz * nh.no_dof) * t_tar;
+        double factor = sqrt(ke_des / nh.ke_cur), facsq = ke_des / nh.ke_cur;
+        for (int i = 0; i < 3 * natms; i++) xd[i] *= factor;
+        for (int k = 0; k < 6; k++) nh.ke_curr[k] *= facsq;
+        nh.ke_cur *= facsq;
+        nh.t_cur *= facsq;
+    } else {
+        nh_ke(o, &nh, mass, xd);
+        if (nh.ke_cur == 0) return -1;
+        double ke_des = (boltz * nh.no_dof) * t_tar;
+        double factor = sqrt(ke_des / nh.ke_cur), facsq = factor * factor;
+        for (int i = 0; i < 3 * natms; i++) xd[i] *= factor;
+        for (int k = 0; k < 6; k++) nh.ke_curr[k] *= facsq;
+        nh.ke_cur *= facsq;
+        nh.t_cur *= facsq;
+    }
+    double* f = calloc((size_t)natms * 3 + 1, sizeof(double));
+    double en[7] = {0, 0, 0, 0, 0, 0, 0};
+    orc_force(o, 1, f, en);
+    for (int i = 0; i < no_ch; i++) nh.eta_m[i] = boltz * t_tar / (nh.t_freq * nh.t_freq);
+    nh.eta_m[0] *= nh.no_dof;
+    for (int i = 0; i < no_ch; i++) nh.eta_d[i] = 0.0;
+    for (int i = 1; i < no_ch; i++)
+        nh.eta_dd[i] = (nh.eta_m[i - 1] * nh.eta_d[i - 1] * nh.eta_d[i - 1] - boltz * t_tar) / nh.eta_m[i];
+    for (int i = 0; i < natms; i++)
+        for (int k = 0; k < 3; k++) o->x0[i * 3 + k] = 0.0;
+    for (int step = 0; step < nsteps; step++) {
+        nh_update_T(o, &nh, xd, dt2);
+        nh_update_x_d(o, &nh, mass, xd, f, dt2);
+        nh_update_x(o, xd, dt);
+        update_0(o);
+        memset(f, 0, sizeof(double) * (size_t)natms * 3);
+        orc_force(o, step == nsteps - 1 ? 1 : 0, f, en);
+        nh_update_x_d(o, &nh, mass, xd, f, dt2);
+        nh_update_T(o, &nh, xd, dt2);
+    }
+    if (thermo) {
+        for (int k = 0; k < 7; k++) thermo[k] = en[k];
+        thermo[7] = nh.ke_cur;
+        thermo[8] = nh.t_cur;
+        for (int i = 0; i < no_ch; i++) thermo[9 + i] = nh.eta_d[i];
+    }
+    free(f);
+    return 0;
 }

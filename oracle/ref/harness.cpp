@@ -15,6 +15,13 @@
  *   force / energy / crd / cdot / calcg call the ForceField virtuals.
  *   lbfgs   = Min_LBFGS (min_l-bfgs.cpp) constructed, init, run, fin, with
  *             the energy of every force_calc logged by the oracle subclass.
+ *   md      = MD_NH "nvt" (md_nh.cpp) constructed, time_step / boltzmann set,
+ *             init, run, then the owned x and x_d and one force_calc(1) at
+ *             the final state written before fin.  Velocities are either
+ *             given (x_d added and filled, then rescaled by init_vel) or made
+ *             by create_vel.  x_0 is zeroed first: MD_NH::init never calls
+ *             Atoms::store_0, so the reader's never-written x_0 would
+ *             otherwise decide whether the first step rebuilds.
  *
  * Two harness-side measures (no change to reference arithmetic):
  *   - OracleDMD<Base>::coef restates ff_dmd_I.cpp:735-796 but routes "FS" to
@@ -50,6 +57,7 @@
 #include "ff_dmd_II.h"
 #include "ff_dmd.h"
 #include "min_l-bfgs.h"
+#include "md_nh.h"
 
 using namespace MAPP_NS;
 
@@ -429,6 +437,54 @@ void do_time(const std::string& what, int reps, const std::string& prefix)
     meta(prefix, "time_%s %d %.9g", what.c_str(), reps, t1 - t0);
 }
 
+/* MD_NH (md_nh.cpp) run on the scripted MD-mode system */
+void do_md(double t_tar, const std::string& period, int no_it, int no_ch, double dt, double boltz, int seed,
+           int steps, const std::string& xd_path, const std::string& prefix)
+{
+    Atoms* atoms = H.mapp->atoms;
+    int natms = atoms->natms;
+    if (xd_path != "-") {
+        std::vector<char> raw = read_raw(xd_path);
+        if (atoms->find_exist("x_d") < 0) atoms->add<double>(0, 3, "x_d");
+        double* xd = vec<double>("x_d");
+        memcpy(xd, raw.data(), sizeof(double) * (size_t)natms * 3);
+    }
+    double* x0 = nullptr;
+    atoms->vectors[1].ret(x0);
+    for (int i = 0; i < natms * atoms->vectors[1].dim; i++) x0[i] = 0.0;
+    char tbuf[64];
+    snprintf(tbuf, sizeof(tbuf), "%.17g", t_tar);
+    std::vector<std::string> a = {"md", "nh", "nvt", "temp", tbuf, period, "eta_iteration", std::to_string(no_it),
+                                  "eta_chains", std::to_string(no_ch)};
+    if (seed > 0) {
+        a.push_back("create_vel");
+        a.push_back(std::to_string(seed));
+    }
+    std::vector<char*> argv;
+    for (auto& t : a) argv.push_back(strdup(t.c_str()));
+    MD_NH* md = new MD_NH(H.mapp, (int)argv.size(), argv.data());
+    md->dt = dt;
+    md->boltz = boltz;
+    md->init();
+    double t0 = MPI_Wtime();
+    md->run(steps);
+    double t1 = MPI_Wtime();
+    write_raw(prefix + ".x.bin", vec<double>("x"), sizeof(double) * (size_t)atoms->natms * 3);
+    write_raw(prefix + ".xd.bin", vec<double>("x_d"), sizeof(double) * (size_t)atoms->natms * 3);
+    int f_n = atoms->find("f");
+    double* f = nullptr;
+    atoms->vectors[f_n].ret(f);
+    for (int i = 0; i < 3 * atoms->natms; i++) f[i] = 0.0;
+    double en[7] = {0, 0, 0, 0, 0, 0, 0};
+    H.mapp->forcefield->force_calc(1, en);
+    meta(prefix, "en %.17g %.17g %.17g %.17g %.17g %.17g %.17g", en[0], en[1], en[2], en[3], en[4], en[5], en[6]);
+    meta(prefix, "natms %d", atoms->natms);
+    meta(prefix, "time_run %.9g", t1 - t0);
+    md->fin();
+    delete md;
+    for (char* t : argv) free(t);
+}
+
 void run_command(const std::string& line)
 {
     std::istringstream is(line);
@@ -450,6 +506,13 @@ void run_command(const std::string& line)
     else if (cmd == "setx") { std::string xp, p; rs >> xp >> p; do_setx(xp, p); }
     else if (cmd == "setc") { std::string cp; rs >> cp; do_setc(cp); }
     else if (cmd == "lbfgs") { int m, k; double tol; std::string p; rs >> m >> k >> tol >> p; do_lbfgs(m, k, tol, p); }
+    else if (cmd == "md") {
+        double T, dt, kb;
+        std::string period, xdp, p;
+        int it, ch, seed, n;
+        rs >> T >> period >> it >> ch >> dt >> kb >> seed >> n >> xdp >> p;
+        do_md(T, period, it, ch, dt, kb, seed, n, xdp, p);
+    }
     else if (cmd == "time") { std::string w, p; int n; rs >> w >> n >> p; do_time(w, n, p); }
     else { fprintf(stderr, "harness: unknown command %s\n", cmd.c_str()); exit(2); }
 }

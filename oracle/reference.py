@@ -107,6 +107,18 @@ class RefRun:
         self.steps.append(("lbfgs", tag))
         return self.add(f"lbfgs {m} {max_iter} {energy_tol!r} {self._p(tag)}")
 
+    def md(self, t_tar: float, t_period: float, steps: int, dt: float, boltz: float, xd=None, seed=0,
+           eta_iteration=1, eta_chains=3, tag="md"):
+        """The reference MD_NH nvt run (construct with init=False): velocities
+        ``xd`` [natms][3] in the reader's atom order, or create_vel with ``seed``."""
+        xp = "-"
+        if xd is not None:
+            xp = self._p(tag + ".xd_in.bin")
+            np.ascontiguousarray(xd, dtype=np.float64).tofile(xp)
+        self.steps.append(("md", tag))
+        return self.add(f"md {t_tar!r} {t_period!r} {eta_iteration} {eta_chains} {dt!r} {boltz!r} {seed} {steps} "
+                        f"{xp} {self._p(tag)}")
+
     def time(self, what: str, reps: int, tag="t"):
         self.steps.append(("time", tag))
         return self.add(f"time {what} {reps} {self._p(tag)}")

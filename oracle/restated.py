@@ -71,6 +71,9 @@ def lib():
         L.orc_lbfgs.argtypes = [P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, dp,
                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_lbfgs.restype = C.c_int
+        L.orc_md_nh.argtypes = [P, dp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                dp, C.c_int, dp]
+        L.orc_md_nh.restype = C.c_int
         _lib = L
     return _lib
 
@@ -270,3 +273,17 @@ class Oracle:
                               C.byref(err), C.byref(nev))
         x = self.x_all()[: self.counts()["natms"]]
         return {"code": err.value, "line_searches": nls, "evals": nev.value, "energies": e[: nls + 1], "x": x}
+
+    def md_nh(self, t_tar, t_period, steps, dt, boltz, xd=None, seed=0, eta_iteration=1, eta_chains=3):
+        """MD_NH nvt run (orc_md_nh): returns dict(x, xd, energy, virial, ke, t, eta_d)."""
+        n = self.counts()["natms"]
+        v = np.zeros((n, 3)) if xd is None else np.array(xd, dtype=np.float64).reshape(n, 3).copy()
+        mass = np.asarray(self.cfg.masses, dtype=np.float64)
+        th = np.zeros(9 + eta_chains)
+        rc = lib().orc_md_nh(self.h, mass, t_tar, t_period, eta_iteration, eta_chains, dt, boltz, seed, v.ravel(),
+                             steps, th)
+        if rc != 0:
+            raise ValueError("orc_md_nh rejected the run (zero velocities or chain settings)")
+        x = self.x_all()[:n]
+        return {"x": x, "xd": v, "energy": th[0], "virial": th[1:7], "ke": th[7], "t": th[8],
+                "eta_d": th[9:9 + eta_chains]}
