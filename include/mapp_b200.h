@@ -306,6 +306,26 @@ int mg_cfg_free(mg_cfg* c);
 int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings,
                  int lbfgs_cluster, mg_cell_result* r, mg_batch_stats* stats);
 
+/* ---- Nose-Hoover molecular dynamics ------------------------------------- */
+/* MD_NH "md nh nvt temp t_tar t_period eta_iteration .. eta_chains .." with
+   time_step dt and boltzmann boltz, then "run nsteps" (md_nh.cpp:23-330
+   constructor options, init :385-567, run :636-677), without a barostat and
+   without a dof vector, for an initialised EAM / FS system whose species
+   masses were given to mg_atoms_set_types.  Velocities: seed > 0 draws them as
+   create_vel does (Park-Miller Gaussian, md_nh.cpp:1211-1280); otherwise
+   xd_in (natms * 3, host or device) is rescaled to t_tar as init_vel does
+   (zero velocities are an MG_ERR_ARG, where the reference aborts).  As in the
+   reference, x_0 is not stored at init, so the first step rebuilds the ghosts
+   and the list.  On return the system holds the final positions (read them
+   with mg_atoms_get_x) and forces; xd_out (natms * 3, may be NULL) receives
+   the velocities; thermo (9 + eta_chains doubles, may be NULL) the energy and
+   six virial terms of force_calc(1) at the final positions, ke_cur, t_cur and
+   the chain velocities eta_d; rebuilds (may be NULL) the number of list
+   rebuilds during the run. */
+int mg_md_nh(mg_system* s, double t_tar, double t_period, int eta_iteration, int eta_chains, double dt,
+             double boltz, int seed, const double* xd_in, int nsteps, double* xd_out, double* thermo,
+             int* rebuilds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,8 @@ SIGNATURES = {
     "mg_batch_relax": (C.c_int, [_P, _P]),
     "mg_batch_cell_result": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mg_min_lbfgs": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _P, _P]),
+    "mg_md_nh": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _P,
+                           C.c_int, _P, _P, _I]),
     "mg_cfg_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mg_cfg_info": (C.c_int, [_P, _I, _I, _P, _I]),
     "mg_cfg_types": (C.c_int, [_P, _P, C.c_int, _P]),
@@ -346,6 +348,23 @@ class System:
         _check(load_library().mg_min_lbfgs(self.h, m, max_iter, fmax_tol, energy_tol, max_halvings, cluster,
                                            C.byref(r), C.byref(st)))
         return ({k: getattr(r, k) for k, _ in CellResult._fields_}, {k: getattr(st, k) for k, _ in BatchStats._fields_})
+
+    def md_nh(self, t_tar, t_period, steps, dt, boltz, xd=None, seed=0, eta_iteration=1, eta_chains=3):
+        """Nose-Hoover NVT run of this EAM / FS system on the device (mg_md_nh).
+        xd: initial velocities [natms][3] (rescaled to t_tar), or seed > 0 for
+        create_vel.  Returns dict(x, xd, energy, virial, ke, t, eta_d, rebuilds)."""
+        n = self.natms
+        xin = None
+        if seed <= 0:
+            xin = np.ascontiguousarray(np.asarray(xd, dtype=np.float64).reshape(n, 3))
+        vout = np.zeros((n, 3))
+        th = np.zeros(9 + eta_chains)
+        nreb = C.c_int(0)
+        _check(load_library().mg_md_nh(self.h, t_tar, t_period, eta_iteration, eta_chains, dt, boltz, seed,
+                                       None if xin is None else xin.ctypes.data, steps, vout.ctypes.data,
+                                       th.ctypes.data, C.byref(nreb)))
+        return {"x": self.get_x(), "xd": vout, "energy": th[0], "virial": th[1:7], "ke": th[7], "t": th[8],
+                "eta_d": th[9:9 + eta_chains], "rebuilds": nreb.value}
 
     def last_time(self, phase):
         ms = C.c_double(0.0)

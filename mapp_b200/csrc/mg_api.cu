@@ -1634,3 +1634,32 @@ void mg::system_box(mg_system* s, double* H_out)
         for (int j = 0; j < 3; j++) H_out[3 * i + j] = s->H[i][j];
 }
 int mg::system_natms(mg_system* s) { return s->natms; }
+int mg::system_check_ready(mg_system* s)
+{
+    CHK(check_sys(s));
+    if (!s->initialized) return fail(MG_ERR_STATE, "ff_init must run first");
+    return MG_OK;
+}
+void mg::system_masses(mg_system* s, double* out)
+{
+    for (int t = 0; t < s->nt; t++) out[t] = t < (int)s->masses.size() ? s->masses[t] : 0.0;
+}
+int mg::system_rebuild(mg_system* s)
+{
+    if (s->natms == 0) return MG_OK;
+    CU(launch_x2s(s->d, s->st));
+    return rebuild(s);
+}
+int mg::system_enqueue_force(mg_system* s, int st_clc, int zero, int* rows)
+{
+    if (s->style != STYLE_EAM && s->style != STYLE_FS)
+        return fail(MG_ERR_UNSUPPORTED, "the device MD loop drives EAM / FS force fields");
+    Dev& d = s->d;
+    if (zero) {
+        CU(cudaMemsetAsync(d.f, 0, (size_t)s->natms * s->x_dim * sizeof(double), s->st));
+        CU(cudaMemsetAsync(d.rho, 0, (size_t)s->natms * sizeof(double), s->st));
+    }
+    CU(s->style == STYLE_EAM ? launch_eam_force(d, st_clc, rows, s->st) : launch_fs_force(d, st_clc, rows, s->st));
+    return MG_OK;
+}
+double* mg::system_red_out(mg_system* s) { return s->red_out; }

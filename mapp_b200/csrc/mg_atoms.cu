@@ -242,19 +242,7 @@ __global__ void k_refresh_x(Dev d)
     if (k >= d.nph) return;
     int g = d.natms + k;
     int r = d.root[g];
-    double4 p = d.pos[r];
-    unsigned long long ch = d.gchain[g];
-    for (int s = 0; s < kMaxChain; s++) {
-        unsigned code = (unsigned)(ch >> (4 * s)) & 15u;
-        if (!(code & 8u)) break;
-        int dim = (code >> 1) & 3, dir = code & 1;
-        for (int j = 0; j <= dim; j++) {
-            double v = comp3(p, j);
-            set3(p, j, dir == 0 ? dadd(v, d.H[dim][j]) : dsub(v, d.H[dim][j]));
-        }
-    }
-    p.w = 0.0;
-    d.pos[g] = p;
+    d.pos[g] = ghost_image(d, d.gchain[g], d.pos[r]);
     for (int a = 0; a < d.x_dim - 3; a++) d.alpha[(size_t)g * d.nt + a] = d.alpha[(size_t)r * d.nt + a];
 }
 

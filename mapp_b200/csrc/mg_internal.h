@@ -129,6 +129,25 @@ __host__ __device__ inline int comp_idx(int i, int j)
     return i < j ? (j + 1) * j / 2 + i : (i + 1) * i / 2 + j;
 }
 
+#ifdef __CUDACC__
+// A ghost's position from its root's: the shifts +-H[dim][0..dim] of its chain
+// applied in creation order with round-to-nearest adds, as Atoms::update
+// refreshes x along the swap chain (atoms.cpp:1320-1352).
+__device__ __forceinline__ double4 ghost_image(const Dev& d, unsigned long long ch, double4 p)
+{
+    for (int s = 0; s < kMaxChain; s++) {
+        unsigned code = (unsigned)(ch >> (4 * s)) & 15u;
+        if (!(code & 8u)) break;
+        int dim = (code >> 1) & 3, dir = code & 1;
+        p.x = dir == 0 ? __dadd_rn(p.x, d.H[dim][0]) : __dsub_rn(p.x, d.H[dim][0]);
+        if (dim >= 1) p.y = dir == 0 ? __dadd_rn(p.y, d.H[dim][1]) : __dsub_rn(p.y, d.H[dim][1]);
+        if (dim >= 2) p.z = dir == 0 ? __dadd_rn(p.z, d.H[dim][2]) : __dsub_rn(p.z, d.H[dim][2]);
+    }
+    p.w = 0.0;
+    return p;
+}
+#endif
+
 // training box of the learned form (inputs outside it fall back to quadrature)
 struct MlpBox {
     float r_lo, r_hi, w_lo, w_hi;
@@ -204,7 +223,7 @@ const char* internal_last_error();
 int num_sms();
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-// accessors of a single system for the batched form (mg_api.cu)
+// accessors of a single system for the batched form and the MD loop (mg_api.cu)
 Dev& system_dev(mg_system* s);
 cudaStream_t system_stream(mg_system* s);
 int system_device(mg_system* s);
@@ -212,5 +231,14 @@ void system_shape(mg_system* s, int* style, int* nt, int* x_dim, int* form, doub
 double system_skin(mg_system* s);
 void system_box(mg_system* s, double* H_out);
 int system_natms(mg_system* s);
+// MG_OK when ff_init has run (else records the error and returns its code)
+int system_check_ready(mg_system* s);
+void system_masses(mg_system* s, double* out);
+// x2s of the owned atoms, then the ghost / bin / list rebuild (Atoms::update_0's rebuild branch)
+int system_rebuild(mg_system* s);
+// enqueue force_calc's device work only (zero f and rho unless the caller has,
+// the EAM / FS passes); capturable
+int system_enqueue_force(mg_system* s, int st_clc, int zero, int* rows);
+double* system_red_out(mg_system* s);
 
 }  // namespace mg

@@ -20,6 +20,7 @@ CASES = [
     ("eam", dict(n=4, seed=7), 300.0, 0.1, 300, 5, 1, 3),
     ("eam", dict(n=4, nt=2, fmt="FS", seed=8), 600.0, 0.05, 200, 0, 2, 4),
     ("fs", dict(n=4, nt=2, seed=9), 450.0, 0.2, 150, 11, 1, 5),
+    ("eam", dict(n=4, seed=7, skin=0.1), 900.0, 1.0, 300, 5, 1, 3),
 ]
 
 
@@ -31,7 +32,7 @@ def _same(a, b):
 
 
 @pytest.mark.parametrize("kind,kw,T,period,steps,seed,it,ch", CASES,
-                         ids=["eam-create_vel", "eam2-init_vel-it2-ch4", "fs2-create_vel-ch5"])
+                         ids=["eam-create_vel", "eam2-init_vel-it2-ch4", "fs2-create_vel-ch5", "eam-skin0.1-rebuilds"])
 def test_md_nh_bit_exact(tmp_path, kind, kw, T, period, steps, seed, it, ch):
     w = fx.write_workload(str(tmp_path / "w"), kind, **kw)
     n = w["cfg"].natms
