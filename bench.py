@@ -441,6 +441,48 @@ def run_single_lbfgs(mb, w, device):
     return out
 
 
+MD_DT = 0.0982269    # 1 fs in the reference's sqrt(amu A^2 / eV) time unit
+MD_KB = 8.617333e-5  # eV / K
+
+
+def run_md(mb, fx, device, steps=1000, ref_steps=300):
+    """Nose-Hoover NVT of the FCC 10^3 EAM crystal (4000 atoms, a = 3.615 A,
+    sites displaced by sigma = 0.05 A, setfl tables of species A): create_vel
+    at 300 K, thermostat period 100 fs, 1000 steps of 1 fs through mg_md_nh,
+    timed on the host clock around the call (velocity set-up, the initial
+    force, every step, rebuilds and the copies out included); beside it the
+    reference's own MD_NH on the same system for ref_steps steps on one core."""
+    d = tempfile.mkdtemp(prefix="mapp_md_")
+    w = fx.write_workload(d, "eam", n=10)
+    period = 100 * MD_DT
+    s = mb.system_from_workload(w, device=device)
+    s.md_nh(300.0, period, 20, MD_DT, MD_KB, seed=4321)  # warm-up: module load, graph paths
+    s.close()
+    s = mb.system_from_workload(w, device=device)
+    t0 = time.perf_counter()
+    r = s.md_nh(300.0, period, steps, MD_DT, MD_KB, seed=4321)
+    wall = time.perf_counter() - t0
+    n = s.natms
+    out = {"atoms": n, "steps": steps, "wall_s": wall, "ms_per_step": wall * 1e3 / steps,
+           "atom_steps_per_s": n * steps / wall, "rebuilds": r["rebuilds"], "final_T": r["t"],
+           "final_energy": r["energy"],
+           "config": "FCC 10^3 EAM (setfl, species A), create_vel 300 K, period 100 fs, dt 1 fs, skin 0.5 A",
+           "kernels_per_step": 6, "timing": "host clock around mg_md_nh (set-up, steps, rebuilds, copies out)"}
+    s.close()
+    from oracle import reference
+
+    if reference.available():
+        rr = reference.RefRun(w, workdir=os.path.join(d, "ref"), init=False)
+        rr.md(300.0, period, ref_steps, MD_DT, MD_KB, seed=4321)
+        meta = rr.run(timeout=1800)["md"]["meta"]
+        t_ref = float(meta["time_run"])
+        out["cpu_baseline"] = {"value": n * ref_steps / t_ref, "unit": "atom-steps/s", "cores": 1,
+                               "kind": "reference",
+                               "sample": f"reference MD_NH::run, {ref_steps} steps of the same system, {t_ref:.2f} s"}
+        out["speedup_vs_reference_core"] = out["atom_steps_per_s"] / out["cpu_baseline"]["value"]
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -508,6 +550,7 @@ def run_ours(args):
     if not args.skip_forms:
         forms["batched"] = run_batched(mb, fx, local)
         forms["single_lbfgs"] = run_single_lbfgs(mb, w, local)
+        forms["md_nh"] = run_md(mb, fx, local)
         forms["large"] = run_large_forms(mb, fx, local, s)
     s.set_form(form_id)
 
