@@ -13,8 +13,9 @@
  *   DMD_I / DMD_II / DMD  force_calc / energy_calc / create_2nd_neigh_lst /
  *           c_d_calc / calc_g / interpolate_m (ff_dmd_I.cpp:88-668,1760-2674;
  *           ff_dmd_II.cpp:2151-2630; ff_dmd.cpp:2221-2606)
- *   callers Min_LBFGS + LineSearch_BackTrack (min_l-bfgs.cpp, line_search.cpp)
- *           and MD_NH without a barostat (md_nh.cpp, rand_engine.cpp)
+ *   callers Min_LBFGS + LineSearch_BackTrack (min_l-bfgs.cpp, line_search.cpp),
+ *           MD_NH without a barostat (md_nh.cpp, rand_engine.cpp) and
+ *           Clock_Adams (clock_adams.cpp)
  *
  * so that, compiled with -ffp-contract=off like the reference, it reproduces
  * the reference's doubles bit for bit (pinned by tests against the compiled
@@ -2122,4 +2123,147 @@ int orc_md_nh(orc_t* o, const double* mass, double t_tar, double t_period, int n
     }
     free(f);
     return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Clock_Adams (clock_adams.cpp): fixed-step Adams-Moulton integration of the
+ * DMD concentrations, each step solved by nonlinear conjugate gradient on
+ * calc_g with box constraints c in [0, 1].
+ * ------------------------------------------------------------------------- */
+
+/* Clock_Adams::solve (clock_adams.cpp:246-365); a, g, g0, c0, h: natms * nt */
+static double adams_solve(orc_t* o, double delta_t, double bet, const double* a, double* g, double* g0, double* c0,
+                          double* h, long* n_calc_g)
+{
+    const int n = o->natms * o->nt;
+    double* c = o->c;
+    double* c_d = o->c_d;
+    const double min_gamma = 1.0e-16, slope = 0.4, gamma_red = 0.8;
+    double gamma, max_gamma = 1.0, inner, tmp, ratio, g0_g0, g_g, g_g0, g_h, curr_cost, ideal_cost, cost;
+    int chk;
+    curr_cost = orc_calc_g(o, 0, delta_t * bet, a, g);
+    (*n_calc_g)++;
+    orc_c_d_calc(o, NULL);
+    ratio = 1.0;
+    for (int i = 0; i < n; i++) {
+        tmp = c_d[i] * delta_t + c[i];
+        if (tmp > 1.0) ratio = MINV((1.0 - c[i]) / (tmp - c[i]), ratio);
+        else if (tmp < 0.0) ratio = MINV((c[i] - 0.0) / (c[i] - tmp), ratio);
+    }
+    for (int i = 0; i < n; i++) c[i] += c_d[i] * delta_t * ratio;
+    refresh_vec(o, c, o->nt);
+    memcpy(h, g, sizeof(double) * n);
+    inner = 0.0;
+    for (int i = 0; i < n; i++) inner += g[i] * g[i];
+    g0_g0 = inner;
+    g_h = g0_g0;
+    int iter = 0;
+    while (curr_cost > 1.0e-8 && iter < 50 && max_gamma > min_gamma) {
+        memcpy(g0, g, sizeof(double) * n);
+        memcpy(c0, c, sizeof(double) * n);
+        gamma = 1.0;
+        for (int i = 0; i < n; i++) {
+            tmp = c0[i] + h[i];
+            if (tmp > 1.0) gamma = MINV((1.0 - c0[i]) / (tmp - c0[i]), gamma);
+            else if (tmp < 0.0) gamma = MINV((c0[i] - 0.0) / (c0[i] - tmp), gamma);
+        }
+        max_gamma = gamma;
+        chk = 1;
+        cost = curr_cost;
+        while (chk && max_gamma > min_gamma) {
+            for (int i = 0; i < n; i++) c[i] = c0[i] + max_gamma * h[i];
+            refresh_vec(o, c, o->nt);
+            curr_cost = orc_calc_g(o, 1, delta_t * bet, a, g);
+            (*n_calc_g)++;
+            ideal_cost = cost - slope * max_gamma * g_h;
+            if (curr_cost < ideal_cost) chk = 0;
+            max_gamma *= gamma_red;
+            if (max_gamma <= 0.0) {
+                memcpy(c, c0, sizeof(double) * n);
+                refresh_vec(o, c, o->nt);
+            }
+        }
+        curr_cost = orc_calc_g(o, 0, delta_t * bet, a, g);
+        (*n_calc_g)++;
+        inner = 0.0;
+        for (int i = 0; i < n; i++) inner += g[i] * g0[i];
+        g_g0 = inner;
+        inner = 0.0;
+        for (int i = 0; i < n; i++) inner += g[i] * g[i];
+        g_g = inner;
+        ratio = (g_g - g_g0) / g0_g0;
+        g0_g0 = g_g;
+        inner = 0.0;
+        for (int i = 0; i < n; i++) {
+            h[i] *= ratio;
+            h[i] += g[i];
+            inner += h[i] * g[i];
+        }
+        g_h = inner;
+        if (g_h < 0.0) {
+            memcpy(h, g, sizeof(double) * n);
+            g_h = g_g;
+        }
+        iter++;
+    }
+    return curr_cost;
+}
+
+/*
+ * "clock adams order no_steps delta_t" then run: Clock_Adams::init
+ * (clock_adams.cpp:128-167) after the set-up of orc_init -- the crd list and
+ * one force_calc(1), which fills the per-pair buffers calc_g and c_d_calc
+ * read -- and Clock_Adams::run (clock_adams.cpp:187-240).
+ * err (no_steps doubles, may be NULL) receives each step's final cost; the
+ * return value is the number of calc_g calls, or -1 for an order outside
+ * 1..6 (the reference aborts).  The owned and ghost c are left in the state.
+ */
+long orc_clock_adams(orc_t* o, int order, int no_steps, double delta_t, double* err)
+{
+    static const double kBeta[6][6] = {
+        {1.0},
+        {1.0 / 2.0, 1.0 / 2.0},
+        {5.0 / 12.0, 8.0 / 12.0, -1.0 / 12.0},
+        {9.0 / 24.0, 19.0 / 24.0, -5.0 / 24.0, 1.0 / 24.0},
+        {251.0 / 720.0, 646.0 / 720.0, -264.0 / 720.0, 106.0 / 720.0, -19.0 / 720.0},
+        {475.0 / 1440.0, 1427.0 / 1440.0, -798.0 / 1440.0, 482.0 / 1440.0, -173.0 / 1440.0, 27.0 / 1440.0}};
+    if (!o->dmd || order < 1 || order > 6) return -1;
+    const double* beta = kBeta[order - 1];
+    const int n = o->natms * o->nt;
+    double en[7];
+    orc_create_2nd_neigh_lst(o);
+    double* f = calloc((size_t)o->natms * o->x_dim + 1, sizeof(double));
+    orc_force(o, 1, f, en);
+    free(f);
+    double* a = calloc((size_t)n + 1, sizeof(double));
+    double* g = calloc((size_t)n + 1, sizeof(double));
+    double* g0 = calloc((size_t)n + 1, sizeof(double));
+    double* c0 = calloc((size_t)n + 1, sizeof(double));
+    double* h = calloc((size_t)n + 1, sizeof(double));
+    double* y = calloc((size_t)(order > 1 ? order - 1 : 1) * n + 1, sizeof(double));
+    int* slot = calloc(order > 1 ? order - 1 : 1, sizeof(int));
+    for (int j = 0; j < order - 1; j++) slot[j] = j;
+    long n_calc_g = 0;
+    for (int istep = 0; istep < no_steps; istep++) {
+        double cur;
+        if (istep < order) {
+            for (int i = 0; i < n; i++) a[i] = -o->c[i];
+            cur = adams_solve(o, delta_t, 1.0, a, g, g0, c0, h, &n_calc_g);
+        } else {
+            for (int i = 0; i < n; i++) {
+                a[i] = -o->c[i];
+                for (int j = 0; j < order - 1; j++) a[i] -= delta_t * beta[j + 1] * y[(size_t)slot[j] * n + i];
+            }
+            cur = adams_solve(o, delta_t, beta[0], a, g, g0, c0, h, &n_calc_g);
+        }
+        if (err) err[istep] = cur;
+        if (order > 1) {
+            int last = slot[order - 2];
+            for (int i = order - 2; i > 0; i--) slot[i] = slot[i - 1];
+            slot[0] = last;
+            memcpy(y + (size_t)slot[0] * n, o->c_d, sizeof(double) * n);
+        }
+    }
+    free(a); free(g); free(g0); free(c0); free(h); free(y); free(slot);
+    return n_calc_g;
 }

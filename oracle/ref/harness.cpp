@@ -15,6 +15,8 @@
  *   force / energy / crd / cdot / calcg call the ForceField virtuals.
  *   lbfgs   = Min_LBFGS (min_l-bfgs.cpp) constructed, init, run, fin, with
  *             the energy of every force_calc logged by the oracle subclass.
+ *   adams   = Clock_Adams (clock_adams.cpp) constructed, init, run, then the
+ *             owned c and the number of calc_g calls written before fin.
  *   md      = MD_NH "nvt" (md_nh.cpp) constructed, time_step / boltzmann set,
  *             init, run, then the owned x and x_d and one force_calc(1) at
  *             the final state written before fin.  Velocities are either
@@ -58,6 +60,7 @@
 #include "ff_dmd.h"
 #include "min_l-bfgs.h"
 #include "md_nh.h"
+#include "clock_adams.h"
 
 using namespace MAPP_NS;
 
@@ -128,8 +131,15 @@ public:
         return Base::energy_calc();
     }
 
+    double calc_g(int chk, double alpha, double* a, double* g) override
+    {
+        n_calc_g++;
+        return Base::calc_g(chk, alpha, a, g);
+    }
+
     std::vector<double>* force_log = nullptr;  // en_st[0] of every force_calc while set
     long n_energy = 0;
+    long n_calc_g = 0;
 
 private:
     bool route_fs_;
@@ -437,6 +447,42 @@ void do_time(const std::string& what, int reps, const std::string& prefix)
     meta(prefix, "time_%s %d %.9g", what.c_str(), reps, t1 - t0);
 }
 
+template <class Base>
+bool calc_g_count(ForceField* ff, long* n)
+{
+    OracleDMD<Base>* o = dynamic_cast<OracleDMD<Base>*>(ff);
+    if (!o) return false;
+    *n = o->n_calc_g;
+    return true;
+}
+
+/* Clock_Adams (clock_adams.cpp) run on the scripted DMD system */
+void do_adams(int order, int steps, const std::string& dt, const std::string& prefix)
+{
+    Atoms* atoms = H.mapp->atoms;
+    ForceField* ff = H.mapp->forcefield;
+    std::vector<std::string> a = {"clock", "adams", std::to_string(order), std::to_string(steps), dt};
+    std::vector<char*> argv;
+    for (auto& t : a) argv.push_back(strdup(t.c_str()));
+    long n0 = 0, n1 = 0;
+    calc_g_count<ForceField_DMD_I>(ff, &n0) || calc_g_count<ForceField_DMD>(ff, &n0) ||
+        calc_g_count<ForceField_DMD_II>(ff, &n0);
+    Clock_Adams* ck = new Clock_Adams(H.mapp, (int)argv.size(), argv.data());
+    ck->init();
+    double t0 = MPI_Wtime();
+    ck->run();
+    double t1 = MPI_Wtime();
+    calc_g_count<ForceField_DMD_I>(ff, &n1) || calc_g_count<ForceField_DMD>(ff, &n1) ||
+        calc_g_count<ForceField_DMD_II>(ff, &n1);
+    write_raw(prefix + ".c.bin", vec<double>("c"), sizeof(double) * (size_t)atoms->natms * H.nt);
+    meta(prefix, "n_calc_g %ld", n1 - n0);
+    meta(prefix, "natms %d", atoms->natms);
+    meta(prefix, "time_run %.9g", t1 - t0);
+    ck->fin();
+    delete ck;
+    for (char* t : argv) free(t);
+}
+
 /* MD_NH (md_nh.cpp) run on the scripted MD-mode system */
 void do_md(double t_tar, const std::string& period, int no_it, int no_ch, double dt, double boltz, int seed,
            int steps, const std::string& xd_path, const std::string& prefix)
@@ -506,6 +552,12 @@ void run_command(const std::string& line)
     else if (cmd == "setx") { std::string xp, p; rs >> xp >> p; do_setx(xp, p); }
     else if (cmd == "setc") { std::string cp; rs >> cp; do_setc(cp); }
     else if (cmd == "lbfgs") { int m, k; double tol; std::string p; rs >> m >> k >> tol >> p; do_lbfgs(m, k, tol, p); }
+    else if (cmd == "adams") {
+        int order, n;
+        std::string dt, p;
+        rs >> order >> n >> dt >> p;
+        do_adams(order, n, dt, p);
+    }
     else if (cmd == "md") {
         double T, dt, kb;
         std::string period, xdp, p;

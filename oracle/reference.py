@@ -107,6 +107,11 @@ class RefRun:
         self.steps.append(("lbfgs", tag))
         return self.add(f"lbfgs {m} {max_iter} {energy_tol!r} {self._p(tag)}")
 
+    def adams(self, order: int, steps: int, dt: float, tag="adams"):
+        """The reference Clock_Adams: init, run, fin (construct with init=False)."""
+        self.steps.append(("adams", tag))
+        return self.add(f"adams {order} {steps} {dt!r} {self._p(tag)}")
+
     def md(self, t_tar: float, t_period: float, steps: int, dt: float, boltz: float, xd=None, seed=0,
            eta_iteration=1, eta_chains=3, tag="md"):
         """The reference MD_NH nvt run (construct with init=False): velocities

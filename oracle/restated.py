@@ -74,6 +74,8 @@ def lib():
         L.orc_md_nh.argtypes = [P, dp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                 dp, C.c_int, dp]
         L.orc_md_nh.restype = C.c_int
+        L.orc_clock_adams.argtypes = [P, C.c_int, C.c_int, C.c_double, dp]
+        L.orc_clock_adams.restype = C.c_long
         _lib = L
     return _lib
 
@@ -287,3 +289,14 @@ class Oracle:
         x = self.x_all()[:n]
         return {"x": x, "xd": v, "energy": th[0], "virial": th[1:7], "ke": th[7], "t": th[8],
                 "eta_d": th[9:9 + eta_chains]}
+
+    def clock_adams(self, order, steps, dt):
+        """Clock_Adams init + run (orc_clock_adams): returns dict(c, err, n_calc_g)."""
+        err = np.zeros(max(steps, 1))
+        n = lib().orc_clock_adams(self.h, order, steps, dt, err)
+        if n < 0:
+            raise ValueError("orc_clock_adams rejected the run (order outside 1..6 or not DMD)")
+        c = self.counts()["natms"]
+        cc = np.zeros((c + self.counts()["nph"]) * self.nt)
+        lib().orc_get_c(self.h, cc)
+        return {"c": cc.reshape(-1, self.nt)[:c], "err": err[:steps], "n_calc_g": int(n)}
