@@ -122,8 +122,9 @@ int mg_neighbor_counts(mg_system* s, int* natms, int* natms_ph, long long* no_pa
 int mg_neighbor_get_list(mg_system* s, int* sizes, int* pairs);
 
 /* ---- diagnostics ------------------------------------------------------ */
-/* Per-atom double vectors of the force field, owned + ghost entries:
-   "E", "dE", "ddE", "n", "c_d" (owned only), "rho" (EAM/FS: F'(rho)). */
+/* Per-atom double vectors of the force field, owned entries (natms * nt, or
+   natms for "rho"): "E", "dE", "ddE", "n", "c_d", "c" (DMD), "rho" (EAM/FS:
+   F'(rho)). */
 int mg_get_vector(mg_system* s, const char* name, double* out);
 /* Per-atom int vectors: "crd" (owned + ghost). */
 int mg_get_int_vector(mg_system* s, const char* name, int* out);
@@ -305,6 +306,18 @@ int mg_cfg_free(mg_cfg* c);
    and counts, stats the launch statistics (either may be NULL). */
 int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings,
                  int lbfgs_cluster, mg_cell_result* r, mg_batch_stats* stats);
+
+/* ---- concentration clock -------------------------------------------------- */
+/* Clock_Adams "clock adams order nsteps delta_t" then run (clock_adams.cpp:
+   13-124 constructor, init :128-167, run :187-240, solve :246-365) for an
+   initialised DMD system in the plain form: fixed-step Adams-Moulton steps of
+   the concentrations, each solved by the reference's box-constrained
+   nonlinear conjugate gradient on calc_g.  The vectors stay on the device;
+   only the scalars that steer the solve cross to the host.  On return the
+   system holds the final c (read with mg_get_vector "c"); err (nsteps
+   doubles, may be NULL) receives each step's final calc_g cost and n_calc_g
+   (may be NULL) the number of calc_g evaluations. */
+int mg_clock_adams(mg_system* s, int order, int nsteps, double delta_t, double* err, long long* n_calc_g);
 
 /* ---- Nose-Hoover molecular dynamics ------------------------------------- */
 /* MD_NH "md nh nvt temp t_tar t_period eta_iteration .. eta_chains .." with

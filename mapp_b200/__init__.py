@@ -76,6 +76,7 @@ SIGNATURES = {
     "mg_batch_relax": (C.c_int, [_P, _P]),
     "mg_batch_cell_result": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mg_min_lbfgs": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _P, _P]),
+    "mg_clock_adams": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, _P, C.POINTER(C.c_longlong)]),
     "mg_md_nh": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _P,
                            C.c_int, _P, _P, _I]),
     "mg_cfg_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
@@ -348,6 +349,14 @@ class System:
         _check(load_library().mg_min_lbfgs(self.h, m, max_iter, fmax_tol, energy_tol, max_halvings, cluster,
                                            C.byref(r), C.byref(st)))
         return ({k: getattr(r, k) for k, _ in CellResult._fields_}, {k: getattr(st, k) for k, _ in BatchStats._fields_})
+
+    def clock_adams(self, order, steps, dt):
+        """Adams clock of this DMD system on the device (mg_clock_adams).
+        Returns dict(c, err, n_calc_g)."""
+        err = np.zeros(max(steps, 1))
+        ncg = C.c_longlong(0)
+        _check(load_library().mg_clock_adams(self.h, order, steps, dt, err.ctypes.data, C.byref(ncg)))
+        return {"c": self.vector("c"), "err": err[:steps], "n_calc_g": int(ncg.value)}
 
     def md_nh(self, t_tar, t_period, steps, dt, boltz, xd=None, seed=0, eta_iteration=1, eta_chains=3):
         """Nose-Hoover NVT run of this EAM / FS system on the device (mg_md_nh).

@@ -16,7 +16,7 @@ OUT = os.path.join(HERE, "libmapp_b200.so")
 BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["mg_api.cu", "mg_atoms.cu", "mg_eam.cu", "mg_dmd.cu", "mg_dmd32.cu", "mg_mlp.cu", "mg_noalloc.cu", "mg_batch.cu", "mg_cfg.cu", "mg_md.cu"]
+SOURCES = ["mg_api.cu", "mg_atoms.cu", "mg_eam.cu", "mg_dmd.cu", "mg_dmd32.cu", "mg_mlp.cu", "mg_noalloc.cu", "mg_batch.cu", "mg_cfg.cu", "mg_md.cu", "mg_clock.cu"]
 HEADERS = ["mg_internal.h", "mg_reduce.cuh", "mg_dmd_common.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -1365,6 +1365,7 @@ int mg_get_vector(mg_system* s, const char* name, double* out)
     else if (!strcmp(name, "ddE")) src = d.ddE, count = (size_t)s->natms * nt;
     else if (!strcmp(name, "n")) src = d.n, count = (size_t)s->natms * nt;
     else if (!strcmp(name, "c_d")) src = d.c_d, count = (size_t)s->natms * nt;
+    else if (!strcmp(name, "c") && s->dmd) src = d.c, count = (size_t)s->natms * nt;
     else if (!strcmp(name, "rho")) src = d.rho, count = (size_t)s->natms;
     else return fail(MG_ERR_ARG, "unknown vector %s", name);
     CHK(copy_out(s, out, src, count * sizeof(double)));
@@ -1663,3 +1664,24 @@ int mg::system_enqueue_force(mg_system* s, int st_clc, int zero, int* rows)
     return MG_OK;
 }
 double* mg::system_red_out(mg_system* s) { return s->red_out; }
+int mg::system_enqueue_calc_g(mg_system* s, int chk, double alpha, int* rows)
+{
+    if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "calc_g needs a DMD force field");
+    if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before calc_g");
+    Dev& d = s->d;
+    CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
+    CU(launch_dmd_calc_g(d, chk, alpha, rows, s->st));
+    CU(launch_reduce_partials(d, *rows, 1, s->red_out, s->st));
+    return MG_OK;
+}
+int mg::system_enqueue_c_d(mg_system* s)
+{
+    if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "c_d_calc needs a DMD force field");
+    if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before c_d_calc");
+    Dev& d = s->d;
+    size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
+    CU(cudaMemsetAsync(d.E, 0, bytes, s->st));
+    CU(cudaMemsetAsync(d.c_d, 0, bytes, s->st));
+    CU(launch_dmd_cdot(d, s->st));
+    return MG_OK;
+}

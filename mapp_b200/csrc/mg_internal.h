@@ -240,5 +240,9 @@ int system_rebuild(mg_system* s);
 // the EAM / FS passes); capturable
 int system_enqueue_force(mg_system* s, int st_clc, int zero, int* rows);
 double* system_red_out(mg_system* s);
+// enqueue calc_g's device work on the system's a_in (cost * 4 left in red_out[0],
+// g in the system's g unless chk) and c_d_calc's (c_d in the system's c_d); capturable
+int system_enqueue_calc_g(mg_system* s, int chk, double alpha, int* rows);
+int system_enqueue_c_d(mg_system* s);
 
 }  // namespace mg
