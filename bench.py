@@ -483,6 +483,45 @@ def run_md(mb, fx, device, steps=1000, ref_steps=300):
     return out
 
 
+def run_adams(mb, w, device, order=2, steps=20, ref_steps=1):
+    """Adams clock of the 32000-site DMD_I system (mg_clock_adams): order 2,
+    dt = 1e-3 tau with tau = 1 / rms(c_d) at the start, 20 steps, timed on the
+    host clock around the call (crd list, initial force, every calc_g / c_d
+    and the scalar read-backs included); beside it the reference's own
+    Clock_Adams on the same system for ref_steps steps on one core."""
+    s = mb.system_from_workload(w, device=device)
+    s.create_2nd_neigh_lst()
+    s.force_calc(1)
+    cd = s.c_d_calc()
+    tau = 1.0 / float(np.sqrt(np.mean(cd * cd)))
+    dt = 1e-3 * tau
+    s.clock_adams(order, 2, dt)  # warm-up
+    s.close()
+    s = mb.system_from_workload(w, device=device)
+    t0 = time.perf_counter()
+    r = s.clock_adams(order, steps, dt)
+    wall = time.perf_counter() - t0
+    n = s.natms
+    out = {"sites": n, "order": order, "steps": steps, "dt": dt, "tau": tau, "wall_s": wall,
+           "ms_per_step": wall * 1e3 / steps, "calc_g_calls": r["n_calc_g"],
+           "ms_per_calc_g": wall * 1e3 / max(r["n_calc_g"], 1), "final_cost_max": float(np.max(r["err"])),
+           "site_steps_per_s": n * steps / wall,
+           "timing": "host clock around mg_clock_adams (crd list, initial force, solves)"}
+    s.close()
+    from oracle import reference
+
+    if reference.available():
+        rr = reference.RefRun(w, workdir=tempfile.mkdtemp(prefix="mapp_adams_"), init=False)
+        rr.adams(order, ref_steps, dt)
+        meta = rr.run(timeout=1800)["adams"]["meta"]
+        t_ref = float(meta["time_run"])
+        out["cpu_baseline"] = {"value": n * ref_steps / t_ref, "unit": "site-steps/s", "cores": 1, "kind": "reference",
+                               "sample": f"reference Clock_Adams::run, {ref_steps} step(s) of the same system "
+                                         f"({meta['n_calc_g']} calc_g), {t_ref:.2f} s"}
+        out["speedup_vs_reference_core"] = out["site_steps_per_s"] / out["cpu_baseline"]["value"]
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -551,6 +590,7 @@ def run_ours(args):
         forms["batched"] = run_batched(mb, fx, local)
         forms["single_lbfgs"] = run_single_lbfgs(mb, w, local)
         forms["md_nh"] = run_md(mb, fx, local)
+        forms["clock_adams"] = run_adams(mb, w, local)
         forms["large"] = run_large_forms(mb, fx, local, s)
     s.set_form(form_id)
 
