@@ -292,6 +292,20 @@ int mg_cfg_types(const mg_cfg* c, char* names, int name_len, double* masses);
    natms * nt (DMD), velocity natms * 3 (MD); any may be NULL */
 int mg_cfg_atoms(const mg_cfg* c, double* x_frac, int* type, double* conc, double* velocity);
 int mg_cfg_free(mg_cfg* c);
+/* WriteCFG::write_file (write_cfg.cpp:119-433) for the default vector set
+   ("write cfg n prefix x" in MD mode, "... x c" in DMD mode; no auxiliary
+   vectors, no id sorting): writes <prefix>.<step as %08d>.cfg, and in DMD
+   mode the companion .usr file, byte for byte as the reference formats them
+   (six decimals, positions as unwrapped fractional coordinates).
+   mg_cfg_write_arrays takes host arrays: names ntypes slots of name_len
+   chars, masses ntypes, H the 3x3 lower-triangular box, x natms * x_dim
+   Cartesian (x_dim 3, or 3 + ntypes in DMD mode with the alphas), type
+   natms (MD) or c natms * ntypes (DMD).  mg_cfg_write writes an initialised
+   system's current owned state. */
+int mg_cfg_write_arrays(const char* prefix, int step, int dmd, int natms, int ntypes, const char* names,
+                        int name_len, const double* masses, const double* H, const double* x, const int* type,
+                        const double* c);
+int mg_cfg_write(mg_system* s, const char* prefix, int step);
 
 /* ---- device-resident minimiser for one system ---------------------------- */
 /* Min_LBFGS::run with LineSearch_BackTrack::line_min (min_l-bfgs.cpp:616-773,

@@ -84,6 +84,9 @@ SIGNATURES = {
     "mg_cfg_types": (C.c_int, [_P, _P, C.c_int, _P]),
     "mg_cfg_atoms": (C.c_int, [_P, _P, _P, _P, _P]),
     "mg_cfg_free": (C.c_int, [_P]),
+    "mg_cfg_write_arrays": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int, _P, _P,
+                                      _P, _P, _P]),
+    "mg_cfg_write": (C.c_int, [_P, C.c_char_p, C.c_int]),
 }
 
 
@@ -375,6 +378,11 @@ class System:
         return {"x": self.get_x(), "xd": vout, "energy": th[0], "virial": th[1:7], "ke": th[7], "t": th[8],
                 "eta_d": th[9:9 + eta_chains], "rebuilds": nreb.value}
 
+    def write_cfg(self, prefix, step=0):
+        """WriteCFG's file of this system's current state (mg_cfg_write)."""
+        _check(load_library().mg_cfg_write(self.h, str(prefix).encode(), step))
+        return "%s.%08d.cfg" % (prefix, step)
+
     def last_time(self, phase):
         ms = C.c_double(0.0)
         _check(load_library().mg_last_time(self.h, phase.encode(), C.byref(ms)))
@@ -487,6 +495,26 @@ def read_cfg(path: str, dmd: bool = False) -> dict:
         return out
     finally:
         L.mg_cfg_free(h)
+
+
+def write_cfg(prefix: str, step: int, names, masses, H, x, type=None, c=None):
+    """WriteCFG's file for host arrays (mg_cfg_write_arrays): x is Cartesian,
+    natms x 3 (MD, with type) or natms x (3 + nt) with the alphas (DMD, with c).
+    Returns the path of the .cfg file written."""
+    L = load_library()
+    dmd = c is not None
+    nt = len(names)
+    name_len = max(len(n) for n in names) + 1
+    nb = b"".join(n.encode().ljust(name_len, b"\0") for n in names)
+    m = np.ascontiguousarray(masses, dtype=np.float64)
+    Hm = np.ascontiguousarray(np.asarray(H, dtype=np.float64).reshape(9))
+    xa = np.ascontiguousarray(x, dtype=np.float64)
+    ta = None if dmd else np.ascontiguousarray(type, dtype=np.int32)
+    ca = np.ascontiguousarray(c, dtype=np.float64) if dmd else None
+    _check(L.mg_cfg_write_arrays(str(prefix).encode(), step, int(dmd), xa.shape[0], nt, nb, name_len, m.ctypes.data,
+                                 Hm.ctypes.data, xa.ctypes.data, None if dmd else ta.ctypes.data,
+                                 ca.ctypes.data if dmd else None))
+    return "%s.%08d.cfg" % (prefix, step)
 
 
 def system_from_workload(w: dict, device: int = 0, skin: float = 0.5) -> System:

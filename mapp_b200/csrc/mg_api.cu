@@ -1685,3 +1685,34 @@ int mg::system_enqueue_c_d(mg_system* s)
     CU(launch_dmd_cdot(d, s->st));
     return MG_OK;
 }
+
+// WriteCFG::write_file for the system's current owned state (the arrays
+// writer, mg_cfg.cu, does the formatting)
+extern "C" int mg_cfg_write(mg_system* s, const char* prefix, int step)
+{
+    CHK(check_sys(s));
+    if (!s->initialized) return fail(MG_ERR_STATE, "ff_init must run before a CFG is written");
+    const int n = s->natms, nt = s->nt;
+    int name_len = 1;
+    for (auto& nm : s->names) name_len = std::max(name_len, (int)nm.size() + 1);
+    std::vector<char> names((size_t)nt * name_len, 0);
+    for (int t = 0; t < nt; t++) memcpy(&names[(size_t)t * name_len], s->names[t].data(), s->names[t].size());
+    std::vector<double> x((size_t)n * s->x_dim + 1), c;
+    std::vector<int> type;
+    double H[9];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) H[3 * i + j] = s->H[i][j];
+    if (n > 0) {
+        CHK(mg_atoms_get_x(s, x.data()));
+        if (s->dmd) {
+            c.resize((size_t)n * nt);
+            CU(cudaMemcpyAsync(c.data(), s->d.c, c.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+        } else {
+            type.resize(n);
+            CU(cudaMemcpyAsync(type.data(), s->d.type, n * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+        }
+        CU(cudaStreamSynchronize(s->st));
+    }
+    return mg_cfg_write_arrays(prefix, step, s->dmd, n, nt, names.data(), name_len, s->masses.data(), H, x.data(),
+                               s->dmd ? nullptr : type.data(), s->dmd ? c.data() : nullptr);
+}

@@ -4,7 +4,10 @@
 // positions wrapped into [0, 1), species from the mass / name lines, MD
 // velocities (times R, in the frame of the file's box, as the reference
 // converts them) and DMD rows (s, alpha per species, c per species).
-// Host code only; no device memory is touched.
+// The writer restates WriteCFG::write_file (write_cfg.cpp:119-433) for the
+// default vector set (x, and c in DMD mode), without auxiliary vectors or id
+// sorting.  Host code only, except that mg_cfg_write first reads the
+// system's owned state back from the device.
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -341,6 +344,100 @@ int mg_cfg_atoms(const mg_cfg* c, double* x_frac, int* type, double* conc, doubl
 int mg_cfg_free(mg_cfg* c)
 {
     delete c;
+    return MG_OK;
+}
+
+int mg_cfg_write_arrays(const char* prefix, int step, int dmd, int natms, int ntypes, const char* names,
+                        int name_len, const double* masses, const double* H, const double* x, const int* type,
+                        const double* conc)
+{
+    if (!prefix || !names || !masses || !H || (natms > 0 && !x)) return cfail(MG_ERR_ARG, "null argument");
+    if (natms < 0 || ntypes < 1 || ntypes > mg::kMaxTypes || name_len < 1) return cfail(MG_ERR_ARG, "bad counts");
+    if (natms > 0 && (dmd ? !conc : !type)) return cfail(MG_ERR_ARG, dmd ? "null c" : "null type");
+    const int nt = ntypes, x_dim = dmd ? 3 + nt : 3;
+    // B = H^-1 as ReadCFG builds it (M3INV, init.h:72-85; read_cfg.cpp:453)
+    double A[3][3], B[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) A[i][j] = H[3 * i + j];
+    B[0][0] = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+    B[1][1] = A[2][2] * A[0][0] - A[2][0] * A[0][2];
+    B[2][2] = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+    B[1][0] = A[1][2] * A[2][0] - A[1][0] * A[2][2];
+    B[2][1] = A[2][0] * A[0][1] - A[2][1] * A[0][0];
+    B[0][2] = A[0][1] * A[1][2] - A[0][2] * A[1][1];
+    B[2][0] = A[1][0] * A[2][1] - A[2][0] * A[1][1];
+    B[0][1] = A[2][1] * A[0][2] - A[0][1] * A[2][2];
+    B[1][2] = A[0][2] * A[1][0] - A[1][2] * A[0][0];
+    double det = A[0][0] * B[0][0] + A[0][1] * B[1][0] + A[0][2] * B[2][0];
+    if (det == 0.0) return cfail(MG_ERR_ARG, "H determinant is zero");
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) B[i][j] /= det;
+    std::vector<char> name(name_len + 1, 0);
+    auto nm = [&](int t) {
+        memcpy(name.data(), names + (size_t)t * name_len, name_len);
+        name[name_len] = 0;
+        return (const char*)name.data();
+    };
+    char path[4096];
+    snprintf(path, sizeof(path), "%s.%08d.cfg", prefix, step);
+    FILE* fp = fopen(path, "w");
+    if (!fp) return cfail(MG_ERR_FILE, "cannot open %s", path);
+    fprintf(fp, "Number of particles = %d\n", natms);
+    fprintf(fp, "A = 1 Angstrom (basic length-scale)\n");
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) fprintf(fp, "H0(%d,%d) = %lf A\n", i + 1, j + 1, H[3 * i + j]);
+    fprintf(fp, ".NO_VELOCITY.\n");
+    fprintf(fp, "entry_count = %d\n", dmd ? x_dim + nt : 3);
+    // x2s_no_correction (atoms.cpp:1901-1920): fractional coordinates, not wrapped
+    double row[3 + mg::kMaxTypes];
+    auto s_of = [&](int i) {
+        const double* xi = x + (size_t)i * x_dim;
+        for (int k = 0; k < x_dim; k++) row[k] = xi[k];
+        for (int j = 0; j < 3; j++) {
+            row[j] = row[j] * B[j][j];
+            for (int k = j + 1; k < 3; k++) row[j] += B[k][j] * row[k];
+        }
+    };
+    if (!dmd) {
+        for (int t = 0; t < nt; t++) {
+            fprintf(fp, "%lf \n%s \n", masses[t], nm(t));
+            for (int i = 0; i < natms; i++) {
+                if (type[i] != t) continue;
+                s_of(i);
+                for (int k = 0; k < 3; k++) fprintf(fp, "%lf ", row[k]);
+                fprintf(fp, "\n");
+            }
+        }
+        fclose(fp);
+        return MG_OK;
+    }
+    int icomp = 0;
+    if (nt == 1) fprintf(fp, "auxiliary[%d] = alpha [reduced unit]\n", icomp++);
+    else
+        for (int k = 0; k < nt; k++) fprintf(fp, "auxiliary[%d] = alpha_%d [reduced unit]\n", icomp++, k);
+    if (nt > 1)
+        for (int k = 0; k < nt; k++) fprintf(fp, "auxiliary[%d] = c_%d [reduced unit]\n", icomp++, k);
+    else
+        fprintf(fp, "auxiliary[%d] = c [reduced unit]\n", icomp++);
+    for (int t = 0; t < nt; t++) fprintf(fp, "%lf \n%s \n", masses[t], nm(t));
+    for (int i = 0; i < natms; i++) {
+        s_of(i);
+        for (int k = 0; k < x_dim; k++) fprintf(fp, "%lf ", row[k]);
+        for (int k = 0; k < nt; k++) fprintf(fp, "%lf ", conc[(size_t)i * nt + k]);
+        fprintf(fp, "\n");
+    }
+    fclose(fp);
+    // the companion .usr file of 1 - c, indexed as the reference indexes it:
+    // entry i of the flat natms x nt array for atom i (write_cfg.cpp:415-420)
+    snprintf(path, sizeof(path), "%s.%08d.usr", prefix, step);
+    FILE* fu = fopen(path, "w");
+    if (!fu) return cfail(MG_ERR_FILE, "cannot open %s", path);
+    for (int i = 0; i < natms; i++) {
+        double tmp = 1.0 - conc[i];
+        fprintf(fu, "%f %f %f", tmp, tmp, tmp);
+        fprintf(fu, "\n");
+    }
+    fclose(fu);
     return MG_OK;
 }
 

@@ -15,6 +15,8 @@
  *   force / energy / crd / cdot / calcg call the ForceField virtuals.
  *   lbfgs   = Min_LBFGS (min_l-bfgs.cpp) constructed, init, run, fin, with
  *             the energy of every force_calc logged by the oracle subclass.
+ *   writecfg = WriteCFG (write_cfg.cpp) "write cfg 1 prefix x [c]" and one
+ *             write_file(step) of the current state.
  *   adams   = Clock_Adams (clock_adams.cpp) constructed, init, run, then the
  *             owned c and the number of calc_g calls written before fin.
  *   md      = MD_NH "nvt" (md_nh.cpp) constructed, time_step / boltzmann set,
@@ -61,6 +63,7 @@
 #include "min_l-bfgs.h"
 #include "md_nh.h"
 #include "clock_adams.h"
+#include "write_cfg.h"
 
 using namespace MAPP_NS;
 
@@ -447,6 +450,19 @@ void do_time(const std::string& what, int reps, const std::string& prefix)
     meta(prefix, "time_%s %d %.9g", what.c_str(), reps, t1 - t0);
 }
 
+/* WriteCFG (write_cfg.cpp) with the default vector set, one file */
+void do_writecfg(const std::string& prefix, int step)
+{
+    std::vector<std::string> a = {"write", "cfg", "1", prefix, "x"};
+    if (H.dmd) a.push_back("c");
+    std::vector<char*> argv;
+    for (auto& t : a) argv.push_back(strdup(t.c_str()));
+    WriteCFG* wr = new WriteCFG(H.mapp, (int)argv.size(), argv.data());
+    wr->write_file(step);
+    delete wr;
+    for (char* t : argv) free(t);
+}
+
 template <class Base>
 bool calc_g_count(ForceField* ff, long* n)
 {
@@ -552,6 +568,12 @@ void run_command(const std::string& line)
     else if (cmd == "setx") { std::string xp, p; rs >> xp >> p; do_setx(xp, p); }
     else if (cmd == "setc") { std::string cp; rs >> cp; do_setc(cp); }
     else if (cmd == "lbfgs") { int m, k; double tol; std::string p; rs >> m >> k >> tol >> p; do_lbfgs(m, k, tol, p); }
+    else if (cmd == "writecfg") {
+        std::string p;
+        int step;
+        rs >> p >> step;
+        do_writecfg(p, step);
+    }
     else if (cmd == "adams") {
         int order, n;
         std::string dt, p;

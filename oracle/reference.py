@@ -107,6 +107,10 @@ class RefRun:
         self.steps.append(("lbfgs", tag))
         return self.add(f"lbfgs {m} {max_iter} {energy_tol!r} {self._p(tag)}")
 
+    def writecfg(self, prefix: str, step: int = 0):
+        """The reference WriteCFG's file of the current state (x, and c in DMD mode)."""
+        return self.add(f"writecfg {prefix} {step}")
+
     def adams(self, order: int, steps: int, dt: float, tag="adams"):
         """The reference Clock_Adams: init, run, fin (construct with init=False)."""
         self.steps.append(("adams", tag))

@@ -139,3 +139,22 @@ def test_compressed_lattice_grows_the_list(tmp_path, kind):
     assert sizes.max() > (96 if kind == "dmd" else 64)
     check_state(s, o)
     check_forces(s, o, kind == "dmd")
+
+
+@pytest.mark.parametrize("kind,kw", [("eam", dict(n=3, sigma=0.05, nt=2, fmt="FS")),
+                                     ("dmd", dict(n=3, sigma=0.02, style="DMD_I"))], ids=["eam2", "dmd"])
+def test_write_cfg_of_a_system_matches_reference(tmp_path, kind, kw):
+    """mg_cfg_write of an initialised system: the same bytes as the reference's
+    WriteCFG after its own set-up (the positions after set-up are bit-exact)."""
+    mb = _mb()
+    from oracle import reference
+
+    if not reference.available():
+        pytest.skip("reference harness not built")
+    w = fx.write_workload(str(tmp_path / "w"), kind, **kw)
+    ref_prefix = str(tmp_path / "ref_out")
+    reference.RefRun(w, workdir=str(tmp_path / "ref")).writecfg(ref_prefix, 3).run()
+    s = mb.system_from_workload(w)
+    path = s.write_cfg(str(tmp_path / "ours"), 3)
+    with open(path, "rb") as a, open(ref_prefix + ".00000003.cfg", "rb") as b:
+        assert a.read() == b.read()
