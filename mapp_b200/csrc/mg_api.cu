@@ -226,6 +226,7 @@ struct mg_system {
     double* d_phiT = nullptr;
     double* d_FT = nullptr;
     float* d_pkT = nullptr;
+    double* d_pk64 = nullptr;
     float* d_pkC = nullptr;
     int* cursor = nullptr;
     int crd_built = 0;
@@ -685,6 +686,22 @@ int upload_tables(mg_system* s)
         CHK(dalloc(&s->d_pkT, pk.size()));
         CU(cudaMemcpy(s->d_pkT, pk.data(), pk.size() * sizeof(float), cudaMemcpyHostToDevice));
         d.pkT = reinterpret_cast<const float4*>(s->d_pkT);
+        // plain form: the same pairing, coefficients copied unchanged
+        std::vector<double> pk64((size_t)nt * nt * nr * 8, 0.0);
+        for (int a = 0; a < nt; a++)
+            for (int b = 0; b < nt; b++)
+                for (int m = 0; m < nr; m++) {
+                    double* dst = pk64.data() + (((size_t)(a * nt + b) * nr + m) * 8);
+                    const double* rr = s->rhoT.data() + ((size_t)(b * nt + a) * nr + m) * 8;
+                    for (int k = 0; k < 4; k++) dst[k] = rr[k];
+                    if (a >= b) {
+                        const double* pp = s->phiT.data() + ((size_t)comp_idx(a, b) * nr + m) * 8;
+                        for (int k = 0; k < 4; k++) dst[4 + k] = pp[k];
+                    }
+                }
+        CHK(dalloc(&s->d_pk64, pk64.size()));
+        CU(cudaMemcpy(s->d_pk64, pk64.data(), pk64.size() * sizeof(double), cudaMemcpyHostToDevice));
+        d.pk64 = s->d_pk64;
         // Coarse copy for the precision form's pass 1: kCoarseKnots knots over
         // [0, rc], each interval the cubic Hermite piece through the fine
         // spline's value and slope at its ends (fine interpolant evaluated as in
@@ -811,7 +828,7 @@ int mg_destroy(mg_system* s)
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->st);
     Dev& d = s->d;
-    void* ptrs[] = {d.prf, s->d_pkT, s->d_pkC, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
+    void* ptrs[] = {d.prf, s->d_pkT, s->d_pk64, s->d_pkC, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
                     d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status,
                     s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};

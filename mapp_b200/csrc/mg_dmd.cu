@@ -30,6 +30,9 @@ namespace {
 #ifndef MG_DMD_MINB
 #define MG_DMD_MINB 3
 #endif
+#ifndef MG_DMD_PACK
+#define MG_DMD_PACK true
+#endif
 
 template <int NT, int NQ>
 __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int row0)
@@ -77,8 +80,10 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int 
                     bool hit = false;
                     if (in_cut) {
                         double alpha = (ai[a] * aj[b]) / (ai[a] + aj[b]);
-                        hit = (a >= b) ? smear<true, true, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr, gda, f0, fdr, fda)
-                                       : smear<false, true, NQ>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr, gda, f0, fdr, fda);
+                        hit = (a >= b) ? smear<true, true, NQ, MG_DMD_PACK>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr,
+                                                                            gda, f0, fdr, fda, a * NT + b)
+                                       : smear<false, true, NQ, MG_DMD_PACK>(d, rs, ps, r, r_inv, rsq, alpha, g0, gdr,
+                                                                             gda, f0, fdr, fda, a * NT + b);
                     }
                     if (!hit) g0 = gdr = gda = f0 = fdr = fda = 0.0;
                     __stcs(out + (S::RHO + rs) * mp, g0);

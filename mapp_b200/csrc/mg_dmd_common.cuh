@@ -59,10 +59,13 @@ __device__ __forceinline__ void embed_F(const Dev& d, int a, double Ev, double& 
 // against the cut-offs) are computed exactly as the reference does; powers of
 // alpha and 1/r come from rsqrt, which moves results by ulps only (the node and
 // table-index decisions they feed are continuous in the result).
-template <bool kPhi, bool kDeriv, int NQ>
+// kPack: read the node knots from the paired table d.pk64 (record kslot =
+// a*nt+b of the ordered species pair, rho at +0, phi at +4) instead of the
+// separate rho / phi tables; the coefficients are the same doubles.
+template <bool kPhi, bool kDeriv, int NQ, bool kPack = false>
 __device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double r, double r_inv, double rsq,
                                       double alpha, double& g0, double& g_dr, double& g_da, double& f0, double& f_dr,
-                                      double& f_da)
+                                      double& f_da, int kslot = 0)
 {
     if (d.alpha_min < alpha && alpha < d.alpha_max) {
         const int nq = NQ > 0 ? NQ : d.nq;
@@ -72,8 +75,8 @@ __device__ __forceinline__ bool smear(const Dev& d, int rslot, int pslot, double
         double upper = (r + d.rc) * asq, lower = (r - d.rc) * asq;
         if (!(lower < d.xi[nq - 1])) return false;
         double fa = 0.0, fb = 0.0, fc = 0.0, ga = 0.0, gb = 0.0, gc = 0.0;
-        const double* rt = d.rhoT + (size_t)rslot * d.nr * 8;
-        const double* pt = d.phiT + (size_t)pslot * d.nr * 8;
+        const double* rt = kPack ? d.pk64 + (size_t)kslot * d.nr * 8 : d.rhoT + (size_t)rslot * d.nr * 8;
+        const double* pt = kPack ? rt + 4 : d.phiT + (size_t)pslot * d.nr * 8;
 #pragma unroll
         for (int q = 0; q < (NQ > 0 ? NQ : kMaxQuad); q++) {
             if (NQ == 0 && q >= nq) break;

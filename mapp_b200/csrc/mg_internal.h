@@ -100,6 +100,10 @@ struct Dev {
     // precision form: per ordered species pair (a,b) and knot, one 32-byte
     // sector {rho c0..c3 of slot b*nt+a, phi c0..c3 of slot COMP(a,b) (zero when a < b)}
     const float4* pkT;
+    // the plain form's copy of the same pairing in FP64: per ordered species
+    // pair (a,b) and knot one 64-byte record {rho c0..c3, phi c0..c3}, so the
+    // two knots a quadrature node needs share one cache line
+    const double* pk64;
     // the same splines resampled onto kCoarseKnots knots over [0, rc] (FP32,
     // packed the same way), small enough for a shared-memory copy in pass 1
     const float4* pkC;
