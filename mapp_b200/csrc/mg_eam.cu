@@ -20,10 +20,31 @@ namespace {
 
 __device__ __forceinline__ int owner(const Dev& d, int j) { return j < d.natms ? j : d.root[j]; }
 
+// One knot row of a spline table (8 doubles: c0..c3 of the value, c4..c6 of
+// the derivative, one pad) as two 32-byte read-only loads.
+struct Row8 {
+    double4 v, dv;
+};
+__device__ __forceinline__ Row8 row8(const double* __restrict__ row)
+{
+    Row8 r;
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(r.v.x), "=d"(r.v.y), "=d"(r.v.z), "=d"(r.v.w) : "l"(row));
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+        : "=d"(r.dv.x), "=d"(r.dv.y), "=d"(r.dv.z), "=d"(r.dv.w)
+        : "l"(row + 4));
+    return r;
+}
+
+// Resident blocks per SM the EAM pass 1 is compiled for (64 registers a
+// thread at 4): a small system's warps then fit one wave.
+#ifndef MG_EAM_MINB
+#define MG_EAM_MINB 4
+#endif
+
 // EAM pass 1 (ff_eam.cpp:95-177).  energy_only skips forces and stored
 // derivatives (ForceField_eam::energy_calc, ff_eam.cpp:297-338).
 template <bool kEnergyOnly>
-__global__ void __launch_bounds__(kFFBlock) k_eam_pass1(Dev d, int st_clc, int row0)
+__global__ void __launch_bounds__(kFFBlock, MG_EAM_MINB) k_eam_pass1(Dev d, int st_clc, int row0)
 {
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
@@ -49,14 +70,14 @@ __global__ void __launch_bounds__(kFFBlock) k_eam_pass1(Dev d, int st_clc, int r
                 int m = min((int)p, d.nr - 2);
                 p -= m;
                 p = fmin(p, 1.0);
-                const double* cf = d.rhoT + ((size_t)(ti * nt + tj) * d.nr + m) * 8;
-                double rho_iv = ((cf[3] * p + cf[2]) * p + cf[1]) * p + cf[0];
-                double drho_i = (cf[6] * p + cf[5]) * p + cf[4];
-                const double* cg = d.rhoT + ((size_t)(tj * nt + ti) * d.nr + m) * 8;
-                double rho_jv = ((cg[3] * p + cg[2]) * p + cg[1]) * p + cg[0];
-                double drho_j = (cg[6] * p + cg[5]) * p + cg[4];
-                const double* ch = d.phiT + ((size_t)comp_idx(ti, tj) * d.nr + m) * 8;
-                double z2 = ((ch[3] * p + ch[2]) * p + ch[1]) * p + ch[0];
+                const Row8 cf = row8(d.rhoT + ((size_t)(ti * nt + tj) * d.nr + m) * 8);
+                double rho_iv = ((cf.v.w * p + cf.v.z) * p + cf.v.y) * p + cf.v.x;
+                double drho_i = (cf.dv.z * p + cf.dv.y) * p + cf.dv.x;
+                const Row8 cg = row8(d.rhoT + ((size_t)(tj * nt + ti) * d.nr + m) * 8);
+                double rho_jv = ((cg.v.w * p + cg.v.z) * p + cg.v.y) * p + cg.v.x;
+                double drho_j = (cg.dv.z * p + cg.dv.y) * p + cg.dv.x;
+                const Row8 ch = row8(d.phiT + ((size_t)comp_idx(ti, tj) * d.nr + m) * 8);
+                double z2 = ((ch.v.w * p + ch.v.z) * p + ch.v.y) * p + ch.v.x;
                 double phi = z2 * r_inv;
                 rho_i += rho_iv;
                 bool own_j = j < d.natms;
@@ -64,7 +85,7 @@ __global__ void __launch_bounds__(kFFBlock) k_eam_pass1(Dev d, int st_clc, int r
                 double w = own_j ? 1.0 : 0.5;
                 acc[0] += w * phi;
                 if (!kEnergyOnly) {
-                    double z2p = (ch[6] * p + ch[5]) * p + ch[4];
+                    double z2p = (ch.dv.z * p + ch.dv.y) * p + ch.dv.x;
                     double dphi = z2p * r_inv - phi * r_inv;
                     double fpair = -dphi * r_inv;
                     fx += fpair * dx0;
