@@ -13,7 +13,8 @@
  *   DMD_I / DMD_II / DMD  force_calc / energy_calc / create_2nd_neigh_lst /
  *           c_d_calc / calc_g / interpolate_m (ff_dmd_I.cpp:88-668,1760-2674;
  *           ff_dmd_II.cpp:2151-2630; ff_dmd.cpp:2221-2606)
- *   callers Min_LBFGS + LineSearch_BackTrack (min_l-bfgs.cpp, line_search.cpp),
+ *   callers Min_LBFGS, Min_CG + LineSearch_BackTrack (min_l-bfgs.cpp, min_cg.cpp,
+ *           line_search.cpp),
  *           MD_NH without a barostat (md_nh.cpp, rand_engine.cpp) and
  *           Clock_Adams (clock_adams.cpp)
  *
@@ -1740,6 +1741,58 @@ static double ls_energy(orc_t* o, const double* x_prev, const double* h, double 
     return orc_energy(o);
 }
 
+
+/* LineSearch_BackTrack::line_min, DMD and fixed-box branch
+   (line_search.cpp:223-241, 300-340; c = 0.4, rho = 0.5, alpha_max = 1,
+   d_max = 1): normalises h in place; on success curr_energy and alpha_m are
+   the accepted point's, on ALPHAMIN the state is back at x0 (energy(0)). */
+static int line_min(orc_t* o, const double* x0, double* h, const double* f, double* curr_energy, double* alpha_m,
+                    double* ls_alpha_min, int max_halvings, double* xw, double* fw, int* nevals)
+{
+    const int nt = o->nt;
+    const size_t n = (size_t)o->natms * o->x_dim;
+    int err = ORC_LS_S;
+    double min_h = INFINITY;
+    for (int i = 0; i < o->natms; i++)
+        for (int j = 0; j < nt; j++) min_h = MINV(min_h, o->x[(size_t)i * (3 + nt) + 3 + j]);
+    min_h *= 0.99;
+    *ls_alpha_min = MINV(*ls_alpha_min, min_h);
+    double hh = 0.0;
+    for (size_t j = 0; j < n; j++) hh += h[j] * h[j];
+    hh = 1.0 / sqrt(hh);
+    for (size_t j = 0; j < n; j++) h[j] *= hh;
+    double fh = 0.0;
+    for (size_t j = 0; j < n; j++) fh += f[j] * h[j];
+    if (fh <= 0) err = ORC_LS_F_DOWNHILL;
+    double max_h = 0.0;
+    if (err == ORC_LS_S) {
+        for (size_t j = 0; j < n; j++) max_h = MAXV(max_h, fabs(h[j]));
+        if (max_h == 0) err = ORC_LS_F_GRAD0;
+    }
+    double a = 0.0;
+    if (err == ORC_LS_S) {
+        a = MINV(1.0, max_h);
+        if (a <= *ls_alpha_min) err = ORC_LS_F_ALPHAMIN;
+    }
+    int halvings = 0;
+    while (err == ORC_LS_S) {
+        double ideal_energy = *curr_energy - a * 0.4 * fh;
+        double cur = ls_energy(o, x0, h, a, xw, nevals, fw);
+        if (cur <= ideal_energy) {
+            *curr_energy = cur;
+            *alpha_m = a;
+            break;
+        }
+        a *= 0.5;
+        halvings++;
+        if (a <= *ls_alpha_min || (max_halvings > 0 && halvings >= max_halvings)) {
+            *curr_energy = ls_energy(o, x0, h, 0.0, xw, nevals, fw);
+            err = ORC_LS_F_ALPHAMIN;
+        }
+    }
+    return err;
+}
+
 /*
  * Min_LBFGS::init tail and Min_LBFGS::run, fixed-box branch
  * (min_l-bfgs.cpp:277-286, 616-773), with LineSearch_BackTrack::line_min, DMD
@@ -1767,7 +1820,7 @@ static double ls_energy(orc_t* o, const double* x_prev, const double* h, double 
 int orc_lbfgs(orc_t* o, int m, int max_iter, double energy_tol, double fmax_tol, int max_halvings,
               int ls_force_energy, double* e_hist, int* err_out, int* nevals_out)
 {
-    const int xd = o->x_dim, nt = o->nt;
+    const int xd = o->x_dim;
     const size_t n = (size_t)o->natms * xd;
     double* f = calloc(n, sizeof(double));
     double* h = calloc(n, sizeof(double));
@@ -1818,47 +1871,8 @@ int orc_lbfgs(orc_t* o, int m, int max_iter, double energy_tol, double fmax_tol,
         double prev_energy = curr_energy;
         /* line_min(curr_energy, alpha_m) */
         double alpha_m = 0.0;
-        {
-            double min_h = INFINITY;
-            for (int i = 0; i < o->natms; i++)
-                for (int j = 0; j < nt; j++) min_h = MINV(min_h, o->x[(size_t)i * (3 + nt) + 3 + j]);
-            min_h *= 0.99;
-            ls_alpha_min = MINV(ls_alpha_min, min_h);
-            double hh = 0.0;
-            for (size_t j = 0; j < n; j++) hh += h[j] * h[j];
-            hh = 1.0 / sqrt(hh);
-            for (size_t j = 0; j < n; j++) h[j] *= hh;
-            double fh = 0.0;
-            for (size_t j = 0; j < n; j++) fh += f[j] * h[j];
-            nls++;
-            if (fh <= 0) err = ORC_LS_F_DOWNHILL;
-            double max_h = 0.0;
-            if (err == ORC_LS_S) {
-                for (size_t j = 0; j < n; j++) max_h = MAXV(max_h, fabs(h[j]));
-                if (max_h == 0) err = ORC_LS_F_GRAD0;
-            }
-            double a = 0.0;
-            if (err == ORC_LS_S) {
-                a = MINV(1.0, max_h);
-                if (a <= ls_alpha_min) err = ORC_LS_F_ALPHAMIN;
-            }
-            int halvings = 0;
-            while (err == ORC_LS_S) {
-                double ideal_energy = curr_energy - a * 0.4 * fh;
-                double cur = ls_energy(o, x0, h, a, xw, &nevals, fw);
-                if (cur <= ideal_energy) {
-                    curr_energy = cur;
-                    alpha_m = a;
-                    break;
-                }
-                a *= 0.5;
-                halvings++;
-                if (a <= ls_alpha_min || (max_halvings > 0 && halvings >= max_halvings)) {
-                    curr_energy = ls_energy(o, x0, h, 0.0, xw, &nevals, fw);
-                    err = ORC_LS_F_ALPHAMIN;
-                }
-            }
-        }
+        nls++;
+        err = line_min(o, x0, h, f, &curr_energy, &alpha_m, &ls_alpha_min, max_halvings, xw, fw, &nevals);
         if (err == ORC_LS_S && prev_energy - curr_energy < energy_tol) err = ORC_MIN_F_TOLERANCE;
         if (err == ORC_LS_S && istp == max_iter) err = ORC_MIN_F_MAX_ITER;
         orc_force(o, 1, f, en);
@@ -1907,6 +1921,85 @@ int orc_lbfgs(orc_t* o, int m, int max_iter, double energy_tol, double fmax_tol,
     if (err_out) *err_out = err;
     if (nevals_out) *nevals_out = nevals;
     free(f); free(h); free(x0); free(f0); free(xw); free(fw); free(sv); free(yv); free(s_list); free(rho); free(alpha);
+    return nls;
+}
+
+/*
+ * Min_CG::init tail and Min_CG::run, fixed-box branch (min_cg.cpp:185-205,
+ * 449-562): Polak-Ribiere conjugate gradient with the same line_min as
+ * orc_lbfgs (which normalises h in place, so the next direction is
+ * h = ratio * h_normalised + f).  Stopping, fmax_tol, max_halvings and
+ * ls_force_energy as in orc_lbfgs; f0_f0 == 0 ends with LS_F_GRAD0
+ * (min_cg.cpp:466-470).  Returns the number of line searches.
+ */
+int orc_cg(orc_t* o, int max_iter, double energy_tol, double fmax_tol, int max_halvings, int ls_force_energy,
+           double* e_hist, int* err_out, int* nevals_out)
+{
+    const int xd = o->x_dim;
+    const size_t n = (size_t)o->natms * xd;
+    double* f = calloc(n, sizeof(double));
+    double* h = calloc(n, sizeof(double));
+    double* x0 = calloc(n, sizeof(double));
+    double* f0 = calloc(n, sizeof(double));
+    double* xw = calloc(n, sizeof(double));
+    double* fw = ls_force_energy ? calloc(n, sizeof(double)) : NULL;
+    int nevals = 0, nls = 0;
+    double en[7];
+    orc_force(o, 1, f, en);
+    nevals++;
+    double curr_energy = en[0];
+    if (e_hist) e_hist[0] = curr_energy;
+    double ls_alpha_min = 0.0, inner, f0_f0, f_f, f_f0, f_h, ratio;
+    int istp = 0, err = ORC_LS_S;
+    memcpy(h, f, n * sizeof(double));
+    inner = 0.0;
+    for (size_t i = 0; i < n; i++) inner += f[i] * f[i];
+    f0_f0 = inner;
+    while (err == ORC_LS_S) {
+        if (f0_f0 == 0.0) {
+            err = ORC_LS_F_GRAD0;
+            continue;
+        }
+        for (int i = 0; i < o->natms; i++)
+            for (int k = 0; k < xd; k++) x0[(size_t)i * xd + k] = o->x[(size_t)i * xd + k];
+        memcpy(f0, f, n * sizeof(double));
+        double prev_energy = curr_energy, alpha_m = 0.0;
+        nls++;
+        err = line_min(o, x0, h, f, &curr_energy, &alpha_m, &ls_alpha_min, max_halvings, xw, fw, &nevals);
+        if (err == ORC_LS_S && prev_energy - curr_energy < energy_tol) err = ORC_MIN_F_TOLERANCE;
+        if (err == ORC_LS_S && istp == max_iter) err = ORC_MIN_F_MAX_ITER;
+        memset(f, 0, n * sizeof(double));
+        orc_force(o, 1, f, en);
+        nevals++;
+        curr_energy = en[0];
+        if (e_hist) e_hist[istp + 1] = curr_energy;
+        if (err == ORC_LS_S && fmax_tol > 0.0) {
+            double fm = 0.0;
+            for (size_t j = 0; j < n; j++) fm = MAXV(fm, fabs(f[j]));
+            if (fm < fmax_tol) err = ORC_MIN_F_TOLERANCE;
+        }
+        if (err) continue;
+        inner = 0.0;
+        for (size_t i = 0; i < n; i++) inner += f[i] * f[i];
+        f_f = inner;
+        inner = 0.0;
+        for (size_t i = 0; i < n; i++) inner += f[i] * f0[i];
+        f_f0 = inner;
+        ratio = (f_f - f_f0) / (f0_f0);
+        inner = 0.0;
+        for (size_t i = 0; i < n; i++) {
+            h[i] *= ratio;
+            h[i] += f[i];
+            inner += h[i] * f[i];
+        }
+        f_h = inner;
+        if (f_h < 0.0) memcpy(h, f, n * sizeof(double));
+        f0_f0 = f_f;
+        istp++;
+    }
+    if (err_out) *err_out = err;
+    if (nevals_out) *nevals_out = nevals;
+    free(f); free(h); free(x0); free(f0); free(xw); free(fw);
     return nls;
 }
 

@@ -15,6 +15,7 @@
  *   force / energy / crd / cdot / calcg call the ForceField virtuals.
  *   lbfgs   = Min_LBFGS (min_l-bfgs.cpp) constructed, init, run, fin, with
  *             the energy of every force_calc logged by the oracle subclass.
+ *   cg      = Min_CG (min_cg.cpp), the same way.
  *   writecfg = WriteCFG (write_cfg.cpp) "write cfg 1 prefix x [c]" and one
  *             write_file(step) of the current state.
  *   adams   = Clock_Adams (clock_adams.cpp) constructed, init, run, then the
@@ -61,6 +62,7 @@
 #include "ff_dmd_II.h"
 #include "ff_dmd.h"
 #include "min_l-bfgs.h"
+#include "min_cg.h"
 #include "md_nh.h"
 #include "clock_adams.h"
 #include "write_cfg.h"
@@ -151,6 +153,13 @@ private:
 /* the reference minimiser with its protected result fields exposed */
 struct LbfgsRun : public Min_LBFGS {
     LbfgsRun(MAPP* m, int narg, char** arg) : Min_LBFGS(m, narg, arg) {}
+    int code() const { return err; }
+    double energy() const { return curr_energy; }
+};
+
+/* the reference CG minimiser with its protected result fields exposed */
+struct CgRun : public Min_CG {
+    CgRun(MAPP* m, int narg, char** arg) : Min_CG(m, narg, arg) {}
     int code() const { return err; }
     double energy() const { return curr_energy; }
 };
@@ -265,6 +274,34 @@ void do_lbfgs(int m, int max_iter, double etol, const std::string& prefix)
     std::vector<double> log;
     if (!ff_log(&log, nullptr)) { fprintf(stderr, "harness: lbfgs needs an oracle DMD force field\n"); exit(2); }
     LbfgsRun* mn = new LbfgsRun(H.mapp, (int)argv.size(), argv.data());
+    mn->init();
+    mn->run();
+    long n_energy = 0;
+    ff_log(nullptr, &n_energy);
+    Atoms* atoms = H.mapp->atoms;
+    double* x = vec<double>("x");
+    write_raw(prefix + ".x.bin", x, sizeof(double) * (size_t)atoms->natms * H.x_dim);
+    write_raw(prefix + ".ehist.bin", log.data(), sizeof(double) * log.size());
+    meta(prefix, "code %d", mn->code());
+    meta(prefix, "energy %.17g", mn->energy());
+    meta(prefix, "n_force %d", (int)log.size());
+    meta(prefix, "n_energy %ld", n_energy);
+    mn->fin();
+    delete mn;
+    for (char* t : argv) free(t);
+}
+
+/* Min_CG (min_cg.cpp) run on the scripted system, outputs as do_lbfgs */
+void do_cg(int max_iter, double etol, const std::string& prefix)
+{
+    char buf[64];
+    snprintf(buf, sizeof(buf), "%.17g", etol);
+    std::vector<std::string> a = {"min", "cg", "max_iteration", std::to_string(max_iter), "energy_tol", buf};
+    std::vector<char*> argv;
+    for (auto& t : a) argv.push_back(strdup(t.c_str()));
+    std::vector<double> log;
+    if (!ff_log(&log, nullptr)) { fprintf(stderr, "harness: cg needs an oracle DMD force field\n"); exit(2); }
+    CgRun* mn = new CgRun(H.mapp, (int)argv.size(), argv.data());
     mn->init();
     mn->run();
     long n_energy = 0;
@@ -567,6 +604,7 @@ void run_command(const std::string& line)
     else if (cmd == "calcg") { int chk; double a; std::string ap, p; rs >> chk >> a >> ap >> p; do_calcg(chk, a, ap, p); }
     else if (cmd == "setx") { std::string xp, p; rs >> xp >> p; do_setx(xp, p); }
     else if (cmd == "setc") { std::string cp; rs >> cp; do_setc(cp); }
+    else if (cmd == "cg") { int k; double tol; std::string p; rs >> k >> tol >> p; do_cg(k, tol, p); }
     else if (cmd == "lbfgs") { int m, k; double tol; std::string p; rs >> m >> k >> tol >> p; do_lbfgs(m, k, tol, p); }
     else if (cmd == "writecfg") {
         std::string p;

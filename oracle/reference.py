@@ -107,6 +107,11 @@ class RefRun:
         self.steps.append(("lbfgs", tag))
         return self.add(f"lbfgs {m} {max_iter} {energy_tol!r} {self._p(tag)}")
 
+    def cg(self, max_iter: int, energy_tol: float, tag="cg"):
+        """The reference Min_CG: init, run, fin (construct with init=False)."""
+        self.steps.append(("cg", tag))
+        return self.add(f"cg {max_iter} {energy_tol!r} {self._p(tag)}")
+
     def writecfg(self, prefix: str, step: int = 0):
         """The reference WriteCFG's file of the current state (x, and c in DMD mode)."""
         return self.add(f"writecfg {prefix} {step}")

@@ -71,6 +71,9 @@ def lib():
         L.orc_lbfgs.argtypes = [P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, dp,
                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_lbfgs.restype = C.c_int
+        L.orc_cg.argtypes = [P, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, dp, C.POINTER(C.c_int),
+                             C.POINTER(C.c_int)]
+        L.orc_cg.restype = C.c_int
         L.orc_md_nh.argtypes = [P, dp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                 dp, C.c_int, dp]
         L.orc_md_nh.restype = C.c_int
@@ -273,6 +276,16 @@ class Oracle:
         nev = C.c_int(0)
         nls = lib().orc_lbfgs(self.h, m, max_iter, energy_tol, fmax_tol, max_halvings, int(ls_force_energy), e,
                               C.byref(err), C.byref(nev))
+        x = self.x_all()[: self.counts()["natms"]]
+        return {"code": err.value, "line_searches": nls, "evals": nev.value, "energies": e[: nls + 1], "x": x}
+
+    def cg(self, max_iter=10000, energy_tol=1e-8, fmax_tol=0.0, max_halvings=0, ls_force_energy=False):
+        """Min_CG run (orc_cg): returns dict(code, line_searches, evals, energies, x) as lbfgs()."""
+        e = np.zeros(max_iter + 2)
+        err = C.c_int(0)
+        nev = C.c_int(0)
+        nls = lib().orc_cg(self.h, max_iter, energy_tol, fmax_tol, max_halvings, int(ls_force_energy), e,
+                           C.byref(err), C.byref(nev))
         x = self.x_all()[: self.counts()["natms"]]
         return {"code": err.value, "line_searches": nls, "evals": nev.value, "energies": e[: nls + 1], "x": x}
 

@@ -80,3 +80,28 @@ def test_reference_dmd_forces_are_not_the_energy_gradient():
     assert 1e-3 < e1_3 < 0.2
     assert 1e-3 < e1_10 < 0.2
     assert e2_10 > 0.2
+
+
+@needs_ref
+@pytest.mark.parametrize("style", ["DMD_I", "DMD_II", "DMD"])
+def test_cg_restatement_matches_reference_bit_for_bit(style):
+    """One species: 60 iterations of the reference's Min_CG (Polak-Ribiere with
+    the same backtracking line search), every force_calc energy and the final
+    x identical to orc_cg's."""
+    w = fx.write_workload(tempfile.mkdtemp(), "dmd", n=3, sigma=0.03, nt=1, style=style)
+    r = reference.RefRun(w, init=False).cg(60, 1e-12).run()["cg"]
+    o = Oracle(w).cg(60, 1e-12)
+    assert o["code"] == int(r["meta"]["code"])
+    assert np.array_equal(o["energies"], r["ehist"])
+    assert np.array_equal(o["x"].ravel(), r["x"])
+
+
+@needs_ref
+def test_cg_two_species_reference_fails_its_first_line_search():
+    """Two species: Min_CG's line search meets the same energy_calc defect as
+    Min_LBFGS's and stops with LS_F_ALPHAMIN; the restatement agrees."""
+    w = fx.write_workload(tempfile.mkdtemp(), "dmd", n=3, sigma=0.03, style="DMD_I")
+    r = reference.RefRun(w, init=False).cg(20, 1e-12).run()["cg"]
+    o = Oracle(w).cg(20, 1e-12)
+    assert int(r["meta"]["code"]) == o["code"] == 3
+    assert np.array_equal(o["energies"], r["ehist"])
