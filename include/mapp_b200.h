@@ -46,6 +46,9 @@ typedef struct mg_system mg_system;
                                  Kahan-compensated per-site sums, FP64 totals      */
 #define MG_FORM_MLP 2         /* learned form: BF16 MLP replaces DMD quadrature    */
 
+#define MG_MIN_LBFGS 0        /* Min_LBFGS's two-loop direction (min_l-bfgs.cpp)    */
+#define MG_MIN_CG 1           /* Min_CG's Polak-Ribiere direction (min_cg.cpp)      */
+
 /* ---- library ---------------------------------------------------------- */
 const char* mg_last_error(void);
 int mg_version(void);
@@ -258,6 +261,9 @@ int mg_batch_add_cell(mg_batch* b, int natms, const double* H, const double* x_f
 int mg_batch_set_params(mg_batch* b, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings);
 /* MG_FORM_FP64 or MG_FORM_FP32 force passes */
 int mg_batch_set_form(mg_batch* b, int form);
+/* MG_MIN_LBFGS (default) or MG_MIN_CG: Min_CG::run's fixed-box branch
+   (min_cg.cpp:449-562) with the same line search; m is unused for CG */
+int mg_batch_set_method(mg_batch* b, int method);
 /* autotune = 1: time candidate launch shapes on the batch (or read them from
    cache_path, a text file of earlier choices, which is then extended);
    0: built-in shapes.  The search covers the blocks per SM of the two pair
@@ -320,6 +326,12 @@ int mg_cfg_write(mg_system* s, const char* prefix, int step);
    and counts, stats the launch statistics (either may be NULL). */
 int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings,
                  int lbfgs_cluster, mg_cell_result* r, mg_batch_stats* stats);
+/* Min_CG::run (min_cg.cpp:449-562, fixed box) with LineSearch_BackTrack
+   for the system itself on the device, as mg_min_lbfgs does for Min_LBFGS:
+   the conjugate direction h = ratio h + f (ratio = (f.f - f.f0) / f0.f0,
+   h = f when h.f < 0) instead of the two-loop recursion. */
+int mg_min_cg(mg_system* s, int max_iter, double fmax_tol, double energy_tol, int max_halvings, int cluster,
+              mg_cell_result* r, mg_batch_stats* stats);
 
 /* ---- concentration clock -------------------------------------------------- */
 /* Clock_Adams "clock adams order nsteps delta_t" then run (clock_adams.cpp:

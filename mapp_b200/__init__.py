@@ -22,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmapp_b200.so")
 
 MG_FORM_FP64, MG_FORM_FP32, MG_FORM_MLP = 0, 1, 2
+MG_MIN_LBFGS, MG_MIN_CG = 0, 1
 ERRORS = {1: "ARG", 2: "FILE", 3: "FORMAT", 4: "STATE", 5: "CUDA", 6: "CAPACITY", 7: "UNSUPPORTED", 8: "TIMEOUT"}
 
 # Every exported entry point of include/mapp_b200.h with its ctypes signature.
@@ -76,6 +77,8 @@ SIGNATURES = {
     "mg_batch_relax": (C.c_int, [_P, _P]),
     "mg_batch_cell_result": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mg_min_lbfgs": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _P, _P]),
+    "mg_min_cg": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _P, _P]),
+    "mg_batch_set_method": (C.c_int, [_P, C.c_int]),
     "mg_clock_adams": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, _P, C.POINTER(C.c_longlong)]),
     "mg_md_nh": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _P,
                            C.c_int, _P, _P, _I]),
@@ -383,6 +386,15 @@ class System:
         _check(load_library().mg_cfg_write(self.h, str(prefix).encode(), step))
         return "%s.%08d.cfg" % (prefix, step)
 
+    def min_cg(self, max_iter=10000, fmax_tol=1e-5, energy_tol=1e-8, max_halvings=60, cluster=0):
+        """Device-resident conjugate-gradient relaxation of this system (mg_min_cg);
+        returns (result, stats) dicts like min_lbfgs."""
+        r = CellResult()
+        st = BatchStats()
+        _check(load_library().mg_min_cg(self.h, max_iter, fmax_tol, energy_tol, max_halvings, cluster, C.byref(r),
+                                        C.byref(st)))
+        return ({k: getattr(r, k) for k, _ in CellResult._fields_}, {k: getattr(st, k) for k, _ in BatchStats._fields_})
+
     def last_time(self, phase):
         ms = C.c_double(0.0)
         _check(load_library().mg_last_time(self.h, phase.encode(), C.byref(ms)))
@@ -439,6 +451,10 @@ class Batch:
 
     def set_form(self, form):
         _check(load_library().mg_batch_set_form(self.h, form))
+
+    def set_method(self, method):
+        """MG_MIN_LBFGS (default) or MG_MIN_CG."""
+        _check(load_library().mg_batch_set_method(self.h, method))
 
     def set_tuning(self, autotune=True, cache_path=None):
         _check(load_library().mg_batch_set_tuning(self.h, int(autotune),

@@ -67,6 +67,7 @@ struct CellState {
 
 struct BatchParams {
     int m, max_iter, max_halvings;
+    int cg;  // 1: Min_CG's Polak-Ribiere direction instead of the L-BFGS two-loop
     double fmax_tol, energy_tol, skin_sq;
 };
 
@@ -202,6 +203,7 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
     for (int k = 0; k < kBMaxM; k++) rho[k] = S->rho[k];
     int code = kRunning, next = PH_TRIAL;
     bool new_dir = false;
+    double cg_beta = 0.0;  // CG: the ratio of this step's direction update
 
     if (phase == PH_FIRST) {
         // Min_LBFGS::init: the first force_calc gives curr_energy
@@ -224,7 +226,21 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
             if (E_prev - E_curr < P.energy_tol) code = kTolerance;
             else if (iter == P.max_iter) code = kMaxIter;
             else if (P.fmax_tol > 0.0 && max_f < P.fmax_tol) code = kTolerance;
-            if (code == kRunning) {
+            if (code == kRunning && P.cg) {
+                // Min_CG::run after its force_calc (min_cg.cpp:526-558): f.f,
+                // f.f0, the Polak-Ribiere ratio; ratio keeps f0.f0 between steps
+                double ff = 0.0, ff0 = 0.0;
+                for (int e = t0; e < n; e += ts) {
+                    ff += f[e] * f[e];
+                    ff0 += f[e] * f0[e];
+                }
+                ff = cred<CS, 0>(ff, sh, &slot_sh);
+                ff0 = cred<CS, 0>(ff0, sh, &slot_sh);
+                cg_beta = (ff - ff0) / ratio;
+                ratio = ff;
+                iter++;
+                new_dir = true;
+            } else if (code == kRunning) {
                 int slot;
                 if (k_it == P.m) {
                     slot = head;
@@ -266,7 +282,38 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
         }
     }
 
-    if (new_dir) {
+    if (new_dir && P.cg) {
+        // Min_CG: h = f at the start (f0.f0 = f.f kept in ratio), else
+        // h = beta h + f with h.f < 0 falling back to h = f; then x_prev = x,
+        // f_prev = f and f0.f0 == 0 ends the run (min_cg.cpp:452-481, 546-558)
+        phase_sync<CS>();
+        if (phase == PH_FIRST) {
+            double ff = 0.0;
+            for (int e = t0; e < n; e += ts) {
+                h[e] = f[e];
+                ff += f[e] * f[e];
+            }
+            ratio = cred<CS, 0>(ff, sh, &slot_sh);
+        } else {
+            double fhv = 0.0;
+            for (int e = t0; e < n; e += ts) {
+                double he = h[e] * cg_beta;
+                he += f[e];
+                h[e] = he;
+                fhv += he * f[e];
+            }
+            fhv = cred<CS, 0>(fhv, sh, &slot_sh);
+            if (fhv < 0.0)
+                for (int e = t0; e < n; e += ts) h[e] = f[e];
+        }
+        for (int k = t0; k < nat; k += ts)
+            for (int q = 0; q < xd; q++) x0[(size_t)k * xd + q] = xget(d, base + k, q);
+        for (int e = t0; e < n; e += ts) f0[e] = f[e];
+        if (ratio == 0.0) {
+            code = kGrad0;
+            new_dir = false;
+        }
+    } else if (new_dir) {
         // h = f, x_prev = x, f_prev = f, then the two-loop recursion
         phase_sync<CS>();
         for (int k = t0; k < nat; k += ts)
@@ -295,6 +342,8 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
             const double be = cred<CS, 0>(in, sh, &slot_sh) * rho[slot];
             for (int e = t0; e < n; e += ts) h[e] -= (be + al[i]) * sv[e];
         }
+    }
+    if (new_dir) {
         // line_min: alpha_min from the smallest alpha coordinate, |h| = 1,
         // downhill test, first step min(1, max|h|)
         double mn = INFINITY;
@@ -593,7 +642,7 @@ std::map<std::string, std::vector<int>> g_tune_mem;
 struct mg_batch {
     mg_system* builder = nullptr;
     int device = 0, nt = 0, xd = 0, form = MG_FORM_FP64;
-    int m = 5, max_iter = 10000, max_halvings = 60;
+    int m = 5, max_iter = 10000, max_halvings = 60, cg = 0;
     double fmax_tol = 1e-5, energy_tol = 1e-8, skin = 0.5;
     int autotune = 0;
     std::string cache_path;
@@ -651,6 +700,7 @@ BatchParams params(mg_batch* b)
 {
     BatchParams P;
     P.m = b->m;
+    P.cg = b->cg;
     P.max_iter = b->max_iter;
     P.max_halvings = b->max_halvings;
     P.fmax_tol = b->fmax_tol;
@@ -1101,6 +1151,17 @@ int mg_batch_set_params(mg_batch* b, int m, int max_iter, double fmax_tol, doubl
     return MG_OK;
 }
 
+int mg_batch_set_method(mg_batch* b, int method)
+{
+    BCHK(check_batch(b));
+    if (method != MG_MIN_LBFGS && method != MG_MIN_CG) return bfail(MG_ERR_ARG, "method must be MG_MIN_LBFGS or MG_MIN_CG");
+    if ((method == MG_MIN_CG) != (b->cg != 0)) {
+        b->cg = method == MG_MIN_CG;
+        destroy_graph(b);
+    }
+    return MG_OK;
+}
+
 int mg_batch_set_form(mg_batch* b, int form)
 {
     BCHK(check_batch(b));
@@ -1284,8 +1345,8 @@ int mg_batch_cell_result(mg_batch* b, int cell, double* x, double* f, mg_cell_re
     return MG_OK;
 }
 
-int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings,
-                 int lbfgs_cluster, mg_cell_result* r, mg_batch_stats* stats)
+static int min_single(mg_system* s, int method, int m, int max_iter, double fmax_tol, double energy_tol,
+                      int max_halvings, int lbfgs_cluster, mg_cell_result* r, mg_batch_stats* stats)
 {
     if (!s) return bfail(MG_ERR_ARG, "null mg_system");
     int style = -1, nt = 0, xd = 0, form = 0;
@@ -1293,9 +1354,9 @@ int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double ener
     system_shape(s, &style, &nt, &xd, &form, B);
     system_box(s, H);
     const int natms = system_natms(s);
-    if (natms < 1) return bfail(MG_ERR_STATE, "mg_min_lbfgs needs an initialised system with sites");
+    if (natms < 1) return bfail(MG_ERR_STATE, "the device minimiser needs an initialised system with sites");
     if (form != MG_FORM_FP64 && form != MG_FORM_FP32)
-        return bfail(MG_ERR_UNSUPPORTED, "mg_min_lbfgs runs the FP64 or FP32 force passes");
+        return bfail(MG_ERR_UNSUPPORTED, "the device minimiser runs the FP64 or FP32 force passes");
     // the current state as one cell: fractional positions (x2s) and alpha, c
     std::vector<double> x((size_t)natms * xd), xs((size_t)natms * xd), c((size_t)natms * nt);
     BCHK(mg_atoms_get_x(s, x.data()));
@@ -1312,6 +1373,7 @@ int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double ener
     } guard{b};
     BCHK(mg_batch_add_cell(b, natms, H, xs.data(), c.data(), nullptr));
     BCHK(mg_batch_set_params(b, m, max_iter, fmax_tol, energy_tol, max_halvings));
+    BCHK(mg_batch_set_method(b, method));
     BCHK(mg_batch_set_form(b, form));
     if (lbfgs_cluster > 0) BCHK(mg_batch_set_launch(b, 0, 0, 1024, lbfgs_cluster));
     else BCHK(mg_batch_set_tuning(b, 1, nullptr));
@@ -1327,6 +1389,18 @@ int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double ener
     BCHK(mg_atoms_set(s, natms, xs.data(), nullptr, c.data()));
     BCHK(mg_ff_init(s));
     return MG_OK;
+}
+
+int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings,
+                 int lbfgs_cluster, mg_cell_result* r, mg_batch_stats* stats)
+{
+    return min_single(s, MG_MIN_LBFGS, m, max_iter, fmax_tol, energy_tol, max_halvings, lbfgs_cluster, r, stats);
+}
+
+int mg_min_cg(mg_system* s, int max_iter, double fmax_tol, double energy_tol, int max_halvings, int cluster,
+              mg_cell_result* r, mg_batch_stats* stats)
+{
+    return min_single(s, MG_MIN_CG, 1, max_iter, fmax_tol, energy_tol, max_halvings, cluster, r, stats);
 }
 
 }  // extern "C"
