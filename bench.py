@@ -363,7 +363,8 @@ def run_batched(mb, fx, device, ncells=512):
 
 
 def run_large_forms(mb, fx, device, mlp_source):
-    """The precision form on FCC 40^3 = 256000 sites and the learned form on
+    """The precision form on FCC 40^3 = 256000 sites (then the 256000-site
+    workflow: 200 CG iterations in the precision form, 10 Adams steps) and the learned form on
     FCC 50^3 = 500000 sites (same distributions as the 32000-site system),
     each against the plain FP64 form on the same system: time per force call
     (L2 flushed before each), max|dF|, |dE|/site and, for the precision form,
@@ -419,6 +420,31 @@ def run_large_forms(mb, fx, device, mlp_source):
                 rec["fallback_rows"] = int(counts[1])
             out[f"{form}_{natms}_sites"] = rec
             s.set_form(mb.MG_FORM_FP64)
+        if n == 40:
+            # the 256000-site workflow: 200 conjugate-gradient iterations in the
+            # precision form (mg_min_cg), then Adams-clock steps of order 2 on
+            # the relaxed state (plain form; dt = 1e-3 / rms(c_d))
+            s.set_form(mb.MG_FORM_FP32)
+            t0 = time.perf_counter()
+            r, st = s.min_cg(200, 1e-5, 1e-8, 60, cluster=0)
+            wall = time.perf_counter() - t0
+            out["cg_fp32_256000_sites"] = {
+                "iterations": r["iterations"], "evaluations": r["evaluations"], "stop_code": r["code"],
+                "energy": r["energy"], "max_f": r["max_f"], "wall_s": wall, "relax_ms": st["relax_ms"],
+                "build_ms": st["build_ms"], "tune_ms": st["tune_ms"],
+                "ms_per_evaluation": st["relax_ms"] / max(r["evaluations"], 1),
+                "lbfgs_cluster": st["lbfgs_cluster"]}
+            s.set_form(mb.MG_FORM_FP64)
+            s.create_2nd_neigh_lst()
+            s.force_calc(1)
+            cd = s.c_d_calc()
+            dt = 1e-3 / float(np.sqrt(np.mean(cd * cd)))
+            t0 = time.perf_counter()
+            ra = s.clock_adams(2, 10, dt)
+            wall = time.perf_counter() - t0
+            out["adams_256000_sites"] = {"order": 2, "steps": 10, "dt": dt, "wall_s": wall,
+                                         "ms_per_step": wall * 1e3 / 10, "calc_g_calls": ra["n_calc_g"],
+                                         "final_cost_max": float(np.max(ra["err"]))}
         s.close()
     return out
 
