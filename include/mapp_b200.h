@@ -46,6 +46,8 @@ typedef struct mg_system mg_system;
                                  Kahan-compensated per-site sums, FP64 totals      */
 #define MG_FORM_MLP 2         /* learned form: BF16 MLP replaces DMD quadrature    */
 
+#define MG_LAUNCH_WHOLE_GPU -1 /* lbfgs_cluster: a one-cell batch's step on every SM */
+
 #define MG_MIN_LBFGS 0        /* Min_LBFGS's two-loop direction (min_l-bfgs.cpp)    */
 #define MG_MIN_CG 1           /* Min_CG's Polak-Ribiere direction (min_cg.cpp)      */
 
@@ -236,7 +238,8 @@ typedef struct mg_batch_stats {
     int bps1, bps2;         /* blocks per SM of force pass 1 and pass 2 */
     int lbfgs_threads;      /* threads per CTA of the L-BFGS step */
     int from_cache;         /* launch shapes read from the tuning cache */
-    int lbfgs_cluster;      /* CTAs per cell of the L-BFGS step (a thread-block cluster) */
+    int lbfgs_cluster;      /* CTAs per cell of the L-BFGS step (a thread-block cluster),
+                               or MG_LAUNCH_WHOLE_GPU */
 } mg_batch_stats;
 
 typedef struct mg_cell_result {
@@ -273,7 +276,8 @@ int mg_batch_set_tuning(mg_batch* b, int autotune, const char* cache_path);
 /* fixed launch shapes instead of autotuning: blocks per SM of force pass 1
    and pass 2 (0: built-in), threads per CTA (32..1024) and CTAs per cell
    (1, 2, 4, 8 or 16: a thread-block cluster whose CTAs share the cell's
-   vectors) of the L-BFGS step */
+   vectors; MG_LAUNCH_WHOLE_GPU for a batch of one cell: one CTA per SM) of
+   the L-BFGS step */
 int mg_batch_set_launch(mg_batch* b, int bps1, int bps2, int lbfgs_threads, int lbfgs_cluster);
 int mg_batch_relax(mg_batch* b, mg_batch_stats* stats);
 /* final state of one cell: x = natms * (3 + nt) Cartesian positions and
@@ -318,7 +322,10 @@ int mg_cfg_write(mg_system* s, const char* prefix, int step);
    line_search.cpp:223-342) for the system itself, on the GPU: the same
    algorithm, stop codes and line-search energies as the batched form (one
    cell), with the L-BFGS vector work of each step spread over a
-   thread-block cluster of lbfgs_cluster CTAs (1, 2, 4, 8 or 16; 0 = autotune).
+   thread-block cluster of lbfgs_cluster CTAs (1, 2, 4, 8 or 16), or on every SM
+   (MG_LAUNCH_WHOLE_GPU: one CTA per SM, launched cooperatively, reductions
+   through a global array after grid barriers whose waits give up after 2 s
+   with MG_ERR_TIMEOUT); 0 = autotune among all of them.
    It replaces the reference's host loop, which copies x and f through the
    boundary on every force evaluation.  The system (DMD style, initialised,
    FP64 or FP32 form) starts from its current state and holds the final state

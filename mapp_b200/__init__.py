@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(HERE, "libmapp_b200.so")
 
 MG_FORM_FP64, MG_FORM_FP32, MG_FORM_MLP = 0, 1, 2
 MG_MIN_LBFGS, MG_MIN_CG = 0, 1
+MG_LAUNCH_WHOLE_GPU = -1
 ERRORS = {1: "ARG", 2: "FILE", 3: "FORMAT", 4: "STATE", 5: "CUDA", 6: "CAPACITY", 7: "UNSUPPORTED", 8: "TIMEOUT"}
 
 # Every exported entry point of include/mapp_b200.h with its ctypes signature.

@@ -31,6 +31,7 @@
 // cell of the L-BFGS step are timed on the batch itself and the choice is
 // kept in a cache keyed by the batch's shape.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -83,6 +84,11 @@ struct BatchView {
     unsigned long long* t0;
     int* budget;
     long long* iters;
+    // whole-GPU step of a single cell (CS = 0): barrier [count, generation],
+    // per-CTA partials [2][kMaxGridCtas], and a wait-timeout flag
+    unsigned int* gbar;
+    double* gpart;
+    int* gerr;
 };
 
 __device__ __forceinline__ unsigned long long global_ns()
@@ -124,31 +130,105 @@ __device__ __forceinline__ double block_red(double v, double* sh)
 }
 
 // A cell's L-BFGS step runs on a thread-block cluster of CS CTAs (one CTA when
-// CS = 1).  Element e of the cell's vectors belongs to thread e mod (CS * T) of
-// the cluster in every loop; reductions combine the CTAs' block results through
-// distributed shared memory in rank order, so every thread of the cluster gets
-// the same value.
+// CS = 1), or, for a batch of one cell, on the whole GPU (CS = 0: one CTA per
+// SM, launched cooperatively so that all are resident).  Element e of the
+// cell's vectors belongs to thread e mod (CTAs * T) in every loop; reductions
+// combine the CTAs' block results in CTA order -- through distributed shared
+// memory in a cluster, through a global array after a grid barrier on the
+// whole GPU -- so every thread gets the same value.
+constexpr int kMaxGridCtas = 1024;
+constexpr unsigned long long kGridWaitNs = 2000000000ull;  // a barrier wait gives up after 2 s
+
+struct RedCtx {
+    double* sh;    // shared [32]
+    double* slot;  // shared, one double (cluster mode)
+    int* par;      // shared, which half of gpart the next reduction uses (grid mode)
+    unsigned int* gbar;
+    double* gpart;
+    int* gerr;
+};
+
 template <int CS>
-__device__ __forceinline__ void phase_sync()
+__device__ __forceinline__ int nctas() { return CS == 0 ? (int)gridDim.x : CS; }
+template <int CS>
+__device__ __forceinline__ int cell_idx() { return CS == 0 ? 0 : (int)blockIdx.x / CS; }
+template <int CS>
+__device__ __forceinline__ int rank_idx() { return CS == 0 ? (int)blockIdx.x : (int)blockIdx.x % CS; }
+
+// Grid barrier of the whole-GPU step (sense by generation count).  A wait
+// that outlasts kGridWaitNs, or sees another CTA's timeout, sets *gerr and
+// returns, so a stuck barrier ends the launch instead of hanging it.
+__device__ __forceinline__ void grid_sync(const RedCtx& R)
 {
-    if (CS == 1) __syncthreads();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = R.gbar + 1;
+        const unsigned int g = *gen;
+        __threadfence();
+        if (atomicAdd(R.gbar, 1u) == gridDim.x - 1) {
+            atomicExch(R.gbar, 0u);
+            __threadfence();
+            atomicAdd(R.gbar + 1, 1u);
+        } else {
+            const unsigned long long t_start = global_ns();
+            while (*gen == g) {
+                if (*(volatile int*)R.gerr) break;
+                if (global_ns() - t_start > kGridWaitNs) {
+                    atomicExch(R.gerr, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+template <int CS>
+__device__ __forceinline__ void phase_sync(const RedCtx& R)
+{
+    if (CS == 0) grid_sync(R);
+    else if (CS == 1) __syncthreads();
     else cooperative_groups::this_cluster().sync();
 }
 
-template <int CS, int OP>
-__device__ __forceinline__ double cred(double v, double* sh, double* slot)
+template <int OP>
+__device__ __forceinline__ double red_op(double a, double b)
 {
-    double b = block_red<OP>(v, sh);
+    return OP == 0 ? a + b : (OP == 1 ? fmax(a, b) : fmin(a, b));
+}
+
+template <int CS, int OP>
+__device__ __forceinline__ double cred(double v, const RedCtx& R)
+{
+    double b = block_red<OP>(v, R.sh);
     if (CS == 1) return b;
-    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
-    if (threadIdx.x == 0) *slot = b;
-    cl.sync();
-    double r = *cl.map_shared_rank(slot, 0);
+    if (CS == 0) {
+        double* buf = R.gpart + (size_t)(*R.par) * kMaxGridCtas;
+        if (threadIdx.x == 0) buf[blockIdx.x] = b;
+        grid_sync(R);
+        if (threadIdx.x < 32) {
+            double a = OP == 0 ? 0.0 : (OP == 1 ? -INFINITY : INFINITY);
+            for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) a = red_op<OP>(a, __ldcg(buf + k));
 #pragma unroll
-    for (int k = 1; k < CS; k++) {
-        const double t = *cl.map_shared_rank(slot, k);
-        r = OP == 0 ? r + t : (OP == 1 ? fmax(r, t) : fmin(r, t));
+            for (int o = 16; o > 0; o >>= 1) a = red_op<OP>(a, __shfl_xor_sync(0xffffffffu, a, o));
+            if (threadIdx.x == 0) {
+                R.sh[0] = a;
+                *R.par ^= 1;
+            }
+        }
+        __syncthreads();
+        const double r = R.sh[0];
+        __syncthreads();
+        return r;
     }
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    if (threadIdx.x == 0) *R.slot = b;
+    cl.sync();
+    double r = *cl.map_shared_rank(R.slot, 0);
+#pragma unroll
+    for (int k = 1; k < CS; k++) r = red_op<OP>(r, *cl.map_shared_rank(R.slot, k));
     cl.sync();  // no CTA overwrites its slot before every CTA has read it
     return r;
 }
@@ -156,14 +236,14 @@ __device__ __forceinline__ double cred(double v, double* sh, double* slot)
 // x = x0 + a h over the cell; returns the largest squared displacement of a
 // site from its position at the last list build
 template <int CS>
-__device__ double set_trial(const Dev& d, const BatchView& B, int base, int nat, double a, double* sh, double* slot,
-                           int t0, int ts)
+__device__ double set_trial(const Dev& d, const BatchView& B, int base, int nat, double a, const RedCtx& R, int t0,
+                           int ts)
 {
     const int xd = d.x_dim;
     const double* x0 = B.x0 + (size_t)base * xd;
     const double* h = B.h + (size_t)base * xd;
     double dmax = 0.0;
-    phase_sync<CS>();
+    phase_sync<CS>(R);
     for (int k = t0; k < nat; k += ts) {
         const int i = base + k;
         for (int q = 0; q < xd; q++) xset(d, i, q, x0[(size_t)k * xd + q] + a * h[(size_t)k * xd + q]);
@@ -171,7 +251,7 @@ __device__ double set_trial(const Dev& d, const BatchView& B, int base, int nat,
         const double dx = p.x - p0.x, dy = p.y - p0.y, dz = p.z - p0.z;
         dmax = fmax(dmax, dx * dx + dy * dy + dz * dz);
     }
-    return cred<CS, 1>(dmax, sh, slot);
+    return cred<CS, 1>(dmax, R);
 }
 
 // One L-BFGS step of every running cell, after the force evaluation of its
@@ -183,8 +263,12 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
 {
     __shared__ double sh[32];
     __shared__ double slot_sh;
-    const int c = blockIdx.x / CS, rank = blockIdx.x % CS;
-    const int t0 = rank * blockDim.x + threadIdx.x, ts = CS * blockDim.x;
+    __shared__ int par_sh;
+    if (threadIdx.x == 0) par_sh = 0;
+    __syncthreads();
+    const RedCtx R{sh, &slot_sh, &par_sh, B.gbar, B.gpart, B.gerr};
+    const int c = cell_idx<CS>(), rank = rank_idx<CS>();
+    const int t0 = rank * blockDim.x + threadIdx.x, ts = nctas<CS>() * blockDim.x;
     CellState* S = B.st + c;
     const int phase = S->phase;
     if (phase == PH_DONE || phase == PH_PAUSED) return;
@@ -222,7 +306,7 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
             E_curr = E_new;
             double fm = 0.0;
             for (int e = t0; e < n; e += ts) fm = fmax(fm, fabs(f[e]));
-            max_f = cred<CS, 1>(fm, sh, &slot_sh);
+            max_f = cred<CS, 1>(fm, R);
             if (E_prev - E_curr < P.energy_tol) code = kTolerance;
             else if (iter == P.max_iter) code = kMaxIter;
             else if (P.fmax_tol > 0.0 && max_f < P.fmax_tol) code = kTolerance;
@@ -234,8 +318,8 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
                     ff += f[e] * f[e];
                     ff0 += f[e] * f0[e];
                 }
-                ff = cred<CS, 0>(ff, sh, &slot_sh);
-                ff0 = cred<CS, 0>(ff0, sh, &slot_sh);
+                ff = cred<CS, 0>(ff, R);
+                ff0 = cred<CS, 0>(ff0, R);
                 cg_beta = (ff - ff0) / ratio;
                 ratio = ff;
                 iter++;
@@ -259,8 +343,8 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
                     in1 += sv_e * yv_e;
                     in2 += yv_e * yv_e;
                 }
-                in1 = cred<CS, 0>(in1, sh, &slot_sh);
-                in2 = cred<CS, 0>(in2, sh, &slot_sh);
+                in1 = cred<CS, 0>(in1, R);
+                in2 = cred<CS, 0>(in2, R);
                 ratio = -in1 / in2;
                 rho[slot] = 1.0 / in1;
                 iter++;
@@ -271,12 +355,12 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
             halvings++;
             if (alpha_m <= ls_alpha_min || (P.max_halvings > 0 && halvings >= P.max_halvings)) {
                 // energy(0): back to x0, whose forces and energy are f0 and E_curr
-                phase_sync<CS>();
+                phase_sync<CS>(R);
                 for (int k = t0; k < nat; k += ts)
                     for (int q = 0; q < xd; q++) xset(d, base + k, q, x0[(size_t)k * xd + q]);
                 for (int e = t0; e < n; e += ts) f[e] = f0[e];
                 code = kAlphaMin;
-            } else if (set_trial<CS>(d, B, base, nat, alpha_m, sh, &slot_sh, t0, ts) > P.skin_sq) {
+            } else if (set_trial<CS>(d, B, base, nat, alpha_m, R, t0, ts) > P.skin_sq) {
                 next = PH_PAUSED;
             }
         }
@@ -286,14 +370,14 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
         // Min_CG: h = f at the start (f0.f0 = f.f kept in ratio), else
         // h = beta h + f with h.f < 0 falling back to h = f; then x_prev = x,
         // f_prev = f and f0.f0 == 0 ends the run (min_cg.cpp:452-481, 546-558)
-        phase_sync<CS>();
+        phase_sync<CS>(R);
         if (phase == PH_FIRST) {
             double ff = 0.0;
             for (int e = t0; e < n; e += ts) {
                 h[e] = f[e];
                 ff += f[e] * f[e];
             }
-            ratio = cred<CS, 0>(ff, sh, &slot_sh);
+            ratio = cred<CS, 0>(ff, R);
         } else {
             double fhv = 0.0;
             for (int e = t0; e < n; e += ts) {
@@ -302,7 +386,7 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
                 h[e] = he;
                 fhv += he * f[e];
             }
-            fhv = cred<CS, 0>(fhv, sh, &slot_sh);
+            fhv = cred<CS, 0>(fhv, R);
             if (fhv < 0.0)
                 for (int e = t0; e < n; e += ts) h[e] = f[e];
         }
@@ -315,7 +399,7 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
         }
     } else if (new_dir) {
         // h = f, x_prev = x, f_prev = f, then the two-loop recursion
-        phase_sync<CS>();
+        phase_sync<CS>(R);
         for (int k = t0; k < nat; k += ts)
             for (int q = 0; q < xd; q++) x0[(size_t)k * xd + q] = xget(d, base + k, q);
         for (int e = t0; e < n; e += ts) {
@@ -329,7 +413,7 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
             const double* yv = B.y + (size_t)slot * B.vstride + vb;
             double in = 0.0;
             for (int e = t0; e < n; e += ts) in += h[e] * sv[e];
-            al[i] = cred<CS, 0>(in, sh, &slot_sh) * rho[slot];
+            al[i] = cred<CS, 0>(in, R) * rho[slot];
             for (int e = t0; e < n; e += ts) h[e] -= al[i] * yv[e];
         }
         for (int e = t0; e < n; e += ts) h[e] *= ratio;
@@ -339,7 +423,7 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
             const double* yv = B.y + (size_t)slot * B.vstride + vb;
             double in = 0.0;
             for (int e = t0; e < n; e += ts) in += h[e] * yv[e];
-            const double be = cred<CS, 0>(in, sh, &slot_sh) * rho[slot];
+            const double be = cred<CS, 0>(in, R) * rho[slot];
             for (int e = t0; e < n; e += ts) h[e] -= (be + al[i]) * sv[e];
         }
     }
@@ -349,30 +433,30 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
         double mn = INFINITY;
         for (int k = t0; k < nat; k += ts)
             for (int t = 0; t < nt; t++) mn = fmin(mn, d.alpha[(size_t)(base + k) * nt + t]);
-        mn = cred<CS, 2>(mn, sh, &slot_sh) * 0.99;
+        mn = cred<CS, 2>(mn, R) * 0.99;
         ls_alpha_min = fmin(ls_alpha_min, mn);
         double hh = 0.0;
         for (int e = t0; e < n; e += ts) hh += h[e] * h[e];
-        hh = 1.0 / sqrt(cred<CS, 0>(hh, sh, &slot_sh));
+        hh = 1.0 / sqrt(cred<CS, 0>(hh, R));
         double fhl = 0.0, mh = 0.0;
         for (int e = t0; e < n; e += ts) {
             h[e] *= hh;
             fhl += f[e] * h[e];
             mh = fmax(mh, fabs(h[e]));
         }
-        fh = cred<CS, 0>(fhl, sh, &slot_sh);
-        mh = cred<CS, 1>(mh, sh, &slot_sh);
+        fh = cred<CS, 0>(fhl, R);
+        mh = cred<CS, 1>(mh, R);
         if (fh <= 0) code = kDownhill;
         else if (mh == 0) code = kGrad0;
         else {
             alpha_m = fmin(1.0, mh);
             halvings = 0;
             if (alpha_m <= ls_alpha_min) code = kAlphaMin;
-            else if (set_trial<CS>(d, B, base, nat, alpha_m, sh, &slot_sh, t0, ts) > P.skin_sq) next = PH_PAUSED;
+            else if (set_trial<CS>(d, B, base, nat, alpha_m, R, t0, ts) > P.skin_sq) next = PH_PAUSED;
         }
     }
     if (code != kRunning) next = PH_DONE;
-    phase_sync<CS>();  // every CTA of the cluster has read the state before it changes
+    phase_sync<CS>(R);  // every CTA of the cluster has read the state before it changes
     if (rank == 0 && threadIdx.x == 0) {
         S->phase = next;
         S->code = code;
@@ -407,7 +491,7 @@ __global__ void k_loop_test(BatchView B, cudaGraphConditionalHandle handle)
     if (threadIdx.x == 0) {
         int left = --(*B.budget);
         (*B.iters)++;
-        cudaGraphSetConditional(handle, (sh_n > 0 && left > 0) ? 1u : 0u);
+        cudaGraphSetConditional(handle, (sh_n > 0 && left > 0 && *B.gerr == 0) ? 1u : 0u);
     }
 }
 
@@ -495,8 +579,12 @@ __global__ void __launch_bounds__(1024) k_lbfgs_probe(Dev d, BatchView B, int m,
 {
     __shared__ double sh[32];
     __shared__ double slot_sh;
-    const int c = blockIdx.x / CS, rank = blockIdx.x % CS;
-    const int t0 = rank * blockDim.x + threadIdx.x, ts = CS * blockDim.x;
+    __shared__ int par_sh;
+    if (threadIdx.x == 0) par_sh = 0;
+    __syncthreads();
+    const RedCtx R{sh, &slot_sh, &par_sh, B.gbar, B.gpart, B.gerr};
+    const int c = cell_idx<CS>(), rank = rank_idx<CS>();
+    const int t0 = rank * blockDim.x + threadIdx.x, ts = nctas<CS>() * blockDim.x;
     const int xd = d.x_dim, n = B.nat[c] * xd;
     const size_t vb = (size_t)B.base[c] * xd;
     double acc = 0.0;
@@ -504,15 +592,33 @@ __global__ void __launch_bounds__(1024) k_lbfgs_probe(Dev d, BatchView B, int m,
         const double* a = (r < 2 * m ? (r & 1 ? B.y : B.s) + (size_t)(r >> 1) * B.vstride : B.h) + vb;
         double in = 0.0;
         for (int e = t0; e < n; e += ts) in += a[e] * d.f[vb + e];
-        acc += cred<CS, 0>(in, sh, &slot_sh);
+        acc += cred<CS, 0>(in, R);
     }
     if (rank == 0 && threadIdx.x == 0) out[c] = acc;
 }
 
-// launch of a per-cell kernel on clusters of cs CTAs (cs = 1: plain launch)
+// launch of a per-cell kernel on clusters of cs CTAs (cs = 1: plain launch;
+// cs = 0: one cell on one CTA per SM, cooperative so that all are resident)
 template <class... A>
 cudaError_t launch_cells(void (*kern)(A...), int cs, int ncells, int threads, cudaStream_t st, A... args)
 {
+    if (cs == 0) {
+        if (ncells != 1) return cudaErrorInvalidValue;
+        int per_sm = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)std::min(num_sms(), kMaxGridCtas), 1, 1);
+        cfg.blockDim = dim3((unsigned)threads, 1, 1);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, kern, args...);
+    }
     if (cs == 1) {
         kern<<<ncells, threads, 0, st>>>(args...);
         return cudaGetLastError();
@@ -536,6 +642,7 @@ cudaError_t launch_step(int cs, int ncells, int threads, cudaStream_t st, const 
                         const BatchParams& P)
 {
     switch (cs) {
+    case 0: return launch_cells(k_lbfgs_step<0>, 0, ncells, threads, st, d, B, P);
     case 1: return launch_cells(k_lbfgs_step<1>, 1, ncells, threads, st, d, B, P);
     case 2: return launch_cells(k_lbfgs_step<2>, 2, ncells, threads, st, d, B, P);
     case 4: return launch_cells(k_lbfgs_step<4>, 4, ncells, threads, st, d, B, P);
@@ -549,6 +656,7 @@ cudaError_t launch_probe(int cs, int ncells, int threads, cudaStream_t st, const
                          double* out)
 {
     switch (cs) {
+    case 0: return launch_cells(k_lbfgs_probe<0>, 0, ncells, threads, st, d, B, m, out);
     case 1: return launch_cells(k_lbfgs_probe<1>, 1, ncells, threads, st, d, B, m, out);
     case 2: return launch_cells(k_lbfgs_probe<2>, 2, ncells, threads, st, d, B, m, out);
     case 4: return launch_cells(k_lbfgs_probe<4>, 4, ncells, threads, st, d, B, m, out);
@@ -663,6 +771,9 @@ struct mg_batch {
     DArr<unsigned long long> t0;
     DArr<int> budget;
     DArr<long long> iters;
+    DArr<unsigned int> gbar;  // whole-GPU step: barrier words
+    DArr<double> gpart;       // whole-GPU step: per-CTA partials
+    DArr<int> gerr;           // whole-GPU step: a barrier wait timed out
     // launch shapes
     int bps1 = 0, bps2 = 0, lbt = 256, lcs = 1;  // pass grids, L-BFGS threads per CTA and CTAs per cell
     bool tuned = false, from_cache = false;
@@ -693,6 +804,9 @@ BatchView view(mg_batch* b)
     v.t0 = b->t0.p;
     v.budget = b->budget.p;
     v.iters = b->iters.p;
+    v.gbar = b->gbar.p;
+    v.gpart = b->gpart.p;
+    v.gerr = b->gerr.p;
     return v;
 }
 
@@ -1036,7 +1150,10 @@ int autotune(mg_batch* b)
     const int tc[][2] = {{128, 1}, {256, 1}, {512, 1}, {1024, 1}, {512, 2}, {1024, 2}, {1024, 4}, {1024, 8}, {1024, 16}};
     best = 1e30f;
     int bestt = 256, bestc = 1;
-    for (const auto& t : tc) {
+    std::vector<std::array<int, 2>> shapes;
+    for (const auto& t : tc) shapes.push_back({t[0], t[1]});
+    if (b->cells.size() == 1) shapes.push_back({1024, 0});  // one cell: also the whole GPU
+    for (const auto& t : shapes) {
         BCHK(time_probe(b, t[0], t[1], 5, &ms));
         if (ms < best) {
             best = ms;
@@ -1196,9 +1313,13 @@ int mg_batch_set_launch(mg_batch* b, int bps1, int bps2, int lbfgs_threads, int 
     BCHK(check_batch(b));
     const bool ok_t = lbfgs_threads >= 32 && lbfgs_threads <= 1024 && lbfgs_threads % 32 == 0;
     const bool ok_c = lbfgs_cluster == 1 || lbfgs_cluster == 2 || lbfgs_cluster == 4 || lbfgs_cluster == 8 ||
-                      lbfgs_cluster == 16;
+                      lbfgs_cluster == 16 || lbfgs_cluster == MG_LAUNCH_WHOLE_GPU;
     if (bps1 < 0 || bps2 < 0 || !ok_t || !ok_c)
-        return bfail(MG_ERR_ARG, "need bps >= 0, 32..1024 threads (multiple of 32), cluster 1, 2, 4, 8 or 16");
+        return bfail(MG_ERR_ARG, "need bps >= 0, 32..1024 threads (multiple of 32), cluster 1, 2, 4, 8, 16 or "
+                                 "MG_LAUNCH_WHOLE_GPU");
+    if (lbfgs_cluster == MG_LAUNCH_WHOLE_GPU && b->cells.size() > 1)
+        return bfail(MG_ERR_ARG, "the whole-GPU step takes a batch of one cell");
+    if (lbfgs_cluster == MG_LAUNCH_WHOLE_GPU) lbfgs_cluster = 0;
     b->autotune = 0;
     b->tuned = false;
     b->bps1 = bps1;
@@ -1227,6 +1348,11 @@ int mg_batch_relax(mg_batch* b, mg_batch_stats* stats)
     BCHK(b->t0.exact(1));
     BCHK(b->budget.exact(1));
     BCHK(b->iters.exact(1));
+    BCHK(b->gbar.exact(2));
+    BCHK(b->gpart.exact(2 * (size_t)kMaxGridCtas));
+    BCHK(b->gerr.exact(1));
+    BCU(cudaMemsetAsync(b->gbar.p, 0, 2 * sizeof(unsigned int), b->st));
+    BCU(cudaMemsetAsync(b->gerr.p, 0, sizeof(int), b->st));
     BCU(cudaMemsetAsync(b->vec.p, 0, vs * (3 + 2 * (size_t)b->m) * sizeof(double), b->st));
     BCU(cudaMemsetAsync(b->state.p, 0, ncells * sizeof(CellState), b->st));
     BCU(cudaMemsetAsync(b->active.p, 1, ncells, b->st));
@@ -1249,7 +1375,10 @@ int mg_batch_relax(mg_batch* b, mg_batch_stats* stats)
         BCU(cudaMemcpyAsync(b->budget.p, &budget, sizeof(int), cudaMemcpyHostToDevice, b->st));
         BCU(cudaGraphLaunch(b->gexec, b->st));
         BCU(cudaMemcpyAsync(hs.data(), b->state.p, ncells * sizeof(CellState), cudaMemcpyDeviceToHost, b->st));
+        int gerr_h = 0;
+        BCU(cudaMemcpyAsync(&gerr_h, b->gerr.p, sizeof(int), cudaMemcpyDeviceToHost, b->st));
         BCU(cudaStreamSynchronize(b->st));
+        if (gerr_h) return bfail(MG_ERR_TIMEOUT, "a grid barrier of the whole-GPU step timed out");
         int paused = 0, running = 0;
         for (const CellState& s : hs) {
             paused += s.phase == PH_PAUSED;
@@ -1306,7 +1435,7 @@ int mg_batch_relax(mg_batch* b, mg_batch_stats* stats)
         stats->bps1 = b->bps1;
         stats->bps2 = b->bps2;
         stats->lbfgs_threads = b->lbt;
-        stats->lbfgs_cluster = b->lcs;
+        stats->lbfgs_cluster = b->lcs == 0 ? MG_LAUNCH_WHOLE_GPU : b->lcs;
         stats->from_cache = b->from_cache ? 1 : 0;
     }
     return MG_OK;
@@ -1375,7 +1504,7 @@ static int min_single(mg_system* s, int method, int m, int max_iter, double fmax
     BCHK(mg_batch_set_params(b, m, max_iter, fmax_tol, energy_tol, max_halvings));
     BCHK(mg_batch_set_method(b, method));
     BCHK(mg_batch_set_form(b, form));
-    if (lbfgs_cluster > 0) BCHK(mg_batch_set_launch(b, 0, 0, 1024, lbfgs_cluster));
+    if (lbfgs_cluster != 0) BCHK(mg_batch_set_launch(b, 0, 0, 1024, lbfgs_cluster));
     else BCHK(mg_batch_set_tuning(b, 1, nullptr));
     BCHK(mg_batch_relax(b, stats));
     mg_cell_result res;

@@ -204,7 +204,7 @@ def test_batch_cg_matches_oracle_per_cell():
     Later, as a cell stalls, an Armijo test or the energy tolerance can fall
     within the last bits of energies the GPU sums in another order, and the
     two runs may stop a few iterations apart; the full runs are then compared
-    by their stop reason and final energy."""
+    by their stop reason and final energy (1e-8 relative)."""
     from oracle.restated import Oracle
 
     mb = _mb()
@@ -241,7 +241,10 @@ def test_batch_cg_matches_oracle_per_cell():
         ro = Oracle(w).cg(200, 1e-8, fmax_tol=1e-5, max_halvings=60, ls_force_energy=True)
         e_ref = ro["energies"][-1]
         assert {r["code"], ro["code"]} <= {3, 5}, (k, r, ro["code"])
-        assert abs(r["energy"] - e_ref) <= 1e-9 * abs(e_ref)
+        # stalled runs that stopped a few iterations apart: energies within
+        # 1e-8 relative (the last iterations of a stall lower the energy by
+        # about 1e-7 eV each)
+        assert abs(r["energy"] - e_ref) <= 1e-8 * abs(e_ref)
 
 
 def test_min_cg_single_system_matches_oracle(tmp_path):
@@ -257,6 +260,34 @@ def test_min_cg_single_system_matches_oracle(tmp_path):
     ro = Oracle(w).cg(60, 1e-8, fmax_tol=1e-5, max_halvings=60, ls_force_energy=True)
     e_ref = ro["energies"][-1]
     assert r["code"] == ro["code"] or {r["code"], ro["code"]} <= {3, 5}
+    assert r["iterations"] == ro["line_searches"] - 1
+    assert abs(r["energy"] - e_ref) <= 1e-12 * abs(e_ref)
+    L = w["cfg"].L
+    dx = s.get_x() - ro["x"]
+    dx[:, :3] -= L * np.round(dx[:, :3] / L)
+    assert np.max(np.abs(dx)) <= 1e-9
+
+
+@pytest.mark.parametrize("method", ["lbfgs", "cg"])
+def test_single_system_step_on_the_whole_gpu(tmp_path, method):
+    """The one-cell step on every SM (MG_LAUNCH_WHOLE_GPU: cooperative launch,
+    grid barriers, reductions in CTA order) follows the oracle like the
+    cluster step does."""
+    mb = _mb()
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=6, sigma=0.03, style="DMD_I")
+    s = mb.system_from_workload(w)
+    o = Oracle(w)
+    if method == "lbfgs":
+        r, st = s.min_lbfgs(5, 8, 0.0, 1e-12, 60, cluster=mb.MG_LAUNCH_WHOLE_GPU)
+        ro = o.lbfgs(5, 8, 1e-12, fmax_tol=0.0, max_halvings=60, ls_force_energy=True)
+    else:
+        r, st = s.min_cg(8, 0.0, 1e-12, 60, cluster=mb.MG_LAUNCH_WHOLE_GPU)
+        ro = o.cg(8, 1e-12, fmax_tol=0.0, max_halvings=60, ls_force_energy=True)
+    assert st["lbfgs_cluster"] == mb.MG_LAUNCH_WHOLE_GPU
+    e_ref = ro["energies"][-1]
+    assert r["code"] == ro["code"]
     assert r["iterations"] == ro["line_searches"] - 1
     assert abs(r["energy"] - e_ref) <= 1e-12 * abs(e_ref)
     L = w["cfg"].L
