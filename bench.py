@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--skip-forms", action="store_true", help="skip the FP32, learned and batched forms (profiling runs)")
     p.add_argument("--form", default="fp64", choices=["fp64", "fp32", "mlp"],
                    help="form of the timed force_calc steps (fp32 / mlp imply --skip-forms; for profiling)")
+    p.add_argument("--eam-cells", type=int, default=0,
+                   help="instead: time EAM force_calc (the MD crystal's potential) on FCC n^3 atoms (profiling)")
     return p.parse_args()
 
 
@@ -720,10 +722,41 @@ def run_ours(args):
     return 0
 
 
+def run_eam(args):
+    """EAM force_calc of the Nose-Hoover crystal's potential (species A setfl
+    tables) on FCC n^3 atoms, a = 3.615 A, sites displaced by 0.05 A: the MD
+    loop's force path timed alone (CUDA events of the library), one JSON line.
+    A profiling entry; the default run reports the MD loop itself."""
+    import torch
+    import mapp_b200 as mb
+    from mapp_b200 import fixtures as fx
+
+    w = fx.write_workload(tempfile.mkdtemp(prefix="mapp_eam_"), "eam", n=args.eam_cells)
+    s = mb.system_from_workload(w)
+    f = torch.zeros((s.natms, 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        s.force_calc(1, f=f)
+    t = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        s.force_calc(1, f=f)
+        t += s.last_time("force")
+    ms = t / args.steps
+    print(json.dumps({"metric": "EAM atom-force evals/s", "value": s.natms / (ms * 1e-3), "unit": "atom-force evals/s",
+                      "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "dtype": "f64",
+                      "config": {"workload": f"FCC {args.eam_cells}^3 EAM (species A setfl)", "atoms": s.natms,
+                                 "pairs": s.counts()["npairs"]}}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.eam_cells > 0:
+        return run_eam(args)
     return run_ours(args)
 
 

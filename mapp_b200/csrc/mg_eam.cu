@@ -73,7 +73,8 @@ __global__ void __launch_bounds__(kFFBlock, MG_EAM_MINB) k_eam_pass1(Dev d, int 
                 const Row8 cf = row8(d.rhoT + ((size_t)(ti * nt + tj) * d.nr + m) * 8);
                 double rho_iv = ((cf.v.w * p + cf.v.z) * p + cf.v.y) * p + cf.v.x;
                 double drho_i = (cf.dv.z * p + cf.dv.y) * p + cf.dv.x;
-                const Row8 cg = row8(d.rhoT + ((size_t)(tj * nt + ti) * d.nr + m) * 8);
+                // the j-side density row is the same row when the species agree
+                const Row8 cg = tj == ti ? cf : row8(d.rhoT + ((size_t)(tj * nt + ti) * d.nr + m) * 8);
                 double rho_jv = ((cg.v.w * p + cg.v.z) * p + cg.v.y) * p + cg.v.x;
                 double drho_j = (cg.dv.z * p + cg.dv.y) * p + cg.dv.x;
                 const Row8 ch = row8(d.phiT + ((size_t)comp_idx(ti, tj) * d.nr + m) * 8);
