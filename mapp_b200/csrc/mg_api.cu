@@ -866,7 +866,7 @@ int mg_set_form(mg_system* s, int form)
     if (form == MG_FORM_MLP && !s->mlp_ready)
         return fail(MG_ERR_STATE, "the learned form needs mg_mlp_init (and normally mg_mlp_train) first");
     if (form != MG_FORM_FP64 && form != MG_FORM_FP32 && form != MG_FORM_MLP)
-        return fail(MG_ERR_UNSUPPORTED, "form %d is not available in this build", form);
+        return fail(MG_ERR_UNSUPPORTED, "form %d is not available", form);
     s->form = form;
     s->d.form = form;
     return MG_OK;
@@ -995,7 +995,7 @@ int mg_ff_coef(mg_system* s, int narg, const char* const* arg)
             if (narg != 3) return fail(MG_ERR_ARG, "one file is needed for eam");
             CHK(read_tables(s, arg[2], false));
         } else if (!strcmp(arg[1], "FuncFL")) {
-            return fail(MG_ERR_UNSUPPORTED, "FuncFL tables are not supported by this build; convert to SetFL");
+            return fail(MG_ERR_UNSUPPORTED, "FuncFL tables are not supported; convert to SetFL");
         } else
             return fail(MG_ERR_ARG, "wrong coeff command for eam Force Field");
         // ff_eam.cpp:424-425
@@ -1029,7 +1029,7 @@ int mg_ff_coef(mg_system* s, int narg, const char* const* arg)
             if (narg != 8) return fail(MG_ERR_ARG, "one file is needed for eam");
             CHK(read_tables(s, arg[7], true));
         } else if (!strcmp(arg[6], "SetFL") || !strcmp(arg[6], "FuncFL")) {
-            return fail(MG_ERR_UNSUPPORTED, "DMD styles read FS tables in this build (got %s)", arg[6]);
+            return fail(MG_ERR_UNSUPPORTED, "DMD styles read FS tables (got %s)", arg[6]);
         } else
             return fail(MG_ERR_ARG, "wrong coeff command for eam Force Field");
         for (int i = 0; i < s->nt; i++) {

@@ -423,7 +423,7 @@ def dmd_coef_args(pot_path: str, r_crd=3.0, n_quad=3, alpha_min=20.0, alpha_max=
 def write_workload(dirpath: str, kind: str, **kw) -> dict:
     """Write a complete workload (cfg + potential + script) and describe it.
 
-    kind: "eam" (configs[0]-style FCC EAM), "fs" (analytic FS), "dmd" (binary DMD).
+    kind: "eam" (FCC EAM crystal, tabulated), "fs" (analytic FS), "dmd" (binary DMD).
     """
     os.makedirs(dirpath, exist_ok=True)
     skin = kw.pop("skin", 0.5)

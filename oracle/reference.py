@@ -1,6 +1,6 @@
 """Runs the compiled reference (oracle/_ref/mapp_ref_harness) on a workload.
 
-Test infrastructure only (the oracle is the checker, never the product).  The
+Test infrastructure only (the oracle tests the library and is never part of it).  The
 harness executable links the unmodified reference objects; see
 oracle/ref/harness.cpp for the call sequences it reproduces.  Each run is a
 separate process, so a reference abort cannot take the caller down.

@@ -1,6 +1,6 @@
 """ctypes wrapper around the C restatement oracle (oracle/mapp_oracle.c).
 
-Test infrastructure only: the checker for the GPU library, never the product.
+Test infrastructure only: what the GPU library is tested against, never part of it.
 ``OracleRun`` mirrors the reference harness (oracle/reference.py): it takes a
 workload written by ``mapp_b200.fixtures.write_workload`` and reproduces the
 reference's call sequence (Min_LBFGS::init order) in the restatement.
