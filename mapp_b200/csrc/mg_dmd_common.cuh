@@ -38,7 +38,11 @@ __device__ __forceinline__ double calc_ent(double x)
 __device__ __forceinline__ void embed_F(const Dev& d, int a, double Ev, double& tmp0, double& tmp1, double* dd)
 {
     double p = Ev * d.drho_inv;
-    int m = min((int)p, d.nr - 2);
+    // the upper clamp is the reference's (nr - 2, defect kept); the lower one
+    // only matters for a negative density, which the learned form's untrained
+    // network can produce: the first knot's polynomial is extrapolated instead
+    // of reading before the table
+    int m = max(0, min((int)p, d.nr - 2));
     p -= m;
     p = fmin(p, 1.0);
     double p2 = p * p, p3 = p2 * p, p4 = p3 * p;

@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kFFBlock) k_eam_embed(Dev d, int row0)
     if (i < d.natms) {
         double rv = d.rho[i];
         double p = rv * d.drho_inv;
-        int m = min((int)p, d.nr - 2);
+        int m = max(0, min((int)p, d.nr - 2));  // lower clamp: never index before the table
         p -= m;
         p = fmin(p, 1.0);
         const double* cf = d.FT + ((size_t)d.type[i] * (d.nrho + 1) + m) * d.Fw;
