@@ -40,6 +40,7 @@ typedef struct mg_system mg_system;
 #define MG_ERR_CAPACITY 6     /* a device buffer limit could not be met          */
 #define MG_ERR_UNSUPPORTED 7  /* feature not available for this style / form      */
 #define MG_ERR_TIMEOUT 8      /* a bounded device-side wait ran out               */
+#define MG_ERR_DOMAIN 9       /* an integration left its domain (reference aborts) */
 
 #define MG_FORM_FP64 0        /* plain form: FP64 arithmetic throughout            */
 #define MG_FORM_FP32 1        /* precision form: FP32 pair/quadrature/spline,
@@ -110,7 +111,8 @@ int mg_ff_create_2nd_neigh_lst(mg_system* s);
    (may be NULL). Uses the per-pair densities of the last force_calc. */
 int mg_ff_c_d_calc(mg_system* s, double* c_d);
 /* ForceField::calc_g (ff_dmd_I.cpp:2402-2674): a and g are natms * ntypes;
-   *cost receives the return value; chk != 0 computes the cost only. */
+   *cost receives the return value; chk != 0 computes the cost only and
+   leaves g zeroed, as the reference does. */
 int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g, double* cost);
 /* ForceField::fin (releases the per-pair scratch and FF vectors). */
 int mg_ff_fin(mg_system* s);
@@ -351,6 +353,43 @@ int mg_min_cg(mg_system* s, int max_iter, double fmax_tol, double energy_tol, in
    doubles, may be NULL) receives each step's final calc_g cost and n_calc_g
    (may be NULL) the number of calc_g evaluations. */
 int mg_clock_adams(mg_system* s, int order, int nsteps, double delta_t, double* err, long long* n_calc_g);
+
+/* The options of "clock bdf nsteps [key value ...]" (clock_bdf.cpp:14-111);
+   mg_bdf_defaults fills the constructor's defaults (clock_bdf.cpp:14-24).
+   initial_del_t < 0 means "not given": the first step is then
+   a_tol / rms(c_d) clamped to [min_del_t, max_del_t] (clock_bdf.cpp:257-269). */
+typedef struct mg_bdf_opts {
+    int max_order;        /* 6 (at most 12 here)  */
+    int max_iter;         /* 50                   */
+    double min_gamma;     /* 1e-10                */
+    double gamma_red;     /* 0.8 ("red_gamma")    */
+    double slope;         /* 0.4                  */
+    double m_tol;         /* 1e-10                */
+    double a_tol;         /* 1e-6                 */
+    double e_tol;         /* 0: no early stop     */
+    double min_del_t;     /* 1e-12                */
+    double max_del_t;     /* 1e4                  */
+    double initial_del_t; /* -1: from rms(c_d)    */
+} mg_bdf_opts;
+void mg_bdf_defaults(mg_bdf_opts* o);
+/* Clock_BDF init + run (clock_bdf.cpp:201-275, 479-884) for an initialised
+   DMD system in the plain form: variable-order (1..max_order),
+   variable-step BDF steps of the concentrations, each solved by the
+   reference's box-constrained nonlinear conjugate gradient on calc_g, with
+   the reference's error estimates and step/order control.  opts may be NULL
+   (the defaults).  The run ends after nsteps steps or when
+   rms(c_d) / e_tol < 1.  The vectors stay on the device; only the scalars
+   that steer the solve and the step control cross to the host.  On return
+   the system holds the final c; hist (3 * nsteps doubles, may be NULL)
+   receives per step its size, the order it ran at and the time after it;
+   steps_taken and n_calc_g (may be NULL) the steps run and the calc_g
+   evaluations.  Where the reference aborts (c outside [0, 1] after a solve)
+   this returns MG_ERR_DOMAIN, as it does when the reference's unbounded
+   step-size retry loops would not end (100000 retries).  The error estimate
+   reads a local time the reference never sets (clock_bdf.cpp:838-854); the
+   reference built with gcc -O2 evaluates it as 0.0 and so does this. */
+int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, double* hist, int* steps_taken,
+                 long long* n_calc_g);
 
 /* ---- Nose-Hoover molecular dynamics ------------------------------------- */
 /* MD_NH "md nh nvt temp t_tar t_period eta_iteration .. eta_chains .." with

@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(HERE, "libmapp_b200.so")
 MG_FORM_FP64, MG_FORM_FP32, MG_FORM_MLP = 0, 1, 2
 MG_MIN_LBFGS, MG_MIN_CG = 0, 1
 MG_LAUNCH_WHOLE_GPU = -1
-ERRORS = {1: "ARG", 2: "FILE", 3: "FORMAT", 4: "STATE", 5: "CUDA", 6: "CAPACITY", 7: "UNSUPPORTED", 8: "TIMEOUT"}
+ERRORS = {1: "ARG", 2: "FILE", 3: "FORMAT", 4: "STATE", 5: "CUDA", 6: "CAPACITY", 7: "UNSUPPORTED", 8: "TIMEOUT", 9: "DOMAIN"}
 
 # Every exported entry point of include/mapp_b200.h with its ctypes signature.
 _P = C.c_void_p
@@ -81,6 +81,8 @@ SIGNATURES = {
     "mg_min_cg": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _P, _P]),
     "mg_batch_set_method": (C.c_int, [_P, C.c_int]),
     "mg_clock_adams": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, _P, C.POINTER(C.c_longlong)]),
+    "mg_bdf_defaults": (None, [_P]),
+    "mg_clock_bdf": (C.c_int, [_P, C.c_int, _P, _P, _I, C.POINTER(C.c_longlong)]),
     "mg_md_nh": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _P,
                            C.c_int, _P, _P, _I]),
     "mg_cfg_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
@@ -117,6 +119,14 @@ class FsCoeffs(C.Structure):
                 ("t1", (C.c_double * 4) * 4), ("t2", (C.c_double * 4) * 4),
                 ("cut_rho", C.c_double * 10), ("cut_phi", C.c_double * 10),
                 ("k1", C.c_double * 10), ("k2", C.c_double * 10), ("k3", C.c_double * 10)]
+
+
+class BdfOpts(C.Structure):
+    """mg_bdf_opts: the options of "clock bdf" (clock_bdf.cpp:14-111)."""
+    _fields_ = [("max_order", C.c_int), ("max_iter", C.c_int), ("min_gamma", C.c_double),
+                ("gamma_red", C.c_double), ("slope", C.c_double), ("m_tol", C.c_double), ("a_tol", C.c_double),
+                ("e_tol", C.c_double), ("min_del_t", C.c_double), ("max_del_t", C.c_double),
+                ("initial_del_t", C.c_double)]
 
 
 class MGError(RuntimeError):
@@ -364,6 +374,28 @@ class System:
         ncg = C.c_longlong(0)
         _check(load_library().mg_clock_adams(self.h, order, steps, dt, err.ctypes.data, C.byref(ncg)))
         return {"c": self.vector("c"), "err": err[:steps], "n_calc_g": int(ncg.value)}
+
+    def clock_bdf(self, steps, **opts):
+        """BDF clock of this DMD system on the device (mg_clock_bdf); options
+        as the fields of BdfOpts (unset ones keep the reference's defaults).
+        Returns dict(c, n_calc_g, steps, del_t, order, t): per step its size,
+        the order it ran at and the time after it; t is the final time."""
+        lib = load_library()
+        o = BdfOpts()
+        lib.mg_bdf_defaults(C.byref(o))
+        names = {k for k, _ in BdfOpts._fields_}
+        for k, v in opts.items():
+            if k not in names:
+                raise ValueError(f"unknown clock bdf option {k}")
+            setattr(o, k, v)
+        hist = np.zeros(3 * max(steps, 1))
+        ncg = C.c_longlong(0)
+        taken = C.c_int(0)
+        _check(lib.mg_clock_bdf(self.h, steps, C.byref(o), hist.ctypes.data, C.byref(taken), C.byref(ncg)))
+        k = taken.value
+        h = hist[: 3 * k].reshape(-1, 3)
+        return {"c": self.vector("c"), "n_calc_g": int(ncg.value), "steps": k, "del_t": h[:, 0],
+                "order": h[:, 1].astype(int), "t": float(h[-1, 2]) if k else 0.0}
 
     def md_nh(self, t_tar, t_period, steps, dt, boltz, xd=None, seed=0, eta_iteration=1, eta_chains=3):
         """Nose-Hoover NVT run of this EAM / FS system on the device (mg_md_nh).

@@ -1306,7 +1306,7 @@ int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g
     CHK(timed_end(s, &s->t_g));
     double tot[2] = {0, 0};
     CU(cudaMemcpyAsync(tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
-    if (!chk) CHK(copy_out(s, g, d.g, bytes));
+    CHK(copy_out(s, g, d.g, bytes));
     CU(cudaStreamSynchronize(s->st));
     if (cost) *cost = tot[0] * 0.25;
     return MG_OK;

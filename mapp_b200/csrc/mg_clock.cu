@@ -27,7 +27,7 @@ constexpr int kCkBlock = 256;
 constexpr int kMaxOrder = 6;
 
 // slots of the device scalar block
-enum { SC_RATIO = 0, SC_GG0 = 1, SC_GG = 2, SC_GH = 3, SC_GAMMA = 4, SC_G0G0 = 5, SC_COUNT = 8 };
+enum { SC_RATIO = 0, SC_GG0 = 1, SC_GG = 2, SC_GH = 3, SC_GAMMA = 4, SC_G0G0 = 5, SC_A = 6, SC_B = 7, SC_COUNT = 8 };
 
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
@@ -214,6 +214,121 @@ __global__ void __launch_bounds__(kCkBlock) k_ck_direction(CkView V, double rati
     if (reduce_last<1, false>(v, V, tot) && threadIdx.x == 0) V.sc[SC_GH] = tot[0];
 }
 
+// ---- BDF clock (clock_bdf.cpp) ---------------------------------------------
+
+constexpr int kMaxBdfOrder = 12;
+
+struct BdfVecs {
+    double* y_0;
+    double* e_n;
+    double* dy;
+};
+
+// the interpolation's history terms (clock_bdf.cpp:345-352): alpha_y[j] and
+// beta * dalpha_y[j] against y[j]
+struct BdfHist {
+    const double* y[kMaxBdfOrder];
+    double ay[kMaxBdfOrder];
+    double bdy[kMaxBdfOrder];
+    int q;
+};
+
+// Clock_BDF::interpolate's vector part (clock_bdf.cpp:343-360): the predictor
+// y_0 and calc_g's a; SC_A receives -1 when some y_0 leaves [0, 1], else 1
+__global__ void __launch_bounds__(kCkBlock) k_bdf_interp(CkView V, BdfVecs B, BdfHist Y, double b_dady0, double ady0)
+{
+    const int i = blockIdx.x * kCkBlock + threadIdx.x;
+    double v[1] = {1.0};
+    if (i < V.n) {
+        const double dyi = B.dy[i];
+        double a = dmul(b_dady0, dyi), y0 = dmul(ady0, dyi);
+        for (int j = 0; j < Y.q; j++) {
+            const double yj = Y.y[j][i];
+            a = dadd(a, dmul(Y.bdy[j], yj));
+            y0 = dadd(y0, dmul(Y.ay[j], yj));
+        }
+        V.a[i] = dsub(a, y0);
+        B.y_0[i] = y0;
+        if (y0 < 0.0 || y0 > 1.0) v[0] = -1.0;
+    }
+    double tot[1];
+    if (reduce_last<1, true>(v, V, tot) && threadIdx.x == 0) V.sc[SC_A] = tot[0];
+}
+
+// the bound of the explicit predictor step y[0] + dy del_t (clock_bdf.cpp:
+// 706-714)
+__global__ void __launch_bounds__(kCkBlock) k_bdf_predict_bound(CkView V, const double* y0, const double* dy, double dt)
+{
+    const int i = blockIdx.x * kCkBlock + threadIdx.x;
+    double v[1] = {1.0};
+    if (i < V.n) v[0] = box_bound(y0[i], dadd(dmul(dy[i], dt), y0[i]), 1.0);
+    double tot[1];
+    if (reduce_last<1, true>(v, V, tot) && threadIdx.x == 0) V.sc[SC_RATIO] = tot[0];
+}
+
+// c = y[0] + dy del_t ratio (clock_bdf.cpp:716-717)
+__global__ void __launch_bounds__(kCkBlock) k_bdf_predict(CkView V, const double* y0, const double* dy, double dt)
+{
+    const int i = blockIdx.x * kCkBlock + threadIdx.x;
+    if (i >= V.n) return;
+    V.c[i] = dadd(y0[i], dmul(dmul(dy[i], dt), V.sc[SC_RATIO]));
+}
+
+// the step's error sums (clock_bdf.cpp:856-863) and the domain check
+// (clock_bdf.cpp:876-878): sum (y_0 - c)^2, sum c_d^2, count of c outside [0, 1]
+__global__ void __launch_bounds__(kCkBlock) k_bdf_err(CkView V, BdfVecs B)
+{
+    const int i = blockIdx.x * kCkBlock + threadIdx.x;
+    double v[3] = {0.0, 0.0, 0.0};
+    if (i < V.n) {
+        const double ci = V.c[i], t = dsub(B.y_0[i], ci), cd = V.c_d[i];
+        v[0] = dmul(t, t);
+        v[1] = dmul(cd, cd);
+        v[2] = (ci < 0.0 || ci > 1.0) ? 1.0 : 0.0;
+    }
+    double tot[3];
+    if (reduce_last<3, false>(v, V, tot) && threadIdx.x == 0) {
+        V.sc[SC_GG0] = tot[0];
+        V.sc[SC_GG] = tot[1];
+        V.sc[SC_GH] = tot[2];
+    }
+}
+
+struct BdfHiLo {
+    const double* y[kMaxBdfOrder];
+    double lwr[kMaxBdfOrder];
+    double q_n, hi_pre, lwr_y, lwr_dy, c1_c0;
+    int hi, lo, m;
+};
+
+// Clock_BDF::hi_lo_err_est's vector part (clock_bdf.cpp:436-464): the
+// higher- and lower-order error sums, then e_n = c - y_0
+__global__ void __launch_bounds__(kCkBlock) k_bdf_hilo(CkView V, BdfVecs B, BdfHiLo P)
+{
+    const int i = blockIdx.x * kCkBlock + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (i < V.n) {
+        const double ci = V.c[i], y0 = B.y_0[i];
+        if (P.hi) {
+            const double t = dmul(dsub(dsub(ci, y0), dmul(P.q_n, B.e_n[i])), P.hi_pre);
+            v[0] = dmul(t, t);
+        }
+        if (P.lo) {
+            double t = dmul(P.lwr_y, ci);
+            t = dadd(t, dmul(P.lwr_dy, V.c_d[i]));
+            for (int j = 0; j < P.m; j++) t = dadd(t, dmul(P.lwr[j], P.y[j][i]));
+            t = dmul(t, P.c1_c0);
+            v[1] = dmul(t, t);
+        }
+        B.e_n[i] = dsub(ci, y0);
+    }
+    double tot[2];
+    if (reduce_last<2, false>(v, V, tot) && threadIdx.x == 0) {
+        V.sc[SC_GG0] = tot[0];
+        V.sc[SC_GG] = tot[1];
+    }
+}
+
 constexpr double kBeta[6][6] = {
     {1.0, 0, 0, 0, 0, 0},
     {1.0 / 2.0, 1.0 / 2.0, 0, 0, 0, 0},
@@ -338,6 +453,250 @@ struct Clock {
     }
 };
 
+// Clock_BDF's run (clock_bdf.cpp:479-675) over the device vectors: the
+// interpolation coefficients, error prefactors and step/order control are
+// scalar host work on the time history, exactly as the reference computes
+// them; the vectors y_0, e_n, dy and the history y[0..max_order) stay on the
+// device.
+struct Bdf {
+    Clock* ck = nullptr;
+    mg_bdf_opts p{};
+    int n = 0, dof_tot = 0, hi_ord_avail = 0, lo_ord_avail = 0;
+    BdfVecs B{};
+    std::vector<double*> y;  // y[0] newest; rotated by pointer as the reference does
+    std::vector<double> t;
+    double alpha_y[kMaxBdfOrder + 1], dalpha_y[kMaxBdfOrder + 1], lwr_alpha[kMaxBdfOrder + 1];
+    double alpha_dy_0 = 0, dalpha_dy_0 = 0, beta = 0, err = 0, lo_err = 0, hi_err = 0, eq_ratio = 0;
+
+    int grid() const { return ck->V.nblocks; }
+
+    // Clock_BDF::interpolate (clock_bdf.cpp:295-368) -> 1 or -1
+    int interpolate(double del_t, int q, int* ret)
+    {
+        double tmp0, tmp1, c0 = 1.0, c1 = 0.0, c2 = 0.0, c3, t_new = t[0] + del_t;
+        for (int i = 1; i < q; i++) {
+            tmp0 = (t_new - t[0]) / (t[i] - t[0]);
+            tmp1 = tmp0 * tmp0;
+            for (int j = 1; j < q; j++)
+                if (i != j) tmp1 *= (t_new - t[j]) / (t[i] - t[j]);
+            alpha_y[i] = tmp1;
+            c0 *= (t_new - t[i]) / (t[0] - t[i]);
+            c1 += 1.0 / (t[0] - t[i]);
+            c2 += 1.0 / (t_new - t[i]);
+        }
+        alpha_y[0] = (1.0 - (t_new - t[0]) * c1) * c0;
+        alpha_dy_0 = c0 * (t_new - t[0]);
+        c3 = 2.0 / (t_new - t[0]);
+        dalpha_dy_0 = alpha_dy_0 * (c2 + 0.5 * c3);
+        dalpha_y[0] = c0 * (c2 - c1 + (t_new - t[0]) * c1 * c2);
+        for (int i = 1; i < q; i++) dalpha_y[i] = alpha_y[i] * (c2 + c3 - 1.0 / (t_new - t[i]));
+        tmp0 = 0.0;
+        for (int i = 0; i < q; i++) tmp0 += 1.0 / (double)(i + 1);
+        beta = del_t / tmp0;
+        BdfHist H{};
+        H.q = q;
+        for (int j = 0; j < q; j++) {
+            H.y[j] = y[j];
+            H.ay[j] = alpha_y[j];
+            H.bdy[j] = beta * dalpha_y[j];
+        }
+        k_bdf_interp<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, B, H, beta * dalpha_dy_0, alpha_dy_0);
+        KCU(cudaGetLastError());
+        KCHK(ck->read_scalars());
+        *ret = ck->host_sc[SC_A] < 0.0 ? -1 : 1;
+        return MG_OK;
+    }
+
+    // Clock_BDF::solve (clock_bdf.cpp:677-884); *out = the cost ratio.  The
+    // error estimate there reads an uninitialised local curr_t
+    // (clock_bdf.cpp:838-854) which the reference built with gcc -O2
+    // evaluates as 0.0; so does this.
+    int solve(double del_t, int q, double* out)
+    {
+        const mg_bdf_opts& o = p;
+        double gamma, max_gamma = 1.0, ratio, g0_g0, g_g, g_g0, g_h, curr_cost, ideal_cost, cost;
+        int chk;
+        k_bdf_predict_bound<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, y[0], B.dy, del_t);
+        k_bdf_predict<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, y[0], B.dy, del_t);
+        KCU(cudaGetLastError());
+        KCHK(ck->refresh_c());
+        KCHK(ck->calc_g(0, beta, &curr_cost));
+        k_ck_h_from_g<<<grid(), kCkBlock, 0, ck->st>>>(ck->V);
+        KCU(cudaGetLastError());
+        KCHK(ck->read_scalars());
+        g0_g0 = ck->host_sc[SC_G0G0];
+        g_h = g0_g0;
+        int iter = 0;
+        while (curr_cost > o.m_tol * (double)dof_tot && iter < o.max_iter && max_gamma > o.min_gamma) {
+            k_ck_begin<<<grid(), kCkBlock, 0, ck->st>>>(ck->V);
+            KCU(cudaGetLastError());
+            KCHK(ck->read_scalars());
+            // min(0.99, the box bounds along h) (clock_bdf.cpp:744-759)
+            gamma = ck->host_sc[SC_GAMMA] < 0.99 ? ck->host_sc[SC_GAMMA] : 0.99;
+            max_gamma = gamma * 0.9;
+            chk = 1;
+            cost = curr_cost;
+            while (chk && max_gamma > o.min_gamma) {
+                k_ck_trial<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, max_gamma);
+                KCU(cudaGetLastError());
+                KCHK(ck->refresh_c());
+                // the dot products g.g0, g.g ride along with the cost readback
+                KCHK(ck->calc_g(0, beta, &curr_cost, true));
+                ideal_cost = cost - o.slope * max_gamma * g_h;
+                if (curr_cost < ideal_cost) chk = 0;
+                max_gamma *= o.gamma_red;
+                if (max_gamma <= o.min_gamma) {
+                    KCU(cudaMemcpyAsync(ck->V.c, ck->V.c0, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                        ck->st));
+                    KCHK(ck->refresh_c());
+                    // the cost-only call zeroes g, so the dots become 0
+                    KCHK(ck->calc_g(1, beta, &curr_cost, true));
+                }
+            }
+            if (chk == 0) {
+                g_g0 = ck->host_sc[SC_GG0];
+                g_g = ck->host_sc[SC_GG];
+                ratio = (g_g - g_g0) / g0_g0;
+                g0_g0 = g_g;
+                k_ck_direction<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, ratio);
+                KCU(cudaGetLastError());
+                KCHK(ck->read_scalars());
+                g_h = ck->host_sc[SC_GH];
+                if (g_h < 0.0) {
+                    KCU(cudaMemcpyAsync(ck->V.h, ck->V.g, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                        ck->st));
+                    g_h = g_g;
+                }
+            }
+            iter++;
+        }
+        double a_1 = 1.0, curr_t = 0.0, l1_q = 0.0, err_pre_fac;
+        for (int i = 0; i < q; i++) {
+            l1_q += 1.0 / (curr_t - t[i]);
+            if (i != 0) a_1 *= (curr_t - t[i]) / (t[0] - t[i]);
+        }
+        err_pre_fac = -1.0 / (l1_q * (1.0 + a_1));
+        k_bdf_err<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, B);
+        KCU(cudaGetLastError());
+        KCHK(ck->read_scalars());
+        eq_ratio = sqrt(ck->host_sc[SC_GG] / (double)dof_tot) / o.e_tol;
+        err = sqrt(ck->host_sc[SC_GG0] / ((double)dof_tot * o.a_tol));
+        err *= fabs(err_pre_fac);
+        if (ck->host_sc[SC_GH] != 0.0) return internal_fail(MG_ERR_DOMAIN, "c exceeded the domain");
+        *out = curr_cost / (o.m_tol * (double)dof_tot);
+        return MG_OK;
+    }
+
+    // Clock_BDF::hi_lo_err_est (clock_bdf.cpp:372-476)
+    int hi_lo(double del_t, int q)
+    {
+        double curr_t = t[0] + del_t, c0 = 0.0, c1 = 1.0, tmp0;
+        double a_0 = 1.0, a_1 = 1.0, l1_q = 0.0, hi_a_0, hi_a_1, hi_l1_q, lo_err_pre_fac;
+        BdfHiLo P{};
+        P.q_n = 1.0;
+        P.hi_pre = 1.0;
+        for (int i = 0; i < q; i++) {
+            l1_q += 1.0 / (curr_t - t[i]);
+            a_0 *= curr_t - t[i];
+            if (i != 0) a_1 *= (curr_t - t[i]) / (t[0] - t[i]);
+        }
+        if (hi_ord_avail) {
+            hi_a_0 = hi_a_1 = 1.0;
+            for (int i = 0; i < q; i++) {
+                hi_a_0 *= t[0] - t[i + 1];
+                if (i != 0) hi_a_1 *= (t[0] - t[i + 1]) / (t[1] - t[i + 1]);
+            }
+            P.q_n = (a_0 / hi_a_0) * (1.0 + a_1) / (1.0 + hi_a_1) * (del_t / (t[0] - t[1]));
+            hi_l1_q = l1_q + 1.0 / (curr_t - t[q]);
+            P.hi_pre = -(curr_t - t[q]) / (q + 2);
+            P.hi_pre *= 1.0 / (hi_l1_q * (1.0 + a_1) * del_t * del_t);
+        }
+        if (lo_ord_avail) {
+            lo_err_pre_fac = -del_t * a_0 / (curr_t - t[q - 1]);
+            c0 = 0.0;
+            c1 = 1.0;
+            for (int i = 0; i < q - 1; i++) {
+                tmp0 = 1.0 / (curr_t - t[i]);
+                c0 += tmp0;
+                c1 *= tmp0;
+                lwr_alpha[i] = tmp0 * tmp0;
+                for (int j = 0; j < q - 1; j++)
+                    if (i != j) lwr_alpha[i] *= 1.0 / (t[i] - t[j]);
+                lwr_alpha[i] *= lo_err_pre_fac;
+            }
+            P.lwr_dy = c1 * lo_err_pre_fac;
+            P.lwr_y = -c0 * c1 * lo_err_pre_fac;
+            P.c1_c0 = c1 / c0;
+            P.m = q - 1;
+            for (int j = 0; j < q - 1; j++) {
+                P.lwr[j] = lwr_alpha[j];
+                P.y[j] = y[j];
+            }
+        }
+        P.hi = hi_ord_avail;
+        P.lo = lo_ord_avail;
+        k_bdf_hilo<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, B, P);
+        KCU(cudaGetLastError());
+        KCHK(ck->read_scalars());
+        lo_err = sqrt(ck->host_sc[SC_GG] / ((double)dof_tot * p.a_tol));
+        hi_err = sqrt(ck->host_sc[SC_GG0] / ((double)dof_tot * p.a_tol));
+        return MG_OK;
+    }
+};
+
+int bdf_check(const mg_bdf_opts& o)
+{
+    const char* m = nullptr;
+    if (o.min_gamma <= 0.0) m = "min_gamma should be larger than zero";
+    else if (o.gamma_red <= 0.0 || o.gamma_red >= 1.0) m = "gamma_red should be between zero and one";
+    else if (o.slope <= 0.0 || o.slope >= 1.0) m = "slope should be between zero and one";
+    else if (o.max_iter <= 0) m = "max_iter should be larger than zero";
+    else if (o.max_order <= 0) m = "max_order should be larger than zero";
+    else if (o.m_tol <= 0.0) m = "m_tol should be larger than zero";
+    else if (o.a_tol <= 0.0) m = "a_tol should be larger than zero";
+    else if (o.e_tol < 0.0) m = "e_tol should be larger than zero";
+    else if (o.min_del_t <= 0.0) m = "min_del_t should be larger than zero";
+    else if (o.max_del_t <= 0.0) m = "max_del_t should be larger than zero";
+    else if (o.min_del_t >= o.max_del_t) m = "max_del_t should be larger than min_del_t";
+    else if (o.initial_del_t == 0.0) m = "initial_del_t should be larger than zero";
+    if (m) return internal_fail(MG_ERR_ARG, m);
+    if (o.max_order > kMaxBdfOrder) return internal_fail(MG_ERR_UNSUPPORTED, "max_order above 12");
+    return MG_OK;
+}
+
+// the clock's set-up shared by the Adams and BDF clocks: DMD style in the
+// plain form, then Clock::init's crd list and force_calc(1), which fills the
+// per-pair buffers c_d_calc and calc_g read
+int clock_setup(mg_system* s, const char* what)
+{
+    KCHK(system_check_ready(s));
+    int style = -1, nt = 0, x_dim = 0, form = 0;
+    system_shape(s, &style, &nt, &x_dim, &form, nullptr);
+    if (style != STYLE_DMD_I && style != STYLE_DMD_II && style != STYLE_DMD) {
+        std::string m = std::string("the ") + what + " clock integrates DMD concentrations";
+        return internal_fail(MG_ERR_UNSUPPORTED, m.c_str());
+    }
+    if (form != MG_FORM_FP64) {
+        std::string m = std::string("the ") + what + " clock runs calc_g in the plain FP64 form";
+        return internal_fail(MG_ERR_UNSUPPORTED, m.c_str());
+    }
+    return MG_OK;
+}
+
+int clock_force_init(mg_system* s)
+{
+    int style = -1, nt = 0, x_dim = 0, form = 0;
+    system_shape(s, &style, &nt, &x_dim, &form, nullptr);
+    const int natms = system_natms(s);
+    KCHK(mg_ff_create_2nd_neigh_lst(s));
+    double* fdev = nullptr;
+    KCU(cudaMalloc(&fdev, ((size_t)natms * x_dim + 1) * sizeof(double)));
+    double en[7];
+    int rc = mg_ff_force_calc(s, 1, fdev, en);
+    cudaFree(fdev);
+    return rc;
+}
+
 }  // namespace
 
 }  // namespace mg
@@ -346,12 +705,9 @@ using namespace mg;
 
 extern "C" int mg_clock_adams(mg_system* s, int order, int nsteps, double delta_t, double* err, long long* n_calc_g)
 {
-    KCHK(system_check_ready(s));
+    KCHK(clock_setup(s, "Adams"));
     int style = -1, nt = 0, x_dim = 0, form = 0;
     system_shape(s, &style, &nt, &x_dim, &form, nullptr);
-    if (style != STYLE_DMD_I && style != STYLE_DMD_II && style != STYLE_DMD)
-        return internal_fail(MG_ERR_UNSUPPORTED, "the Adams clock integrates DMD concentrations");
-    if (form != MG_FORM_FP64) return internal_fail(MG_ERR_UNSUPPORTED, "the Adams clock runs calc_g in the plain FP64 form");
     if (order < 1 || order > 6) {
         char msg[96];
         snprintf(msg, sizeof(msg), "BDF cannot operate with order: %d", order);  // the reference's text
@@ -362,17 +718,7 @@ extern "C" int mg_clock_adams(mg_system* s, int order, int nsteps, double delta_
     Clock ck;
     ck.s = s;
     ck.st = system_stream(s);
-    // Clock_Adams::init after the set-up: the crd list and force_calc(1), which
-    // fills the per-pair buffers c_d_calc and calc_g read
-    KCHK(mg_ff_create_2nd_neigh_lst(s));
-    {
-        double* fdev = nullptr;
-        KCU(cudaMalloc(&fdev, ((size_t)natms * x_dim + 1) * sizeof(double)));
-        double en[7];
-        int rc = mg_ff_force_calc(s, 1, fdev, en);
-        cudaFree(fdev);
-        if (rc != MG_OK) return rc;
-    }
+    KCHK(clock_force_init(s));
     const int n = natms * nt;
     if (n == 0 || nsteps == 0) {
         if (n_calc_g) *n_calc_g = 0;
@@ -425,6 +771,184 @@ extern "C" int mg_clock_adams(mg_system* s, int order, int nsteps, double delta_
         }
     }
     KCU(cudaStreamSynchronize(ck.st));
+    if (n_calc_g) *n_calc_g = ck.n_calc_g;
+    return MG_OK;
+}
+
+extern "C" void mg_bdf_defaults(mg_bdf_opts* o)
+{
+    if (!o) return;
+    // Clock_BDF's constructor defaults (clock_bdf.cpp:14-24)
+    o->max_order = 6;
+    o->max_iter = 50;
+    o->min_gamma = 1.0e-10;
+    o->gamma_red = 0.8;
+    o->slope = 0.4;
+    o->m_tol = 1.0e-10;
+    o->a_tol = 1.0e-6;
+    o->e_tol = 0.0;
+    o->min_del_t = 1.0e-12;
+    o->max_del_t = 1.0e4;
+    o->initial_del_t = -1.0;
+}
+
+extern "C" int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, double* hist, int* steps_taken,
+                            long long* n_calc_g)
+{
+    KCHK(clock_setup(s, "BDF"));
+    if (nsteps <= 0) return internal_fail(MG_ERR_ARG, "no of steps should be greater than zero");
+    mg_bdf_opts o;
+    mg_bdf_defaults(&o);
+    if (opts) o = *opts;
+    KCHK(bdf_check(o));
+    int style = -1, nt = 0, x_dim = 0, form = 0;
+    system_shape(s, &style, &nt, &x_dim, &form, nullptr);
+    const int natms = system_natms(s);
+    Clock ck;
+    ck.s = s;
+    ck.st = system_stream(s);
+    // Clock_BDF::init (clock_bdf.cpp:201-275)
+    KCHK(clock_force_init(s));
+    const int n = natms * nt;
+    if (steps_taken) *steps_taken = 0;
+    if (n_calc_g) *n_calc_g = 0;
+    if (n == 0) return MG_OK;
+    const int mo = o.max_order, nblocks = div_up(n, kCkBlock);
+    const size_t vec = ((size_t)n + 31) / 32 * 32;
+    const size_t total = vec * (6 + mo) + (size_t)nblocks * 8 + SC_COUNT + 8;
+    KCU(cudaMalloc(&ck.block, total * sizeof(double)));
+    Dev& d = system_dev(s);
+    ck.V.c = d.c;
+    ck.V.c_d = d.c_d;
+    ck.V.g = d.g;
+    ck.V.a = d.a_in;
+    ck.V.g0 = ck.block;
+    ck.V.c0 = ck.block + vec;
+    ck.V.h = ck.block + 2 * vec;
+    Bdf b;
+    b.ck = &ck;
+    b.p = o;
+    b.n = n;
+    b.dof_tot = n;
+    b.B.y_0 = ck.block + 3 * vec;
+    b.B.e_n = ck.block + 4 * vec;
+    b.B.dy = ck.block + 5 * vec;
+    for (int j = 0; j < mo; j++) b.y.push_back(ck.block + (6 + j) * vec);
+    b.t.assign(mo + 1, 0.0);
+    ck.V.part = ck.block + (6 + mo) * vec;
+    ck.V.sc = ck.V.part + (size_t)nblocks * 8;
+    ck.V.counter = reinterpret_cast<unsigned int*>(ck.V.sc + SC_COUNT);
+    ck.V.n = n;
+    ck.V.nblocks = nblocks;
+    KCU(cudaMemsetAsync(ck.block, 0, total * sizeof(double), ck.st));
+    KCHK(system_enqueue_c_d(s));
+    const size_t bytes = (size_t)n * sizeof(double);
+    double initial_del_t = o.initial_del_t;
+    if (initial_del_t < 0.0) {
+        // y_0 is still zero: the error kernel's second sum is sum c_d^2
+        k_bdf_err<<<nblocks, kCkBlock, 0, ck.st>>>(ck.V, b.B);
+        KCU(cudaGetLastError());
+        KCHK(ck.read_scalars());
+        double sum = sqrt(ck.host_sc[SC_GG] / (double)n);
+        initial_del_t = o.a_tol / sum > o.min_del_t ? o.a_tol / sum : o.min_del_t;
+        initial_del_t = initial_del_t < o.max_del_t ? initial_del_t : o.max_del_t;
+    }
+    KCU(cudaMemcpyAsync(b.y[0], d.c, bytes, cudaMemcpyDeviceToDevice, ck.st));
+    KCU(cudaMemcpyAsync(b.B.dy, d.c_d, bytes, cudaMemcpyDeviceToDevice, ck.st));
+    // Clock_BDF::run (clock_bdf.cpp:479-675); the reference's retry loops on a
+    // predictor outside [0, 1] have no bound, these give up after 100000 tries
+    const long kMaxRetries = 100000;
+    double del_t = initial_del_t, del_t_tmp, err1, ratio = 1.0, cost = 0.0, lo_ratio, hi_ratio;
+    int ord = 1, chk = 1, const_stp = 0, istep = 0;
+    long guard = 0;
+    b.eq_ratio = 1.0;
+    while (b.eq_ratio >= 1.0 && istep < nsteps) {
+        KCHK(b.interpolate(del_t, ord, &chk));
+        while (chk == -1) {
+            if (++guard > kMaxRetries) return internal_fail(MG_ERR_DOMAIN, "the predictor stays outside [0, 1]");
+            del_t *= 0.8;
+            del_t = del_t > o.min_del_t ? del_t : o.min_del_t;
+            KCHK(b.interpolate(del_t, ord, &chk));
+        }
+        KCHK(b.solve(del_t, ord, &cost));
+        while (b.err >= 1.0 || cost >= 1.0) {
+            if (++guard > kMaxRetries) return internal_fail(MG_ERR_DOMAIN, "the step size does not settle");
+            err1 = b.err > cost ? b.err : cost;
+            ratio = pow(0.5 / err1, 1.0 / (double)(ord + 1));
+            if (ratio < 0.5) ratio = 0.5;
+            else if (ratio > 0.9) ratio = 0.9;
+            del_t_tmp = del_t * ratio;
+            del_t = del_t_tmp < o.min_del_t ? o.min_del_t : del_t_tmp;
+            KCHK(b.interpolate(del_t, ord, &chk));
+            while (chk == -1) {
+                if (++guard > kMaxRetries) return internal_fail(MG_ERR_DOMAIN, "the predictor stays outside [0, 1]");
+                del_t *= 0.8;
+                KCHK(b.interpolate(del_t, ord, &chk));
+            }
+            KCHK(b.solve(del_t, ord, &cost));
+        }
+        double* tmp_y = b.y[mo - 1];
+        for (int i = mo - 1; i > 0; i--) {
+            b.t[i] = b.t[i - 1];
+            b.y[i] = b.y[i - 1];
+        }
+        b.y[0] = tmp_y;
+        b.t[0] += del_t;
+        KCU(cudaMemcpyAsync(b.y[0], d.c, bytes, cudaMemcpyDeviceToDevice, ck.st));
+        KCU(cudaMemcpyAsync(b.B.dy, d.c_d, bytes, cudaMemcpyDeviceToDevice, ck.st));
+        b.lo_ord_avail = (ord != 1 && const_stp > ord + 1) ? 1 : 0;
+        b.hi_ord_avail = ((ord < mo && istep != 0) && const_stp > ord + 1) ? 1 : 0;
+        KCHK(b.hi_lo(del_t, ord));
+        if (hist) {
+            hist[3 * istep] = del_t;
+            hist[3 * istep + 1] = ord;
+            hist[3 * istep + 2] = b.t[0];
+        }
+        if (b.hi_ord_avail && b.lo_ord_avail) {
+            lo_ratio = pow(0.5 / b.lo_err, 1.0 / (double)ord);
+            hi_ratio = pow(0.5 / b.hi_err, 1.0 / (double)(ord + 2));
+            ratio = pow(0.5 / b.err, 1.0 / (double)(ord + 1));
+            if (hi_ratio > lo_ratio && hi_ratio > ratio) {
+                ord++;
+                ratio = hi_ratio;
+            } else if (lo_ratio > hi_ratio && lo_ratio > ratio) {
+                ord--;
+                ratio = lo_ratio;
+            }
+        } else if (b.hi_ord_avail == 1 && b.lo_ord_avail == 0) {
+            hi_ratio = pow(0.5 / b.hi_err, 1.0 / (double)(ord + 2));
+            ratio = pow(0.5 / b.err, 1.0 / (double)(ord + 1));
+            if (hi_ratio > ratio) {
+                ord++;
+                ratio = hi_ratio;
+            }
+        } else if (b.hi_ord_avail == 0 && b.lo_ord_avail == 1) {
+            lo_ratio = pow(0.5 / b.lo_err, 1.0 / (double)ord);
+            ratio = pow(0.5 / b.err, 1.0 / (double)(ord + 1));
+            if (lo_ratio > ratio) {
+                ord--;
+                ratio = lo_ratio;
+            }
+        } else
+            ratio = pow(0.5 / b.err, 1.0 / (double)(ord + 1));
+        if (ratio >= 2.0) {
+            ratio = 2.0;
+            const_stp = 0;
+        } else if (ratio <= 0.5) {
+            ratio = 0.5;
+            const_stp = 0;
+        } else {
+            ratio = 1.0;
+            const_stp++;
+        }
+        del_t_tmp = ratio * del_t;
+        if (del_t_tmp > o.max_del_t) del_t = o.max_del_t;
+        else if (del_t_tmp < o.min_del_t) del_t = o.min_del_t;
+        else del_t = del_t_tmp;
+        istep++;
+    }
+    KCU(cudaStreamSynchronize(ck.st));
+    if (steps_taken) *steps_taken = istep;
     if (n_calc_g) *n_calc_g = ck.n_calc_g;
     return MG_OK;
 }

@@ -613,14 +613,16 @@ __global__ void __launch_bounds__(kFFBlock) k_g_srates(Dev d, double alpha)
 }
 
 template <int NT>
-__global__ void __launch_bounds__(kFFBlock) k_g_cost(Dev d, int row0)
+__global__ void __launch_bounds__(kFFBlock) k_g_cost(Dev d, int row0, int chk)
 {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     if (idx < d.natms * NT) {
         double s = d.s[idx];
         acc[0] = s * s;
-        d.g[idx] = -s;
+        // the cost-only call leaves g zeroed, as the reference's does
+        // (g cleared at ff_dmd_I.cpp:2444-2445, return before the g terms)
+        d.g[idx] = chk ? 0.0 : -s;
         d.t[idx] = 0.0;
         d.v[idx] = 0.0;
     }
@@ -859,7 +861,7 @@ cudaError_t dmd_calc_g_ntp(const Dev& d, int chk, double alpha, int* nb, cudaStr
     k_mu_nfinal<NT><<<gs, kFFBlock, 0, st>>>(d, d.style == STYLE_DMD_II ? 3 : 2);
     k_g_sinit<NT><<<gs, kFFBlock, 0, st>>>(d);
     k_g_srates<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
-    k_g_cost<NT><<<gs, kFFBlock, 0, st>>>(d, 0);
+    k_g_cost<NT><<<gs, kFFBlock, 0, st>>>(d, 0, chk);
     *nb = gs;
     if (!chk) {
         k_g_trates<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);

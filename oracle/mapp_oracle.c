@@ -2360,3 +2360,379 @@ long orc_clock_adams(orc_t* o, int order, int no_steps, double delta_t, double* 
     free(a); free(g); free(g0); free(c0); free(h); free(y); free(slot);
     return n_calc_g;
 }
+
+/* ---------------------------------------------------------------------------
+ * Clock_BDF (clock_bdf.cpp): variable-order, variable-step BDF integration of
+ * the DMD concentrations, each step solved by box-constrained nonlinear CG on
+ * calc_g.
+ * ------------------------------------------------------------------------- */
+
+typedef struct {
+    int no_steps, max_order, max_iter;
+    double min_gamma, gamma_red, slope, m_tol, a_tol, e_tol, min_del_t, max_del_t, initial_del_t;
+} orc_bdf_opts;
+
+typedef struct {
+    orc_t* o;
+    orc_bdf_opts p;
+    int n, dof_tot, hi_ord_avail, lo_ord_avail;
+    double *y_0, *e_n, *a, *g, *g0, *c0, *h, *dy, *t, **y, *alpha_y, *dalpha_y, *lwr_alpha;
+    double alpha_dy_0, dalpha_dy_0, beta, err, lo_err, hi_err, eq_ratio, lwr_alpha_dy, lwr_alpha_y;
+    long n_calc_g;
+} orc_bdf_t;
+
+/* Clock_BDF::interpolate (clock_bdf.cpp:295-368) */
+static int bdf_interpolate(orc_bdf_t* B, double del_t, int q)
+{
+    double tmp0, tmp1, c0 = 1.0, c1 = 0.0, c2 = 0.0, c3, t_new = B->t[0] + del_t;
+    double* t = B->t;
+    for (int i = 1; i < q; i++) {
+        tmp0 = (t_new - t[0]) / (t[i] - t[0]);
+        tmp1 = tmp0 * tmp0;
+        for (int j = 1; j < q; j++)
+            if (i != j) tmp1 *= (t_new - t[j]) / (t[i] - t[j]);
+        B->alpha_y[i] = tmp1;
+        c0 *= (t_new - t[i]) / (t[0] - t[i]);
+        c1 += 1.0 / (t[0] - t[i]);
+        c2 += 1.0 / (t_new - t[i]);
+    }
+    B->alpha_y[0] = (1.0 - (t_new - t[0]) * c1) * c0;
+    B->alpha_dy_0 = c0 * (t_new - t[0]);
+    c3 = 2.0 / (t_new - t[0]);
+    B->dalpha_dy_0 = B->alpha_dy_0 * (c2 + 0.5 * c3);
+    B->dalpha_y[0] = c0 * (c2 - c1 + (t_new - t[0]) * c1 * c2);
+    for (int i = 1; i < q; i++) B->dalpha_y[i] = B->alpha_y[i] * (c2 + c3 - 1.0 / (t_new - t[i]));
+    tmp0 = 0.0;
+    for (int i = 0; i < q; i++) tmp0 += 1.0 / (double)(i + 1);
+    B->beta = del_t / tmp0;
+    int ret = 1;
+    for (int i = 0; i < B->n && ret == 1; i++) {
+        B->a[i] = B->beta * B->dalpha_dy_0 * B->dy[i];
+        B->y_0[i] = B->alpha_dy_0 * B->dy[i];
+        for (int j = 0; j < q; j++) {
+            B->a[i] += B->beta * B->dalpha_y[j] * B->y[j][i];
+            B->y_0[i] += B->alpha_y[j] * B->y[j][i];
+        }
+        B->a[i] -= B->y_0[i];
+        if (B->y_0[i] < 0.0 || B->y_0[i] > 1.0) ret = -1;
+    }
+    return ret;
+}
+
+/* Clock_BDF::solve (clock_bdf.cpp:677-884).  The error estimate reads a local
+   curr_t that the reference never sets (clock_bdf.cpp:838-854); the reference
+   built with gcc -O2 evaluates it as 0.0 (it materialises the value as a
+   zeroed register), and so does this restatement.  Returns the cost ratio, or
+   -1 when c leaves [0, 1] (the reference aborts). */
+static double bdf_solve(orc_bdf_t* B, double del_t, int q)
+{
+    orc_t* o = B->o;
+    const int n = B->n;
+    double* c = o->c;
+    double gamma, max_gamma = 1.0, inner, tmp, tmp1, ratio, g0_g0, g_g, g_g0, g_h, curr_cost, ideal_cost, cost;
+    int chk;
+    ratio = 1.0;
+    for (int i = 0; i < n; i++) {
+        tmp = B->dy[i] * del_t + B->y[0][i];
+        if (tmp > 1.0) ratio = MINV((1.0 - B->y[0][i]) / (tmp - B->y[0][i]), ratio);
+        else if (tmp < 0.0) ratio = MINV((B->y[0][i] - 0.0) / (B->y[0][i] - tmp), ratio);
+    }
+    for (int i = 0; i < n; i++) c[i] = B->y[0][i] + B->dy[i] * del_t * ratio;
+    refresh_vec(o, c, o->nt);
+    curr_cost = orc_calc_g(o, 0, B->beta, B->a, B->g);
+    B->n_calc_g++;
+    memcpy(B->h, B->g, sizeof(double) * n);
+    inner = 0.0;
+    for (int i = 0; i < n; i++) inner += B->g[i] * B->g[i];
+    g0_g0 = inner;
+    g_h = g0_g0;
+    int iter = 0;
+    while (curr_cost > B->p.m_tol * (double)B->dof_tot && iter < B->p.max_iter && max_gamma > B->p.min_gamma) {
+        memcpy(B->g0, B->g, sizeof(double) * n);
+        memcpy(B->c0, c, sizeof(double) * n);
+        gamma = 0.99;
+        for (int i = 0; i < n; i++) {
+            tmp = B->c0[i] + B->h[i];
+            if (tmp > 1.0) gamma = MINV((1.0 - B->c0[i]) / (tmp - B->c0[i]), gamma);
+            else if (tmp < 0.0) gamma = MINV((B->c0[i] - 0.0) / (B->c0[i] - tmp), gamma);
+        }
+        max_gamma = gamma;
+        max_gamma *= 0.9;
+        chk = 1;
+        cost = curr_cost;
+        while (chk && max_gamma > B->p.min_gamma) {
+            for (int i = 0; i < n; i++) c[i] = B->c0[i] + max_gamma * B->h[i];
+            refresh_vec(o, c, o->nt);
+            curr_cost = orc_calc_g(o, 0, B->beta, B->a, B->g);
+            B->n_calc_g++;
+            ideal_cost = cost - B->p.slope * max_gamma * g_h;
+            if (curr_cost < ideal_cost) chk = 0;
+            max_gamma *= B->p.gamma_red;
+            if (max_gamma <= B->p.min_gamma) {
+                memcpy(c, B->c0, sizeof(double) * n);
+                refresh_vec(o, c, o->nt);
+                curr_cost = orc_calc_g(o, 1, B->beta, B->a, B->g);
+                B->n_calc_g++;
+            }
+        }
+        if (chk == 0) {
+            inner = 0.0;
+            for (int i = 0; i < n; i++) inner += B->g[i] * B->g0[i];
+            g_g0 = inner;
+            inner = 0.0;
+            for (int i = 0; i < n; i++) inner += B->g[i] * B->g[i];
+            g_g = inner;
+            ratio = (g_g - g_g0) / g0_g0;
+            g0_g0 = g_g;
+            inner = 0.0;
+            for (int i = 0; i < n; i++) {
+                B->h[i] *= ratio;
+                B->h[i] += B->g[i];
+                inner += B->h[i] * B->g[i];
+            }
+            g_h = inner;
+            if (g_h < 0.0) {
+                memcpy(B->h, B->g, sizeof(double) * n);
+                g_h = g_g;
+            }
+        }
+        iter++;
+    }
+    double a_1 = 1.0, curr_t = 0.0, l1_q = 0.0, err_pre_fac, tmp0, err_lcl;
+    for (int i = 0; i < q; i++) {
+        l1_q += 1.0 / (curr_t - B->t[i]);
+        if (i != 0) a_1 *= (curr_t - B->t[i]) / (B->t[0] - B->t[i]);
+    }
+    err_pre_fac = -1.0 / (l1_q * (1.0 + a_1));
+    err_lcl = 0.0;
+    tmp1 = 0.0;
+    for (int i = 0; i < n; i++) {
+        tmp0 = (B->y_0[i] - c[i]);
+        tmp1 += o->c_d[i] * o->c_d[i];
+        err_lcl += tmp0 * tmp0;
+    }
+    B->eq_ratio = sqrt(tmp1 / (double)B->dof_tot) / B->p.e_tol;
+    B->err = sqrt(err_lcl / ((double)B->dof_tot * B->p.a_tol));
+    B->err *= fabs(err_pre_fac);
+    for (int i = 0; i < n; i++)
+        if (c[i] < 0.0 || c[i] > 1.0) return -1.0;
+    return curr_cost / (B->p.m_tol * (double)B->dof_tot);
+}
+
+/* Clock_BDF::hi_lo_err_est (clock_bdf.cpp:372-476) */
+static void bdf_hi_lo(orc_bdf_t* B, double del_t, int q)
+{
+    orc_t* o = B->o;
+    double* t = B->t;
+    const double* c = o->c;
+    const double* c_d = o->c_d;
+    double curr_t = t[0] + del_t, c0 = 0.0, c1 = 1.0, tmp0;
+    double a_0 = 1.0, a_1 = 1.0, l1_q = 0.0;
+    double hi_a_0, hi_a_1, hi_l1_q, Q_n = 1.0, hi_err_pre_fac = 1.0, lo_err_pre_fac;
+    for (int i = 0; i < q; i++) {
+        l1_q += 1.0 / (curr_t - t[i]);
+        a_0 *= curr_t - t[i];
+        if (i != 0) a_1 *= (curr_t - t[i]) / (t[0] - t[i]);
+    }
+    if (B->hi_ord_avail) {
+        hi_a_0 = hi_a_1 = 1.0;
+        for (int i = 0; i < q; i++) {
+            hi_a_0 *= t[0] - t[i + 1];
+            if (i != 0) hi_a_1 *= (t[0] - t[i + 1]) / (t[1] - t[i + 1]);
+        }
+        Q_n = (a_0 / hi_a_0) * (1.0 + a_1) / (1.0 + hi_a_1) * (del_t / (t[0] - t[1]));
+        hi_l1_q = l1_q + 1.0 / (curr_t - t[q]);
+        hi_err_pre_fac = -(curr_t - t[q]) / (q + 2);
+        hi_err_pre_fac *= 1.0 / (hi_l1_q * (1.0 + a_1) * del_t * del_t);
+    }
+    if (B->lo_ord_avail) {
+        lo_err_pre_fac = -del_t * a_0 / (curr_t - t[q - 1]);
+        c0 = 0.0;
+        c1 = 1.0;
+        for (int i = 0; i < q - 1; i++) {
+            tmp0 = 1.0 / (curr_t - t[i]);
+            c0 += tmp0;
+            c1 *= tmp0;
+            B->lwr_alpha[i] = tmp0 * tmp0;
+            for (int j = 0; j < q - 1; j++)
+                if (i != j) B->lwr_alpha[i] *= 1.0 / (t[i] - t[j]);
+            B->lwr_alpha[i] *= lo_err_pre_fac;
+        }
+        B->lwr_alpha_dy = c1 * lo_err_pre_fac;
+        B->lwr_alpha_y = -c0 * c1 * lo_err_pre_fac;
+    }
+    double lo = 0.0, hi = 0.0;
+    for (int i = 0; i < B->n; i++) {
+        if (B->hi_ord_avail) {
+            tmp0 = (c[i] - B->y_0[i]) - Q_n * B->e_n[i];
+            tmp0 *= hi_err_pre_fac;
+            hi += tmp0 * tmp0;
+        }
+        if (B->lo_ord_avail) {
+            tmp0 = B->lwr_alpha_y * c[i];
+            tmp0 += B->lwr_alpha_dy * c_d[i];
+            for (int j = 0; j < q - 1; j++) tmp0 += B->lwr_alpha[j] * B->y[j][i];
+            tmp0 *= c1 / c0;
+            lo += tmp0 * tmp0;
+        }
+        B->e_n[i] = c[i] - B->y_0[i];
+    }
+    B->lo_err = sqrt(lo / ((double)B->dof_tot * B->p.a_tol));
+    B->hi_err = sqrt(hi / ((double)B->dof_tot * B->p.a_tol));
+}
+
+/*
+ * "clock bdf no_steps [options]" then run: Clock_BDF::init (clock_bdf.cpp:
+ * 201-275) after the set-up of orc_init (crd list, force_calc(1), c_d_calc,
+ * the initial step from rms(c_d) when initial_del_t < 0) and Clock_BDF::run
+ * (clock_bdf.cpp:479-675).  hist (3 * no_steps doubles, may be NULL) receives
+ * per step the step size, the order and the time after it.  Returns the
+ * number of steps taken, -1 for c leaving [0, 1] (the reference aborts), -2
+ * when a step-size loop of the reference would not end (more than 100000
+ * retries).  *n_calc_g counts the calc_g calls.
+ */
+int orc_clock_bdf(orc_t* o, const orc_bdf_opts* opts, double* hist, long* n_calc_g)
+{
+    if (!o->dmd || opts->max_order < 1) return -2;
+    orc_bdf_t B;
+    memset(&B, 0, sizeof(B));
+    B.o = o;
+    B.p = *opts;
+    const int n = o->natms * o->nt, mo = opts->max_order;
+    B.n = n;
+    B.dof_tot = n;
+    double en[7];
+    orc_create_2nd_neigh_lst(o);
+    double* f = calloc((size_t)o->natms * o->x_dim + 1, sizeof(double));
+    orc_force(o, 1, f, en);
+    free(f);
+    double* block = calloc((size_t)(n + 1) * (9 + mo) + 4 * (size_t)mo + 8, sizeof(double));
+    double* p = block;
+    B.y_0 = p; p += n + 1;
+    B.e_n = p; p += n + 1;
+    B.a = p; p += n + 1;
+    B.g = p; p += n + 1;
+    B.g0 = p; p += n + 1;
+    B.c0 = p; p += n + 1;
+    B.h = p; p += n + 1;
+    B.dy = p; p += n + 1;
+    B.t = p; p += mo + 1;
+    B.alpha_y = p; p += mo + 1;
+    B.dalpha_y = p; p += mo + 1;
+    B.lwr_alpha = p; p += mo + 1;
+    B.y = calloc(mo, sizeof(double*));
+    for (int i = 0; i < mo; i++) {
+        B.y[i] = p;
+        p += n + 1;
+    }
+    B.t[0] = 0.0;
+    orc_c_d_calc(o, NULL);
+    double initial_del_t = opts->initial_del_t;
+    if (initial_del_t < 0.0) {
+        double sum = 0.0;
+        for (int i = 0; i < n; i++) sum += o->c_d[i] * o->c_d[i];
+        sum = sqrt(sum / (double)B.dof_tot);
+        initial_del_t = MAXV(opts->a_tol / sum, opts->min_del_t);
+        initial_del_t = MINV(initial_del_t, opts->max_del_t);
+    }
+    memcpy(B.y[0], o->c, sizeof(double) * n);
+    memcpy(B.dy, o->c_d, sizeof(double) * n);
+    double del_t = initial_del_t, del_t_tmp, err1, ratio = 1.0, cost, lo_ratio, hi_ratio;
+    int ord = 1, chk, const_stp = 0, istep = 0, rc = 0;
+    B.eq_ratio = 1.0;
+    long guard = 0;
+    while (B.eq_ratio >= 1.0 && istep < opts->no_steps) {
+        chk = bdf_interpolate(&B, del_t, ord);
+        while (chk == -1) {
+            if (++guard > 100000) { rc = -2; goto out; }
+            del_t *= 0.8;
+            del_t = MAXV(del_t, opts->min_del_t);
+            chk = bdf_interpolate(&B, del_t, ord);
+        }
+        cost = bdf_solve(&B, del_t, ord);
+        if (cost < 0.0) { rc = -1; goto out; }
+        while (B.err >= 1.0 || cost >= 1.0) {
+            if (++guard > 100000) { rc = -2; goto out; }
+            err1 = MAXV(B.err, cost);
+            ratio = pow(0.5 / err1, 1.0 / (double)(ord + 1));
+            if (ratio < 0.5) ratio = 0.5;
+            else if (ratio > 0.9) ratio = 0.9;
+            del_t_tmp = del_t * ratio;
+            if (del_t_tmp < opts->min_del_t) del_t = opts->min_del_t;
+            else del_t = del_t_tmp;
+            chk = bdf_interpolate(&B, del_t, ord);
+            while (chk == -1) {
+                if (++guard > 100000) { rc = -2; goto out; }
+                del_t *= 0.8;
+                chk = bdf_interpolate(&B, del_t, ord);
+            }
+            cost = bdf_solve(&B, del_t, ord);
+            if (cost < 0.0) { rc = -1; goto out; }
+        }
+        double* tmp_y = B.y[mo - 1];
+        for (int i = mo - 1; i > 0; i--) {
+            B.t[i] = B.t[i - 1];
+            B.y[i] = B.y[i - 1];
+        }
+        B.y[0] = tmp_y;
+        B.t[0] += del_t;
+        memcpy(B.y[0], o->c, sizeof(double) * n);
+        memcpy(B.dy, o->c_d, sizeof(double) * n);
+        B.lo_ord_avail = (ord != 1 && const_stp > ord + 1) ? 1 : 0;
+        B.hi_ord_avail = ((ord < mo && istep != 0) && const_stp > ord + 1) ? 1 : 0;
+        bdf_hi_lo(&B, del_t, ord);
+        if (hist) {
+            hist[3 * istep] = del_t;
+            hist[3 * istep + 1] = ord;
+            hist[3 * istep + 2] = B.t[0];
+        }
+        if (B.hi_ord_avail && B.lo_ord_avail) {
+            lo_ratio = pow(0.5 / B.lo_err, 1.0 / (double)ord);
+            hi_ratio = pow(0.5 / B.hi_err, 1.0 / (double)(ord + 2));
+            ratio = pow(0.5 / B.err, 1.0 / (double)(ord + 1));
+            if (hi_ratio > lo_ratio && hi_ratio > ratio) {
+                ord++;
+                ratio = hi_ratio;
+            } else if (lo_ratio > hi_ratio && lo_ratio > ratio) {
+                ord--;
+                ratio = lo_ratio;
+            }
+        } else if (B.hi_ord_avail == 1 && B.lo_ord_avail == 0) {
+            hi_ratio = pow(0.5 / B.hi_err, 1.0 / (double)(ord + 2));
+            ratio = pow(0.5 / B.err, 1.0 / (double)(ord + 1));
+            if (hi_ratio > ratio) {
+                ord++;
+                ratio = hi_ratio;
+            }
+        } else if (B.hi_ord_avail == 0 && B.lo_ord_avail == 1) {
+            lo_ratio = pow(0.5 / B.lo_err, 1.0 / (double)ord);
+            ratio = pow(0.5 / B.err, 1.0 / (double)(ord + 1));
+            if (lo_ratio > ratio) {
+                ord--;
+                ratio = lo_ratio;
+            }
+        } else
+            ratio = pow(0.5 / B.err, 1.0 / (double)(ord + 1));
+        if (ratio >= 2.0) {
+            ratio = 2.0;
+            const_stp = 0;
+        } else if (ratio <= 0.5) {
+            ratio = 0.5;
+            const_stp = 0;
+        } else {
+            ratio = 1.0;
+            const_stp++;
+        }
+        del_t_tmp = ratio * del_t;
+        if (del_t_tmp > opts->max_del_t) del_t = opts->max_del_t;
+        else if (del_t_tmp < opts->min_del_t) del_t = opts->min_del_t;
+        else del_t = del_t_tmp;
+        istep++;
+    }
+    rc = istep;
+out:
+    if (n_calc_g) *n_calc_g = B.n_calc_g;
+    free(B.y);
+    free(block);
+    return rc;
+}

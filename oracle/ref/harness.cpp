@@ -20,6 +20,7 @@
  *             write_file(step) of the current state.
  *   adams   = Clock_Adams (clock_adams.cpp) constructed, init, run, then the
  *             owned c and the number of calc_g calls written before fin.
+ *   bdf     = Clock_BDF (clock_bdf.cpp) the same way, plus the final time.
  *   md      = MD_NH "nvt" (md_nh.cpp) constructed, time_step / boltzmann set,
  *             init, run, then the owned x and x_d and one force_calc(1) at
  *             the final state written before fin.  Velocities are either
@@ -65,6 +66,7 @@
 #include "min_cg.h"
 #include "md_nh.h"
 #include "clock_adams.h"
+#include "clock_bdf.h"
 #include "write_cfg.h"
 
 using namespace MAPP_NS;
@@ -162,6 +164,12 @@ struct CgRun : public Min_CG {
     CgRun(MAPP* m, int narg, char** arg) : Min_CG(m, narg, arg) {}
     int code() const { return err; }
     double energy() const { return curr_energy; }
+};
+
+/* the reference BDF clock with its protected time exposed */
+struct BdfRun : public Clock_BDF {
+    BdfRun(MAPP* m, int narg, char** arg) : Clock_BDF(m, narg, arg) {}
+    double time() const { return t[0]; }
 };
 
 struct Harness {
@@ -536,6 +544,38 @@ void do_adams(int order, int steps, const std::string& dt, const std::string& pr
     for (char* t : argv) free(t);
 }
 
+/* Clock_BDF (clock_bdf.cpp) "clock bdf steps [key value ...]" run on the
+   scripted DMD system */
+void do_bdf(int steps, const std::string& opts, const std::string& prefix)
+{
+    Atoms* atoms = H.mapp->atoms;
+    ForceField* ff = H.mapp->forcefield;
+    std::vector<std::string> a = {"clock", "bdf", std::to_string(steps)};
+    std::istringstream os(opts);
+    std::string tok;
+    while (os >> tok) a.push_back(tok);
+    std::vector<char*> argv;
+    for (auto& t : a) argv.push_back(strdup(t.c_str()));
+    long n0 = 0, n1 = 0;
+    calc_g_count<ForceField_DMD_I>(ff, &n0) || calc_g_count<ForceField_DMD>(ff, &n0) ||
+        calc_g_count<ForceField_DMD_II>(ff, &n0);
+    BdfRun* ck = new BdfRun(H.mapp, (int)argv.size(), argv.data());
+    ck->init();
+    double t0 = MPI_Wtime();
+    ck->run();
+    double t1 = MPI_Wtime();
+    calc_g_count<ForceField_DMD_I>(ff, &n1) || calc_g_count<ForceField_DMD>(ff, &n1) ||
+        calc_g_count<ForceField_DMD_II>(ff, &n1);
+    write_raw(prefix + ".c.bin", vec<double>("c"), sizeof(double) * (size_t)atoms->natms * H.nt);
+    meta(prefix, "n_calc_g %ld", n1 - n0);
+    meta(prefix, "t %.17g", ck->time());
+    meta(prefix, "natms %d", atoms->natms);
+    meta(prefix, "time_run %.9g", t1 - t0);
+    ck->fin();
+    delete ck;
+    for (char* t : argv) free(t);
+}
+
 /* MD_NH (md_nh.cpp) run on the scripted MD-mode system */
 void do_md(double t_tar, const std::string& period, int no_it, int no_ch, double dt, double boltz, int seed,
            int steps, const std::string& xd_path, const std::string& prefix)
@@ -617,6 +657,13 @@ void run_command(const std::string& line)
         std::string dt, p;
         rs >> order >> n >> dt >> p;
         do_adams(order, n, dt, p);
+    }
+    else if (cmd == "bdf") {
+        int n;
+        std::string p, opts;
+        rs >> n >> p;
+        std::getline(rs, opts);
+        do_bdf(n, opts, p);
     }
     else if (cmd == "md") {
         double T, dt, kb;

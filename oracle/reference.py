@@ -121,6 +121,14 @@ class RefRun:
         self.steps.append(("adams", tag))
         return self.add(f"adams {order} {steps} {dt!r} {self._p(tag)}")
 
+    def bdf(self, steps: int, tag="bdf", **opts):
+        """The reference Clock_BDF "clock bdf steps [key value ...]": init, run,
+        fin (construct with init=False).  Option keys as in the reference's
+        script (gamma_red is spelled red_gamma there)."""
+        self.steps.append(("bdf", tag))
+        kv = " ".join(f"{'red_gamma' if k == 'gamma_red' else k} {v!r}" for k, v in opts.items())
+        return self.add(f"bdf {steps} {self._p(tag)} {kv}")
+
     def md(self, t_tar: float, t_period: float, steps: int, dt: float, boltz: float, xd=None, seed=0,
            eta_iteration=1, eta_chains=3, tag="md"):
         """The reference MD_NH nvt run (construct with init=False): velocities

@@ -79,8 +79,24 @@ def lib():
         L.orc_md_nh.restype = C.c_int
         L.orc_clock_adams.argtypes = [P, C.c_int, C.c_int, C.c_double, dp]
         L.orc_clock_adams.restype = C.c_long
+        L.orc_clock_bdf.argtypes = [P, C.POINTER(BdfOpts), dp, C.POINTER(C.c_long)]
+        L.orc_clock_bdf.restype = C.c_int
         _lib = L
     return _lib
+
+
+class BdfOpts(C.Structure):
+    """orc_bdf_opts: the options of "clock bdf" (clock_bdf.cpp:14-24 defaults)."""
+    _fields_ = [("no_steps", C.c_int), ("max_order", C.c_int), ("max_iter", C.c_int),
+                ("min_gamma", C.c_double), ("gamma_red", C.c_double), ("slope", C.c_double),
+                ("m_tol", C.c_double), ("a_tol", C.c_double), ("e_tol", C.c_double),
+                ("min_del_t", C.c_double), ("max_del_t", C.c_double), ("initial_del_t", C.c_double)]
+
+
+# Clock_BDF's constructor defaults (clock_bdf.cpp:14-24); the script keyword for
+# gamma_red is "red_gamma" (clock_bdf.cpp:46)
+BDF_DEFAULTS = dict(max_order=6, max_iter=50, min_gamma=1.0e-10, gamma_red=0.8, slope=0.4, m_tol=1.0e-10,
+                    a_tol=1.0e-6, e_tol=0.0, min_del_t=1.0e-12, max_del_t=1.0e4, initial_del_t=-1.0)
 
 
 def _numbers(lines):
@@ -313,3 +329,44 @@ class Oracle:
         cc = np.zeros((c + self.counts()["nph"]) * self.nt)
         lib().orc_get_c(self.h, cc)
         return {"c": cc.reshape(-1, self.nt)[:c], "err": err[:steps], "n_calc_g": int(n)}
+
+    def clock_bdf(self, steps, **opts):
+        """Clock_BDF init + run (orc_clock_bdf): returns dict(c, n_calc_g, steps,
+        del_t, order, t) -- per step the size, the order it ran at and the time
+        after it; ``t`` is the final time.  Options as BDF_DEFAULTS."""
+        bad = set(opts) - set(BDF_DEFAULTS)
+        if bad:
+            raise ValueError(f"unknown clock bdf options {sorted(bad)}")
+        p = dict(BDF_DEFAULTS, **opts)
+        # the constructor's checks (clock_bdf.cpp:29-31, 104-134)
+        checks = [(steps <= 0, "no of steps should be greater than zero"),
+                  (p["min_gamma"] <= 0.0, "min_gamma should be larger than zero"),
+                  (not 0.0 < p["gamma_red"] < 1.0, "gamma_red should be between zero and one"),
+                  (not 0.0 < p["slope"] < 1.0, "slope should be between zero and one"),
+                  (p["max_iter"] <= 0, "max_iter should be larger than zero"),
+                  (p["max_order"] <= 0, "max_order should be larger than zero"),
+                  (p["m_tol"] <= 0.0, "m_tol should be larger than zero"),
+                  (p["a_tol"] <= 0.0, "a_tol should be larger than zero"),
+                  (p["e_tol"] < 0.0, "e_tol should be larger than zero"),
+                  (p["min_del_t"] <= 0.0, "min_del_t should be larger than zero"),
+                  (p["max_del_t"] <= 0.0, "max_del_t should be larger than zero"),
+                  (p["min_del_t"] >= p["max_del_t"], "max_del_t should be larger than min_del_t"),
+                  ("initial_del_t" in opts and opts["initial_del_t"] <= 0.0,
+                   "initial_del_t should be larger than zero")]
+        for bad_opt, msg in checks:
+            if bad_opt:
+                raise ValueError(msg)
+        o = BdfOpts(no_steps=steps, **p)
+        hist = np.zeros(3 * max(steps, 1))
+        ncg = C.c_long(0)
+        rc = lib().orc_clock_bdf(self.h, C.byref(o), hist, C.byref(ncg))
+        if rc == -1:
+            raise ValueError("c exceeded the domain")
+        if rc < 0:
+            raise ValueError("orc_clock_bdf rejected the run (not DMD, or a step-size loop that does not end)")
+        c = self.counts()["natms"]
+        cc = np.zeros((c + self.counts()["nph"]) * self.nt)
+        lib().orc_get_c(self.h, cc)
+        h = hist[: 3 * rc].reshape(-1, 3)
+        return {"c": cc.reshape(-1, self.nt)[:c], "n_calc_g": int(ncg.value), "steps": rc, "del_t": h[:, 0],
+                "order": h[:, 1].astype(int), "t": float(h[-1, 2]) if rc else 0.0}
