@@ -871,6 +871,7 @@ extern "C" int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, d
             KCHK(b.interpolate(del_t, ord, &chk));
         }
         KCHK(b.solve(del_t, ord, &cost));
+        double tried = del_t;
         while (b.err >= 1.0 || cost >= 1.0) {
             if (++guard > kMaxRetries) return internal_fail(MG_ERR_DOMAIN, "the step size does not settle");
             err1 = b.err > cost ? b.err : cost;
@@ -885,6 +886,10 @@ extern "C" int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, d
                 del_t *= 0.8;
                 KCHK(b.interpolate(del_t, ord, &chk));
             }
+            // a retry at the step size just tried repeats that solve exactly:
+            // the reference would loop for ever
+            if (del_t == tried) return internal_fail(MG_ERR_DOMAIN, "the step cannot shrink below min_del_t");
+            tried = del_t;
             KCHK(b.solve(del_t, ord, &cost));
         }
         double* tmp_y = b.y[mo - 1];

@@ -2589,7 +2589,8 @@ static void bdf_hi_lo(orc_bdf_t* B, double del_t, int q)
  * per step the step size, the order and the time after it.  Returns the
  * number of steps taken, -1 for c leaving [0, 1] (the reference aborts), -2
  * when a step-size loop of the reference would not end (more than 100000
- * retries).  *n_calc_g counts the calc_g calls.
+ * retries), -3 when a step is retried at the size it just failed at (at
+ * min_del_t), which the reference repeats for ever.  *n_calc_g counts the calc_g calls.
  */
 int orc_clock_bdf(orc_t* o, const orc_bdf_opts* opts, double* hist, long* n_calc_g)
 {
@@ -2651,6 +2652,7 @@ int orc_clock_bdf(orc_t* o, const orc_bdf_opts* opts, double* hist, long* n_calc
         }
         cost = bdf_solve(&B, del_t, ord);
         if (cost < 0.0) { rc = -1; goto out; }
+        double tried = del_t;
         while (B.err >= 1.0 || cost >= 1.0) {
             if (++guard > 100000) { rc = -2; goto out; }
             err1 = MAXV(B.err, cost);
@@ -2666,6 +2668,10 @@ int orc_clock_bdf(orc_t* o, const orc_bdf_opts* opts, double* hist, long* n_calc
                 del_t *= 0.8;
                 chk = bdf_interpolate(&B, del_t, ord);
             }
+            /* a retry at the step size just tried repeats that solve exactly:
+               the reference would loop for ever */
+            if (del_t == tried) { rc = -3; goto out; }
+            tried = del_t;
             cost = bdf_solve(&B, del_t, ord);
             if (cost < 0.0) { rc = -1; goto out; }
         }

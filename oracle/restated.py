@@ -362,6 +362,8 @@ class Oracle:
         rc = lib().orc_clock_bdf(self.h, C.byref(o), hist, C.byref(ncg))
         if rc == -1:
             raise ValueError("c exceeded the domain")
+        if rc == -3:
+            raise ValueError("the step cannot shrink below min_del_t (the reference would retry for ever)")
         if rc < 0:
             raise ValueError("orc_clock_bdf rejected the run (not DMD, or a step-size loop that does not end)")
         c = self.counts()["natms"]

@@ -1,5 +1,6 @@
-"""Device Adams clock (mg_clock_adams) against the restated Clock_Adams,
-itself pinned bit for bit to the reference's clock_adams.cpp.
+"""Device Adams and BDF clocks (mg_clock_adams, mg_clock_bdf) against the
+restated Clock_Adams and Clock_BDF, themselves pinned bit for bit to the
+reference's clock_adams.cpp and clock_bdf.cpp.
 
 The device computes calc_g and the dot products of the conjugate-gradient
 solve with parallel sums, so costs and directions differ from the
@@ -9,6 +10,12 @@ make the same number of calc_g calls.  Bars: equal calc_g counts,
 concentrations within 1e-9 absolute, step costs within 1e-6 relative
 (costs near the 1e-8 convergence threshold carry the rounding of a
 cancellation) or 1e-16 absolute.
+
+The BDF clock's step-size and order decisions are thresholds on error
+estimates computed from the same parallel sums; on these runs they come out
+the same as the oracle's, so the step sizes and orders are compared exactly
+in count and order and within 1e-9 relative in size, the calc_g counts
+exactly, the concentrations within 1e-9 absolute.
 """
 import numpy as np
 import pytest
@@ -97,3 +104,80 @@ def test_clock_adams_errors(tmp_path):
     s.set_form(mb.MG_FORM_FP32)
     with pytest.raises(mb.MGError):
         s.clock_adams(2, 2, 1e-6)
+
+
+def _compare_bdf(r, o):
+    assert r["steps"] == o["steps"]
+    assert np.array_equal(r["order"], o["order"])
+    assert np.all(np.abs(r["del_t"] - o["del_t"]) <= 1e-9 * np.abs(o["del_t"]))
+    assert abs(r["t"] - o["t"]) <= 1e-9 * abs(o["t"])
+    assert r["n_calc_g"] == o["n_calc_g"]
+    assert float(np.max(np.abs(r["c"].ravel() - o["c"].ravel()))) <= 1e-9
+
+
+BDF_CASES = [
+    # style, n, nt, steps, options
+    ("DMD_I", 4, 2, 20, {}),
+    ("DMD_I", 4, 2, 12, dict(max_order=2, max_iter=20)),
+    ("DMD_II", 4, 2, 25, {}),
+    ("DMD_II", 4, 2, 60, dict(a_tol=1e-5)),
+    ("DMD", 4, 2, 25, dict(a_tol=1e-4)),
+    ("DMD_II", 3, 3, 15, dict(initial_del_t=1e-3, m_tol=1e-9, max_del_t=50.0)),
+]
+BDF_IDS = ["dmd-i-default", "dmd-i-o2-it20", "dmd-ii-default", "dmd-ii-atol1e-5-60", "dmd-atol1e-4", "dmd-ii-3sp"]
+
+
+@pytest.mark.parametrize("style,n,nt,steps,opts", BDF_CASES, ids=BDF_IDS)
+def test_clock_bdf_matches_oracle(tmp_path, style, n, nt, steps, opts):
+    mb = _lib_or_skip()
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=n, nt=nt, sigma=0.02, style=style)
+    s = mb.system_from_workload(w)
+    r = s.clock_bdf(steps, **opts)
+    o = Oracle(w).clock_bdf(steps, **opts)
+    _compare_bdf(r, o)
+
+
+def test_clock_bdf_e_tol_stops_early(tmp_path):
+    mb = _lib_or_skip()
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=4, sigma=0.02, style="DMD_II")
+    e_tol = 0.5 / rate_scale(w) * 4.0
+    r = mb.system_from_workload(w).clock_bdf(10, e_tol=e_tol)
+    o = Oracle(w).clock_bdf(10, e_tol=e_tol)
+    assert o["steps"] < 10
+    _compare_bdf(r, o)
+
+
+def test_clock_bdf_full_size_32000_sites(tmp_path):
+    """FCC 20^3 binary DMD_II (32000 sites), 20 steps from the default first
+    step: the order rises to 2 on the way."""
+    mb = _lib_or_skip()
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=20, a=3.58, sigma=0.0, style="DMD_II", seed=4321)
+    r = mb.system_from_workload(w).clock_bdf(20)
+    o = Oracle(w).clock_bdf(20)
+    _compare_bdf(r, o)
+    assert o["order"].max() == 2
+
+
+def test_clock_bdf_errors(tmp_path):
+    mb = _lib_or_skip()
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=3, sigma=0.02)
+    s = mb.system_from_workload(w)
+    with pytest.raises(mb.MGError, match="max_order should be larger than zero"):
+        s.clock_bdf(2, max_order=0)
+    with pytest.raises(mb.MGError, match="no of steps"):
+        s.clock_bdf(0)
+    with pytest.raises(mb.MGError, match="max_del_t should be larger than min_del_t"):
+        s.clock_bdf(2, min_del_t=1.0, max_del_t=0.5)
+    tau = rate_scale(w)
+    with pytest.raises(mb.MGError, match="min_del_t"):
+        s.clock_bdf(5, max_order=2, a_tol=1e-30, initial_del_t=1e-2 * tau, min_del_t=1e-2 * tau,
+                    max_del_t=2e-2 * tau)
+    we = fx.write_workload(str(tmp_path / "e"), "eam", n=3)
+    with pytest.raises(mb.MGError):
+        mb.system_from_workload(we).clock_bdf(2)

@@ -94,3 +94,14 @@ def test_clock_bdf_bad_options(tmp_path, opts, msg):
         ref.run()
     with pytest.raises(ValueError, match=msg):
         Oracle(w).clock_bdf(2, **opts)
+
+
+def test_clock_bdf_stall_at_min_del_t(tmp_path):
+    """A step whose error test fails at min_del_t is retried at the same size
+    for ever by the reference (clock_bdf.cpp:513-540); the restatement stops
+    with an error instead (the reference is not run: it would not end)."""
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=3, sigma=0.02, style="DMD_I")
+    tau = 1.0 / rms_c_d(w)
+    with pytest.raises(ValueError, match="min_del_t"):
+        Oracle(w).clock_bdf(5, max_order=2, a_tol=1e-30, initial_del_t=1e-2 * tau, min_del_t=1e-2 * tau,
+                            max_del_t=2e-2 * tau)
