@@ -366,7 +366,8 @@ def run_batched(mb, fx, device, ncells=512):
 
 def run_large_forms(mb, fx, device, mlp_source):
     """The precision form on FCC 40^3 = 256000 sites (then the 256000-site
-    workflow: 200 CG iterations in the precision form, 10 Adams steps) and the learned form on
+    workflow: 200 CG iterations in the precision form, 10 Adams steps, 100
+    BDF steps of order at most 2) and the learned form on
     FCC 50^3 = 500000 sites (same distributions as the 32000-site system),
     each against the plain FP64 form on the same system: time per force call
     (L2 flushed before each), max|dF|, |dE|/site and, for the precision form,
@@ -447,6 +448,27 @@ def run_large_forms(mb, fx, device, mlp_source):
             out["adams_256000_sites"] = {"order": 2, "steps": 10, "dt": dt, "wall_s": wall,
                                          "ms_per_step": wall * 1e3 / 10, "calc_g_calls": ra["n_calc_g"],
                                          "final_cost_max": float(np.max(ra["err"]))}
+            # 100 BDF steps of order at most 2 from 1e-3 tau on the same
+            # lattice with the DMD_II force field (with DMD_I the reference's
+            # Clock_BDF stalls against the [0, 1] box, see run_bdf)
+            d2 = tempfile.mkdtemp(prefix="mapp_bdf256_")
+            w2 = fx.write_workload(d2, "dmd", n=40, a=WORKLOAD["a"], sigma=0.0, style="DMD_II", seed=4321)
+            s2 = mb.system_from_workload(w2, device=device)
+            s2.create_2nd_neigh_lst()
+            s2.force_calc(1)
+            cd2 = s2.c_d_calc()
+            tau2 = 1.0 / float(np.sqrt(np.mean(cd2 * cd2)))
+            s2.close()
+            s2 = mb.system_from_workload(w2, device=device)
+            t0 = time.perf_counter()
+            rb = s2.clock_bdf(100, max_order=2, initial_del_t=1e-3 * tau2)
+            wall = time.perf_counter() - t0
+            s2.close()
+            out["bdf2_256000_sites"] = {"style": "DMD_II", "steps": rb["steps"], "initial_del_t": 1e-3 * tau2,
+                                        "final_time": rb["t"], "orders_used": np.bincount(rb["order"]).tolist(),
+                                        "wall_s": wall, "ms_per_step": wall * 1e3 / max(rb["steps"], 1),
+                                        "calc_g_calls": rb["n_calc_g"],
+                                        "ms_per_calc_g": wall * 1e3 / max(rb["n_calc_g"], 1)}
         s.close()
     return out
 
@@ -550,6 +572,58 @@ def run_adams(mb, w, device, order=2, steps=20, ref_steps=1):
     return out
 
 
+def run_bdf(mb, fx, device, steps=100, ref_steps=5):
+    """BDF clock (mg_clock_bdf) of the 32000-site binary DMD system with the
+    DMD_II force field: "clock bdf 100 max_order 2 initial_del_t 1e-3 tau"
+    (tau = 1 / rms(c_d) at the start), the reference's own step-size and
+    order control, timed on the host clock around the call (crd list,
+    initial force, every calc_g and the scalar read-backs included).  DMD_II
+    because with DMD_I the reference's own Clock_BDF stops progressing on
+    this lattice: its calc_g never refreshes c_d, so the predictor keeps the
+    initial rates and drives a site against the [0, 1] box, where its retry
+    loop never ends.  Beside it the reference's Clock_BDF for the first
+    ref_steps steps on one core, and ours over the same steps."""
+    d = tempfile.mkdtemp(prefix="mapp_bdf_")
+    w = fx.write_workload(d, "dmd", n=20, a=WORKLOAD["a"], sigma=0.0, style="DMD_II", seed=4321)
+    s = mb.system_from_workload(w, device=device)
+    s.create_2nd_neigh_lst()
+    s.force_calc(1)
+    cd = s.c_d_calc()
+    tau = 1.0 / float(np.sqrt(np.mean(cd * cd)))
+    opts = dict(max_order=2, initial_del_t=1e-3 * tau)
+    s.clock_bdf(3, **opts)  # warm-up
+    s.close()
+    s = mb.system_from_workload(w, device=device)
+    n = s.natms
+    t0 = time.perf_counter()
+    r = s.clock_bdf(steps, **opts)
+    wall = time.perf_counter() - t0
+    s.close()
+    s = mb.system_from_workload(w, device=device)
+    t0 = time.perf_counter()
+    rs = s.clock_bdf(ref_steps, **opts)
+    wall_s = time.perf_counter() - t0
+    s.close()
+    out = {"sites": n, "style": "DMD_II", "max_order": 2, "steps": r["steps"], "initial_del_t": opts["initial_del_t"],
+           "tau": tau, "final_time": r["t"], "orders_used": np.bincount(r["order"]).tolist(), "wall_s": wall,
+           "ms_per_step": wall * 1e3 / max(r["steps"], 1), "calc_g_calls": r["n_calc_g"],
+           "ms_per_calc_g": wall * 1e3 / max(r["n_calc_g"], 1), "site_steps_per_s": n * r["steps"] / wall,
+           "first_steps": {"steps": rs["steps"], "wall_s": wall_s, "calc_g_calls": rs["n_calc_g"]},
+           "timing": "host clock around mg_clock_bdf (crd list, initial force, solves, step control)"}
+    from oracle import reference
+
+    if reference.available():
+        rr = reference.RefRun(w, workdir=tempfile.mkdtemp(prefix="mapp_bdf_ref_"), init=False)
+        rr.bdf(ref_steps, **opts)
+        meta = rr.run(timeout=1800)["bdf"]["meta"]
+        t_ref = float(meta["time_run"])
+        out["cpu_baseline"] = {"value": n * ref_steps / t_ref, "unit": "site-steps/s", "cores": 1, "kind": "reference",
+                               "sample": f"reference Clock_BDF::run, the first {ref_steps} steps of the same run "
+                                         f"({meta['n_calc_g']} calc_g), {t_ref:.2f} s"}
+        out["speedup_vs_reference_core_same_steps"] = t_ref / wall_s
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -619,6 +693,7 @@ def run_ours(args):
         forms["single_lbfgs"] = run_single_lbfgs(mb, w, local)
         forms["md_nh"] = run_md(mb, fx, local)
         forms["clock_adams"] = run_adams(mb, w, local)
+        forms["clock_bdf"] = run_bdf(mb, fx, local)
         forms["large"] = run_large_forms(mb, fx, local, s)
     s.set_form(form_id)
 

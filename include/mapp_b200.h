@@ -385,8 +385,9 @@ void mg_bdf_defaults(mg_bdf_opts* o);
    steps_taken and n_calc_g (may be NULL) the steps run and the calc_g
    evaluations.  Where the reference aborts (c outside [0, 1] after a solve)
    this returns MG_ERR_DOMAIN, as it does where the reference's unbounded
-   step-size retry loops would not end: a retry at the size just tried (at
-   min_del_t) or 100000 retries.  The error estimate
+   step-size retry loops would not end: a predictor outside [0, 1] at
+   min_del_t, a retry at the size just tried (at min_del_t), or 100000
+   retries.  The error estimate
    reads a local time the reference never sets (clock_bdf.cpp:838-854); the
    reference built with gcc -O2 evaluates it as 0.0 and so does this. */
 int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, double* hist, int* steps_taken,

@@ -866,6 +866,10 @@ extern "C" int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, d
         KCHK(b.interpolate(del_t, ord, &chk));
         while (chk == -1) {
             if (++guard > kMaxRetries) return internal_fail(MG_ERR_DOMAIN, "the predictor stays outside [0, 1]");
+            // at min_del_t the clamped retry repeats the same interpolation:
+            // the reference would loop for ever
+            if (del_t == o.min_del_t)
+                return internal_fail(MG_ERR_DOMAIN, "the predictor leaves [0, 1] even at min_del_t");
             del_t *= 0.8;
             del_t = del_t > o.min_del_t ? del_t : o.min_del_t;
             KCHK(b.interpolate(del_t, ord, &chk));

@@ -2590,7 +2590,9 @@ static void bdf_hi_lo(orc_bdf_t* B, double del_t, int q)
  * number of steps taken, -1 for c leaving [0, 1] (the reference aborts), -2
  * when a step-size loop of the reference would not end (more than 100000
  * retries), -3 when a step is retried at the size it just failed at (at
- * min_del_t), which the reference repeats for ever.  *n_calc_g counts the calc_g calls.
+ * min_del_t), which the reference repeats for ever, -4 when the predictor
+ * leaves [0, 1] even at min_del_t, where the reference's clamped retry loop
+ * (clock_bdf.cpp:504-510) never ends.  *n_calc_g counts the calc_g calls.
  */
 int orc_clock_bdf(orc_t* o, const orc_bdf_opts* opts, double* hist, long* n_calc_g)
 {
@@ -2646,6 +2648,9 @@ int orc_clock_bdf(orc_t* o, const orc_bdf_opts* opts, double* hist, long* n_calc
         chk = bdf_interpolate(&B, del_t, ord);
         while (chk == -1) {
             if (++guard > 100000) { rc = -2; goto out; }
+            /* at min_del_t the clamped retry repeats the same interpolation:
+               the reference would loop for ever */
+            if (del_t == opts->min_del_t) { rc = -4; goto out; }
             del_t *= 0.8;
             del_t = MAXV(del_t, opts->min_del_t);
             chk = bdf_interpolate(&B, del_t, ord);

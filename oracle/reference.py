@@ -126,7 +126,10 @@ class RefRun:
         fin (construct with init=False).  Option keys as in the reference's
         script (gamma_red is spelled red_gamma there)."""
         self.steps.append(("bdf", tag))
-        kv = " ".join(f"{'red_gamma' if k == 'gamma_red' else k} {v!r}" for k, v in opts.items())
+        def text(v):
+            return str(int(v)) if isinstance(v, (int, np.integer)) else repr(float(v))
+
+        kv = " ".join(f"{'red_gamma' if k == 'gamma_red' else k} {text(v)}" for k, v in opts.items())
         return self.add(f"bdf {steps} {self._p(tag)} {kv}")
 
     def md(self, t_tar: float, t_period: float, steps: int, dt: float, boltz: float, xd=None, seed=0,

@@ -362,6 +362,8 @@ class Oracle:
         rc = lib().orc_clock_bdf(self.h, C.byref(o), hist, C.byref(ncg))
         if rc == -1:
             raise ValueError("c exceeded the domain")
+        if rc == -4:
+            raise ValueError("the predictor leaves [0, 1] even at min_del_t (the reference would retry for ever)")
         if rc == -3:
             raise ValueError("the step cannot shrink below min_del_t (the reference would retry for ever)")
         if rc < 0:

@@ -181,3 +181,14 @@ def test_clock_bdf_errors(tmp_path):
     we = fx.write_workload(str(tmp_path / "e"), "eam", n=3)
     with pytest.raises(mb.MGError):
         mb.system_from_workload(we).clock_bdf(2)
+
+
+def test_clock_bdf_predictor_stall(tmp_path):
+    """Where the reference's predictor retry loop would never end (DMD_I on
+    an undisplaced lattice, see the oracle's test) the device clock stops
+    with MG_ERR_DOMAIN."""
+    mb = _lib_or_skip()
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=4, a=3.58, sigma=0.0, style="DMD_I", seed=4321)
+    tau = rate_scale(w)
+    with pytest.raises(mb.MGError, match="even at min_del_t"):
+        mb.system_from_workload(w).clock_bdf(100, max_order=2, initial_del_t=1e-3 * tau)

@@ -105,3 +105,16 @@ def test_clock_bdf_stall_at_min_del_t(tmp_path):
     with pytest.raises(ValueError, match="min_del_t"):
         Oracle(w).clock_bdf(5, max_order=2, a_tol=1e-30, initial_del_t=1e-2 * tau, min_del_t=1e-2 * tau,
                             max_del_t=2e-2 * tau)
+
+
+def test_clock_bdf_predictor_stall(tmp_path):
+    """DMD_I's calc_g never refreshes c_d (ff_dmd_I.cpp:2402-2674), so
+    Clock_BDF keeps predicting with the initial rates (clock_bdf.cpp:565) and
+    on this undisplaced lattice drives a site against the [0, 1] box; the
+    reference's clamped retry loop (clock_bdf.cpp:504-510) then repeats at
+    min_del_t for ever (the compiled reference was seen still running after
+    120 s).  The restatement stops with an error at that point."""
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=4, a=3.58, sigma=0.0, style="DMD_I", seed=4321)
+    tau = 1.0 / rms_c_d(w)
+    with pytest.raises(ValueError, match="even at min_del_t"):
+        Oracle(w).clock_bdf(100, max_order=2, initial_del_t=1e-3 * tau)
