@@ -184,11 +184,17 @@ def test_clock_bdf_errors(tmp_path):
 
 
 def test_clock_bdf_predictor_stall(tmp_path):
-    """Where the reference's predictor retry loop would never end (DMD_I on
-    an undisplaced lattice, see the oracle's test) the device clock stops
-    with MG_ERR_DOMAIN."""
+    """Where the reference's clamped predictor retry loop would never end (the
+    predictor leaves [0, 1] even at min_del_t) the device clock stops with
+    MG_ERR_DOMAIN, as the oracle does: here the first step may not be
+    shorter than 10 tau, which carries most sites out of the box."""
     mb = _lib_or_skip()
-    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=4, a=3.58, sigma=0.0, style="DMD_I", seed=4321)
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=4, sigma=0.02, style="DMD_I")
     tau = rate_scale(w)
+    opts = dict(max_order=2, initial_del_t=10.0 * tau, min_del_t=10.0 * tau, max_del_t=20.0 * tau)
+    with pytest.raises(ValueError, match="even at min_del_t"):
+        Oracle(w).clock_bdf(5, **opts)
     with pytest.raises(mb.MGError, match="even at min_del_t"):
-        mb.system_from_workload(w).clock_bdf(100, max_order=2, initial_del_t=1e-3 * tau)
+        mb.system_from_workload(w).clock_bdf(5, **opts)
