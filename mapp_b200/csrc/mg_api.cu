@@ -760,9 +760,17 @@ int timed_begin(mg_system* s)
     return MG_OK;
 }
 
-int timed_end(mg_system* s, double* slot)
+// marks the end of the timed work; the caller reads the time with
+// timed_read after its own stream synchronisation, so that the result copies
+// queue behind the kernels without a host round trip between them
+int timed_end(mg_system* s)
 {
     CU(cudaEventRecord(s->ev1, s->st));
+    return MG_OK;
+}
+
+int timed_read(mg_system* s, double* slot)
+{
     CU(cudaEventSynchronize(s->ev1));
     float ms = 0;
     cudaEventElapsedTime(&ms, s->ev0, s->ev1);
@@ -1103,12 +1111,14 @@ int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
     CU(launch_skin_check(d, s->skin * s->skin, d.status + 5, s->st));
     int flag = 0;
     CU(cudaMemcpyAsync(&flag, d.status + 5, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    // the ghost refresh is queued before the flag is known: it only writes
+    // the ghost slots, which a rebuild recreates anyway, and in the usual
+    // no-rebuild case it runs while the host waits for the flag
+    CU(launch_refresh_x(d, s->st));
     CU(cudaStreamSynchronize(s->st));
     if (flag) {
         CU(launch_x2s(d, s->st));
         CHK(rebuild(s));
-    } else {
-        CU(launch_refresh_x(d, s->st));
     }
     if (rebuilt) *rebuilt = flag;
     return MG_OK;
@@ -1189,16 +1199,17 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     }
     double tot[8] = {0};
     CU(launch_reduce_partials(d, rows, 7, s->red_out, s->st));
-    CHK(timed_end(s, &s->t_force));
+    CHK(timed_end(s));
+    CU(cudaMemcpyAsync(tot, s->red_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CHK(copy_out(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
+    CU(cudaStreamSynchronize(s->st));
+    CHK(timed_read(s, &s->t_force));
     if (s->dmd)
         for (int k = 0; k < 3; k++) {
             float ms = 0;
             cudaEventElapsedTime(&ms, s->evk[k], s->evk[k + 1]);
             s->t_k[k] = ms;
         }
-    CU(cudaMemcpyAsync(tot, s->red_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
-    CHK(copy_out(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
-    CU(cudaStreamSynchronize(s->st));
     if (en_st) {
         if (st_clc)
             for (int i = 0; i < 7; i++) en_st[i] = tot[i];
@@ -1228,9 +1239,10 @@ int mg_ff_energy_calc(mg_system* s, double* energy)
     }
     double tot[8] = {0};
     CU(launch_reduce_partials(d, rows, 1, s->red_out, s->st));
-    CHK(timed_end(s, &s->t_energy));
+    CHK(timed_end(s));
     CU(cudaMemcpyAsync(tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
+    CHK(timed_read(s, &s->t_energy));
     if (energy) *energy = tot[0];
     return MG_OK;
 }
@@ -1276,9 +1288,10 @@ int mg_ff_c_d_calc(mg_system* s, double* c_d)
     CU(cudaMemsetAsync(d.E, 0, bytes, s->st));
     CU(cudaMemsetAsync(d.c_d, 0, bytes, s->st));
     CU(launch_dmd_cdot(d, s->st));
-    CHK(timed_end(s, &s->t_cd));
+    CHK(timed_end(s));
     CHK(copy_out(s, c_d, d.c_d, bytes));
     CU(cudaStreamSynchronize(s->st));
+    CHK(timed_read(s, &s->t_cd));
     return MG_OK;
 }
 
@@ -1303,11 +1316,12 @@ int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g
     int rows = 0;
     CU(launch_dmd_calc_g(d, chk, alpha, &rows, s->st));
     CU(launch_reduce_partials(d, rows, 1, s->red_out, s->st));
-    CHK(timed_end(s, &s->t_g));
+    CHK(timed_end(s));
     double tot[2] = {0, 0};
     CU(cudaMemcpyAsync(tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CHK(copy_out(s, g, d.g, bytes));
     CU(cudaStreamSynchronize(s->st));
+    CHK(timed_read(s, &s->t_g));
     if (cost) *cost = tot[0] * 0.25;
     return MG_OK;
 }
