@@ -607,6 +607,113 @@ int read_tables(mg_system* s, const char* path, bool fs_layout)
     return MG_OK;
 }
 
+// the 4-point Lagrange interpolation of ForceField_eam::set_funcfl
+// (ff_eam.cpp:565-580); tab[0] = 0 and the value at grid index m is tab[m + 1]
+double lagrange4(const std::vector<double>& tab, int n_src, double d_src, double x)
+{
+    const double sixth = 1.0 / 6.0;
+    double p = x / d_src + 1.0;
+    int k = static_cast<int>(p);
+    k = k < n_src - 2 ? k : n_src - 2;
+    k = k > 2 ? k : 2;
+    p -= k;
+    p = p < 2.0 ? p : 2.0;
+    double c1 = -sixth * p * (p - 1.0) * (p - 2.0);
+    double c2 = 0.5 * (p * p - 1.0) * (p - 2.0);
+    double c3 = -0.5 * p * (p + 1.0) * (p - 2.0);
+    double c4 = sixth * p * (p * p - 1.0);
+    return c1 * tab[k - 1] + c2 * tab[k] + c3 * tab[k + 1] + c4 * tab[k + 2];
+}
+
+// funcfl files, one per type (ForceField_eam::set_funcfl, ff_eam.cpp:433-670):
+// a comment line, "Z mass a lattice", "nrho drho nr dr cut", then F, Z(r) and
+// rho(r).  The tables are regridded onto nr = int(max_r / max_dr + 0.5) points
+// of max_dr; nrho comes from the same r expression (ff_eam.cpp:547-548); the
+// pair term is 27.2 * 0.529 * Z_i Z_j.  For more than one type the reference
+// writes type i's density to slot i*(i+1) (ff_eam.cpp:583), which it never
+// allocated; here every slot b*nt+a holds type a's density, as for setfl.
+int read_funcfl(mg_system* s, int nfiles, const char* const* files)
+{
+    const int nt = s->nt;
+    if (nfiles != nt) return fail(MG_ERR_ARG, "no of types and number of files should be equal in eam");
+    std::vector<int> nrs(nt), nrhos(nt);
+    std::vector<double> drs(nt), drhos(nt);
+    std::vector<std::vector<double>> tF(nt), tZ(nt), tR(nt);
+    for (int t = 0; t < nt; t++) {
+        std::vector<std::string> lines;
+        CHK(read_all(files[t], lines));
+        if (lines.size() < 3) return fail(MG_ERR_FORMAT, "eam potential file ended immaturely");
+        std::vector<std::string> h = tokens(lines[2]);
+        if (h.size() != 5) return fail(MG_ERR_FORMAT, "wrong line in eam file: %s", lines[2].c_str());
+        nrhos[t] = atoi(h[0].c_str());
+        drhos[t] = atof(h[1].c_str());
+        nrs[t] = atoi(h[2].c_str());
+        drs[t] = atof(h[3].c_str());
+        if (nrs[t] < 5 || nrhos[t] < 5 || !(drs[t] > 0.0) || !(drhos[t] > 0.0))
+            return fail(MG_ERR_FORMAT, "table sizes too small (nr=%d nrho=%d)", nrs[t], nrhos[t]);
+        const size_t tot = (size_t)nrhos[t] + 2 * (size_t)nrs[t];
+        std::vector<double> v;
+        v.reserve(tot);
+        for (size_t li = 3; li < lines.size() && v.size() < tot; li++) {
+            std::vector<std::string> tk = tokens(lines[li]);
+            if (v.size() + tk.size() > tot) return fail(MG_ERR_FORMAT, "eam potential file ended immaturely");
+            for (const std::string& x : tk) v.push_back(atof(x.c_str()));
+        }
+        if (v.size() < tot) return fail(MG_ERR_FORMAT, "eam potential file ended immaturely");
+        tF[t].assign(1, 0.0);
+        tF[t].insert(tF[t].end(), v.begin(), v.begin() + nrhos[t]);
+        tZ[t].assign(1, 0.0);
+        tZ[t].insert(tZ[t].end(), v.begin() + nrhos[t], v.begin() + nrhos[t] + nrs[t]);
+        tR[t].assign(1, 0.0);
+        tR[t].insert(tR[t].end(), v.begin() + nrhos[t] + nrs[t], v.end());
+    }
+    double maxr = 0.0, maxrho = 0.0, maxdr = 0.0, maxdrho = 0.0;
+    for (int t = 0; t < nt; t++) {
+        double r = static_cast<double>(nrs[t] - 1) * drs[t], rh = static_cast<double>(nrhos[t] - 1) * drhos[t];
+        maxr = maxr > r ? maxr : r;
+        maxrho = maxrho > rh ? maxrho : rh;
+        maxdr = maxdr > drs[t] ? maxdr : drs[t];
+        maxdrho = maxdrho > drhos[t] ? maxdrho : drhos[t];
+    }
+    const int nr = static_cast<int>(maxr / maxdr + 0.5), nrho = static_cast<int>(maxr / maxdr + 0.5);
+    const double dr = maxdr, drho = maxdrho;
+    if (nr < 5 || nrho < 5) return fail(MG_ERR_FORMAT, "table sizes too small (nr=%d nrho=%d)", nr, nrho);
+    s->nr = nr;
+    s->nrho = nrho;
+    s->dr = dr;
+    s->drho = drho;
+    s->Fw = 7;
+    const int ncomp = nt * (nt + 1) / 2;
+    s->FT.assign((size_t)nt * (nrho + 1) * s->Fw, 0.0);
+    s->rhoT.assign((size_t)nt * nt * nr * 8, 0.0);
+    s->phiT.assign((size_t)ncomp * nr * 8, 0.0);
+    for (int a = 0; a < nt; a++) {
+        double* Fd = s->FT.data() + (size_t)a * (nrho + 1) * s->Fw;
+        for (int j = 0; j < nrho; j++) Fd[(size_t)j * s->Fw] = lagrange4(tF[a], nrhos[a], drhos[a], static_cast<double>(j) * drho);
+        spline7(nrho, drho, Fd, s->Fw);
+    }
+    for (int a = 0; a < nt; a++) {
+        std::vector<double> col(nr);
+        for (int j = 0; j < nr; j++) col[j] = lagrange4(tR[a], nrs[a], drs[a], static_cast<double>(j) * dr);
+        for (int b = 0; b < nt; b++) {
+            double* dst = s->rhoT.data() + (size_t)(b * nt + a) * nr * 8;
+            for (int j = 0; j < nr; j++) dst[(size_t)j * 8] = col[j];
+            spline7(nr, dr, dst, 8);
+        }
+    }
+    for (int a = 0; a < nt; a++)
+        for (int b = a; b < nt; b++) {
+            double* dst = s->phiT.data() + (size_t)comp_idx(a, b) * nr * 8;
+            for (int j = 0; j < nr; j++) {
+                double r = static_cast<double>(j) * dr;
+                double t0 = lagrange4(tZ[a], nrs[a], drs[a], r), t1 = lagrange4(tZ[b], nrs[b], drs[b], r);
+                dst[(size_t)j * 8] = 27.2 * 0.529 * t0 * t1;
+            }
+            spline7(nr, dr, dst, 8);
+        }
+    return MG_OK;
+}
+
 // analytic FS coefficient file (ff_fs.cpp:113-335)
 int read_fs_coeffs(mg_system* s, const char* path)
 {
@@ -1003,7 +1110,7 @@ int mg_ff_coef(mg_system* s, int narg, const char* const* arg)
             if (narg != 3) return fail(MG_ERR_ARG, "one file is needed for eam");
             CHK(read_tables(s, arg[2], false));
         } else if (!strcmp(arg[1], "FuncFL")) {
-            return fail(MG_ERR_UNSUPPORTED, "FuncFL tables are not supported; convert to SetFL");
+            CHK(read_funcfl(s, narg - 2, arg + 2));
         } else
             return fail(MG_ERR_ARG, "wrong coeff command for eam Force Field");
         // ff_eam.cpp:424-425

@@ -169,6 +169,36 @@ def write_fs(path: str, t: EamTables):
             _write_values(fp, row)
 
 
+# funcfl grid: deliberately not the setfl one, so that the reference's
+# regridding onto nr - 1 points (and nrho taken from the r grid) is exercised
+FUNCFL_NR = 2500
+FUNCFL_NRHO = 2000
+FUNCFL_RHO_MAX = 40.0
+ZCONST = 27.2 * 0.529  # eV A: r*phi = ZCONST * Z_i(r) Z_j(r) in the funcfl convention
+
+
+def write_funcfl(path: str, sp: "Species", nr=FUNCFL_NR, nrho=FUNCFL_NRHO, rho_max=FUNCFL_RHO_MAX):
+    """One single-element funcfl file: a comment line; "Z mass a lattice";
+    "nrho drho nr dr cut"; then F(rho) on nrho points, the effective charge
+    Z(r) and rho(r) on nr points.  Z(r) = sqrt(r phi(r) / ZCONST), so that the
+    pair term the reader forms, ZCONST Z_i Z_j, is r*phi for like pairs (phi
+    is positive for these species)."""
+    dr = R_CUT / (nr - 1)
+    drho = rho_max / (nrho - 1)
+    r = np.arange(nr, dtype=np.float64) * dr
+    rh = np.arange(nrho, dtype=np.float64) * drho
+    F = -sp.f0 * np.sqrt(rh)
+    z = np.sqrt(np.maximum(r * pair_phi(r, sp.phi0, sp.re, sp.beta_phi), 0.0) / ZCONST)
+    rho = pair_rho(r, sp.re, sp.beta_rho)
+    with open(path, "w") as fp:
+        fp.write("# synthetic funcfl table for species %s generated by mapp_b200.fixtures\n" % sp.name)
+        fp.write("29 %.17g 3.615 fcc\n" % sp.mass)
+        fp.write("%d %.17g %d %.17g %.17g\n" % (nrho, drho, nr, dr, R_CUT))
+        _write_values(fp, F)
+        _write_values(fp, z)
+        _write_values(fp, rho)
+
+
 @dataclass
 class FsCoeffs:
     """Analytic Finnis-Sinclair coefficients (ff_fs.cpp:14-21 functional form)."""
@@ -433,10 +463,19 @@ def write_workload(dirpath: str, kind: str, **kw) -> dict:
         nt = kw.pop("nt", 1)
         fmt = kw.pop("fmt", "SetFL")
         cfg = make_md_config(nt=nt, **kw)
-        tables = make_tables((SPECIES_A, SPECIES_B)[:nt])
-        pot = os.path.join(dirpath, "pot.eam")
-        (write_fs if fmt == "FS" else write_setfl)(pot, tables)
-        out["coef"] = ["ff_coef", fmt, pot]
+        if fmt == "FuncFL":
+            # one single-element file per species
+            pots = []
+            for sp in (SPECIES_A, SPECIES_B)[:nt]:
+                pots.append(os.path.join(dirpath, f"pot_{sp.name}.funcfl"))
+                write_funcfl(pots[-1], sp)
+            pot = pots[0]
+            out["coef"] = ["ff_coef", fmt] + pots
+        else:
+            tables = make_tables((SPECIES_A, SPECIES_B)[:nt])
+            pot = os.path.join(dirpath, "pot.eam")
+            (write_fs if fmt == "FS" else write_setfl)(pot, tables)
+            out["coef"] = ["ff_coef", fmt, pot]
         out["style"] = "EAM"
     elif kind == "fs":
         nt = kw.pop("nt", 1)

@@ -130,6 +130,90 @@ def read_eam_file(path, nt, fs_mode):
     return dict(nr=nr, dr=dr, nrho=nrho, drho=drho, F=F, rho=rho, rphi=rphi)
 
 
+def _lagrange4(tab, n_src, d_src, x):
+    """The 4-point Lagrange interpolation of ForceField_eam::set_funcfl
+    (ff_eam.cpp:565-580): tab holds a leading 0 then the n_src file values,
+    the value at grid index m sits at tab[m + 1]."""
+    sixth = 1.0 / 6.0
+    p = x / d_src + 1.0
+    k = int(p)
+    k = min(k, n_src - 2)
+    k = max(k, 2)
+    p -= k
+    p = min(p, 2.0)
+    c1 = -sixth * p * (p - 1.0) * (p - 2.0)
+    c2 = 0.5 * (p * p - 1.0) * (p - 2.0)
+    c3 = -0.5 * p * (p + 1.0) * (p - 2.0)
+    c4 = sixth * p * (p * p - 1.0)
+    return c1 * tab[k - 1] + c2 * tab[k] + c3 * tab[k + 1] + c4 * tab[k + 2]
+
+
+def read_funcfl_files(paths, nt):
+    """ForceField_eam::set_funcfl (ff_eam.cpp:433-670): one single-element
+    file per type; the tables are regridded onto nr = int(max_r / max_dr +
+    0.5) points of max_dr, and nrho is taken from the same r expression
+    (ff_eam.cpp:547-548, so the F grid has nr points too); the pair term is
+    27.2 * 0.529 * Z_i Z_j.  Returns the setfl-layout columns (F [nt][nrho],
+    rho [nt][nr], r*phi [nt(nt+1)/2][nr]) that the interpolation
+    (ForceField_eam::interpolate) then works on.  For more than one type the
+    reference stores type i's density in slot i*(i+1) (ff_eam.cpp:583), a slot
+    it never allocated; here it is type i's own density, as for setfl."""
+    if len(paths) != nt:
+        raise ValueError("no of types and number of files should be equal in eam")
+    hdr, F0, Z0, R0 = [], [], [], []
+    for path in paths:
+        with open(path) as fp:
+            lines = fp.readlines()
+        if len(lines) < 3:
+            raise ValueError("eam potential file ended immaturely")
+        h = lines[2].split("#")[0].split()
+        if len(h) != 5:
+            raise ValueError("wrong line in eam file")
+        nrho, drho, nr, dr = int(h[0]), float(h[1]), int(h[2]), float(h[3])
+        tot = nrho + 2 * nr
+        v = []
+        for ln in lines[3:]:
+            t = ln.split("#")[0].split()
+            if len(v) + len(t) > tot:
+                raise ValueError("eam potential file ended immaturely")
+            v.extend(float(x) for x in t)
+            if len(v) == tot:
+                break
+        if len(v) < tot:
+            raise ValueError("eam potential file ended immaturely")
+        hdr.append((nrho, drho, nr, dr))
+        F0.append([0.0] + v[:nrho])
+        Z0.append([0.0] + v[nrho:nrho + nr])
+        R0.append([0.0] + v[nrho + nr:])
+    maxr = maxrho = maxdr = maxdrho = 0.0
+    for nrho, drho, nr, dr in hdr:
+        maxr = max(maxr, (nr - 1) * dr)
+        maxrho = max(maxrho, (nrho - 1) * drho)
+        maxdr = max(maxdr, dr)
+        maxdrho = max(maxdrho, drho)
+    nr = int(maxr / maxdr + 0.5)
+    nrho = int(maxr / maxdr + 0.5)
+    dr, drho = maxdr, maxdrho
+    F = np.zeros((nt, nrho))
+    rho = np.zeros((nt, nr))
+    ncomp = nt * (nt + 1) // 2
+    rphi = np.zeros((ncomp, nr))
+    for i in range(nt):
+        for j in range(nrho):
+            F[i, j] = _lagrange4(F0[i], hdr[i][0], hdr[i][1], float(j) * drho)
+        for j in range(nr):
+            rho[i, j] = _lagrange4(R0[i], hdr[i][2], hdr[i][3], float(j) * dr)
+    for i in range(nt):
+        for j in range(i, nt):
+            row = j * (j + 1) // 2 + i
+            for m in range(nr):
+                r = float(m) * dr
+                t0 = _lagrange4(Z0[i], hdr[i][2], hdr[i][3], r)
+                t1 = _lagrange4(Z0[j], hdr[j][2], hdr[j][3], r)
+                rphi[row, m] = 27.2 * 0.529 * t0 * t1
+    return dict(nr=nr, dr=dr, nrho=nrho, drho=drho, F=F, rho=rho, rphi=rphi)
+
+
 def read_fs_coeffs(path, nt):
     rows = []
     with open(path) as fp:
@@ -169,7 +253,10 @@ class Oracle:
         self.h = L.orc_new(STYLES[self.style], self.nt)
         coef = workload["coef"]
         if self.style == "EAM":
-            t = read_eam_file(coef[2], self.nt, coef[1] == "FS")
+            if coef[1] == "FuncFL":
+                t = read_funcfl_files(coef[2:], self.nt)
+            else:
+                t = read_eam_file(coef[2], self.nt, coef[1] == "FS")
             L.orc_set_tables(self.h, t["nr"], t["dr"], t["nrho"], t["drho"], int(coef[1] == "FS"),
                              np.ascontiguousarray(t["F"]), np.ascontiguousarray(t["rho"]), np.ascontiguousarray(t["rphi"]))
         elif self.style == "FS":

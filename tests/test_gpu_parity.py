@@ -85,6 +85,8 @@ CASES = [
     ("eam", dict(n=4)),
     ("eam", dict(n=10)),
     ("eam", dict(n=5, nt=2, fmt="FS")),
+    ("eam", dict(n=5, fmt="FuncFL")),
+    ("eam", dict(n=4, nt=2, fmt="FuncFL")),
     ("fs", dict(n=4, nt=2)),
     ("fs", dict(n=6)),
     ("dmd", dict(n=4, sigma=0.02, style="DMD_I")),

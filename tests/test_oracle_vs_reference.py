@@ -18,6 +18,7 @@ pytestmark = pytest.mark.skipif(not reference.available(), reason="reference har
 CASES = [
     ("eam", dict(n=4)),
     ("eam", dict(n=4, nt=2, fmt="FS")),
+    ("eam", dict(n=4, fmt="FuncFL")),
     ("fs", dict(n=4, nt=2)),
     ("dmd", dict(n=4, sigma=0.02, style="DMD_I")),
     ("dmd", dict(n=4, sigma=0.02, style="DMD_II")),
