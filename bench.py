@@ -52,6 +52,8 @@ def parse():
                    help="form of the timed force_calc steps (fp32 / mlp imply --skip-forms; for profiling)")
     p.add_argument("--eam-cells", type=int, default=0,
                    help="instead: time EAM force_calc (the MD crystal's potential) on FCC n^3 atoms (profiling)")
+    p.add_argument("--clock", default="", choices=["", "adams", "bdf"],
+                   help="instead: run only the 32000-site Adams or BDF clock line, without the CPU reference (profiling)")
     return p.parse_args()
 
 
@@ -554,7 +556,7 @@ def run_md(mb, fx, device, steps=1000, ref_steps=300):
     return out
 
 
-def run_adams(mb, w, device, order=2, steps=20, ref_steps=1):
+def run_adams(mb, w, device, order=2, steps=20, ref_steps=1, with_reference=True):
     """Adams clock of the 32000-site DMD_I system (mg_clock_adams): order 2,
     dt = 1e-3 tau with tau = 1 / rms(c_d) at the start, 20 steps, timed on the
     host clock around the call (crd list, initial force, every calc_g / c_d
@@ -581,7 +583,7 @@ def run_adams(mb, w, device, order=2, steps=20, ref_steps=1):
     s.close()
     from oracle import reference
 
-    if reference.available():
+    if with_reference and reference.available():
         rr = reference.RefRun(w, workdir=tempfile.mkdtemp(prefix="mapp_adams_"), init=False)
         rr.adams(order, ref_steps, dt)
         meta = rr.run(timeout=1800)["adams"]["meta"]
@@ -593,7 +595,7 @@ def run_adams(mb, w, device, order=2, steps=20, ref_steps=1):
     return out
 
 
-def run_bdf(mb, fx, device, steps=100, ref_steps=5):
+def run_bdf(mb, fx, device, steps=100, ref_steps=5, with_reference=True):
     """BDF clock (mg_clock_bdf) of the 32000-site binary DMD system with the
     DMD_II force field: "clock bdf 100 max_order 2 initial_del_t 1e-3 tau"
     (tau = 1 / rms(c_d) at the start), the reference's own step-size and
@@ -633,7 +635,7 @@ def run_bdf(mb, fx, device, steps=100, ref_steps=5):
            "timing": "host clock around mg_clock_bdf (crd list, initial force, solves, step control)"}
     from oracle import reference
 
-    if reference.available():
+    if with_reference and reference.available():
         rr = reference.RefRun(w, workdir=tempfile.mkdtemp(prefix="mapp_bdf_ref_"), init=False)
         rr.bdf(ref_steps, **opts)
         meta = rr.run(timeout=1800)["bdf"]["meta"]
@@ -857,6 +859,21 @@ def main():
         return run_reference(args)
     if args.eam_cells > 0:
         return run_eam(args)
+    if args.clock:
+        import torch
+
+        import mapp_b200 as mb
+        from mapp_b200 import fixtures as fx
+
+        torch.cuda.set_device(0)
+        if args.clock == "bdf":
+            out = run_bdf(mb, fx, 0, with_reference=False)
+        else:
+            w = fx.write_workload(tempfile.mkdtemp(prefix="mapp_adams_w_"), "dmd", n=WORKLOAD["n"], a=WORKLOAD["a"],
+                                  sigma=WORKLOAD["sigma"], style="DMD_I", seed=4321)
+            out = run_adams(mb, w, 0, with_reference=False)
+        print(json.dumps({"clock": args.clock, **out}))
+        return 0
     return run_ours(args)
 
 

@@ -1,5 +1,6 @@
-// Adams clock on the device: Clock_Adams (clock_adams.cpp) for a DMD system,
-// with every concentration-sized vector resident in HBM.
+// Adams and BDF clocks on the device: Clock_Adams (clock_adams.cpp) and
+// Clock_BDF (clock_bdf.cpp) for a DMD system, with every concentration-sized
+// vector resident in HBM.
 //
 // The reference keeps a, g, g0, c0, h and the c_d history on the host and
 // loops over them between calc_g calls, which in a GPU build would move every
@@ -49,9 +50,10 @@ struct CkView {
 };
 
 // Block reduction of NV values, then the fixed-order reduction of all block
-// rows by the last block; MIN selects minima instead of sums.  Returns true
-// in the last block, where tot holds the result in every thread.
-template <int NV, bool MIN>
+// rows by the last block; bit k of MINMASK selects the minimum instead of the
+// sum for value k.  Returns true in the last block, where tot holds the
+// results in every thread.
+template <int NV, unsigned MINMASK>
 __device__ bool reduce_last(double (&v)[NV], const CkView& V, double (&tot)[NV])
 {
     __shared__ double sh[kCkBlock / 32][NV];
@@ -59,17 +61,19 @@ __device__ bool reduce_last(double (&v)[NV], const CkView& V, double (&tot)[NV])
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < NV; k++) {
+        const bool mn = (MINMASK >> k) & 1u;
         double a = v[k];
         for (int o = 16; o > 0; o >>= 1) {
             double b = __shfl_down_sync(0xffffffffu, a, o);
-            a = MIN ? fmin(a, b) : a + b;
+            a = mn ? fmin(a, b) : a + b;
         }
         if (lane == 0) sh[w][k] = a;
     }
     __syncthreads();
     if (threadIdx.x < NV) {
+        const bool mn = (MINMASK >> threadIdx.x) & 1u;
         double a = sh[0][threadIdx.x];
-        for (int j = 1; j < kCkBlock / 32; j++) a = MIN ? fmin(a, sh[j][threadIdx.x]) : a + sh[j][threadIdx.x];
+        for (int j = 1; j < kCkBlock / 32; j++) a = mn ? fmin(a, sh[j][threadIdx.x]) : a + sh[j][threadIdx.x];
         V.part[(size_t)blockIdx.x * 8 + threadIdx.x] = a;
     }
     __threadfence();
@@ -80,22 +84,24 @@ __device__ bool reduce_last(double (&v)[NV], const CkView& V, double (&tot)[NV])
     __threadfence();
 #pragma unroll
     for (int k = 0; k < NV; k++) {
-        double a = MIN ? 1.0 : 0.0;
+        const bool mn = (MINMASK >> k) & 1u;
+        double a = mn ? 1.0 : 0.0;
         for (int b = threadIdx.x; b < V.nblocks; b += kCkBlock) {
             double x = __ldcg(V.part + (size_t)b * 8 + k);
-            a = MIN ? fmin(a, x) : a + x;
+            a = mn ? fmin(a, x) : a + x;
         }
         for (int o = 16; o > 0; o >>= 1) {
             double b = __shfl_down_sync(0xffffffffu, a, o);
-            a = MIN ? fmin(a, b) : a + b;
+            a = mn ? fmin(a, b) : a + b;
         }
         if (lane == 0) sh[w][k] = a;
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < NV; k++) {
+        const bool mn = (MINMASK >> k) & 1u;
         double a = sh[0][k];
-        for (int j = 1; j < kCkBlock / 32; j++) a = MIN ? fmin(a, sh[j][k]) : a + sh[j][k];
+        for (int j = 1; j < kCkBlock / 32; j++) a = mn ? fmin(a, sh[j][k]) : a + sh[j][k];
         tot[k] = a;
     }
     if (threadIdx.x == 0) *V.counter = 0u;
@@ -134,45 +140,16 @@ __global__ void __launch_bounds__(kCkBlock) k_ck_predict_bound(CkView V, double 
     double v[1] = {1.0};
     if (i < V.n) v[0] = box_bound(V.c[i], dadd(dmul(V.c_d[i], dt), V.c[i]), 1.0);
     double tot[1];
-    if (reduce_last<1, true>(v, V, tot) && threadIdx.x == 0) V.sc[SC_RATIO] = tot[0];
+    if (reduce_last<1, 1u>(v, V, tot) && threadIdx.x == 0) V.sc[SC_RATIO] = tot[0];
 }
 
-// c += c_d dt ratio; then h = g and g.g (clock_adams.cpp:277-290)
+// c += c_d dt ratio (clock_adams.cpp:277-283)
 __global__ void __launch_bounds__(kCkBlock) k_ck_predict(CkView V, double dt)
 {
     const int i = blockIdx.x * kCkBlock + threadIdx.x;
     if (i >= V.n) return;
     const double r = V.sc[SC_RATIO];
     V.c[i] = dadd(V.c[i], dmul(dmul(V.c_d[i], dt), r));
-}
-
-__global__ void __launch_bounds__(kCkBlock) k_ck_h_from_g(CkView V)
-{
-    const int i = blockIdx.x * kCkBlock + threadIdx.x;
-    double v[1] = {0.0};
-    if (i < V.n) {
-        const double gi = V.g[i];
-        V.h[i] = gi;
-        v[0] = dmul(gi, gi);
-    }
-    double tot[1];
-    if (reduce_last<1, false>(v, V, tot) && threadIdx.x == 0) V.sc[SC_G0G0] = tot[0];
-}
-
-// start of a conjugate-gradient iteration: g0 = g, c0 = c, and the step bound
-// gamma along h (clock_adams.cpp:296-314)
-__global__ void __launch_bounds__(kCkBlock) k_ck_begin(CkView V)
-{
-    const int i = blockIdx.x * kCkBlock + threadIdx.x;
-    double v[1] = {1.0};
-    if (i < V.n) {
-        const double ci = V.c[i], hi = V.h[i];
-        V.g0[i] = V.g[i];
-        V.c0[i] = ci;
-        v[0] = box_bound(ci, dadd(ci, hi), 1.0);
-    }
-    double tot[1];
-    if (reduce_last<1, true>(v, V, tot) && threadIdx.x == 0) V.sc[SC_GAMMA] = tot[0];
 }
 
 // trial point c = c0 + gamma h (clock_adams.cpp:322-323)
@@ -193,25 +170,58 @@ __global__ void __launch_bounds__(kCkBlock) k_ck_dots(CkView V)
         v[1] = dmul(gi, gi);
     }
     double tot[2];
-    if (reduce_last<2, false>(v, V, tot) && threadIdx.x == 0) {
+    if (reduce_last<2, 0u>(v, V, tot) && threadIdx.x == 0) {
         V.sc[SC_GG0] = tot[0];
         V.sc[SC_GG] = tot[1];
     }
 }
 
-// h = h ratio + g and h.g (clock_adams.cpp:356-366)
-__global__ void __launch_bounds__(kCkBlock) k_ck_direction(CkView V, double ratio)
+// the first direction h = g with g.g, fused with the start of the first
+// conjugate-gradient iteration (g0 = g, c0 = c and the box bound along h):
+// clock_adams.cpp:287-314, clock_bdf.cpp:727-759
+__global__ void __launch_bounds__(kCkBlock) k_ck_first_dir(CkView V)
 {
     const int i = blockIdx.x * kCkBlock + threadIdx.x;
-    double v[1] = {0.0};
+    double v[2] = {0.0, 1.0};
     if (i < V.n) {
-        const double gi = V.g[i];
+        const double gi = V.g[i], ci = V.c[i];
+        V.h[i] = gi;
+        V.g0[i] = gi;
+        V.c0[i] = ci;
+        v[0] = dmul(gi, gi);
+        v[1] = box_bound(ci, dadd(ci, gi), 1.0);
+    }
+    double tot[2];
+    if (reduce_last<2, 2u>(v, V, tot) && threadIdx.x == 0) {
+        V.sc[SC_G0G0] = tot[0];
+        V.sc[SC_GAMMA] = tot[1];
+    }
+}
+
+// the direction update h = h ratio + g with h.g (clock_adams.cpp:356-366,
+// clock_bdf.cpp:810-828), fused with the start of the next iteration:
+// g0 = g, c0 = c, and the box bounds along the new h and along g (the
+// direction restarts from g when h.g < 0)
+__global__ void __launch_bounds__(kCkBlock) k_ck_next_dir(CkView V, double ratio)
+{
+    const int i = blockIdx.x * kCkBlock + threadIdx.x;
+    double v[3] = {0.0, 1.0, 1.0};
+    if (i < V.n) {
+        const double gi = V.g[i], ci = V.c[i];
         const double hi = dadd(dmul(V.h[i], ratio), gi);
         V.h[i] = hi;
+        V.g0[i] = gi;
+        V.c0[i] = ci;
         v[0] = dmul(hi, gi);
+        v[1] = box_bound(ci, dadd(ci, hi), 1.0);
+        v[2] = box_bound(ci, dadd(ci, gi), 1.0);
     }
-    double tot[1];
-    if (reduce_last<1, false>(v, V, tot) && threadIdx.x == 0) V.sc[SC_GH] = tot[0];
+    double tot[3];
+    if (reduce_last<3, 6u>(v, V, tot) && threadIdx.x == 0) {
+        V.sc[SC_GH] = tot[0];
+        V.sc[SC_GAMMA] = tot[1];
+        V.sc[SC_B] = tot[2];
+    }
 }
 
 // ---- BDF clock (clock_bdf.cpp) ---------------------------------------------
@@ -252,7 +262,7 @@ __global__ void __launch_bounds__(kCkBlock) k_bdf_interp(CkView V, BdfVecs B, Bd
         if (y0 < 0.0 || y0 > 1.0) v[0] = -1.0;
     }
     double tot[1];
-    if (reduce_last<1, true>(v, V, tot) && threadIdx.x == 0) V.sc[SC_A] = tot[0];
+    if (reduce_last<1, 1u>(v, V, tot) && threadIdx.x == 0) V.sc[SC_A] = tot[0];
 }
 
 // the bound of the explicit predictor step y[0] + dy del_t (clock_bdf.cpp:
@@ -263,7 +273,7 @@ __global__ void __launch_bounds__(kCkBlock) k_bdf_predict_bound(CkView V, const 
     double v[1] = {1.0};
     if (i < V.n) v[0] = box_bound(y0[i], dadd(dmul(dy[i], dt), y0[i]), 1.0);
     double tot[1];
-    if (reduce_last<1, true>(v, V, tot) && threadIdx.x == 0) V.sc[SC_RATIO] = tot[0];
+    if (reduce_last<1, 1u>(v, V, tot) && threadIdx.x == 0) V.sc[SC_RATIO] = tot[0];
 }
 
 // c = y[0] + dy del_t ratio (clock_bdf.cpp:716-717)
@@ -287,7 +297,7 @@ __global__ void __launch_bounds__(kCkBlock) k_bdf_err(CkView V, BdfVecs B)
         v[2] = (ci < 0.0 || ci > 1.0) ? 1.0 : 0.0;
     }
     double tot[3];
-    if (reduce_last<3, false>(v, V, tot) && threadIdx.x == 0) {
+    if (reduce_last<3, 0u>(v, V, tot) && threadIdx.x == 0) {
         V.sc[SC_GG0] = tot[0];
         V.sc[SC_GG] = tot[1];
         V.sc[SC_GH] = tot[2];
@@ -323,7 +333,7 @@ __global__ void __launch_bounds__(kCkBlock) k_bdf_hilo(CkView V, BdfVecs B, BdfH
         B.e_n[i] = dsub(ci, y0);
     }
     double tot[2];
-    if (reduce_last<2, false>(v, V, tot) && threadIdx.x == 0) {
+    if (reduce_last<2, 0u>(v, V, tot) && threadIdx.x == 0) {
         V.sc[SC_GG0] = tot[0];
         V.sc[SC_GG] = tot[1];
     }
@@ -409,17 +419,16 @@ struct Clock {
         k_ck_predict<<<grid(), kCkBlock, 0, st>>>(V, delta_t);
         KCU(cudaGetLastError());
         KCHK(refresh_c());
-        k_ck_h_from_g<<<grid(), kCkBlock, 0, st>>>(V);
+        // h = g, and the first iteration's g0, c0 and step bound with it
+        k_ck_first_dir<<<grid(), kCkBlock, 0, st>>>(V);
         KCU(cudaGetLastError());
         KCHK(read_scalars());
         g0_g0 = host_sc[SC_G0G0];
         g_h = g0_g0;
+        double bound = host_sc[SC_GAMMA];
         int iter = 0;
         while (curr_cost > 1.0e-8 && iter < 50 && max_gamma > min_gamma) {
-            k_ck_begin<<<grid(), kCkBlock, 0, st>>>(V);
-            KCU(cudaGetLastError());
-            KCHK(read_scalars());
-            max_gamma = host_sc[SC_GAMMA];
+            max_gamma = bound;
             chk = 1;
             cost = curr_cost;
             while (chk && max_gamma > min_gamma) {
@@ -438,13 +447,16 @@ struct Clock {
             g_g = host_sc[SC_GG];
             ratio = (g_g - g_g0) / g0_g0;
             g0_g0 = g_g;
-            k_ck_direction<<<grid(), kCkBlock, 0, st>>>(V, ratio);
+            // the new direction, and the next iteration's g0, c0 and bound
+            k_ck_next_dir<<<grid(), kCkBlock, 0, st>>>(V, ratio);
             KCU(cudaGetLastError());
             KCHK(read_scalars());
             g_h = host_sc[SC_GH];
+            bound = host_sc[SC_GAMMA];
             if (g_h < 0.0) {
                 KCU(cudaMemcpyAsync(V.h, V.g, (size_t)V.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
                 g_h = g_g;
+                bound = host_sc[SC_B];
             }
             iter++;
         }
@@ -521,18 +533,17 @@ struct Bdf {
         KCU(cudaGetLastError());
         KCHK(ck->refresh_c());
         KCHK(ck->calc_g(0, beta, &curr_cost));
-        k_ck_h_from_g<<<grid(), kCkBlock, 0, ck->st>>>(ck->V);
+        // h = g, and the first iteration's g0, c0 and step bound with it
+        k_ck_first_dir<<<grid(), kCkBlock, 0, ck->st>>>(ck->V);
         KCU(cudaGetLastError());
         KCHK(ck->read_scalars());
         g0_g0 = ck->host_sc[SC_G0G0];
         g_h = g0_g0;
+        double bound = ck->host_sc[SC_GAMMA];
         int iter = 0;
         while (curr_cost > o.m_tol * (double)dof_tot && iter < o.max_iter && max_gamma > o.min_gamma) {
-            k_ck_begin<<<grid(), kCkBlock, 0, ck->st>>>(ck->V);
-            KCU(cudaGetLastError());
-            KCHK(ck->read_scalars());
             // min(0.99, the box bounds along h) (clock_bdf.cpp:744-759)
-            gamma = ck->host_sc[SC_GAMMA] < 0.99 ? ck->host_sc[SC_GAMMA] : 0.99;
+            gamma = bound < 0.99 ? bound : 0.99;
             max_gamma = gamma * 0.9;
             chk = 1;
             cost = curr_cost;
@@ -558,14 +569,18 @@ struct Bdf {
                 g_g = ck->host_sc[SC_GG];
                 ratio = (g_g - g_g0) / g0_g0;
                 g0_g0 = g_g;
-                k_ck_direction<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, ratio);
+                // the new direction, and the next iteration's g0, c0 and bound
+                // (a failed line search ends the loop: max_gamma <= min_gamma)
+                k_ck_next_dir<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, ratio);
                 KCU(cudaGetLastError());
                 KCHK(ck->read_scalars());
                 g_h = ck->host_sc[SC_GH];
+                bound = ck->host_sc[SC_GAMMA];
                 if (g_h < 0.0) {
                     KCU(cudaMemcpyAsync(ck->V.h, ck->V.g, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice,
                                         ck->st));
                     g_h = g_g;
+                    bound = ck->host_sc[SC_B];
                 }
             }
             iter++;

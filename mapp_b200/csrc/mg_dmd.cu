@@ -364,12 +364,24 @@ __global__ void k_crd_ghosts(Dev d)
 }
 
 // ---- c_d_calc / calc_g shared passes -------------------------------------
+// Each site's list is walked by an aligned group of lanes: the neighbour
+// list (about 42 entries per site at the bench density) by 16 lanes, the
+// r_crd sub-list (about 6, its half of the 12 first neighbours) by 8, so that
+// few lanes idle; the group's sums close with group_sum.
+#ifndef MG_NBR_LANES
+#define MG_NBR_LANES 16
+#endif
+#ifndef MG_CRD_LANES
+#define MG_CRD_LANES 8
+#endif
+constexpr int kNbrLanes = MG_NBR_LANES;
+constexpr int kCrdLanes = MG_CRD_LANES;
 // E from the stored per-pair densities (ff_dmd_I.cpp:2273-2292).
-template <int NT, typename P>
+template <int NT, typename P, int G>
 __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
 {
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
     double ci[NT], Ei[NT];
 #pragma unroll
@@ -378,7 +390,7 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
         Ei[a] = 0.0;
     }
     int nn = d.nnb[i];
-    for (int k = lane; k < nn; k += 32) {
+    for (int k = lane; k < nn; k += G) {
         long long slot = (long long)d.poff[i] + k;
         int j = d.nbr[(size_t)i * d.maxnb + k];
         double cj[NT], Ej[NT];
@@ -402,7 +414,7 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
     }
 #pragma unroll
     for (int a = 0; a < NT; a++) {
-        double s = warp_sum(Ei[a]);
+        double s = group_sum<G>(Ei[a]);
         if (lane == 0) atomicAdd(&d.E[(size_t)i * NT + a], s);
     }
 }
@@ -432,12 +444,12 @@ __device__ __forceinline__ double dE_flat(const Dev& d, int q)
 }
 
 // chemical-potential pair sums (ff_dmd_I.cpp:2320-2345).
-template <int NT, typename P>
+template <int NT, typename P, int G>
 __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
 {
     using S = Slots<NT>;
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
     double ci[NT], ni[NT], dEi_q[NT];
 #pragma unroll
@@ -447,7 +459,7 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
         dEi_q[a] = dE_flat<NT>(d, i + a);
     }
     int nn = d.nnb[i];
-    for (int k = lane; k < nn; k += 32) {
+    for (int k = lane; k < nn; k += G) {
         long long slot = (long long)d.poff[i] + k;
         int j = d.nbr[(size_t)i * d.maxnb + k];
         double cj[NT], nj[NT], dEj_q[NT];
@@ -474,7 +486,7 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
     }
 #pragma unroll
     for (int a = 0; a < NT; a++) {
-        double s = warp_sum(ni[a]);
+        double s = group_sum<G>(ni[a]);
         if (lane == 0) atomicAdd(&d.n[(size_t)i * NT + a], s);
     }
 }
@@ -528,11 +540,11 @@ __device__ __forceinline__ double rate_sij(const Dev& d, double ni, double nj, d
 }
 
 // c_d over the r_crd sub-list (ff_dmd_I.cpp:2361-2382).
-template <int NT>
+template <int NT, int G>
 __global__ void __launch_bounds__(kFFBlock) k_cd_rates(Dev d)
 {
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
     double ni[NT], ci[NT], cdi[NT];
 #pragma unroll
@@ -542,7 +554,7 @@ __global__ void __launch_bounds__(kFFBlock) k_cd_rates(Dev d)
         cdi[a] = 0.0;
     }
     int nc = d.ncrd[i];
-    for (int k = lane; k < nc; k += 32) {
+    for (int k = lane; k < nc; k += G) {
         int j = d.crdl[(size_t)i * d.maxcrd + k];
         int oj = owner(d, j);
 #pragma unroll
@@ -554,7 +566,7 @@ __global__ void __launch_bounds__(kFFBlock) k_cd_rates(Dev d)
     }
 #pragma unroll
     for (int a = 0; a < NT; a++) {
-        double s = warp_sum(cdi[a]);
+        double s = group_sum<G>(cdi[a]);
         if (lane == 0) atomicAdd(&d.c_d[(size_t)i * NT + a], s);
     }
 }
@@ -570,11 +582,11 @@ __global__ void k_g_sinit(Dev d)
     if (d.style == STYLE_DMD_II) d.c_d[idx] = 0.0;
 }
 
-template <int NT>
+template <int NT, int G>
 __global__ void __launch_bounds__(kFFBlock) k_g_srates(Dev d, double alpha)
 {
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
     double ni[NT], ci[NT], si[NT], cdi[NT];
 #pragma unroll
@@ -585,7 +597,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_srates(Dev d, double alpha)
     }
     bool II = d.style == STYLE_DMD_II;
     int nc = d.ncrd[i];
-    for (int k = lane; k < nc; k += 32) {
+    for (int k = lane; k < nc; k += G) {
         int j = d.crdl[(size_t)i * d.maxcrd + k];
         int oj = owner(d, j);
 #pragma unroll
@@ -603,10 +615,10 @@ __global__ void __launch_bounds__(kFFBlock) k_g_srates(Dev d, double alpha)
     }
 #pragma unroll
     for (int a = 0; a < NT; a++) {
-        double s = warp_sum(si[a]);
+        double s = group_sum<G>(si[a]);
         if (lane == 0) atomicAdd(&d.s[(size_t)i * NT + a], s);
         if (II) {
-            double c2 = warp_sum(cdi[a]);
+            double c2 = group_sum<G>(cdi[a]);
             if (lane == 0) atomicAdd(&d.c_d[(size_t)i * NT + a], c2);
         }
     }
@@ -631,11 +643,11 @@ __global__ void __launch_bounds__(kFFBlock) k_g_cost(Dev d, int row0, int chk)
 
 // t and the first g terms over the crd sub-list (ff_dmd_I.cpp:2582-2608,
 // ff_dmd.cpp:2582-2605, ff_dmd_II.cpp:2529-2564).
-template <int NT>
+template <int NT, int G>
 __global__ void __launch_bounds__(kFFBlock) k_g_trates(Dev d, double alpha)
 {
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
     double ni[NT], ci[NT], si[NT], ti[NT], gi[NT];
 #pragma unroll
@@ -646,7 +658,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_trates(Dev d, double alpha)
         ti[a] = gi[a] = 0.0;
     }
     int nc = d.ncrd[i];
-    for (int k = lane; k < nc; k += 32) {
+    for (int k = lane; k < nc; k += G) {
         int j = d.crdl[(size_t)i * d.maxcrd + k];
         int oj = owner(d, j);
         bool own_j = j < d.natms;
@@ -690,7 +702,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_trates(Dev d, double alpha)
     }
 #pragma unroll
     for (int a = 0; a < NT; a++) {
-        double s = warp_sum(ti[a]), g = warp_sum(gi[a]);
+        double s = group_sum<G>(ti[a]), g = group_sum<G>(gi[a]);
         if (lane == 0) {
             atomicAdd(&d.t[(size_t)i * NT + a], s);
             atomicAdd(&d.g[(size_t)i * NT + a], g);
@@ -699,12 +711,12 @@ __global__ void __launch_bounds__(kFFBlock) k_g_trates(Dev d, double alpha)
 }
 
 // v and the t-weighted g terms over the full list (ff_dmd_I.cpp:2612-2644).
-template <int NT, typename P>
+template <int NT, typename P, int G>
 __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
 {
     using S = Slots<NT>;
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
     double dEi[NT], ti[NT], vi[NT], gi[NT];
 #pragma unroll
@@ -715,7 +727,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
     }
     double ba = d.beta * alpha;
     int nn = d.nnb[i];
-    for (int k = lane; k < nn; k += 32) {
+    for (int k = lane; k < nn; k += G) {
         long long slot = (long long)d.poff[i] + k;
         int j = d.nbr[(size_t)i * d.maxnb + k];
         int oj = owner(d, j);
@@ -750,7 +762,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
     }
 #pragma unroll
     for (int a = 0; a < NT; a++) {
-        double s = warp_sum(vi[a]), g = warp_sum(gi[a]);
+        double s = group_sum<G>(vi[a]), g = group_sum<G>(gi[a]);
         if (lane == 0) {
             atomicAdd(&d.v[(size_t)i * NT + a], s);
             atomicAdd(&d.g[(size_t)i * NT + a], g);
@@ -759,11 +771,11 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
 }
 
 // last g terms with ddE (ff_dmd_I.cpp:2649-2670).
-template <int NT, typename P>
+template <int NT, typename P, int G>
 __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
 {
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
     double wi[NT], gi[NT];
     double ab = alpha * d.beta;
@@ -774,7 +786,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
         gi[a] = 0.0;
     }
     int nn = d.nnb[i];
-    for (int k = lane; k < nn; k += 32) {
+    for (int k = lane; k < nn; k += G) {
         long long slot = (long long)d.poff[i] + k;
         int j = d.nbr[(size_t)i * d.maxnb + k];
         int oj = owner(d, j);
@@ -800,7 +812,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
     }
 #pragma unroll
     for (int a = 0; a < NT; a++) {
-        double g = warp_sum(gi[a]);
+        double g = group_sum<G>(gi[a]);
         if (lane == 0) atomicAdd(&d.g[(size_t)i * NT + a], g);
     }
 }
@@ -836,12 +848,13 @@ cudaError_t dmd_energy_nt(const Dev& d, int* nb, cudaStream_t st)
 template <int NT, typename P>
 cudaError_t dmd_cdot_ntp(const Dev& d, cudaStream_t st)
 {
-    int gw = div_up((long long)d.natms * 32, kFFBlock), gs = div_up((long long)d.natms * NT, kFFBlock);
-    k_mu_E<NT, P><<<gw, kFFBlock, 0, st>>>(d);
+    int gw = div_up((long long)d.natms * kNbrLanes, kFFBlock), gc = div_up((long long)d.natms * kCrdLanes, kFFBlock);
+    int gs = div_up((long long)d.natms * NT, kFFBlock);
+    k_mu_E<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d);
     k_mu_embed<NT><<<gs, kFFBlock, 0, st>>>(d, 0);
-    k_mu_npairs<NT, P><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_npairs<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d);
     k_mu_nfinal<NT><<<gs, kFFBlock, 0, st>>>(d, d.style == STYLE_DMD_II ? 1 : 0);
-    k_cd_rates<NT><<<gw, kFFBlock, 0, st>>>(d);
+    k_cd_rates<NT, kCrdLanes><<<gc, kFFBlock, 0, st>>>(d);
     return cudaGetLastError();
 }
 
@@ -854,19 +867,20 @@ cudaError_t dmd_cdot_nt(const Dev& d, cudaStream_t st)
 template <int NT, typename P>
 cudaError_t dmd_calc_g_ntp(const Dev& d, int chk, double alpha, int* nb, cudaStream_t st)
 {
-    int gw = div_up((long long)d.natms * 32, kFFBlock), gs = div_up((long long)d.natms * NT, kFFBlock);
-    k_mu_E<NT, P><<<gw, kFFBlock, 0, st>>>(d);
+    int gw = div_up((long long)d.natms * kNbrLanes, kFFBlock), gc = div_up((long long)d.natms * kCrdLanes, kFFBlock);
+    int gs = div_up((long long)d.natms * NT, kFFBlock);
+    k_mu_E<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d);
     k_mu_embed<NT><<<gs, kFFBlock, 0, st>>>(d, 1);
-    k_mu_npairs<NT, P><<<gw, kFFBlock, 0, st>>>(d);
+    k_mu_npairs<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d);
     k_mu_nfinal<NT><<<gs, kFFBlock, 0, st>>>(d, d.style == STYLE_DMD_II ? 3 : 2);
     k_g_sinit<NT><<<gs, kFFBlock, 0, st>>>(d);
-    k_g_srates<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
+    k_g_srates<NT, kCrdLanes><<<gc, kFFBlock, 0, st>>>(d, alpha);
     k_g_cost<NT><<<gs, kFFBlock, 0, st>>>(d, 0, chk);
     *nb = gs;
     if (!chk) {
-        k_g_trates<NT><<<gw, kFFBlock, 0, st>>>(d, alpha);
-        k_g_vpass<NT, P><<<gw, kFFBlock, 0, st>>>(d, alpha);
-        k_g_last<NT, P><<<gw, kFFBlock, 0, st>>>(d, alpha);
+        k_g_trates<NT, kCrdLanes><<<gc, kFFBlock, 0, st>>>(d, alpha);
+        k_g_vpass<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d, alpha);
+        k_g_last<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d, alpha);
     }
     return cudaGetLastError();
 }
