@@ -465,6 +465,7 @@ def run_large_forms(mb, fx, device, mlp_source):
             s.force_calc(1)
             cd = s.c_d_calc()
             dt = 1e-3 / float(np.sqrt(np.mean(cd * cd)))
+            s.clock_adams(2, 1, dt)  # warm-up (first-call allocations)
             t0 = time.perf_counter()
             ra = s.clock_adams(2, 10, dt)
             wall = time.perf_counter() - t0
@@ -481,6 +482,7 @@ def run_large_forms(mb, fx, device, mlp_source):
             s2.force_calc(1)
             cd2 = s2.c_d_calc()
             tau2 = 1.0 / float(np.sqrt(np.mean(cd2 * cd2)))
+            s2.clock_bdf(2, max_order=2, initial_del_t=1e-3 * tau2)  # warm-up
             s2.close()
             s2 = mb.system_from_workload(w2, device=device)
             t0 = time.perf_counter()
