@@ -47,6 +47,8 @@ struct CkView {
     double* sc;     // scalars
     unsigned int* counter;
     int n, nblocks;
+    const int* root;  // ghost -> owning site (the system's)
+    int natms, nph, nt;
 };
 
 // Block reduction of NV values, then the fixed-order reduction of all block
@@ -152,11 +154,21 @@ __global__ void __launch_bounds__(kCkBlock) k_ck_predict(CkView V, double dt)
     V.c[i] = dadd(V.c[i], dmul(dmul(V.c_d[i], dt), r));
 }
 
-// trial point c = c0 + gamma h (clock_adams.cpp:322-323)
+// trial point c = c0 + gamma h (clock_adams.cpp:322-323), ghosts included:
+// a ghost takes its owner's trial value, computed the same way, which is what
+// the ghost refresh that follows in the reference (atoms->update(c_n)) copies
 __global__ void __launch_bounds__(kCkBlock) k_ck_trial(CkView V, double gamma)
 {
     const int i = blockIdx.x * kCkBlock + threadIdx.x;
-    if (i < V.n) V.c[i] = dadd(V.c0[i], dmul(gamma, V.h[i]));
+    if (i < V.n) {
+        V.c[i] = dadd(V.c0[i], dmul(gamma, V.h[i]));
+        return;
+    }
+    const int k = i - V.n;
+    if (k >= V.nph * V.nt) return;
+    const int gq = k / V.nt, a = k - gq * V.nt;
+    const size_t o = (size_t)V.root[V.natms + gq] * V.nt + a;
+    V.c[(size_t)(V.natms + gq) * V.nt + a] = dadd(V.c0[o], dmul(gamma, V.h[o]));
 }
 
 // g.g0 and g.g after the line search (clock_adams.cpp:340-352)
@@ -375,6 +387,7 @@ struct Clock {
     ~Clock() { cudaFree(block); }
 
     int grid() const { return V.nblocks; }
+    int trial_grid() const { return div_up(V.n + V.nph * V.nt, kCkBlock); }
 
     // calc_g(chk, alpha, a, g) -> cost (one synchronisation)
     int calc_g(int chk, double alpha, double* cost, bool with_dots = false)
@@ -432,9 +445,8 @@ struct Clock {
             chk = 1;
             cost = curr_cost;
             while (chk && max_gamma > min_gamma) {
-                k_ck_trial<<<grid(), kCkBlock, 0, st>>>(V, max_gamma);
+                k_ck_trial<<<trial_grid(), kCkBlock, 0, st>>>(V, max_gamma);
                 KCU(cudaGetLastError());
-                KCHK(refresh_c());
                 KCHK(calc_g(1, alpha, &curr_cost));
                 ideal_cost = cost - slope * max_gamma * g_h;
                 if (curr_cost < ideal_cost) chk = 0;
@@ -548,9 +560,8 @@ struct Bdf {
             chk = 1;
             cost = curr_cost;
             while (chk && max_gamma > o.min_gamma) {
-                k_ck_trial<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, max_gamma);
+                k_ck_trial<<<ck->trial_grid(), kCkBlock, 0, ck->st>>>(ck->V, max_gamma);
                 KCU(cudaGetLastError());
-                KCHK(ck->refresh_c());
                 // the dot products g.g0, g.g ride along with the cost readback
                 KCHK(ck->calc_g(0, beta, &curr_cost, true));
                 ideal_cost = cost - o.slope * max_gamma * g_h;
@@ -758,6 +769,10 @@ extern "C" int mg_clock_adams(mg_system* s, int order, int nsteps, double delta_
     ck.V.counter = reinterpret_cast<unsigned int*>(ck.V.sc + SC_COUNT);
     ck.V.n = n;
     ck.V.nblocks = nblocks;
+    ck.V.root = d.root;
+    ck.V.natms = natms;
+    ck.V.nph = d.nph;
+    ck.V.nt = nt;
     KCU(cudaMemsetAsync(ck.V.counter, 0, 8 * sizeof(double), ck.st));
     const double* beta = kBeta[order - 1];
     std::vector<int> slot(m);
@@ -855,6 +870,10 @@ extern "C" int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, d
     ck.V.counter = reinterpret_cast<unsigned int*>(ck.V.sc + SC_COUNT);
     ck.V.n = n;
     ck.V.nblocks = nblocks;
+    ck.V.root = d.root;
+    ck.V.natms = natms;
+    ck.V.nph = d.nph;
+    ck.V.nt = nt;
     KCU(cudaMemsetAsync(ck.block, 0, total * sizeof(double), ck.st));
     KCHK(system_enqueue_c_d(s));
     const size_t bytes = (size_t)n * sizeof(double);
