@@ -55,12 +55,9 @@ def test_clock_bdf_bit_exact(tmp_path, style, n, nt, steps, opts):
     assert np.all(np.diff(np.r_[0.0, res["order"]]) <= 1)
 
 
-def test_clock_bdf_order_changes():
+def test_clock_bdf_order_changes(tmp_path):
     """The DMD_II default run above changes order: the history records it."""
-    import tempfile
-
-    d = tempfile.mkdtemp()
-    w = fx.write_workload(d + "/w", "dmd", n=4, sigma=0.02, style="DMD_II")
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=4, sigma=0.02, style="DMD_II")
     res = Oracle(w).clock_bdf(25)
     assert res["order"].max() == 2 and res["order"][-1] == 1
     assert abs(np.sum(res["del_t"]) - res["t"]) <= 1e-12 * res["t"]
