@@ -494,10 +494,8 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
 // per-site finalisation of n; mode as in the oracle:
 //   0 c_d_calc DMD_I/DMD, 1 c_d_calc DMD_II, 2 calc_g DMD_I/DMD, 3 calc_g DMD_II
 template <int NT>
-__global__ void k_mu_nfinal(Dev d, int mode)
+__device__ __forceinline__ void mu_nfinal(const Dev& d, int idx, int mode)
 {
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= d.natms * NT) return;
     int a = idx % NT;
     double la = d.alpha[idx];
     double v = d.n[idx];
@@ -515,6 +513,13 @@ __global__ void k_mu_nfinal(Dev d, int mode)
         v += 1.5 * d.kbT * log(la);
     }
     d.n[idx] = v;
+}
+
+template <int NT>
+__global__ void k_mu_nfinal(Dev d, int mode)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < d.natms * NT) mu_nfinal<NT>(d, idx, mode);
 }
 
 // jump-rate term of one crd pair and species (ff_dmd_I.cpp:2372-2376,
@@ -573,11 +578,13 @@ __global__ void __launch_bounds__(kFFBlock) k_cd_rates(Dev d)
 
 // calc_g: s = 2(c + a) then the rate terms (ff_dmd_I.cpp:2537-2564,
 // ff_dmd_II.cpp:2471-2511); block partial of sum s^2 computed in k_g_cost.
+// (with calc_g's finalisation of n, which needs nothing from other sites)
 template <int NT>
-__global__ void k_g_sinit(Dev d)
+__global__ void k_g_sinit(Dev d, int mode)
 {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= d.natms * NT) return;
+    mu_nfinal<NT>(d, idx, mode);
     d.s[idx] = 2.0 * (d.c[idx] + d.a_in[idx]);
     if (d.style == STYLE_DMD_II) d.c_d[idx] = 0.0;
 }
@@ -872,8 +879,7 @@ cudaError_t dmd_calc_g_ntp(const Dev& d, int chk, double alpha, int* nb, cudaStr
     k_mu_E<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d);
     k_mu_embed<NT><<<gs, kFFBlock, 0, st>>>(d, 1);
     k_mu_npairs<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d);
-    k_mu_nfinal<NT><<<gs, kFFBlock, 0, st>>>(d, d.style == STYLE_DMD_II ? 3 : 2);
-    k_g_sinit<NT><<<gs, kFFBlock, 0, st>>>(d);
+    k_g_sinit<NT><<<gs, kFFBlock, 0, st>>>(d, d.style == STYLE_DMD_II ? 3 : 2);
     k_g_srates<NT, kCrdLanes><<<gc, kFFBlock, 0, st>>>(d, alpha);
     k_g_cost<NT><<<gs, kFFBlock, 0, st>>>(d, 0, chk);
     *nb = gs;
