@@ -221,6 +221,7 @@ struct mg_system {
     size_t scan_tmp_bytes = 0;
     double* stage = nullptr;  // device staging for host arrays
     size_t stage_cap = 0;
+    size_t act_cap = 0;  // capacity of the active-pair sublist (entries)
     double* red_out = nullptr;  // 8 doubles
     double* d_rhoT = nullptr;
     double* d_phiT = nullptr;
@@ -945,7 +946,7 @@ int mg_destroy(mg_system* s)
     Dev& d = s->d;
     void* ptrs[] = {d.prf, s->d_pkT, s->d_pk64, s->d_pkC, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
-                    d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status,
+                    d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status, d.act_j, d.act_slot, d.nact,
                     s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1812,6 +1813,27 @@ int mg::system_enqueue_calc_g(mg_system* s, int chk, double alpha, int* rows)
     CU(launch_reduce_partials(d, *rows, 1, s->red_out, s->st));
     return MG_OK;
 }
+int mg::system_set_active_pairs(mg_system* s, bool on)
+{
+    Dev& d = s->d;
+    if (!on) {
+        d.act_on = 0;
+        return MG_OK;
+    }
+    if (!s->dmd || s->form != MG_FORM_FP64 || s->natms == 0) return MG_OK;
+    const size_t cap = (size_t)s->natms * d.maxnb;
+    if (cap > s->act_cap) {
+        CHK(dalloc(&d.act_j, cap));
+        CHK(dalloc(&d.act_slot, cap));
+        CHK(dalloc(&d.nact, (size_t)s->natms));
+        s->act_cap = cap;
+    }
+    d.act_on = 0;
+    CU(launch_active_pairs(d, s->st));
+    d.act_on = 1;
+    return MG_OK;
+}
+
 int mg::system_enqueue_c_d(mg_system* s)
 {
     if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "c_d_calc needs a DMD force field");

@@ -709,6 +709,14 @@ int clock_setup(mg_system* s, const char* what)
     return MG_OK;
 }
 
+// the clocks keep positions and lists fixed, so calc_g and c_d_calc may walk
+// the active-pair sublist for the whole run; switched off again on every exit
+struct ActivePairs {
+    mg_system* s;
+    explicit ActivePairs(mg_system* sys) : s(sys) {}
+    ~ActivePairs() { system_set_active_pairs(s, false); }
+};
+
 int clock_force_init(mg_system* s)
 {
     int style = -1, nt = 0, x_dim = 0, form = 0;
@@ -720,7 +728,8 @@ int clock_force_init(mg_system* s)
     double en[7];
     int rc = mg_ff_force_calc(s, 1, fdev, en);
     cudaFree(fdev);
-    return rc;
+    if (rc != MG_OK) return rc;
+    return system_set_active_pairs(s, true);
 }
 
 }  // namespace
@@ -744,6 +753,7 @@ extern "C" int mg_clock_adams(mg_system* s, int order, int nsteps, double delta_
     Clock ck;
     ck.s = s;
     ck.st = system_stream(s);
+    ActivePairs active(s);
     KCHK(clock_force_init(s));
     const int n = natms * nt;
     if (n == 0 || nsteps == 0) {
@@ -838,6 +848,7 @@ extern "C" int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, d
     ck.s = s;
     ck.st = system_stream(s);
     // Clock_BDF::init (clock_bdf.cpp:201-275)
+    ActivePairs active(s);
     KCHK(clock_force_init(s));
     const int n = natms * nt;
     if (steps_taken) *steps_taken = 0;

@@ -389,10 +389,11 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
         ci[a] = d.c[(size_t)i * NT + a];
         Ei[a] = 0.0;
     }
-    int nn = d.nnb[i];
+    int nn = d.act_on ? d.nact[i] : d.nnb[i];
     for (int k = lane; k < nn; k += G) {
-        long long slot = (long long)d.poff[i] + k;
-        int j = d.nbr[(size_t)i * d.maxnb + k];
+        const size_t q = (size_t)i * d.maxnb + k;
+        long long slot = d.act_on ? d.act_slot[q] : (long long)d.poff[i] + k;
+        int j = d.act_on ? d.act_j[q] : d.nbr[q];
         double cj[NT], Ej[NT];
 #pragma unroll
         for (int b = 0; b < NT; b++) {
@@ -458,10 +459,11 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
         ni[a] = 0.0;
         dEi_q[a] = dE_flat<NT>(d, i + a);
     }
-    int nn = d.nnb[i];
+    int nn = d.act_on ? d.nact[i] : d.nnb[i];
     for (int k = lane; k < nn; k += G) {
-        long long slot = (long long)d.poff[i] + k;
-        int j = d.nbr[(size_t)i * d.maxnb + k];
+        const size_t q = (size_t)i * d.maxnb + k;
+        long long slot = d.act_on ? d.act_slot[q] : (long long)d.poff[i] + k;
+        int j = d.act_on ? d.act_j[q] : d.nbr[q];
         double cj[NT], nj[NT], dEj_q[NT];
 #pragma unroll
         for (int b = 0; b < NT; b++) {
@@ -733,10 +735,11 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
         vi[a] = gi[a] = 0.0;
     }
     double ba = d.beta * alpha;
-    int nn = d.nnb[i];
+    int nn = d.act_on ? d.nact[i] : d.nnb[i];
     for (int k = lane; k < nn; k += G) {
-        long long slot = (long long)d.poff[i] + k;
-        int j = d.nbr[(size_t)i * d.maxnb + k];
+        const size_t q = (size_t)i * d.maxnb + k;
+        long long slot = d.act_on ? d.act_slot[q] : (long long)d.poff[i] + k;
+        int j = d.act_on ? d.act_j[q] : d.nbr[q];
         int oj = owner(d, j);
         double dEj[NT], tj[NT], vj[NT], gj[NT];
 #pragma unroll
@@ -792,10 +795,11 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
         wi[a] = d.ddE[q] * d.c[q] * d.v[q];
         gi[a] = 0.0;
     }
-    int nn = d.nnb[i];
+    int nn = d.act_on ? d.nact[i] : d.nnb[i];
     for (int k = lane; k < nn; k += G) {
-        long long slot = (long long)d.poff[i] + k;
-        int j = d.nbr[(size_t)i * d.maxnb + k];
+        const size_t q = (size_t)i * d.maxnb + k;
+        long long slot = d.act_on ? d.act_slot[q] : (long long)d.poff[i] + k;
+        int j = d.act_on ? d.act_j[q] : d.nbr[q];
         int oj = owner(d, j);
         double wj[NT], gj[NT];
 #pragma unroll
@@ -822,6 +826,33 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
         double g = group_sum<G>(gi[a]);
         if (lane == 0) atomicAdd(&d.g[(size_t)i * NT + a], g);
     }
+}
+
+// the active sublist (Dev::act_*): a listed pair is active when any of its
+// stored densities or pair energies (the only per-pair values c_d_calc and
+// calc_g read) is non-zero; an inactive pair adds exact zeros there
+template <int NT>
+__global__ void k_active_pairs(Dev d)
+{
+    using S = Slots<NT>;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.natms) return;
+    const int nn = d.nnb[i];
+    int m = 0;
+    for (int k = 0; k < nn; k++) {
+        const long long slot = (long long)d.poff[i] + k;
+        bool on = false;
+#pragma unroll
+        for (int q = 0; q < NT * NT; q++) on |= d.pr[(size_t)(S::RHO + q) * d.maxp + slot] != 0.0;
+#pragma unroll
+        for (int q = 0; q < S::NC; q++) on |= d.pr[(size_t)(S::PHI + q) * d.maxp + slot] != 0.0;
+        if (on) {
+            const size_t o = (size_t)i * d.maxnb + m++;
+            d.act_j[o] = d.nbr[(size_t)i * d.maxnb + k];
+            d.act_slot[o] = slot;
+        }
+    }
+    d.nact[i] = m;
 }
 
 template <int NT>
@@ -938,6 +969,19 @@ cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st)
     case 4: return dmd_cdot_nt<4>(d, st);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_active_pairs(const Dev& d, cudaStream_t st)
+{
+    const int g = div_up(d.natms, kFFBlock);
+    switch (d.nt) {
+    case 1: k_active_pairs<1><<<g, kFFBlock, 0, st>>>(d); break;
+    case 2: k_active_pairs<2><<<g, kFFBlock, 0, st>>>(d); break;
+    case 3: k_active_pairs<3><<<g, kFFBlock, 0, st>>>(d); break;
+    case 4: k_active_pairs<4><<<g, kFFBlock, 0, st>>>(d); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nb, cudaStream_t st)

@@ -87,6 +87,13 @@ struct Dev {
     // per-pair scratch
     double* pr;    // EAM/FS: drhoi[maxp], drhoj[maxp]; DMD: 21 SoA blocks of maxp
     long long maxp;
+    // while act_on: per owned site the listed pairs whose stored densities and
+    // pair energies are not all zero (site j, pair slot), [natms][maxnb], and
+    // their count; c_d_calc and calc_g then walk these instead of the list
+    int* act_j;
+    long long* act_slot;
+    int* nact;
+    int act_on;
     // reductions
     double* partial;   // [nblocks][8]
     int* status;       // [0] overflow of nbr, [1] needed maxnb, [2] overflow crd, [3] needed maxcrd
@@ -218,6 +225,7 @@ cudaError_t launch_dmd_force_mlp(const Dev& d, const MlpState& S, unsigned long 
 cudaError_t launch_dmd_crd(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_active_pairs(const Dev& d, cudaStream_t st);
 
 // records msg as the calling thread's last error and returns code
 int internal_fail(int code, const char* msg);
@@ -248,5 +256,9 @@ double* system_red_out(mg_system* s);
 // g in the system's g unless chk) and c_d_calc's (c_d in the system's c_d); capturable
 int system_enqueue_calc_g(mg_system* s, int chk, double alpha, int* rows);
 int system_enqueue_c_d(mg_system* s);
+// builds the active-pair sublist from the last force_calc's pair values and
+// makes c_d_calc / calc_g walk it (on), or walk the full list again (off);
+// valid while the positions and the list stay as they are
+int system_set_active_pairs(mg_system* s, bool on);
 
 }  // namespace mg
