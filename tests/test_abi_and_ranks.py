@@ -35,6 +35,20 @@ def test_library_exports_every_declared_entry_point():
     assert not missing, missing
 
 
+@pytest.mark.skipif(not os.path.exists(LIB), reason="library not built")
+def test_bdf_defaults_are_the_references():
+    """mg_bdf_defaults (host code, no device call) fills Clock_BDF's
+    constructor defaults (clock_bdf.cpp:14-24), the same ones the oracle's
+    restatement uses."""
+    import mapp_b200 as mb
+    from oracle.restated import BDF_DEFAULTS
+
+    o = mb.BdfOpts()
+    mb.load_library().mg_bdf_defaults(ctypes.byref(o))
+    for k, v in BDF_DEFAULTS.items():
+        assert getattr(o, k) == v, k
+
+
 def test_python_mirror_binds_every_entry_point():
     import mapp_b200
 

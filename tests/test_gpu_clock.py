@@ -174,6 +174,10 @@ def test_clock_bdf_errors(tmp_path):
         s.clock_bdf(0)
     with pytest.raises(mb.MGError, match="max_del_t should be larger than min_del_t"):
         s.clock_bdf(2, min_del_t=1.0, max_del_t=0.5)
+    with pytest.raises(mb.MGError, match="initial_del_t should be larger than zero"):
+        s.clock_bdf(2, initial_del_t=0.0)
+    with pytest.raises(mb.MGError, match="max_order above 12"):
+        s.clock_bdf(2, max_order=13)
     tau = rate_scale(w)
     with pytest.raises(mb.MGError, match="min_del_t"):
         s.clock_bdf(5, max_order=2, a_tol=1e-30, initial_del_t=1e-2 * tau, min_del_t=1e-2 * tau,
