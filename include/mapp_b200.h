@@ -9,8 +9,8 @@
  *   Neighbor    (neighbor.h:46-58)    create_list, neighbor_list, no_pairs
  *   Atoms       (atoms.h:255-287)     H / skin / per-atom vectors, update_0, update(c)
  *
- * so a MAPP ForceField subclass can forward its virtuals one-to-one (see
- * INTEGRATION.md).  Conventions:
+ * so a MAPP ForceField subclass can forward its virtuals one-to-one.
+ * Conventions:
  *   - every function returns MG_OK (0) or an MG_ERR_* code; mg_last_error()
  *     returns the message of the last failure on the calling thread (the
  *     reference prints the same text and exits, error.cpp:29-43);
@@ -190,8 +190,12 @@ int mg_mlp_audit(mg_system* s, double* max_err, long long* counts);
    x, type, nbr_off and nbr must be device memory; natms may not exceed
    MG_NOALLOC_MAX_ATOMS (MG_ERR_CAPACITY otherwise).  The first call on a
    device looks up the scratch's device address with that device current, so
-   make it before any stream capture.  Every call shares the scratch and
-   clears the densities it uses: calls that overlap on the GPU race. */
+   make it before any stream capture; under the CUDA runtime's lazy module
+   loading that first lookup may also load the library's device code on that
+   device, which can allocate and synchronise once, so make the first call
+   during set-up.  Later calls allocate nothing.  Every call shares the
+   scratch and clears the densities it uses: calls that overlap on the GPU
+   race. */
 #define MG_NOALLOC_SCRATCH_BYTES (8u << 20)
 #define MG_NOALLOC_MAX_ATOMS 1000000
 

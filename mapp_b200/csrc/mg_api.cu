@@ -221,14 +221,15 @@ struct mg_system {
     size_t scan_tmp_bytes = 0;
     double* stage = nullptr;  // device staging for host arrays
     size_t stage_cap = 0;
-    size_t act_cap = 0;  // capacity of the active-pair sublist (entries)
+    size_t act_cap = 0;   // capacity of the active-pair sublist (entries)
+    size_t nact_cap = 0;  // and of its per-site counts (sites)
     double* red_out = nullptr;  // 8 doubles
     double* d_rhoT = nullptr;
     double* d_phiT = nullptr;
     double* d_FT = nullptr;
     float* d_pkT = nullptr;
     double* d_pk64 = nullptr;
-    float* d_pkC = nullptr;
+    float* d_pkS = nullptr;
     int* cursor = nullptr;
     int crd_built = 0;
     int npair_blocks = 2;
@@ -246,6 +247,9 @@ struct mg_system {
     double t_k[3] = {0, 0, 0};  // DMD force: pass 1, embedding, pass 2
     long long partial_rows = 0;
     bool tables_uploaded = false;  // device tables match the last ff_coef
+    // the last force_calc ran in the precision form, which stores no per-pair
+    // values; c_d_calc and calc_g have them written first (ensure_pair_values)
+    bool prf_stale = false;
     size_t owned_cap = 0, nbr_cap = 0, crdl_cap = 0;  // element capacities of the per-owned-site, ELL and crd buffers
 };
 
@@ -315,6 +319,11 @@ int ensure_atoms(mg_system* s, size_t need, size_t keep)
     CHK(dalloc(&d.t, cap * nt));
     CHK(dalloc(&d.v, cap * nt));
     CHK(dalloc(&d.crd, cap));
+    if (s->dmd) {
+        CHK(dalloc(&d.srec, cap * kSiteRec));
+        CHK(dalloc(&d.dE32, cap * nt));
+        CHK(dalloc(&d.facc, cap * 8));
+    }
     CHK(dalloc(&s->flags, cap));
     CHK(dalloc(&s->offs, cap));
     size_t tb = scan_temp_bytes((int)cap);
@@ -354,6 +363,9 @@ int ensure_compact(mg_system* s, long long npairs)
         CHK(dalloc(&d.pr, (size_t)cap * s->npair_blocks));
         CHK(dalloc(&d.prf, (size_t)cap * s->npair_blocks));
         d.maxp = cap;
+        d.icut_cap = dmd32_icut_capacity(cap);
+        CHK(dalloc(&d.icut, (size_t)d.icut_cap));
+        if (!d.icut_n) CHK(dalloc(&d.icut_n, (size_t)dmd32_icut_warps()));
     }
     s->pair_cap = cap;
     return MG_OK;
@@ -810,13 +822,17 @@ int upload_tables(mg_system* s)
         CHK(dalloc(&s->d_pk64, pk64.size()));
         CU(cudaMemcpy(s->d_pk64, pk64.data(), pk64.size() * sizeof(double), cudaMemcpyHostToDevice));
         d.pk64 = s->d_pk64;
-        // Coarse copy for the precision form's pass 1: kCoarseKnots knots over
+        // The precision form's shared-memory table: kSplitKnots knots over
         // [0, rc], each interval the cubic Hermite piece through the fine
         // spline's value and slope at its ends (fine interpolant evaluated as in
-        // the force kernels, index clamp nr-2 and p <= 1).  With rho and r*phi
-        // decaying over 0.3-0.6 A the two interpolants differ by ~1e-10 relative,
-        // far below FP32 rounding.
-        const int K = kCoarseKnots;
+        // the force kernels, index clamp nr-2 and p <= 1), and a last row of
+        // zeros for |x| >= rc.  The reference's node test, xi_q inside
+        // ((r - rc) sqrt(alpha), (r + rc) sqrt(alpha)) (ff_dmd_I.cpp:198), is
+        // |r - xi_q / sqrt(alpha)| < rc, so a node it rejects reads the zero row
+        // and adds an exact zero without a test.  For the decaying rho and r*phi
+        // of these tables the resampling error is below FP32 rounding already at
+        // 256 knots.
+        const int K = kSplitKnots, ncomp = nt * (nt + 1) / 2;
         const double rc = (nr - 1) * s->dr, hc = rc / (K - 1);
         auto fine = [&](const double* slot, double r, double& v, double& dv) {
             double pp = r * (1.0 / s->dr);
@@ -826,30 +842,33 @@ int upload_tables(mg_system* s)
             v = ((c[3] * p + c[2]) * p + c[1]) * p + c[0];
             dv = ((3.0 * c[3] * p + 2.0 * c[2]) * p + c[1]) * (1.0 / s->dr);
         };
-        auto hermite = [&](const double* slot, int k, float* dst) {
-            double v0, d0, v1, d1;
-            fine(slot, k * hc, v0, d0);
-            fine(slot, std::min((k + 1) * hc, rc), v1, d1);
-            d0 *= hc;
-            d1 *= hc;
-            dst[0] = (float)v0;
-            dst[1] = (float)d0;
-            dst[2] = (float)(3.0 * (v1 - v0) - 2.0 * d0 - d1);
-            dst[3] = (float)(2.0 * (v0 - v1) + d0 + d1);
+        auto resample = [&](const double* slot, float* dst) {
+            for (int k = 0; k < K - 1; k++) {
+                double v0, d0, v1, d1;
+                fine(slot, k * hc, v0, d0);
+                fine(slot, std::min((k + 1) * hc, rc), v1, d1);
+                d0 *= hc;
+                d1 *= hc;
+                float* o = dst + (size_t)k * 4;
+                o[0] = (float)v0;
+                o[1] = (float)d0;
+                o[2] = (float)(3.0 * (v1 - v0) - 2.0 * d0 - d1);
+                o[3] = (float)(2.0 * (v0 - v1) + d0 + d1);
+            }
+            float* o = dst + (size_t)(K - 1) * 4;
+            o[0] = o[1] = o[2] = o[3] = 0.0f;
         };
-        std::vector<float> pc((size_t)nt * nt * K * 8, 0.0f);
+        std::vector<float> ps((size_t)(nt * nt + ncomp) * K * 4, 0.0f);
         for (int a = 0; a < nt; a++)
             for (int b = 0; b < nt; b++)
-                for (int k = 0; k < K - 1; k++) {
-                    float* dst = pc.data() + (((size_t)(a * nt + b) * K + k) * 8);
-                    hermite(s->rhoT.data() + (size_t)(b * nt + a) * nr * 8, k, dst);
-                    if (a >= b) hermite(s->phiT.data() + (size_t)comp_idx(a, b) * nr * 8, k, dst + 4);
-                }
-        CHK(dalloc(&s->d_pkC, pc.size()));
-        CU(cudaMemcpy(s->d_pkC, pc.data(), pc.size() * sizeof(float), cudaMemcpyHostToDevice));
-        d.pkC = reinterpret_cast<const float4*>(s->d_pkC);
-        d.nrC = K;
-        d.drC_inv = (float)(1.0 / hc);
+                resample(s->rhoT.data() + (size_t)(b * nt + a) * nr * 8, ps.data() + (size_t)(a * nt + b) * K * 4);
+        for (int q = 0; q < ncomp; q++)
+            resample(s->phiT.data() + (size_t)q * nr * 8, ps.data() + (size_t)(nt * nt + q) * K * 4);
+        CHK(dalloc(&s->d_pkS, ps.size()));
+        CU(cudaMemcpy(s->d_pkS, ps.data(), ps.size() * sizeof(float), cudaMemcpyHostToDevice));
+        d.pkS = reinterpret_cast<const float4*>(s->d_pkS);
+        d.nrS = K;
+        d.drS_inv = (float)(1.0 / hc);
     }
     d.Fw = s->Fw;
     d.nr = s->nr;
@@ -859,6 +878,19 @@ int upload_tables(mg_system* s)
     d.dr_inv = 1.0 / s->dr;
     d.drho_inv = 1.0 / s->drho;
     s->tables_uploaded = true;
+    return MG_OK;
+}
+
+// c_d_calc and calc_g read the per-pair densities and pair energies of the last
+// force_calc; the precision form's force call does not store them, so they are
+// written here, once, before the first reader (at the current positions: every
+// caller of the boundary runs these at the positions of its last force_calc)
+int ensure_pair_values(mg_system* s)
+{
+    if (!s->prf_stale || s->form != MG_FORM_FP32) return MG_OK;
+    fill_dev_scalars(s);
+    CU(launch_dmd32_pair_values(s->d, s->st));
+    s->prf_stale = false;
     return MG_OK;
 }
 
@@ -944,7 +976,7 @@ int mg_destroy(mg_system* s)
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->st);
     Dev& d = s->d;
-    void* ptrs[] = {d.prf, s->d_pkT, s->d_pk64, s->d_pkC, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
+    void* ptrs[] = {d.prf, s->d_pkT, s->d_pk64, s->d_pkS, d.icut, d.icut_n, d.srec, d.dE32, d.facc, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
                     d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status, d.act_j, d.act_slot, d.nact,
                     s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};
@@ -1290,18 +1322,23 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     Dev& d = s->d;
     fill_dev_scalars(s);
     CHK(timed_begin(s));
-    CU(cudaMemsetAsync(d.f, 0, (size_t)s->natms * s->x_dim * sizeof(double), s->st));
+    // the precision form's first kernel zeroes f and E itself
+    const bool f32 = s->dmd && s->form == MG_FORM_FP32;
+    if (!f32) CU(cudaMemsetAsync(d.f, 0, (size_t)s->natms * s->x_dim * sizeof(double), s->st));
     int rows = 0;
     if (s->style == STYLE_EAM || s->style == STYLE_FS) {
         CU(cudaMemsetAsync(d.rho, 0, (size_t)s->natms * sizeof(double), s->st));
         CU(s->style == STYLE_EAM ? launch_eam_force(d, st_clc, &rows, s->st) : launch_fs_force(d, st_clc, &rows, s->st));
     } else {
-        CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
-        if (s->form == MG_FORM_FP32) CU(launch_dmd_force_f32(d, st_clc, &rows, s->st, s->evk));
-        else if (s->form == MG_FORM_MLP) {
+        if (!f32) CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
+        if (f32) {
+            CU(launch_dmd_force_f32(d, st_clc, &rows, s->st, s->evk));
+            s->prf_stale = true;
+        } else if (s->form == MG_FORM_MLP) {
             CU(cudaMemsetAsync(s->mlp.audit, 0, 16 * sizeof(float), s->st));
             CU(launch_dmd_force_mlp(d, s->mlp, 0x51ed270b3a5d4e1ull + 0x9e37ull * (++s->mlp_calls), st_clc, &rows,
                                     s->st, s->evk));
+            s->prf_stale = false;
         } else
             CU(launch_dmd_force(d, st_clc, &rows, s->st, s->evk));
     }
@@ -1309,8 +1346,12 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     CU(launch_reduce_partials(d, rows, 7, s->red_out, s->st));
     CHK(timed_end(s));
     CU(cudaMemcpyAsync(tot, s->red_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    int icut_over = 0;
+    if (s->dmd && s->form == MG_FORM_FP32)
+        CU(cudaMemcpyAsync(&icut_over, d.status + 4, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CHK(copy_out(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
     CU(cudaStreamSynchronize(s->st));
+    if (icut_over) return fail(MG_ERR_CAPACITY, "precision form: in-cut pair list overflow");
     CHK(timed_read(s, &s->t_force));
     if (s->dmd)
         for (int k = 0; k < 3; k++) {
@@ -1393,6 +1434,7 @@ int mg_ff_c_d_calc(mg_system* s, double* c_d)
     Dev& d = s->d;
     size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
     CHK(timed_begin(s));
+    CHK(ensure_pair_values(s));
     CU(cudaMemsetAsync(d.E, 0, bytes, s->st));
     CU(cudaMemsetAsync(d.c_d, 0, bytes, s->st));
     CU(launch_dmd_cdot(d, s->st));
@@ -1420,6 +1462,7 @@ int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g
     size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
     CU(cudaMemcpyAsync(d.a_in, a, bytes, is_device_ptr(a) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->st));
     CHK(timed_begin(s));
+    CHK(ensure_pair_values(s));
     CU(cudaMemsetAsync(d.E, 0, bytes, s->st));
     int rows = 0;
     CU(launch_dmd_calc_g(d, chk, alpha, &rows, s->st));
@@ -1807,6 +1850,7 @@ int mg::system_enqueue_calc_g(mg_system* s, int chk, double alpha, int* rows)
 {
     if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "calc_g needs a DMD force field");
     if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before calc_g");
+    CHK(ensure_pair_values(s));
     Dev& d = s->d;
     CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
     CU(launch_dmd_calc_g(d, chk, alpha, rows, s->st));
@@ -1825,8 +1869,11 @@ int mg::system_set_active_pairs(mg_system* s, bool on)
     if (cap > s->act_cap) {
         CHK(dalloc(&d.act_j, cap));
         CHK(dalloc(&d.act_slot, cap));
-        CHK(dalloc(&d.nact, (size_t)s->natms));
         s->act_cap = cap;
+    }
+    if ((size_t)s->natms > s->nact_cap) {
+        CHK(dalloc(&d.nact, (size_t)s->natms));
+        s->nact_cap = (size_t)s->natms;
     }
     d.act_on = 0;
     CU(launch_active_pairs(d, s->st));
@@ -1838,6 +1885,7 @@ int mg::system_enqueue_c_d(mg_system* s)
 {
     if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "c_d_calc needs a DMD force field");
     if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before c_d_calc");
+    CHK(ensure_pair_values(s));
     Dev& d = s->d;
     size_t bytes = (size_t)s->natms * s->nt * sizeof(double);
     CU(cudaMemsetAsync(d.E, 0, bytes, s->st));

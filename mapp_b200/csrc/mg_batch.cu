@@ -765,6 +765,10 @@ struct mg_batch {
     DArr<double4> pos, pos0;
     DArr<double> alpha, c, shift, f, E, dE, pr, partial, cell_E, vec, probe_out;
     DArr<float> prf;
+    DArr<int2> icut;       // the precision form's in-cut pair list
+    DArr<float4> srec;     // and its per-site FP32 records
+    DArr<float> dE32, facc;
+    DArr<unsigned> icut_n;
     DArr<int> root, site_cell, pair_i, pair_j, base, nat;
     DArr<unsigned char> active;
     DArr<CellState> state;
@@ -916,8 +920,14 @@ int build_all(mg_batch* b)
     BCHK(b->dE.exact(nall * nt));
     const int nblk = 3 * nt * nt + 3 * nt * (nt + 1) / 2;
     const size_t maxp = (size_t)pair_fill + 1;
-    if (b->form == MG_FORM_FP32) BCHK(b->prf.exact(maxp * nblk));
-    else BCHK(b->pr.exact(maxp * nblk));
+    if (b->form == MG_FORM_FP32) {
+        BCHK(b->icut.exact((size_t)dmd32_icut_capacity((long long)maxp)));
+        BCHK(b->icut_n.exact((size_t)dmd32_icut_warps()));
+        BCHK(b->srec.exact(nall * kSiteRec));
+        BCHK(b->dE32.exact(nall * nt));
+        BCHK(b->facc.exact((size_t)NT * 8));
+    } else
+        BCHK(b->pr.exact(maxp * nblk));
     const long long rows = 2LL * div_up(pair_fill, kFFBlock) + div_up((long long)NT, kFFBlock) + 64;
     BCHK(b->partial.exact((size_t)rows * 8));
     BCHK(b->cell_E.exact((size_t)ncells));
@@ -943,7 +953,13 @@ int build_all(mg_batch* b)
     bd.E = b->E.p;
     bd.dE = b->dE.p;
     bd.pr = b->pr.p;
-    bd.prf = b->prf.p;
+    bd.prf = nullptr;
+    bd.icut = b->icut.p;
+    bd.icut_n = b->icut_n.p;
+    bd.icut_cap = (long long)b->icut.cap;
+    bd.srec = b->srec.p;
+    bd.dE32 = b->dE32.p;
+    bd.facc = b->facc.p;
     bd.partial = b->partial.p;
     bd.form = b->form;
     bd.site_cell = b->site_cell.p;
@@ -1216,6 +1232,11 @@ int mg_batch_destroy(mg_batch* b)
     b->dE.release();
     b->pr.release();
     b->prf.release();
+    b->icut.release();
+    b->srec.release();
+    b->dE32.release();
+    b->facc.release();
+    b->icut_n.release();
     b->partial.release();
     b->cell_E.release();
     b->vec.release();

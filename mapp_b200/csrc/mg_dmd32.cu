@@ -1,20 +1,51 @@
 // Precision form (MG_FORM_FP32) of ForceField_DMD_I/II/DMD::force_calc
 // (ff_dmd_I.cpp:88-450): the per-pair work -- pair geometry after the cut
 // test, the Gauss-Hermite smearing, the spline lookups and the force
-// projections -- runs in FP32; per-site density and force sums are
-// compensated; the cut test on rsq, the per-site embedding F(E) and the energy
-// and virial totals stay FP64.
+// projections -- runs in FP32; per-site density and force sums are carried in
+// FP64; the cut test on rsq, the per-site embedding F(E) and the energy and
+// virial totals stay FP64.
 //
-// Tables: one 32-byte sector per ordered species pair (a,b) and knot,
-// {rho c0..c3 of density slot b*nt+a, phi c0..c3 of slot COMP(a,b)}, so a
-// quadrature node costs one sector where the FP64 form needs two.
+// Structure of one force call (no per-pair array reaches HBM):
+//   k_dmd32_dens   densities only: per listed pair the cut test, then for the
+//                  in-cut pairs the value of the smeared density of every
+//                  ordered species pair (ff_dmd_I.cpp:178-230, weights w0
+//                  only).  A warp queues its in-cut pairs in shared memory and
+//                  evaluates them 32 at a time, so no lane idles on a pair
+//                  beyond the cut; each full batch of 32 is also appended to
+//                  the in-cut pair list `icut` (padded with i = -1).
+//   k_dmd32_embed  F(E), F'(E), entropy and alpha terms per site (FP64).
+//   k_dmd32_force  per batch of `icut`: the smearing again, now with all three
+//                  weight sets and the pair function, giving the per-pair
+//                  derivatives the reference stores (ff_dmd_I.cpp:231-259),
+//                  projected at once onto the forces (ff_dmd_I.cpp:357-436);
+//                  pair energy and virial.
+// Recomputing the smearing costs one table pass over the in-cut pairs; it
+// replaces the reference's per-pair buffers (21 values per pair for two
+// species), which in FP32 would move about 84 B per listed pair through HBM
+// twice per call.  c_d_calc and calc_g read the per-pair densities and pair
+// energies of the last force_calc; after a precision-form force call they are
+// written on demand by k_dmd32_fill (launch_dmd32_pair_values).
 //
-// Per-site sums: a site's i-side pairs are summed inside the warp with TwoSum
-// (error-free addition) steps, and every contribution is accumulated into the
-// site's FP64 density / force with a fire-and-forget atomic add.  A Kahan
-// (sum, compensation) float pair would need a compare-and-swap round trip per
-// update, which measured 1.5x slower for the whole force call; the FP64
-// accumulator is at least as accurate.
+// Tables: the splines resampled onto kSplitKnots knots over [0, rc] (cubic
+// Hermite pieces through the fine spline's value and slope, FP32) and held in
+// shared memory, one float4 {c0..c3} per knot and slot: the rho slots of the
+// ordered species pairs first (slot a*nt+b holds density slot b*nt+a), then
+// the phi slots in COMP order; row K-1 of a slot is zero, so a quadrature
+// node the reference rejects (|r - xi_q / sqrt(alpha)| >= rc) adds an exact
+// zero without a test.  Rho and phi are separate slots so the 16-byte knot
+// loads of a warp spread over all eight bank groups.
+//
+// Per-site sums: densities are FP64 throughout -- a warp's i-side
+// contributions summed by segmented FP64 shuffles (pairs are in i order
+// inside a batch) and added with one FP64 atomic per site and batch, j-side
+// contributions FP64 atomics; an FP64 accumulator of FP32 terms keeps more
+// bits than a Kahan-compensated FP32 sum and needs no compare-and-swap loop.
+// Forces: i-side runs summed in FP32 over at most 32 terms, then one FP64
+// atomic per site and batch; j-side FP32 vector reductions into a per-site
+// FP32 buffer that k_dmd32_fmerge adds to the FP64 forces.
+#include <mutex>
+#include <unordered_map>
+
 #include "mg_reduce.cuh"
 #include "mg_dmd_common.cuh"
 
@@ -23,6 +54,18 @@ namespace {
 
 #ifndef MG_DMD32_MINB
 #define MG_DMD32_MINB 4
+#endif
+// resident 256-thread blocks per SM the two precision-form pair passes are
+// compiled for (bounds their registers)
+#if defined(MG_DENS_MINB) && MG_DENS_MINB > 0
+#define MG_DENS_BOUNDS __launch_bounds__(kFFBlock, MG_DENS_MINB)
+#else
+#define MG_DENS_BOUNDS __launch_bounds__(kFFBlock)
+#endif
+#if defined(MG_FORCE_MINB) && MG_FORCE_MINB > 0
+#define MG_FORCE_BOUNDS __launch_bounds__(kFFBlock, MG_FORCE_MINB)
+#else
+#define MG_FORCE_BOUNDS __launch_bounds__(kFFBlock)
 #endif
 
 // Accumulate a compensated (hi, lo) FP32 value into an FP64 per-site sum.
@@ -53,105 +96,638 @@ __device__ __forceinline__ float2 seg_sum2(float v, const Seg& s)
     return make_float2(hi, lo);
 }
 
-// ---- pass 1: FP32 smearing, compensated densities -------------------------
-// kSmem = 1: the coarse table (d.pkC) is copied into shared memory first and
-// every knot of the quadrature is read from there, one 1024-thread block per
-// SM; kSmem = 0: the fine packed table through L1 / L2.
-template <int NT, int NQ, int kSmem>
-__global__ void __launch_bounds__(kSmem ? 1024 : kFFBlock, kSmem ? 1 : MG_DMD32_MINB) k_dmd32_pass1(Dev d, int row0)
+// Segments of a warp whose keys are sorted (equal keys in contiguous lanes,
+// padding lanes with key -1 at the end): boundaries from one shuffle and one
+// ballot instead of a match instruction.
+__device__ __forceinline__ Seg seg_sorted(int key)
 {
-    using S = Slots<NT>;
-    extern __shared__ float4 tab_sh[];
     const int lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const size_t mp = (size_t)d.maxp;
-    F32Consts kc = f32_consts(d);
-    const float4* tab = d.pkT;
-    if (kSmem) {
-        const int n4 = NT * NT * d.nrC * 2;
-        for (int k = threadIdx.x; k < n4; k += blockDim.x) tab_sh[k] = __ldg(d.pkC + k);
-        __syncthreads();
-        tab = tab_sh;
-        kc.nr = d.nrC;
-        kc.dr_inv = d.drC_inv;
-        kc.top = (float)(d.nrC - 1);
-        kc.top_m = (float)(d.nrC - 2);
-    }
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < d.npairs; base += stride) {
-        long long p = base + lane;
-        bool valid = p < d.npairs;
-        int i = valid ? d.pair_i[p] : -1;
-        float Ei[NT];
+    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
+    const unsigned upto = heads & (0xffffffffu >> (31 - lane));  // heads at or before this lane
+    const unsigned after = heads & ~(0xffffffffu >> (31 - lane));
+    Seg sg;
+    sg.first = 31 - __clz(upto);
+    sg.last = after ? __ffs(after) - 2 : 31;
+    return sg;
+}
+
+// FP32 sum over the caller's segment (first lane of the segment receives it)
+__device__ __forceinline__ float seg_sumf(float v, const Seg& s)
+{
+    const int lane = threadIdx.x & 31;
 #pragma unroll
-        for (int a = 0; a < NT; a++) Ei[a] = 0.0f;
-        const bool act = valid && site_active(d, i);
-        double epair = 0.0;
-        if (act) {
-            int j = d.pair_j[p];
-            double4 xi = d.pos[i], xj = d.pos[j];
-            float ai[NT], ci[NT], aj[NT], cj[NT], Ej[NT];
+    for (int o = 1; o < 32; o <<= 1) {
+        const float t = __shfl_down_sync(0xffffffffu, v, o);
+        if (lane + o <= s.last) v += t;
+    }
+    return v;
+}
+
+// a site position as one 32-byte read-only load
+__device__ __forceinline__ double4 pos_ld(const Dev& d, int i)
+{
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(d.pos + i));
+    return r;
+}
+
+// ---- split-table smearing ---------------------------------------------------
+
+struct SplitK {
+    float rc, dr_inv, top, alpha_min, alpha_max;
+};
+
+__device__ __forceinline__ SplitK split_consts(const Dev& d)
+{
+    SplitK k;
+    k.rc = (float)d.rc;
+    k.dr_inv = d.drS_inv;
+    k.top = (float)(d.nrS - 1);
+    k.alpha_min = (float)d.alpha_min;
+    k.alpha_max = (float)d.alpha_max;
+    return k;
+}
+
+// knot row and fraction of |x| on the split table: p = min(|x| / h, K - 1),
+// row = floor(p) by a round-down add against 1.5 * 2^23 (exact for
+// 0 <= p < 2^22; FP32 pipe, no conversion instruction), t = p - row in [0, 1)
+struct Knot {
+    int row;
+    float t;
+};
+
+__device__ __forceinline__ Knot knot_at(float x, const SplitK& k)
+{
+    const float p = fminf(fabsf(x) * k.dr_inv, k.top);
+    const float f = __fadd_rd(p, 12582912.0f);
+    Knot r;
+    r.row = __float_as_int(f) - 0x4B400000;
+    r.t = p - (f - 12582912.0f);
+    return r;
+}
+
+__device__ __forceinline__ float horner(const float4 c, float t) { return fmaf(fmaf(fmaf(c.w, t, c.z), t, c.y), t, c.x); }
+
+__device__ __forceinline__ float horner_d(const float4 c, float t)
+{
+    return fmaf(fmaf(3.0f * c.w, t, 2.0f * c.z), t, c.y);
+}
+
+// v with the sign of t (the odd extension of r*phi, ff_dmd_I.cpp:214-215):
+// one bit operation
+__device__ __forceinline__ float with_sign_of(float v, float t)
+{
+    return __int_as_float(__float_as_int(v) ^ (__float_as_int(t) & 0x80000000));
+}
+
+// Node positions t_q = r - xi_q / sqrt(alpha) of the quadrature.  The
+// reference's node test (ff_dmd_I.cpp:198) is |t_q| < rc; the table's zero
+// row for |x| >= rc makes a rejected node add an exact zero, so no node is
+// tested.  NQ = 3: three nodes whose middle one is 0, so it sits at r (knot
+// k0); NQ = 0: d.nq nodes.
+//
+// kInRange: the caller has established alpha_min < alpha < alpha_max.
+
+// Value of the smeared density of one ordered species pair (rho slot tr).
+template <int NQ, bool kInRange>
+__device__ __forceinline__ float dens_value(const Dev& d, const float4* tr, const SplitK& k, float r, float r_inv,
+                                            bool below_rc, float alpha, const Knot& k0)
+{
+    if (kInRange || (k.alpha_min < alpha && alpha < k.alpha_max)) {
+        const float ias = rsqrtf(alpha);
+        float ga;
+        if (NQ == 3) {
+            const float tm = fmaf(-d.xi_f[0], ias, r), tp = fmaf(-d.xi_f[2], ias, r);
+            const Knot km = knot_at(tm, k), kp = knot_at(tp, k);
+            ga = d.w0_f[0] * (horner(tr[km.row], km.t) * tm);
+            ga = fmaf(d.w0_f[1], horner(tr[k0.row], k0.t) * r, ga);
+            ga = fmaf(d.w0_f[2], horner(tr[kp.row], kp.t) * tp, ga);
+        } else {
+            ga = 0.0f;
+            for (int q = 0; q < d.nq; q++) {
+                const float t0 = fmaf(-d.xi_f[q], ias, r);
+                const Knot kq = knot_at(t0, k);
+                ga = fmaf(d.w0_f[q], horner(tr[kq.row], kq.t) * t0, ga);
+            }
+        }
+        return ga * kPiInSqF * r_inv;
+    }
+    if (k.alpha_max <= alpha && below_rc) return horner(tr[k0.row], k0.t);
+    return 0.0f;
+}
+
+// Value of the smeared r*phi of one species pair (phi slot tp) over r: the
+// pair energy term of ff_dmd_I.cpp:226-231 (values only).
+template <int NQ>
+__device__ __forceinline__ float phi_value(const Dev& d, const float4* tp, const SplitK& k, float r, float r_inv,
+                                           bool below_rc, float alpha, const Knot& k0)
+{
+    if (k.alpha_min < alpha && alpha < k.alpha_max) {
+        const float ias = rsqrtf(alpha);
+        float fa = 0.0f;
+        const int nq = NQ == 3 ? 3 : d.nq;
+        for (int q = 0; q < (NQ == 3 ? 3 : kMaxQuad); q++) {
+            if (q >= nq) break;
+            const float t0 = (NQ == 3 && q == 1) ? r : fmaf(-d.xi_f[q], ias, r);
+            const Knot kq = (NQ == 3 && q == 1) ? k0 : knot_at(t0, k);
+            fa = fmaf(d.w0_f[q], with_sign_of(horner(tp[kq.row], kq.t), t0), fa);
+        }
+        return fa * kPiInSqF * r_inv;
+    }
+    if (k.alpha_max <= alpha && below_rc) return horner(tp[k0.row], k0.t) * r_inv;
+    return 0.0f;
+}
+
+// value and r / alpha derivatives of one smeared function
+struct VDer {
+    float v, dr, da;
+};
+
+// Full smearing of one ordered species pair (ff_dmd_I.cpp:178-310): the rho
+// slot tr always, the phi slot tp when kPhi; values and both derivatives with
+// the reference's closing algebra (ff_dmd_I.cpp:231-259, 261-310).
+template <int NQ, bool kPhi, bool kInRange>
+__device__ __forceinline__ void smear_full(const Dev& d, const float4* tr, const float4* tp, const SplitK& k, float r,
+                                           float r_inv, bool below_rc, float alpha, const Knot& k0, VDer& g, VDer& f)
+{
+    g.v = g.dr = g.da = 0.0f;
+    f.v = f.dr = f.da = 0.0f;
+    if (kInRange || (k.alpha_min < alpha && alpha < k.alpha_max)) {
+        const float ias = rsqrtf(alpha), as = alpha * ias, inv_alpha = ias * ias;
+        float ga = 0.f, gb = 0.f, gc = 0.f, fa = 0.f, fb = 0.f, fc = 0.f;
+        const int nq = NQ == 3 ? 3 : d.nq;
+#pragma unroll
+        for (int q = 0; q < (NQ == 3 ? 3 : kMaxQuad); q++) {
+            if (NQ != 3 && q >= nq) break;
+            const float t0 = (NQ == 3 && q == 1) ? r : fmaf(-d.xi_f[q], ias, r);
+            const Knot kq = (NQ == 3 && q == 1) ? k0 : knot_at(t0, k);
+            const float vr = horner(tr[kq.row], kq.t) * t0;
+            ga = fmaf(d.w0_f[q], vr, ga);
+            gb = fmaf(d.w1_f[q], vr, gb);
+            gc = fmaf(d.w2_f[q], vr, gc);
+            if (kPhi) {
+                const float vp = with_sign_of(horner(tp[kq.row], kq.t), t0);
+                fa = fmaf(d.w0_f[q], vp, fa);
+                fb = fmaf(d.w1_f[q], vp, fb);
+                fc = fmaf(d.w2_f[q], vp, fc);
+            }
+        }
+        const float sc = kPiInSqF * r_inv;
+        g.v = ga * sc;
+        g.dr = fmaf(-g.v, r_inv, -2.0f * as * (gb * sc));
+        g.da = fmaf(0.5f, g.v, -gc * sc) * inv_alpha;
+        if (kPhi) {
+            f.v = fa * sc;
+            f.dr = fmaf(-f.v, r_inv, -2.0f * as * (fb * sc));
+            f.da = fmaf(0.5f, f.v, -fc * sc) * inv_alpha;
+        }
+        return;
+    }
+    if (k.alpha_max <= alpha && below_rc) {
+        const float4 cr = tr[k0.row];
+        g.v = horner(cr, k0.t);
+        g.dr = horner_d(cr, k0.t) * k.dr_inv;
+        if (kPhi) {
+            const float4 cp = tp[k0.row];
+            const float z2 = horner(cp, k0.t), z2p = horner_d(cp, k0.t) * k.dr_inv;
+            f.v = z2 * r_inv;
+            f.dr = (z2p - z2 * r_inv) * r_inv;
+        }
+    }
+}
+
+// copies the first nslots slots of the split table into shared memory
+__device__ __forceinline__ void load_split_table(const Dev& d, float4* sh, int nslots)
+{
+    const int n = nslots * d.nrS;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) sh[k] = __ldg(d.pkS + k);
+    __syncthreads();
+}
+
+// alpha and c of site j from its FP32 record (srec: {alpha_0.., c_0..})
+template <int NT>
+__device__ __forceinline__ void load_rec(const Dev& d, int j, float (&al)[NT], float (&cc)[NT])
+{
+    float v[8];
+    const float4 r0 = __ldg(d.srec + (size_t)j * kSiteRec);
+    v[0] = r0.x;
+    v[1] = r0.y;
+    v[2] = r0.z;
+    v[3] = r0.w;
+    if (2 * NT > 4) {
+        const float4 r1 = __ldg(d.srec + (size_t)j * kSiteRec + 1);
+        v[4] = r1.x;
+        v[5] = r1.y;
+        v[6] = r1.z;
+        v[7] = r1.w;
+    }
+#pragma unroll
+    for (int a = 0; a < NT; a++) {
+        al[a] = v[a];
+        cc[a] = v[NT + a];
+    }
+}
+
+// ---- set-up of a precision-form force call ----------------------------------
+// the FP32 site records of every site (owned + ghost); for the owned sites
+// being evaluated, f, E and the j-side force sums zeroed; the in-cut list
+// emptied
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_dmd32_prep(Dev d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) d.status[4] = 0;
+    if (i < d.nall) {
+        float v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            v[a] = (float)d.alpha[(size_t)i * NT + a];
+            v[NT + a] = (float)d.c[(size_t)i * NT + a];
+        }
+        d.srec[(size_t)i * kSiteRec] = make_float4(v[0], v[1], v[2], v[3]);
+        if (2 * NT > 4) d.srec[(size_t)i * kSiteRec + 1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+    if (i < d.natms && site_active(d, i)) {
+        for (int q = 0; q < d.x_dim; q++) d.f[(size_t)i * d.x_dim + q] = 0.0;
+#pragma unroll
+        for (int a = 0; a < NT; a++) d.E[(size_t)i * NT + a] = 0.0;
+        reinterpret_cast<float4*>(d.facc)[(size_t)i * 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+        reinterpret_cast<float4*>(d.facc)[(size_t)i * 2 + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// the j-side FP32 force sums added to the FP64 forces
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_dmd32_fmerge(Dev d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.natms || !site_active(d, i)) return;
+    const float4 a = reinterpret_cast<const float4*>(d.facc)[(size_t)i * 2];
+    const float4 b = reinterpret_cast<const float4*>(d.facc)[(size_t)i * 2 + 1];
+    const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    double* f = d.f + (size_t)i * d.x_dim;
+#pragma unroll
+    for (int q = 0; q < 3 + NT; q++) f[q] += (double)v[q];
+}
+
+// ---- pass A: densities, in-cut pair list ------------------------------------
+constexpr int kQueue = 64;  // per-warp queue of in-cut pairs (two batches)
+
+template <int NT, int NQ>
+__global__ void MG_DENS_BOUNDS k_dmd32_dens(Dev d, int K)
+{
+    extern __shared__ float4 tab[];
+    __shared__ int2 q_ij[kFFWarps][kQueue];
+    __shared__ float q_r[kFFWarps][kQueue];
+    load_split_table(d, tab, NT * NT);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const SplitK k = split_consts(d);
+    const float cut_sq_f = (float)d.cut_sq;
+    const long long stride = (long long)gridDim.x * kFFBlock;
+    long long base = (long long)blockIdx.x * kFFBlock + w * 32;  // this warp's chunk of 32 listed pairs
+    int cnt = 0;                                                 // queued in-cut pairs (warp-uniform)
+    // this warp's region of the in-cut list: K batches of 32 (it tests at most
+    // K chunks of 32 listed pairs), filled from the start; the batch count goes
+    // to icut_n[warp]
+    const int wg = blockIdx.x * kFFWarps + w;
+    int2* region = d.icut + (size_t)wg * K * 32;
+    int nbt = 0;
+    // Software pipeline over this warp's chunks: while a batch is evaluated,
+    // the positions of the next chunk and the pair indices of the one after
+    // are already in flight (a chunk's cut test needs pair -> site -> position,
+    // two dependent gathers).  A lane's j is -1 when it has no pair to test.
+    auto load_idx = [&](long long b, int& i, int& j) {
+        const long long p = b + lane;
+        i = -1;
+        j = -1;
+        if (p < d.npairs) {
+            i = d.pair_i[p];
+            if (site_active(d, i)) j = d.pair_j[p];
+        }
+    };
+    int i1, j1, i2, j2;
+    load_idx(base, i1, j1);
+    double4 xi1 = make_double4(0, 0, 0, 0), xj1 = xi1;
+    if (j1 >= 0) {
+        xi1 = pos_ld(d, i1);
+        xj1 = pos_ld(d, j1);
+    }
+    load_idx(base + stride, i2, j2);
+    while (true) {
+        const bool have = base < d.npairs;
+        if (have) {
+            bool in = false;
+            float rsqf = 0.f;
+            if (j1 >= 0) {
+                const double dx0 = xi1.x - xj1.x, dx1 = xi1.y - xj1.y, dx2 = xi1.z - xj1.z;
+                const double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
+                in = rsq < d.cut_sq_mod;
+                rsqf = (float)rsq;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, in);
+            if (in) {
+                const int slot = cnt + __popc(m & lt);
+                q_ij[w][slot] = make_int2(i1, j1);
+                q_r[w][slot] = rsqf;
+            }
+            cnt += __popc(m);
+            __syncwarp();
+        }
+        // advance the pipeline by one chunk
+        i1 = i2;
+        j1 = j2;
+        if (j1 >= 0) {
+            xi1 = pos_ld(d, i1);
+            xj1 = pos_ld(d, j1);
+        }
+        load_idx(base + 2 * stride, i2, j2);
+        const bool done = !have || base + stride >= d.npairs;
+        // evaluate full batches, and the last partial one once this warp has no chunk left
+        while (cnt >= 32 || (done && cnt > 0)) {
+            const int nb = min(cnt, 32);
+            const bool on = lane < nb;
+            const int2 e = on ? q_ij[w][lane] : make_int2(-1, -1);
+            const float rsqf = on ? q_r[w][lane] : 1.0f;
+            __syncwarp();
+            if (lane < cnt - nb) {
+                q_ij[w][lane] = q_ij[w][nb + lane];
+                q_r[w][lane] = q_r[w][nb + lane];
+            }
+            __syncwarp();
+            cnt -= nb;
+            // append the batch, padded to 32 with i = -1, to this warp's region
+            if (nbt < K) region[(size_t)nbt * 32 + lane] = e;
+            else if (lane == 0) d.status[4] = 1;
+            nbt++;
+            float Ei[NT], Ej[NT], ci[NT], cj[NT], al[NT * NT];
+            float r = 1.0f, r_inv = 1.0f;
+            bool below_rc = false, inr = true;
+#pragma unroll
+            for (int a = 0; a < NT; a++) Ei[a] = Ej[a] = ci[a] = cj[a] = 0.0f;
+#pragma unroll
+            for (int q = 0; q < NT * NT; q++) al[q] = 0.0f;
+            if (on) {
+                float ai[NT], aj[NT];
+                load_rec<NT>(d, e.x, ai, ci);
+                load_rec<NT>(d, e.y, aj, cj);
+                r_inv = rsqrtf(rsqf);
+                r = rsqf * r_inv;
+                below_rc = rsqf < cut_sq_f;
+#pragma unroll
+                for (int a = 0; a < NT; a++)
+#pragma unroll
+                    for (int b = 0; b < NT; b++) {
+                        const float alpha = __fdividef(ai[a] * aj[b], ai[a] + aj[b]);
+                        al[a * NT + b] = alpha;
+                        inr = inr && k.alpha_min < alpha && alpha < k.alpha_max;
+                    }
+            }
+            // every lane's species pairs inside the smeared range: no branches
+            const bool fast = __all_sync(0xffffffffu, inr);
+            if (on) {
+                const Knot k0 = knot_at(r, k);
+#pragma unroll
+                for (int a = 0; a < NT; a++)
+#pragma unroll
+                    for (int b = 0; b < NT; b++) {
+                        const float4* tr = tab + (size_t)(a * NT + b) * d.nrS;
+                        const float g0 = fast ? dens_value<NQ, true>(d, tr, k, r, r_inv, below_rc, al[a * NT + b], k0)
+                                              : dens_value<NQ, false>(d, tr, k, r, r_inv, below_rc, al[a * NT + b], k0);
+                        Ei[a] = fmaf(g0, cj[b], Ei[a]);
+                        Ej[b] = fmaf(g0, ci[a], Ej[b]);
+                    }
+                if (e.y < d.natms) {
+#pragma unroll
+                    for (int b = 0; b < NT; b++)
+                        if (Ej[b] != 0.0f) atomicAdd(&d.E[(size_t)e.y * NT + b], (double)Ej[b]);
+                }
+            }
+            const Seg sg = seg_sorted(e.x);
 #pragma unroll
             for (int a = 0; a < NT; a++) {
-                ai[a] = (float)d.alpha[(size_t)i * NT + a];
-                ci[a] = (float)d.c[(size_t)i * NT + a];
-                aj[a] = (float)d.alpha[(size_t)j * NT + a];
-                cj[a] = (float)d.c[(size_t)j * NT + a];
-                Ej[a] = 0.0f;
+                const double t = seg_sum((double)Ei[a], sg);
+                if (on && lane == sg.first && t != 0.0) atomicAdd(&d.E[(size_t)e.x * NT + a], t);
             }
-            double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
-            double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
-            bool own_j = j < d.natms;
-            bool in_cut = rsq < d.cut_sq_mod;
-            bool below_rc = rsq < d.cut_sq;
-            float rsqf = (float)rsq;
-            float r_inv = rsqrtf(rsqf);
-            float r = rsqf * r_inv;
-            double w = own_j ? 0.5 : 0.25;
-            float* out = d.prf + p;
+        }
+        if (done) break;
+        base += stride;
+    }
+    if (lane == 0) d.icut_n[wg] = (unsigned)min(nbt, K);
+}
+
+// ---- pass B: smearing with derivatives, forces, pair energy, virial ---------
+template <int NT, int NQ>
+__global__ void MG_FORCE_BOUNDS k_dmd32_force(Dev d, int st_clc, int row0, int W, int K)
+{
+    using S = Slots<NT>;
+    extern __shared__ float4 tab[];
+    load_split_table(d, tab, NT * NT + S::NC);
+    const int lane = threadIdx.x & 31;
+    const SplitK k = split_consts(d);
+    const float cut_sq_f = (float)d.cut_sq;
+    // slots (region rg, batch b) of the density pass's W regions of K
+    // batches, region by region (region-major spreads the warps running
+    // together over the system, so their j-side reductions seldom meet on the
+    // same sites; batch-major measured slower)
+    const long long nslot = (long long)W * K;
+    const long long wstride = (long long)gridDim.x * kFFWarps;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    // this thread's virial terms (a few dozen pairs) in FP32; the block and
+    // grid totals are FP64
+    float vir[6] = {0, 0, 0, 0, 0, 0};
+    for (long long t = (long long)blockIdx.x * kFFWarps + (threadIdx.x >> 5); t < nslot; t += wstride) {
+        const long long rg = t / K;
+        if (t - rg * K >= (long long)__ldg(d.icut_n + rg)) continue;  // past the region's last batch
+        const int2 e = d.icut[t * 32 + lane];
+        const bool on = e.x >= 0;
+        float fi[3 + NT];
+#pragma unroll
+        for (int q = 0; q < 3 + NT; q++) fi[q] = 0.0f;
+        double epair = 0.0;
+        float ai[NT], ci[NT], aj[NT], cj[NT], al[NT * NT];
+        bool inr = true;
+#pragma unroll
+        for (int a = 0; a < NT; a++) ai[a] = ci[a] = aj[a] = cj[a] = 0.0f;
+#pragma unroll
+        for (int q = 0; q < NT * NT; q++) al[q] = 0.0f;
+        if (on) {
+            load_rec<NT>(d, e.x, ai, ci);
+            load_rec<NT>(d, e.y, aj, cj);
+#pragma unroll
+            for (int a = 0; a < NT; a++)
+#pragma unroll
+                for (int b = 0; b < NT; b++) {
+                    const float alpha = __fdividef(ai[a] * aj[b], ai[a] + aj[b]);
+                    al[a * NT + b] = alpha;
+                    inr = inr && k.alpha_min < alpha && alpha < k.alpha_max;
+                }
+        }
+        // every lane's species pairs inside the smeared range: no branches
+        const bool fast = __all_sync(0xffffffffu, inr);
+        if (on) {
+            const int i = e.x, j = e.y;
+            const double4 xi = pos_ld(d, i), xj = pos_ld(d, j);
+            const float dx0 = (float)(xi.x - xj.x), dx1 = (float)(xi.y - xj.y), dx2 = (float)(xi.z - xj.z);
+            const float rsqf = fmaf(dx2, dx2, fmaf(dx1, dx1, dx0 * dx0));
+            const float r_inv = rsqrtf(rsqf), r = rsqf * r_inv;
+            const bool below_rc = rsqf < cut_sq_f;
+            const bool own_j = j < d.natms;
+            const int oj = owner(d, j);
+            float dEi[NT], dEj[NT];
+            if (NT == 2) {
+                const float2 ei = __ldg(reinterpret_cast<const float2*>(d.dE32) + i);
+                const float2 ej = __ldg(reinterpret_cast<const float2*>(d.dE32) + oj);
+                dEi[0] = ei.x;
+                dEi[NT - 1] = ei.y;
+                dEj[0] = ej.x;
+                dEj[NT - 1] = ej.y;
+            } else {
+#pragma unroll
+                for (int a = 0; a < NT; a++) {
+                    dEi[a] = __ldg(d.dE32 + (size_t)i * NT + a);
+                    dEj[a] = __ldg(d.dE32 + (size_t)oj * NT + a);
+                }
+            }
+            const Knot k0 = knot_at(r, k);
+            // the per-pair derivatives the reference stores, in its slot order
+            float drr[NT * NT], dra[NT * NT], dpr[S::NC], dpa[S::NC];
+            float ep = 0.0f;
 #pragma unroll
             for (int a = 0; a < NT; a++)
 #pragma unroll
                 for (int b = 0; b < NT; b++) {
                     const int rs = b * NT + a, ps = comp_idx(a, b);
-                    const float4* pk = tab + (size_t)(a * NT + b) * kc.nr * 2;
-                    float g0 = 0, gdr = 0, gda = 0, f0 = 0, fdr = 0, fda = 0;
-                    bool hit = false;
-                    if (in_cut) {
-                        float alpha = __fdividef(ai[a] * aj[b], ai[a] + aj[b]);
-                        hit = (a >= b) ? smear_f<true, NQ, kSmem != 0>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr,
-                                                                      gda, f0, fdr, fda)
-                                       : smear_f<false, NQ, kSmem != 0>(d, kc, pk, r, r_inv, below_rc, alpha, g0, gdr,
-                                                                       gda, f0, fdr, fda);
+                    const float alpha = al[a * NT + b];
+                    const float4* tr = tab + (size_t)(a * NT + b) * d.nrS;
+                    const float4* tp = tab + (size_t)(NT * NT + ps) * d.nrS;
+                    VDer g, f;
+                    if (fast) {
+                        if (a >= b) smear_full<NQ, true, true>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
+                        else smear_full<NQ, false, true>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
+                    } else {
+                        if (a >= b) smear_full<NQ, true, false>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
+                        else smear_full<NQ, false, false>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
                     }
-                    if (!hit) g0 = gdr = gda = f0 = fdr = fda = 0.0f;
-                    __stcs(out + (S::RHO + rs) * mp, g0);
-                    __stcs(out + (S::DRR + rs) * mp, gdr);
-                    __stcs(out + (S::DRA + rs) * mp, gda);
+                    drr[rs] = g.dr;
+                    dra[rs] = g.da;
                     if (a >= b) {
-                        __stcs(out + (S::PHI + ps) * mp, f0);
-                        __stcs(out + (S::DPR + ps) * mp, fdr);
-                        __stcs(out + (S::DPA + ps) * mp, fda);
-                        epair += w * (double)((cj[b] * ci[a] + cj[a] * ci[b]) * f0);
+                        dpr[ps] = f.dr;
+                        dpa[ps] = f.da;
+                        ep = fmaf(cj[b] * ci[a] + cj[a] * ci[b], f.v, ep);
                     }
-                    Ei[a] += g0 * cj[b];
-                    Ej[b] += g0 * ci[a];
                 }
-            if (own_j && in_cut) {
+            epair = (own_j ? 0.5 : 0.25) * (double)ep;
+            // projections (ff_dmd_I.cpp:370-392)
+            float fj[NT];
+            float fsum = 0.0f;
 #pragma unroll
-                for (int b = 0; b < NT; b++) acc_add(&d.E[(size_t)j * NT + b], Ej[b], 0.0f);
+            for (int b = 0; b < NT; b++) fj[b] = 0.0f;
+#pragma unroll
+            for (int a = 0; a < NT; a++)
+#pragma unroll
+                for (int b = 0; b < NT; b++) {
+                    const int ab = a * NT + b, ba = b * NT + a, ps = comp_idx(a, b);
+                    const float cc = ci[a] * cj[b];
+                    const float fpair = -(drr[ab] * dEi[a] + drr[ba] * dEj[b] + dpr[ps]) * cc * r_inv;
+                    const float sa = ai[a] + aj[b];
+                    const float apair = -(dra[ab] * dEi[a] + dra[ba] * dEj[b] + dpa[ps]) * __fdividef(cc, sa * sa);
+                    fsum += fpair;
+                    fi[3 + a] = fmaf(apair, aj[b] * aj[b], fi[3 + a]);
+                    fj[b] = fmaf(apair, ai[a] * ai[a], fj[b]);
+                }
+            fi[0] = dx0 * fsum;
+            fi[1] = dx1 * fsum;
+            fi[2] = dx2 * fsum;
+            if (st_clc) {
+                const float wf = (own_j ? 1.0f : 0.5f) * fsum;
+                vir[0] = fmaf(-wf, dx0 * dx0, vir[0]);
+                vir[1] = fmaf(-wf, dx1 * dx1, vir[1]);
+                vir[2] = fmaf(-wf, dx2 * dx2, vir[2]);
+                vir[3] = fmaf(-wf, dx1 * dx2, vir[3]);
+                vir[4] = fmaf(-wf, dx2 * dx0, vir[4]);
+                vir[5] = fmaf(-wf, dx0 * dx1, vir[5]);
+            }
+            if (own_j) {
+                // j-side sums in FP32, vector reductions (merged into f by k_dmd32_fmerge)
+                float4* fo = reinterpret_cast<float4*>(d.facc) + (size_t)j * 2;
+                atomicAdd(fo, make_float4(-dx0 * fsum, -dx1 * fsum, -dx2 * fsum, fj[0]));
+                if (NT == 2) atomicAdd(reinterpret_cast<float*>(fo + 1), fj[NT - 1]);
+                else if (NT > 2) {
+                    float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+                    t.x = fj[1 % NT];
+                    if (NT > 2) t.y = fj[2 % NT];
+                    if (NT > 3) t.z = fj[3 % NT];
+                    atomicAdd(fo + 1, t);
+                }
             }
         }
-        Seg sg = seg_of(i);
+        // i-side forces: FP32 sums over the batch's run of each site (at most 32
+        // terms, tree order), one FP64 atomic per site and component
+        const Seg sg = seg_sorted(e.x);
 #pragma unroll
-        for (int a = 0; a < NT; a++) {
-            float2 t = seg_sum2(Ei[a], sg);
-            if (valid && lane == sg.first) acc_add(&d.E[(size_t)i * NT + a], t.x, t.y);
+        for (int q = 0; q < 3 + NT; q++) {
+            const float t = seg_sumf(fi[q], sg);
+            if (on && lane == sg.first && t != 0.0f) atomicAdd(d.f + (size_t)e.x * d.x_dim + q, (double)t);
         }
-        if (d.site_cell) cell_energy_add(d, valid ? i : -1, epair);
+        if (d.site_cell) cell_energy_add(d, on ? e.x : -1, epair);
         else acc[0] += epair;
     }
+#pragma unroll
+    for (int q = 0; q < 6; q++) acc[1 + q] = (double)vir[q];
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
+}
+
+// ---- per-pair densities and pair energies for c_d_calc / calc_g -------------
+// One thread per listed pair: the values k_dmd32_dens and k_dmd32_force
+// compute, stored in the reference's slot order into the FP32 pair scratch
+// (rho and phi blocks only; the derivative blocks are not read there).
+template <int NT, int NQ>
+__global__ void __launch_bounds__(kFFBlock) k_dmd32_fill(Dev d)
+{
+    using S = Slots<NT>;
+    extern __shared__ float4 tab[];
+    load_split_table(d, tab, NT * NT + S::NC);
+    const SplitK k = split_consts(d);
+    const float cut_sq_f = (float)d.cut_sq;
+    const size_t mp = (size_t)d.maxp;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.npairs;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int i = d.pair_i[p], j = d.pair_j[p];
+        const double4 xi = d.pos[i], xj = d.pos[j];
+        const double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
+        const double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
+        const bool in = rsq < d.cut_sq_mod;
+        const float rsqf = (float)rsq;
+        const float r_inv = rsqrtf(rsqf), r = rsqf * r_inv;
+        const bool below_rc = rsqf < cut_sq_f;
+        float ai[NT], ci[NT], aj[NT], cj[NT];
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            ai[a] = (float)d.alpha[(size_t)i * NT + a];
+            ci[a] = (float)d.c[(size_t)i * NT + a];
+            aj[a] = (float)d.alpha[(size_t)j * NT + a];
+            cj[a] = (float)d.c[(size_t)j * NT + a];
+        }
+        const Knot k0 = knot_at(r, k);
+        float* out = d.prf + p;
+#pragma unroll
+        for (int a = 0; a < NT; a++)
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                const int rs = b * NT + a, ps = comp_idx(a, b);
+                const float alpha = __fdividef(ai[a] * aj[b], ai[a] + aj[b]);
+                float g0 = 0.0f, f0 = 0.0f;
+                if (in) {
+                    g0 = dens_value<NQ, false>(d, tab + (size_t)(a * NT + b) * d.nrS, k, r, r_inv, below_rc, alpha, k0);
+                    if (a >= b)
+                        f0 = phi_value<NQ>(d, tab + (size_t)(NT * NT + ps) * d.nrS, k, r, r_inv, below_rc, alpha, k0);
+                }
+                out[(S::RHO + rs) * mp] = g0;
+                if (a >= b) out[(S::PHI + ps) * mp] = f0;
+            }
+    }
 }
 
 // ---- per-site embedding (FP64, as in the plain form) ----------------------
@@ -171,6 +747,7 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd32_embed(Dev d, int row0)
             double ca = d.c[q], al = d.alpha[q];
             d.E[q] = tmp0;
             d.dE[q] = tmp1;
+            if (d.dE32) d.dE32[q] = (float)tmp1;
             e += ca * tmp0;
             e += d.kbT * calc_ent(ca);
             e += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
@@ -286,37 +863,84 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD32_MINB) k_dmd32_pass2(Dev d, 
     block_partials<7>(acc, d.partial, row0 + blockIdx.x);
 }
 
+// resident blocks per SM of a force kernel at its dynamic shared memory,
+// cached per device, kernel and size
+int resident_blocks(const void* fn, size_t smem)
+{
+    static std::mutex mu;
+    static std::unordered_map<std::string, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    char key[96];
+    snprintf(key, sizeof(key), "%d:%p:%zu", dev, fn, smem);
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kFFBlock, smem) != cudaSuccess) {
+        cudaGetLastError();
+        nb = 0;
+    }
+    nb = std::max(0, std::min(nb, kMaxPassBlocksPerSM));
+    cache[key] = nb;
+    return nb;
+}
+
+// grid of a persistent pair kernel: resident blocks per SM (capped by the
+// tuning hint when given) on every SM, never more blocks than 256-pair chunks
+int pair_grid(long long npairs, int resident, int hint)
+{
+    int bps = resident;
+    if (hint > 0) bps = std::min(bps, hint);
+    bps = std::max(bps, 1);
+    return persistent_grid(npairs, bps);
+}
+
 template <int NT>
 cudaError_t dmd32_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
 {
-    int g1 = persistent_grid(d.npairs, d.tune_bps > 0 ? d.tune_bps : MG_DMD32_MINB), g2 = div_up(d.natms, kFFBlock);
-    int g3 = persistent_grid(d.npairs, d.tune_bps2 > 0 ? d.tune_bps2 : MG_DMD32_MINB);
-    const size_t tab_bytes = (size_t)NT * NT * d.nrC * 2 * sizeof(float4);
-    const bool smem = d.pkC != nullptr && tab_bytes <= 200 * 1024;
-    if (smem) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_dmd32_pass1<NT, 3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            cudaFuncSetAttribute(k_dmd32_pass1<NT, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            attr = true;
-        }
-        long long need = div_up(d.npairs, 1024LL);
-        g1 = (int)(need < num_sms() ? (need > 0 ? need : 1) : num_sms());
-    }
+    constexpr int NC = NT * (NT + 1) / 2;
+    if (!d.pkS || !d.icut || !d.icut_n) return cudaErrorInvalidValue;
+    const size_t smA = (size_t)NT * NT * d.nrS * sizeof(float4), smB = (size_t)(NT * NT + NC) * d.nrS * sizeof(float4);
+    const bool mid0 = d.nq == 3 && d.xi_f[1] == 0.0f;
+    void (*kA)(Dev, int) = mid0 ? k_dmd32_dens<NT, 3> : k_dmd32_dens<NT, 0>;
+    void (*kB)(Dev, int, int, int, int) = mid0 ? k_dmd32_force<NT, 3> : k_dmd32_force<NT, 0>;
+    const int rA = resident_blocks((const void*)kA, smA), rB = resident_blocks((const void*)kB, smB);
+    if (rA == 0 || rB == 0) return cudaErrorInvalidConfiguration;
+    const int gA = pair_grid(d.npairs, rA, d.tune_bps), gB = pair_grid(d.npairs, rB, d.tune_bps2);
+    const int g2 = div_up(d.natms, kFFBlock), g0 = div_up(std::max(d.nall, 1), kFFBlock);
+    if (!d.srec || !d.dE32 || !d.facc) return cudaErrorInvalidValue;
     if (evs) cudaEventRecord(evs[0], st);
-    if (smem) {
-        if (d.nq == 3) k_dmd32_pass1<NT, 3, 1><<<g1, 1024, tab_bytes, st>>>(d, 0);
-        else k_dmd32_pass1<NT, 0, 1><<<g1, 1024, tab_bytes, st>>>(d, 0);
-    } else {
-        if (d.nq == 3) k_dmd32_pass1<NT, 3, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
-        else k_dmd32_pass1<NT, 0, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
-    }
+    // the density pass's warps each test K chunks of 32 listed pairs and own a
+    // region of K batches of the in-cut list
+    const int W = gA * kFFWarps;
+    const int K = (int)std::max(1LL, (d.npairs + (long long)gA * kFFBlock - 1) / ((long long)gA * kFFBlock));
+    if ((long long)W * K * 32 > d.icut_cap || W > dmd32_icut_warps()) return cudaErrorInvalidValue;
+    k_dmd32_prep<NT><<<g0, kFFBlock, 0, st>>>(d);
+    kA<<<gA, kFFBlock, smA, st>>>(d, K);
     if (evs) cudaEventRecord(evs[1], st);
-    k_dmd32_embed<NT><<<g2, kFFBlock, 0, st>>>(d, g1);
+    k_dmd32_embed<NT><<<g2, kFFBlock, 0, st>>>(d, 0);
     if (evs) cudaEventRecord(evs[2], st);
-    k_dmd32_pass2<NT><<<g3, kFFBlock, 0, st>>>(d, st_clc, g1 + g2);
+    kB<<<gB, kFFBlock, smB, st>>>(d, st_clc, g2, W, K);
+    k_dmd32_fmerge<NT><<<g2, kFFBlock, 0, st>>>(d);
     if (evs) cudaEventRecord(evs[3], st);
-    *nb = g1 + g2 + g3;
+    *nb = g2 + gB;
+    return cudaGetLastError();
+}
+
+template <int NT>
+cudaError_t dmd32_fill_nt(const Dev& d, cudaStream_t st)
+{
+    constexpr int NC = NT * (NT + 1) / 2;
+    if (!d.pkS || !d.prf) return cudaErrorInvalidValue;
+    if (d.npairs == 0) return cudaSuccess;
+    const size_t sm = (size_t)(NT * NT + NC) * d.nrS * sizeof(float4);
+    const bool mid0 = d.nq == 3 && d.xi_f[1] == 0.0f;
+    void (*kf)(Dev) = mid0 ? k_dmd32_fill<NT, 3> : k_dmd32_fill<NT, 0>;
+    const int r = resident_blocks((const void*)kf, sm);
+    if (r == 0) return cudaErrorInvalidConfiguration;
+    kf<<<pair_grid(d.npairs, r, 0), kFFBlock, sm, st>>>(d);
     return cudaGetLastError();
 }
 
@@ -355,6 +979,25 @@ cudaError_t launch_dmd_force_f32(const Dev& d, int st_clc, int* nb, cudaStream_t
     case 4: return dmd32_force_nt<4>(d, st_clc, nb, st, evs);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_dmd32_pair_values(const Dev& d, cudaStream_t st)
+{
+    switch (d.nt) {
+    case 1: return dmd32_fill_nt<1>(d, st);
+    case 2: return dmd32_fill_nt<2>(d, st);
+    case 3: return dmd32_fill_nt<3>(d, st);
+    case 4: return dmd32_fill_nt<4>(d, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+int dmd32_icut_warps() { return num_sms() * kMaxPassBlocksPerSM * kFFWarps; }
+
+long long dmd32_icut_capacity(long long maxp)
+{
+    // every warp of the density pass pads its last batch to 32 entries
+    return maxp + 32LL * num_sms() * kMaxPassBlocksPerSM * kFFWarps;
 }
 
 }  // namespace mg

@@ -37,7 +37,12 @@ enum Style { STYLE_EAM = 0, STYLE_FS = 1, STYLE_DMD_I = 2, STYLE_DMD_II = 3, STY
 
 constexpr int kMaxTypes = 4;
 constexpr int kMaxQuad = 14;
-constexpr int kCoarseKnots = 1024;
+#ifndef MG_SPLIT_KNOTS
+#define MG_SPLIT_KNOTS 512
+#endif
+constexpr int kSplitKnots = MG_SPLIT_KNOTS;  // knots per slot of the precision form's shared-memory table
+constexpr int kMaxPassBlocksPerSM = 8;    // resident 256-thread blocks per SM at most
+constexpr int kSiteRec = 2;               // float4 per site of the precision form's site record (nt <= 4)
 constexpr int kMaxChain = 15;
 
 // Everything a kernel needs, passed by value.
@@ -96,7 +101,8 @@ struct Dev {
     int act_on;
     // reductions
     double* partial;   // [nblocks][8]
-    int* status;       // [0] overflow of nbr, [1] needed maxnb, [2] overflow crd, [3] needed maxcrd
+    int* status;       // [0] overflow of nbr, [1] needed maxnb, [2] overflow crd, [3] needed maxcrd,
+                       // [4] overflow of the precision form's in-cut list
     // tables (device)
     int nr, nrho;
     double dr, drho, dr_inv, drho_inv, rho_max, cut_sq, cut_sq_mod, rc;
@@ -111,12 +117,27 @@ struct Dev {
     // pair (a,b) and knot one 64-byte record {rho c0..c3, phi c0..c3}, so the
     // two knots a quadrature node needs share one cache line
     const double* pk64;
-    // the same splines resampled onto kCoarseKnots knots over [0, rc] (FP32,
-    // packed the same way), small enough for a shared-memory copy in pass 1
-    const float4* pkC;
-    int nrC;
-    float drC_inv;
+    // the precision form's table: the same splines resampled onto nrS =
+    // kSplitKnots knots over [0, rc] (FP32 cubic Hermite pieces, float4
+    // {c0..c3} per knot), rho slots of the ordered species pairs (a*nt+b holds
+    // density slot b*nt+a) then phi slots in COMP order, nrS rows each; row
+    // nrS-1 of a slot is the constant f(rc)
+    const float4* pkS;
+    int nrS;
+    float drS_inv;
+    // in-cut pair list of the precision form, written by its density pass in
+    // batches of 32 (i, j) padded with i = -1: warp w of that pass fills region
+    // w and writes its batch count to icut_n[w]; capacity icut_cap entries
+    int2* icut;
+    unsigned* icut_n;
+    long long icut_cap;
     float* prf;          // FP32 pair scratch, same SoA layout as pr
+    // precision form per-site FP32 records: srec[i*kSiteRec..] = {alpha_0..,
+    // c_0..} of site i (owned + ghost), dE32[i*nt+a] = F'(E) of owned site i,
+    // facc[i*8..] the j-side force sums of owned site i (x, y, z, alpha_0..)
+    float4* srec;
+    float* dE32;
+    float* facc;
     double cut_sk_sq[16];
     // FS analytic
     double fsA[kMaxTypes], fst1[kMaxTypes][kMaxTypes], fst2[kMaxTypes][kMaxTypes];
@@ -208,6 +229,13 @@ cudaError_t launch_dmd_energy(const Dev& d, int* nblocks_out, cudaStream_t st);
 // precision form (MG_FORM_FP32) force_calc; evs as for launch_dmd_force
 cudaError_t launch_dmd_force_f32(const Dev& d, int st_clc, int* nblocks_out, cudaStream_t st, cudaEvent_t* evs);
 // the precision form's embedding and pass 2 after a pass 1 that filled the FP32 pair scratch
+// the precision form's per-pair densities and pair energies (rho and phi blocks
+// of prf) at the current positions, for c_d_calc / calc_g after its force call
+cudaError_t launch_dmd32_pair_values(const Dev& d, cudaStream_t st);
+// entries the in-cut list needs for maxp listed pairs, and the number of
+// per-warp batch counts (icut_n) it needs
+long long dmd32_icut_capacity(long long maxp);
+int dmd32_icut_warps();
 cudaError_t launch_dmd_force_f32_after_pass1(const Dev& d, int st_clc, int row0, int* nblocks_out, cudaStream_t st,
                                              cudaEvent_t* evs);
 // learned form

@@ -14,6 +14,13 @@
 // The scratch is shared by every call: the densities are cleared at the start
 // of each call, and calls that overlap on the GPU (on different streams, or
 // from different threads) race on it.  Callers serialise them.
+//
+// The first call on a device resolves the array's device address there
+// (cudaGetSymbolAddress).  With the runtime's lazy module loading that lookup
+// can be what loads this library's device code onto the device, which may
+// allocate and synchronise once; callers make that first call during set-up.
+// The cached address belongs to the device's current context: after a
+// cudaDeviceReset the cache is stale and this entry point must not be used.
 #include <mutex>
 
 #include "../../include/mapp_b200.h"

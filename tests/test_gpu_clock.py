@@ -202,3 +202,43 @@ def test_clock_bdf_predictor_stall(tmp_path):
         Oracle(w).clock_bdf(5, **opts)
     with pytest.raises(mb.MGError, match="even at min_del_t"):
         mb.system_from_workload(w).clock_bdf(5, **opts)
+
+
+@pytest.mark.parametrize("fail", [False, True], ids=["after-return", "after-domain-error"])
+def test_lists_after_clock(tmp_path, fail):
+    """While a clock runs, c_d_calc and calc_g walk the active-pair sublist of
+    the clock's initial force_calc.  After the clock returns -- normally, or
+    with MG_ERR_DOMAIN from the predictor stall -- they walk the full list
+    again: the sites are then moved and the concentrations reset, and
+    c_d_calc and calc_g must match the oracle on the new state at 1e-10."""
+    mb = _lib_or_skip()
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=4, sigma=0.02, style="DMD_I")
+    s = mb.system_from_workload(w)
+    if fail:
+        tau = rate_scale(w)
+        with pytest.raises(mb.MGError, match="even at min_del_t"):
+            s.clock_bdf(5, max_order=2, initial_del_t=10.0 * tau, min_del_t=10.0 * tau, max_del_t=20.0 * tau)
+    else:
+        s.clock_bdf(5)
+    o = Oracle(w)
+    o.force(1)
+    N = w["cfg"].natms
+    x1 = s.get_x()
+    x1[:, :3] += np.random.default_rng(9).normal(0, 0.08, (N, 3))
+    c = w["cfg"].c.copy()
+    assert s.update_x(x1) == o.update_x(x1)
+    s.update_c(c)
+    o.update_c(c)
+    s.force_calc(1)
+    o.force(1)
+    s.create_2nd_neigh_lst()
+    o.crd()
+    cd, cdo = s.c_d_calc(), o.c_d()
+    assert float(np.max(np.abs(cd - cdo))) <= 1e-10 * float(np.max(np.abs(cdo)))
+    a = np.random.default_rng(3).normal(0, 1e-3, (N, w["cfg"].c.shape[1]))
+    cost, g = s.calc_g(a, 0.01)
+    cost_o, g_o = o.calc_g(a, 0.01)
+    assert abs(cost - cost_o) <= 1e-10 * abs(cost_o)
+    assert float(np.max(np.abs(g - g_o))) <= 1e-10 * float(np.max(np.abs(g_o)))

@@ -66,13 +66,21 @@ def test_noalloc_fs_energy_matches_force_field(tmp_path, nt, n):
     o_d = torch.from_numpy(off).to(dev)
     n_d = torch.from_numpy(np.ascontiguousarray(pairs)).to(dev)
     cf = _coeffs(w["coef"][1], w["cfg"].names, mb)
+    e_devs = [torch.zeros(1, dtype=torch.float64, device=dev) for _ in range(2)]
     for call in range(2):
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         e_host = np.zeros(1)
         mb.fs_energy_noalloc(cf, natms, nall, x_d, t_d, o_d, n_d, e_host)
+        mb.fs_energy_noalloc(cf, natms, nall, x_d, t_d, o_d, n_d, e_devs[call])
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
         assert abs(e_host[0] - e_ref) <= TOL * abs(e_ref), (call, e_host[0], e_ref)
-        e_dev = torch.zeros(1, dtype=torch.float64, device=dev)
-        mb.fs_energy_noalloc(cf, natms, nall, x_d, t_d, o_d, n_d, e_dev)
-        assert abs(float(e_dev.item()) - e_ref) <= TOL * abs(e_ref), (call, float(e_dev.item()), e_ref)
+        assert abs(float(e_devs[call].item()) - e_ref) <= TOL * abs(e_ref), (call, float(e_devs[call].item()), e_ref)
+        if call == 1:
+            # the second call allocates no device memory (the first may load
+            # the library's device code on this device)
+            assert free_after == free_before, (free_before, free_after)
 
 
 def test_noalloc_rejects_oversize_and_host_inputs():
