@@ -36,6 +36,8 @@ sys.path.insert(0, ROOT)
 METRIC = "DMD site-force evals/s, surrogate & FP32 vs FP64 on 1 B200 at max|dF|<=1e-4 eV/A"
 UNIT = "site-force evals/s"
 WORKLOAD = dict(n=20, a=3.58, sigma=0.0, style="DMD_I")
+# flops of one evaluation of the learned form's network 4 -> 64 -> 64 -> 64 -> 6
+MLP_FLOPS_PER_ROW = 2 * (4 * 64 + 64 * 64 + 64 * 64 + 64 * 6)
 
 
 def parse():
@@ -157,47 +159,62 @@ def run_reference(args):
 # clocks sampling during the timed region
 # ---------------------------------------------------------------------------
 class Clocks:
+    """Samples SM clocks, power and throttle reasons with nvidia-smi while the
+    timed work runs (reads only).  Each sample is one nvidia-smi query that
+    exits by itself: a looping nvidia-smi writing to a file buffers its
+    output, and a terminated one can leave the file empty."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device):
+    def __init__(self, device, period_s=0.1):
         self.device = device
-        self.proc = None
-        self.path = tempfile.mktemp(suffix=".csv")
+        self.period = period_s
+        self.rows = []
+        self._stop = None
+        self._thread = None
+
+    def _run(self):
+        cmd = ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits"]
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(cmd, capture_output=True, text=True, timeout=5).stdout
+            except (OSError, subprocess.SubprocessError):
+                return
+            for line in out.splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    self.rows.append(parts)
+            self._stop.wait(self.period)
 
     def __enter__(self):
-        try:
-            self.fp = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=self.fp, stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+        import threading
+
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            self.fp.close()
+        self._stop.set()
+        self._thread.join(timeout=10)
+
+    def count(self):
+        return len(self.rows)
 
     def summary(self):
-        rows = []
-        try:
-            for line in open(self.path):
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        except OSError:
-            return None
+        rows = list(self.rows)
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in rows) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
@@ -229,6 +246,30 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def measure_fp32_peak(n=8192, reps=5):
+    """FP32 denominator for the precision form's compute view: cuBLAS SGEMM
+    (torch.matmul in float32 with TF32 off, so the FP32 FMA pipe), n^3,
+    best of reps, CUDA events."""
+    import torch
+
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    c = a @ b
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    torch.backends.cuda.matmul.allow_tf32 = old
+    del a, b, c
+    return 2.0 * n ** 3 / best / 1e12
+
+
 def measure_fp64_peak(n=4096, reps=5):
     """FP64 denominator for the compute view of the roofline: cuBLAS DGEMM
     (torch.matmul in float64, n^3, 2 n^3 flops) on this GPU, best of reps,
@@ -253,6 +294,14 @@ def measure_fp64_peak(n=4096, reps=5):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def pass2_flops_per_pair(nt):
+    """Algorithmic work of force pass 2 (the projection of the stored
+    derivatives on the forces, ff_dmd_I.cpp:357-436) per half pair inside the
+    smeared cut: about 25 flops per ordered species pair, nt^2 * 25 (100 for
+    the binary system)."""
+    return nt * nt * 25
+
+
 def pass1_flops_per_pair(nt, nq):
     """Algorithmic FP64 work of force pass 1 per half pair inside the smeared
     cut, as counted for this workload's measurement: per ordered species pair
@@ -365,12 +414,16 @@ def run_batched(mb, fx, device, ncells=512):
         mf = np.array([r["max_f"] for r in res])
         codes = np.bincount([r["code"] for r in res], minlength=6).tolist()
         out[name] = {
+            # the lead figure: force evaluations of sites per second over the
+            # whole relaxation; cells stop after about two iterations (their
+            # forces are not the gradient of the energy the line search
+            # tests), so relaxations/s does not measure relaxation work
+            "site_evals_per_s": float(sum(r["evaluations"] * r["natms"] for r in res) / (st["relax_ms"] * 1e-3)),
             "relaxations_per_s": ncells / (st["relax_ms"] * 1e-3),
             "relaxations_per_s_with_build": ncells / ((st["relax_ms"] + st["build_ms"]) * 1e-3),
             "relax_ms": st["relax_ms"], "build_ms": st["build_ms"], "tune_ms_first_run": first["tune_ms"],
             "cell_time_ms_p50": float(np.percentile(t, 50)), "cell_time_ms_p99": float(np.percentile(t, 99)),
             "loop_iterations": st["iterations"], "cell_evaluations": st["evaluations"],
-            "site_evals_per_s": float(sum(r["evaluations"] * r["natms"] for r in res) / (st["relax_ms"] * 1e-3)),
             "stop_codes": {"not_downhill": codes[1], "min_step": codes[3], "max_iter": codes[4],
                            "tolerance": codes[5]},
             "converged_max_f": st["converged"],
@@ -385,6 +438,37 @@ def run_batched(mb, fx, device, ncells=512):
                    "no energy line search reaches max|f| < 1e-5")
     builder.close()
     return out
+
+
+def run_batched_sharded(mb, fx, device, rank, world, ncells=512):
+    """The batched form's 512 cells split over the job's GPUs
+    (mapp_b200.shard): each rank relaxes its share (FP64, one graph launch,
+    the second relaxation timed), the job time is the slowest rank's device
+    time, the per-cell results are gathered on rank 0."""
+    import torch
+
+    from mapp_b200 import shard
+
+    bdir = tempfile.mkdtemp(prefix=f"mapp_batch_sh{rank}_")
+    wb = fx.write_workload(bdir, "dmd", n=2, style="DMD_I")
+    builder = mb.system_from_workload(wb, device=device)
+    cells = fx.make_batch_cells(ncells, seed=2024)
+    st, local = shard.relax_sharded(builder, cells, rank, world, form=mb.MG_FORM_FP64,
+                                    tuning_cache=os.path.join(bdir, "tune.txt"), warm=True)
+    t_job_s = job_max(st["relax_ms"] * 1e-3, "cuda")
+    evals = torch.tensor([float(sum(r["evaluations"] * r["natms"] for _, r in local))], dtype=torch.float64,
+                         device="cuda")
+    import torch.distributed as dist
+
+    dist.all_reduce(evals)
+    res = shard.gather_results(local, ncells)
+    builder.close()
+    if rank != 0:
+        return None
+    return {"cells": ncells, "ranks": world, "site_evals_per_s": float(evals.item()) / t_job_s,
+            "relaxations_per_s": ncells / t_job_s, "job_relax_ms": t_job_s * 1e3,
+            "rank0_cells": st["cells"], "rank0_sites": st["sites"],
+            "cells_gathered": len(res), "assignment": "largest first to the least-loaded rank (by site count)"}
 
 
 def run_large_forms(mb, fx, device, mlp_source):
@@ -702,29 +786,48 @@ def run_ours(args):
         s.mlp_init(1.8, 5.0, 0.05, 0.20, seed=5)
         s.mlp_train(nsamples=2_000_000, steps=20_000, batch=4096, lr=1e-3, seed=11)
     s.set_form(form_id)
-    for _ in range(args.warmup):
-        s.force_calc(1, f=f_dev)
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
     t_dev = 0.0
-    t_p1 = 0.0
+    t_ph = [0.0, 0.0, 0.0]
+    # nvidia-smi samples every 200 ms and takes a moment to start, so the
+    # sampler starts before the warm-up and, after a short timed region, runs
+    # on through further (untimed) steps of the same work until it has a few
+    # samples under this load
     with Clocks(local) as clk:
+        for _ in range(args.warmup):
+            s.force_calc(1, f=f_dev)
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
         wall0 = time.perf_counter()
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
             s.force_calc(1, f=f_dev)
             t_dev += s.last_time("force")
-            t_p1 += s.last_time("force.pass1")
+            for k, ph in enumerate(("force.pass1", "force.embed", "force.pass2")):
+                t_ph[k] += s.last_time(ph)
         torch.cuda.synchronize()
         wall = time.perf_counter() - wall0
+        t_extra = time.perf_counter()
+        while clk.count() < 5 and time.perf_counter() - t_extra < 3.0:
+            for _ in range(20):
+                flush.zero_()
+                s.force_calc(1, f=f_dev)
+            torch.cuda.synchronize()
+    t_p1 = t_ph[0]
     t_dev = job_max(t_dev, "cuda")
     if ws > 1:
         dist.barrier()
     value = job_rate(natms, args.steps, t_dev * 1e-3, ws)
 
+    if ws > 1:
+        # several GPUs: the single-system forms are per-GPU figures; the form
+        # that splits across GPUs is the batched one (cells shared out by
+        # cost, one graph launch per rank, results gathered on rank 0)
+        args.skip_forms = True
     forms = {} if args.skip_forms else run_forms(args, s, mb, natms, f_dev, flush, t_dev)
+    if ws > 1:
+        forms["batched_sharded"] = run_batched_sharded(mb, fx, local, rank, ws)
     if not args.skip_forms:
         forms["batched"] = run_batched(mb, fx, local)
         forms["single_lbfgs"] = run_single_lbfgs(mb, w, local)
@@ -775,8 +878,10 @@ def run_ours(args):
         return 0
 
     peaks, peak_kind = measured_peaks()
-    p1_ms = t_p1 / args.steps
-    flops = pass1_flops_per_pair(nt, 3) * in_cut
+    p1_ms, emb_ms, p2_ms = (t / args.steps for t in t_ph)
+    call_ms = t_dev / args.steps
+    f1 = pass1_flops_per_pair(nt, 3) * in_cut
+    f2 = pass2_flops_per_pair(nt) * in_cut
     bytes_p1 = PASS1_ALG_BYTES_PER_SITE * natms
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved_gbs = bytes_p1 / (p1_ms * 1e-3) / 1e9
@@ -791,34 +896,70 @@ def run_ours(args):
         except (OSError, KeyError, ValueError):
             traffic = None
     clocks = clk.summary()
-    fp64_peak = measure_fp64_peak()
+    tflops = lambda fl, ms: fl / (ms * 1e-3) / 1e12
+    flop_rules = {"pass1": "nt^2 (10 + 22 nq) flops per half pair inside the smeared cut (304 here)",
+                  "pass2": "nt^2 * 25 flops per half pair inside the smeared cut (100 here)",
+                  "force_call": "pass1 + pass2 rules (404 per half pair inside the smeared cut here)"}
+    if args.form == "fp64":
+        peak = measure_fp64_peak()
+        peak_note = "measured in this run: cuBLAS DGEMM (torch.matmul float64 4096^3, best of 5); " \
+                    "MEASURED_PEAKS.json has no FP64 figure"
+        roof = {"bound": "fp64", "kernel": "k_dmd_pass1", "achieved": tflops(f1, p1_ms), "peak": peak,
+                "unit": "TFLOP/s", "frac": tflops(f1, p1_ms) / peak, "traffic": traffic,
+                "launch_ms": p1_ms, "flops_per_launch": f1, "flops_rule": flop_rules["pass1"],
+                "peak_kind": peak_note,
+                "pass2": {"kernel": "k_dmd_pass2", "launch_ms": p2_ms, "flops_per_launch": f2,
+                          "achieved": tflops(f2, p2_ms), "frac": tflops(f2, p2_ms) / peak,
+                          "flops_rule": flop_rules["pass2"]},
+                "force_call": {"ms": call_ms, "flops": f1 + f2, "achieved": tflops(f1 + f2, call_ms),
+                               "frac": tflops(f1 + f2, call_ms) / peak, "flops_rule": flop_rules["force_call"]},
+                "hbm_view": {"achieved_gbs": achieved_gbs, "peak_gbs": hbm, "frac": achieved_gbs / hbm,
+                             "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                             "algorithmic_bytes_per_launch": bytes_p1,
+                             "algorithmic_bytes_rule": f"{PASS1_ALG_BYTES_PER_SITE} B per owned site "
+                                                       "(x, alpha, c read; E written)",
+                             "traffic_note": "pass 1 writes the per-pair scratch the reference keeps (21 FP64 "
+                                             "values per listed pair); that is most of its DRAM traffic"}}
+    elif args.form == "fp32":
+        peak = measure_fp32_peak()
+        fB = f1 + f2  # the force pass evaluates the whole smearing and the projection
+        roof = {"bound": "fp32", "kernel": "k_dmd32_force", "achieved": tflops(fB, p2_ms), "peak": peak,
+                "unit": "TFLOP/s", "frac": tflops(fB, p2_ms) / peak, "traffic": None,
+                "launch_ms": p2_ms, "flops_per_launch": fB,
+                "flops_rule": "pass1 + pass2 rules: the force pass re-evaluates the smearing with derivatives "
+                              "and projects it (404 flops per half pair inside the smeared cut here)",
+                "peak_kind": "measured in this run: cuBLAS SGEMM (torch.matmul float32, TF32 off, 8192^3, best of 5)",
+                "density_pass": {"kernel": "k_dmd32_dens", "launch_ms": p1_ms},
+                "force_call": {"ms": call_ms, "flops": fB, "achieved": tflops(fB, call_ms),
+                               "frac": tflops(fB, call_ms) / peak, "flops_rule": flop_rules["force_call"]}}
+    else:
+        bf16 = float(peaks.get("bf16_tflops", 1590.0))
+        fm = MLP_FLOPS_PER_ROW * nt * nt * in_cut
+        roof = {"bound": "tensor", "kernel": "k_dmd_pass1_mlp", "achieved": tflops(fm, p1_ms), "peak": bf16,
+                "unit": "TFLOP/s", "frac": tflops(fm, p1_ms) / bf16, "traffic": None, "launch_ms": p1_ms,
+                "flops_per_launch": fm,
+                "flops_rule": "network flops per evaluated row x nt^2 rows per half pair inside the smeared cut "
+                              "(rows outside the training box take the quadrature instead)",
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json bf16_tflops)"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_dev / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"fp64": "f64", "fp32": "f32", "mlp": "bf16"}[args.form],
         "data": "synthetic (seeded lattice, alpha and c; random tables of the named potentials)",
         "form": {"fp64": "plain FP64", "fp32": "precision (FP32)", "mlp": "learned (BF16 MLP)"}[args.form],
-        "config": workload_config(args, {"pairs": cnt["npairs"], "pairs_in_smeared_cut": in_cut, "ghosts": cnt["nph"]}),
-        "roofline": {"bound": "hbm", "kernel": "k_dmd_pass1" if args.form == "fp64" else
-                     {"fp32": "k_dmd32_pass1", "mlp": "k_dmd_pass1_mlp"}[args.form],
-                     "achieved": achieved_gbs, "peak": hbm,
-                     "unit": "GB/s", "frac": achieved_gbs / hbm, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": bytes_p1,
-                     "algorithmic_bytes_rule": f"{PASS1_ALG_BYTES_PER_SITE} B per owned site (x, alpha, c read; E written)",
-                     "launch_ms": p1_ms,
-                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "fp64_flops_per_launch": flops,
-                     "fp64_flops_rule": "nt^2 (10 + 22 nq) per half pair inside the smeared cut",
-                     "fp64_tflops_achieved": flops / (p1_ms * 1e-3) / 1e12,
-                     "fp64_peak_tflops": fp64_peak,
-                     "fp64_peak_kind": "measured in this run: cuBLAS DGEMM (torch.matmul float64 4096^3, best of 5)",
-                     "fp64_frac": flops / (p1_ms * 1e-3) / 1e12 / fp64_peak},
+        "config": workload_config(args),
+        "workload_counts": {"pairs": cnt["npairs"], "pairs_in_smeared_cut": in_cut, "ghosts": cnt["nph"]},
+        "roofline": roof,
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": natms * (s.x_dim + nt) * 8, "d2h_bytes_per_step": natms * s.x_dim * 8 + 56,
                 "steps": e2e_steps, "path": "mg_atoms_update_x + mg_atoms_update_c + mg_ff_force_calc, pinned host buffers"},
         "forms": forms,
-        "gpu_launches": 4 * args.steps,
-        "phases_ms": {"force": t_dev / args.steps, "force.pass1": p1_ms, "list_rebuild": t_list,
+        # library kernels per force call: plain pass 1, embedding, pass 2,
+        # reduction; precision prep, density, embedding, force, merge,
+        # reduction; learned pass 1, embedding, pass 2, reduction
+        "gpu_launches": {"fp64": 4, "fp32": 6, "mlp": 4}[args.form] * args.steps,
+        "phases_ms": {"force": t_dev / args.steps, "force.pass1": p1_ms, "force.embed": emb_ms,
+                      "force.pass2": p2_ms, "list_rebuild": t_list,
                       "energy_calc": t_energy, "c_d_calc": t_cd, "calc_g": t_g},
         "wall_s": wall,
         "clocks": clocks,

@@ -285,6 +285,14 @@ int mg_batch_set_tuning(mg_batch* b, int autotune, const char* cache_path);
    vectors; MG_LAUNCH_WHOLE_GPU for a batch of one cell: one CTA per SM) of
    the L-BFGS step */
 int mg_batch_set_launch(mg_batch* b, int bps1, int bps2, int lbfgs_threads, int lbfgs_cluster);
+/* failure limits of a relaxation: at most iteration_budget loop iterations in
+   one launch (0: every cell's max_iter times its halvings, the default), and
+   a grid-barrier wait of the whole-GPU step that gives up after
+   barrier_wait_s seconds (default 2; 0 gives up at the first wait, to test
+   the failure path).  Either running out ends the relaxation with
+   MG_ERR_TIMEOUT and leaves the GPU usable.  The reference has no such
+   limits: its loops end or abort (error.cpp:29-43). */
+int mg_batch_set_limits(mg_batch* b, long long iteration_budget, double barrier_wait_s);
 int mg_batch_relax(mg_batch* b, mg_batch_stats* stats);
 /* final state of one cell: x = natms * (3 + nt) Cartesian positions and
    alpha, f the same shape; either may be NULL */

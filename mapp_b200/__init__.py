@@ -24,6 +24,7 @@ LIB_PATH = os.path.join(HERE, "libmapp_b200.so")
 MG_FORM_FP64, MG_FORM_FP32, MG_FORM_MLP = 0, 1, 2
 MG_MIN_LBFGS, MG_MIN_CG = 0, 1
 MG_LAUNCH_WHOLE_GPU = -1
+MG_ERR_TIMEOUT = 8
 ERRORS = {1: "ARG", 2: "FILE", 3: "FORMAT", 4: "STATE", 5: "CUDA", 6: "CAPACITY", 7: "UNSUPPORTED", 8: "TIMEOUT", 9: "DOMAIN"}
 
 # Every exported entry point of include/mapp_b200.h with its ctypes signature.
@@ -75,6 +76,7 @@ SIGNATURES = {
     "mg_batch_set_form": (C.c_int, [_P, C.c_int]),
     "mg_batch_set_tuning": (C.c_int, [_P, C.c_int, C.c_char_p]),
     "mg_batch_set_launch": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "mg_batch_set_limits": (C.c_int, [_P, C.c_longlong, C.c_double]),
     "mg_batch_relax": (C.c_int, [_P, _P]),
     "mg_batch_cell_result": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mg_min_lbfgs": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _P, _P]),
@@ -495,6 +497,11 @@ class Batch:
 
     def set_launch(self, bps1=0, bps2=0, lbfgs_threads=256, lbfgs_cluster=1):
         _check(load_library().mg_batch_set_launch(self.h, bps1, bps2, lbfgs_threads, lbfgs_cluster))
+
+    def set_limits(self, iteration_budget=0, barrier_wait_s=2.0):
+        """Iteration budget of one launch (0: automatic) and grid-barrier wait
+        limit; running out of either raises MGError (MG_ERR_TIMEOUT)."""
+        _check(load_library().mg_batch_set_limits(self.h, int(iteration_budget), float(barrier_wait_s)))
 
     def relax(self) -> dict:
         st = BatchStats()

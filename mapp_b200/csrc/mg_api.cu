@@ -364,7 +364,7 @@ int ensure_compact(mg_system* s, long long npairs)
         CHK(dalloc(&d.prf, (size_t)cap * s->npair_blocks));
         d.maxp = cap;
         d.icut_cap = dmd32_icut_capacity(cap);
-        CHK(dalloc(&d.icut, (size_t)d.icut_cap));
+        CHK(dalloc(&d.icut, (size_t)d.icut_cap * 2));
         if (!d.icut_n) CHK(dalloc(&d.icut_n, (size_t)dmd32_icut_warps()));
     }
     s->pair_cap = cap;
@@ -1203,6 +1203,7 @@ int mg_ff_coef(mg_system* s, int narg, const char* const* arg)
 
 int mg_ff_init(mg_system* s)
 {
+    MG_NVTX("mg_ff_init");
     CHK(check_sys(s));
     if (!s->types_set || !s->box_set || !s->atoms_set || !s->coef_set)
         return fail(MG_ERR_STATE, "types, box, atoms and ff_coef must be set before init");
@@ -1235,6 +1236,7 @@ int mg_ff_init(mg_system* s)
 
 int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
 {
+    MG_NVTX("mg_atoms_update_x");
     CHK(check_sys(s));
     if (!s->initialized) return fail(MG_ERR_STATE, "init must run before update_0");
     if (s->natms == 0) {
@@ -1266,6 +1268,7 @@ int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
 
 int mg_atoms_update_c(mg_system* s, const double* c)
 {
+    MG_NVTX("mg_atoms_update_c");
     CHK(check_sys(s));
     if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "c exists only in DMD mode");
     if (!s->initialized) return fail(MG_ERR_STATE, "init must run first");
@@ -1312,6 +1315,7 @@ int mg_atoms_get_ghosts(mg_system* s, double* x, int* owner)
 
 int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
 {
+    MG_NVTX("mg_ff_force_calc");
     CHK(check_sys(s));
     if (!s->initialized) return fail(MG_ERR_STATE, "force_calc before init");
     if (s->natms == 0) {
@@ -1370,6 +1374,7 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
 
 int mg_ff_energy_calc(mg_system* s, double* energy)
 {
+    MG_NVTX("mg_ff_energy_calc");
     CHK(check_sys(s));
     if (!s->initialized) return fail(MG_ERR_STATE, "energy_calc before init");
     if (s->natms == 0) {
@@ -1398,6 +1403,7 @@ int mg_ff_energy_calc(mg_system* s, double* energy)
 
 int mg_ff_create_2nd_neigh_lst(mg_system* s)
 {
+    MG_NVTX("mg_ff_create_2nd_neigh_lst");
     CHK(check_sys(s));
     if (!s->dmd) return MG_OK;  // empty in EAM / FS (ff_eam.h:61)
     if (!s->initialized) return fail(MG_ERR_STATE, "create_2nd_neigh_lst before init");
@@ -1427,6 +1433,7 @@ int mg_ff_create_2nd_neigh_lst(mg_system* s)
 
 int mg_ff_c_d_calc(mg_system* s, double* c_d)
 {
+    MG_NVTX("mg_ff_c_d_calc");
     CHK(check_sys(s));
     if (!s->dmd) return MG_OK;
     if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before c_d_calc");
@@ -1447,6 +1454,7 @@ int mg_ff_c_d_calc(mg_system* s, double* c_d)
 
 int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g, double* cost)
 {
+    MG_NVTX("mg_ff_calc_g");
     CHK(check_sys(s));
     if (!s->dmd) {
         if (cost) *cost = 0.0;  // ff_eam.h:62 returns 0
@@ -1494,6 +1502,7 @@ int mg_ff_fin(mg_system* s)
 
 int mg_neighbor_create_list(mg_system* s)
 {
+    MG_NVTX("mg_neighbor_create_list");
     CHK(check_sys(s));
     if (!s->initialized) return fail(MG_ERR_STATE, "init must run first");
     if (s->natms == 0) return MG_OK;
@@ -1684,6 +1693,7 @@ int mg_mlp_state(mg_system* s, float* par_out, const float* par_in, float* scali
 int mg_mlp_train(mg_system* s, long long nsamples, int steps, int batch, double lr, unsigned long long seed,
                  double* final_loss)
 {
+    MG_NVTX("mg_mlp_train");
     CHK(check_sys(s));
     if (!s->mlp_ready) return fail(MG_ERR_STATE, "mg_mlp_init first");
     if (nsamples < 64 || steps < 1 || batch < 64 || batch % 64 || batch / 64 > 4096)

@@ -89,6 +89,7 @@ struct BatchView {
     unsigned int* gbar;
     double* gpart;
     int* gerr;
+    unsigned long long wait_ns;  // a grid-barrier wait gives up after this long
 };
 
 __device__ __forceinline__ unsigned long long global_ns()
@@ -137,7 +138,7 @@ __device__ __forceinline__ double block_red(double v, double* sh)
 // memory in a cluster, through a global array after a grid barrier on the
 // whole GPU -- so every thread gets the same value.
 constexpr int kMaxGridCtas = 1024;
-constexpr unsigned long long kGridWaitNs = 2000000000ull;  // a barrier wait gives up after 2 s
+constexpr double kGridWaitS = 2.0;  // default: a barrier wait gives up after 2 s (mg_batch_set_limits)
 
 struct RedCtx {
     double* sh;    // shared [32]
@@ -146,6 +147,7 @@ struct RedCtx {
     unsigned int* gbar;
     double* gpart;
     int* gerr;
+    unsigned long long wait_ns;
 };
 
 template <int CS>
@@ -156,8 +158,11 @@ template <int CS>
 __device__ __forceinline__ int rank_idx() { return CS == 0 ? (int)blockIdx.x : (int)blockIdx.x % CS; }
 
 // Grid barrier of the whole-GPU step (sense by generation count).  A wait
-// that outlasts kGridWaitNs, or sees another CTA's timeout, sets *gerr and
-// returns, so a stuck barrier ends the launch instead of hanging it.
+// that outlasts R.wait_ns, or sees another CTA's timeout, sets *gerr and
+// returns, so a stuck barrier ends the launch instead of hanging it: the
+// loop test then stops the relaxation, which returns MG_ERR_TIMEOUT.  Every
+// index the step uses comes from the cell's state as the launch read it, so
+// the work a CTA still does after a failed wait stays in bounds.
 __device__ __forceinline__ void grid_sync(const RedCtx& R)
 {
     __syncthreads();
@@ -173,7 +178,7 @@ __device__ __forceinline__ void grid_sync(const RedCtx& R)
             const unsigned long long t_start = global_ns();
             while (*gen == g) {
                 if (*(volatile int*)R.gerr) break;
-                if (global_ns() - t_start > kGridWaitNs) {
+                if (global_ns() - t_start >= R.wait_ns) {
                     atomicExch(R.gerr, 1);
                     break;
                 }
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(1024) k_lbfgs_step(Dev d, BatchView B, BatchPa
     __shared__ int par_sh;
     if (threadIdx.x == 0) par_sh = 0;
     __syncthreads();
-    const RedCtx R{sh, &slot_sh, &par_sh, B.gbar, B.gpart, B.gerr};
+    const RedCtx R{sh, &slot_sh, &par_sh, B.gbar, B.gpart, B.gerr, B.wait_ns};
     const int c = cell_idx<CS>(), rank = rank_idx<CS>();
     const int t0 = rank * blockDim.x + threadIdx.x, ts = nctas<CS>() * blockDim.x;
     CellState* S = B.st + c;
@@ -582,7 +587,7 @@ __global__ void __launch_bounds__(1024) k_lbfgs_probe(Dev d, BatchView B, int m,
     __shared__ int par_sh;
     if (threadIdx.x == 0) par_sh = 0;
     __syncthreads();
-    const RedCtx R{sh, &slot_sh, &par_sh, B.gbar, B.gpart, B.gerr};
+    const RedCtx R{sh, &slot_sh, &par_sh, B.gbar, B.gpart, B.gerr, B.wait_ns};
     const int c = cell_idx<CS>(), rank = rank_idx<CS>();
     const int t0 = rank * blockDim.x + threadIdx.x, ts = nctas<CS>() * blockDim.x;
     const int xd = d.x_dim, n = B.nat[c] * xd;
@@ -754,6 +759,10 @@ struct mg_batch {
     double fmax_tol = 1e-5, energy_tol = 1e-8, skin = 0.5;
     int autotune = 0;
     std::string cache_path;
+    // failure limits (mg_batch_set_limits): iteration budget of one launch
+    // (0: from max_iter and max_halvings) and the grid-barrier wait
+    long long iter_budget = 0;
+    double wait_s = kGridWaitS;
     std::vector<HostCell> cells;
     cudaStream_t st = nullptr;
     // batch numbering
@@ -765,7 +774,7 @@ struct mg_batch {
     DArr<double4> pos, pos0;
     DArr<double> alpha, c, shift, f, E, dE, pr, partial, cell_E, vec, probe_out;
     DArr<float> prf;
-    DArr<int2> icut;       // the precision form's in-cut pair list
+    DArr<int4> icut;       // the precision form's in-cut pair list (two int4 per pair)
     DArr<float4> srec;     // and its per-site FP32 records
     DArr<float> dE32, facc;
     DArr<unsigned> icut_n;
@@ -811,6 +820,7 @@ BatchView view(mg_batch* b)
     v.gbar = b->gbar.p;
     v.gpart = b->gpart.p;
     v.gerr = b->gerr.p;
+    v.wait_ns = (unsigned long long)(b->wait_s * 1e9);
     return v;
 }
 
@@ -921,7 +931,7 @@ int build_all(mg_batch* b)
     const int nblk = 3 * nt * nt + 3 * nt * (nt + 1) / 2;
     const size_t maxp = (size_t)pair_fill + 1;
     if (b->form == MG_FORM_FP32) {
-        BCHK(b->icut.exact((size_t)dmd32_icut_capacity((long long)maxp)));
+        BCHK(b->icut.exact((size_t)dmd32_icut_capacity((long long)maxp) * 2));
         BCHK(b->icut_n.exact((size_t)dmd32_icut_warps()));
         BCHK(b->srec.exact(nall * kSiteRec));
         BCHK(b->dE32.exact(nall * nt));
@@ -956,7 +966,7 @@ int build_all(mg_batch* b)
     bd.prf = nullptr;
     bd.icut = b->icut.p;
     bd.icut_n = b->icut_n.p;
-    bd.icut_cap = (long long)b->icut.cap;
+    bd.icut_cap = (long long)b->icut.cap / 2;
     bd.srec = b->srec.p;
     bd.dE32 = b->dE32.p;
     bd.facc = b->facc.p;
@@ -1351,8 +1361,20 @@ int mg_batch_set_launch(mg_batch* b, int bps1, int bps2, int lbfgs_threads, int 
     return MG_OK;
 }
 
+int mg_batch_set_limits(mg_batch* b, long long iteration_budget, double barrier_wait_s)
+{
+    BCHK(check_batch(b));
+    if (iteration_budget < 0 || !(barrier_wait_s >= 0.0) || barrier_wait_s > 3600.0)
+        return bfail(MG_ERR_ARG, "need iteration_budget >= 0 and 0 <= barrier_wait_s <= 3600");
+    b->iter_budget = iteration_budget;
+    b->wait_s = barrier_wait_s;
+    destroy_graph(b);
+    return MG_OK;
+}
+
 int mg_batch_relax(mg_batch* b, mg_batch_stats* stats)
 {
+    MG_NVTX("mg_batch_relax");
     BCHK(check_batch(b));
     const int ncells = (int)b->cells.size();
     if (ncells == 0) return bfail(MG_ERR_STATE, "no cells in the batch");
@@ -1387,7 +1409,9 @@ int mg_batch_relax(mg_batch* b, mg_batch_stats* stats)
     BCHK(capture_graph(b));
     // iteration budget of one launch: every cell's iterations and halvings, bounded
     const long long per_cell = (long long)(b->max_iter + 2) * (long long)(b->max_halvings > 0 ? b->max_halvings + 1 : 64);
-    const int budget = (int)std::min<long long>(per_cell + 8, 1LL << 30);
+    long long bud = std::min<long long>(per_cell + 8, 1LL << 30);
+    if (b->iter_budget > 0) bud = std::min(bud, b->iter_budget);
+    const int budget = (int)bud;
     int rounds = 0;
     auto t_start = std::chrono::steady_clock::now();
     k_stamp<<<1, 1, 0, b->st>>>(b->t0.p);
@@ -1544,12 +1568,14 @@ static int min_single(mg_system* s, int method, int m, int max_iter, double fmax
 int mg_min_lbfgs(mg_system* s, int m, int max_iter, double fmax_tol, double energy_tol, int max_halvings,
                  int lbfgs_cluster, mg_cell_result* r, mg_batch_stats* stats)
 {
+    MG_NVTX("mg_min_lbfgs");
     return min_single(s, MG_MIN_LBFGS, m, max_iter, fmax_tol, energy_tol, max_halvings, lbfgs_cluster, r, stats);
 }
 
 int mg_min_cg(mg_system* s, int max_iter, double fmax_tol, double energy_tol, int max_halvings, int cluster,
               mg_cell_result* r, mg_batch_stats* stats)
 {
+    MG_NVTX("mg_min_cg");
     return min_single(s, MG_MIN_CG, 1, max_iter, fmax_tol, energy_tol, max_halvings, cluster, r, stats);
 }
 

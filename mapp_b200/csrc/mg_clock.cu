@@ -740,6 +740,7 @@ using namespace mg;
 
 extern "C" int mg_clock_adams(mg_system* s, int order, int nsteps, double delta_t, double* err, long long* n_calc_g)
 {
+    MG_NVTX("mg_clock_adams");
     KCHK(clock_setup(s, "Adams"));
     int style = -1, nt = 0, x_dim = 0, form = 0;
     system_shape(s, &style, &nt, &x_dim, &form, nullptr);
@@ -835,6 +836,7 @@ extern "C" void mg_bdf_defaults(mg_bdf_opts* o)
 extern "C" int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, double* hist, int* steps_taken,
                             long long* n_calc_g)
 {
+    MG_NVTX("mg_clock_bdf");
     KCHK(clock_setup(s, "BDF"));
     if (nsteps <= 0) return internal_fail(MG_ERR_ARG, "no of steps should be greater than zero");
     mg_bdf_opts o;

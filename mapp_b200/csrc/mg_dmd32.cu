@@ -12,7 +12,8 @@
 //                  only).  A warp queues its in-cut pairs in shared memory and
 //                  evaluates them 32 at a time, so no lane idles on a pair
 //                  beyond the cut; each full batch of 32 is also appended to
-//                  the in-cut pair list `icut` (padded with i = -1).
+//                  the in-cut pair list `icut` (padded with i = -1), with the
+//                  pair's geometry, so the force pass gathers no positions.
 //   k_dmd32_embed  F(E), F'(E), entropy and alpha terms per site (FP64).
 //   k_dmd32_force  per batch of `icut`: the smearing again, now with all three
 //                  weight sets and the pair function, giving the per-pair
@@ -379,7 +380,7 @@ __global__ void MG_DENS_BOUNDS k_dmd32_dens(Dev d, int K)
 {
     extern __shared__ float4 tab[];
     __shared__ int2 q_ij[kFFWarps][kQueue];
-    __shared__ float q_r[kFFWarps][kQueue];
+    __shared__ float4 q_x[kFFWarps][kQueue];  // dx, dy, dz (FP32), rsq
     load_split_table(d, tab, NT * NT);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -392,7 +393,7 @@ __global__ void MG_DENS_BOUNDS k_dmd32_dens(Dev d, int K)
     // K chunks of 32 listed pairs), filled from the start; the batch count goes
     // to icut_n[warp]
     const int wg = blockIdx.x * kFFWarps + w;
-    int2* region = d.icut + (size_t)wg * K * 32;
+    int4* region = d.icut + (size_t)wg * K * 32 * 2;
     int nbt = 0;
     // Software pipeline over this warp's chunks: while a batch is evaluated,
     // the positions of the next chunk and the pair indices of the one after
@@ -419,18 +420,18 @@ __global__ void MG_DENS_BOUNDS k_dmd32_dens(Dev d, int K)
         const bool have = base < d.npairs;
         if (have) {
             bool in = false;
-            float rsqf = 0.f;
+            float4 gx = make_float4(0.f, 0.f, 0.f, 0.f);
             if (j1 >= 0) {
                 const double dx0 = xi1.x - xj1.x, dx1 = xi1.y - xj1.y, dx2 = xi1.z - xj1.z;
                 const double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
                 in = rsq < d.cut_sq_mod;
-                rsqf = (float)rsq;
+                gx = make_float4((float)dx0, (float)dx1, (float)dx2, (float)rsq);
             }
             const unsigned m = __ballot_sync(0xffffffffu, in);
             if (in) {
                 const int slot = cnt + __popc(m & lt);
                 q_ij[w][slot] = make_int2(i1, j1);
-                q_r[w][slot] = rsqf;
+                q_x[w][slot] = gx;
             }
             cnt += __popc(m);
             __syncwarp();
@@ -449,17 +450,24 @@ __global__ void MG_DENS_BOUNDS k_dmd32_dens(Dev d, int K)
             const int nb = min(cnt, 32);
             const bool on = lane < nb;
             const int2 e = on ? q_ij[w][lane] : make_int2(-1, -1);
-            const float rsqf = on ? q_r[w][lane] : 1.0f;
+            const float4 gx = on ? q_x[w][lane] : make_float4(0.f, 0.f, 0.f, 1.f);
+            const float rsqf = gx.w;
             __syncwarp();
             if (lane < cnt - nb) {
                 q_ij[w][lane] = q_ij[w][nb + lane];
-                q_r[w][lane] = q_r[w][nb + lane];
+                q_x[w][lane] = q_x[w][nb + lane];
             }
             __syncwarp();
             cnt -= nb;
-            // append the batch, padded to 32 with i = -1, to this warp's region
-            if (nbt < K) region[(size_t)nbt * 32 + lane] = e;
-            else if (lane == 0) d.status[4] = 1;
+            // append the batch, padded to 32 with i = -1, to this warp's
+            // region: per pair {i, j, owner of j} and {dx, dy, dz, rsq}
+            if (nbt < K) {
+                const int oj = on ? owner(d, e.y) : -1;
+                int4* o = region + ((size_t)nbt * 32 + lane) * 2;
+                o[0] = make_int4(e.x, e.y, oj, 0);
+                o[1] = make_int4(__float_as_int(gx.x), __float_as_int(gx.y), __float_as_int(gx.z), __float_as_int(gx.w));
+            } else if (lane == 0)
+                d.status[4] = 1;
             nbt++;
             float Ei[NT], Ej[NT], ci[NT], cj[NT], al[NT * NT];
             float r = 1.0f, r_inv = 1.0f;
@@ -540,7 +548,8 @@ __global__ void MG_FORCE_BOUNDS k_dmd32_force(Dev d, int st_clc, int row0, int W
     for (long long t = (long long)blockIdx.x * kFFWarps + (threadIdx.x >> 5); t < nslot; t += wstride) {
         const long long rg = t / K;
         if (t - rg * K >= (long long)__ldg(d.icut_n + rg)) continue;  // past the region's last batch
-        const int2 e = d.icut[t * 32 + lane];
+        const int4 e = d.icut[(size_t)t * 64 + lane * 2];
+        const int4 ex = d.icut[(size_t)t * 64 + lane * 2 + 1];
         const bool on = e.x >= 0;
         float fi[3 + NT];
 #pragma unroll
@@ -567,14 +576,12 @@ __global__ void MG_FORCE_BOUNDS k_dmd32_force(Dev d, int st_clc, int row0, int W
         // every lane's species pairs inside the smeared range: no branches
         const bool fast = __all_sync(0xffffffffu, inr);
         if (on) {
-            const int i = e.x, j = e.y;
-            const double4 xi = pos_ld(d, i), xj = pos_ld(d, j);
-            const float dx0 = (float)(xi.x - xj.x), dx1 = (float)(xi.y - xj.y), dx2 = (float)(xi.z - xj.z);
-            const float rsqf = fmaf(dx2, dx2, fmaf(dx1, dx1, dx0 * dx0));
+            const int i = e.x, j = e.y, oj = e.z;
+            const float dx0 = __int_as_float(ex.x), dx1 = __int_as_float(ex.y), dx2 = __int_as_float(ex.z);
+            const float rsqf = __int_as_float(ex.w);
             const float r_inv = rsqrtf(rsqf), r = rsqf * r_inv;
             const bool below_rc = rsqf < cut_sq_f;
             const bool own_j = j < d.natms;
-            const int oj = owner(d, j);
             float dEi[NT], dEj[NT];
             if (NT == 2) {
                 const float2 ei = __ldg(reinterpret_cast<const float2*>(d.dE32) + i);

@@ -28,6 +28,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <nvtx3/nvToolsExt.h>
 
 struct mg_system;
 
@@ -126,9 +127,10 @@ struct Dev {
     int nrS;
     float drS_inv;
     // in-cut pair list of the precision form, written by its density pass in
-    // batches of 32 (i, j) padded with i = -1: warp w of that pass fills region
-    // w and writes its batch count to icut_n[w]; capacity icut_cap entries
-    int2* icut;
+    // batches of 32 padded with i = -1, two int4 per pair: {i, j, owner of j,
+    // 0} and the bits of {dx, dy, dz, rsq} (FP32); warp w of that pass fills
+    // region w and writes its batch count to icut_n[w]; capacity icut_cap pairs
+    int4* icut;
     unsigned* icut_n;
     long long icut_cap;
     float* prf;          // FP32 pair scratch, same SoA layout as pr
@@ -254,6 +256,18 @@ cudaError_t launch_dmd_crd(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nblocks_out, cudaStream_t st);
 cudaError_t launch_active_pairs(const Dev& d, cudaStream_t st);
+
+// One NVTX range per hot-path entry point, named after it, so a profiler's
+// timeline shows force_calc, calc_g, list builds and solver runs the way the
+// reference's per-phase timers report them (thermo_dynamics.cpp:188-206).
+// Without an attached tool a range costs one pointer test.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+#define MG_NVTX(name) ::mg::NvtxRange mg_nvtx_range_(name)
 
 // records msg as the calling thread's last error and returns code
 int internal_fail(int code, const char* msg);

@@ -408,6 +408,7 @@ extern "C" int mg_md_nh(mg_system* s, double t_tar, double t_period, int eta_ite
                         double boltz, int seed, const double* xd_in, int nsteps, double* xd_out, double* thermo,
                         int* rebuilds_out)
 {
+    MG_NVTX("mg_md_nh");
     MCHK(system_check_ready(s));
     int style = -1, nt = 0, x_dim = 0, form = 0;
     system_shape(s, &style, &nt, &x_dim, &form, nullptr);

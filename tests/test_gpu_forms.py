@@ -57,3 +57,30 @@ def test_fp32_form_rejected_for_eam(tmp_path):
     with pytest.raises(mb.MGError) as e:
         s.set_form(mb.MG_FORM_FP32)
     assert e.value.code == 7
+
+
+def test_fp32_form_gates_at_256000_sites(tmp_path):
+    """The precision form's gates at the size of its workload definition: FCC
+    40^3 = 256000 sites of the binary DMD_I system, against the FP64 oracle:
+    max|dF| <= 1e-4 eV/A, |dE|/site <= 1e-6 eV, |d mu| <= 2e-6 eV."""
+    mb = _mb()
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=40, a=3.58, sigma=0.0, style="DMD_I", seed=4321)
+    s = mb.system_from_workload(w)
+    s.set_form(mb.MG_FORM_FP32)
+    o = Oracle(w)
+    f, en = s.force_calc(1)
+    fo, eno = o.force(1)
+    N = w["cfg"].natms
+    assert N == 256000
+    assert np.max(np.abs(f - fo)) <= 1e-4
+    assert abs(en[0] - eno[0]) / N <= 1e-6
+    s.create_2nd_neigh_lst()
+    o.crd()
+    s.c_d_calc()
+    o.c_d()
+    to_ev = 8.617333e-5 * 600.0
+    n_gpu = s.vector("n")[:N * 2]
+    n_orc = o.vec(2)[:N * 2]
+    assert np.max(np.abs(n_gpu - n_orc)) * to_ev <= 2e-6
