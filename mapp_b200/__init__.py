@@ -25,6 +25,8 @@ MG_FORM_FP64, MG_FORM_FP32, MG_FORM_MLP = 0, 1, 2
 MG_MIN_LBFGS, MG_MIN_CG = 0, 1
 MG_LAUNCH_WHOLE_GPU = -1
 MG_ERR_TIMEOUT = 8
+MG_MLP_ACT_POLY = 0
+MG_MLP_ACT_TANH = 1
 ERRORS = {1: "ARG", 2: "FILE", 3: "FORMAT", 4: "STATE", 5: "CUDA", 6: "CAPACITY", 7: "UNSUPPORTED", 8: "TIMEOUT", 9: "DOMAIN"}
 
 # Every exported entry point of include/mapp_b200.h with its ctypes signature.
@@ -77,6 +79,7 @@ SIGNATURES = {
     "mg_batch_set_tuning": (C.c_int, [_P, C.c_int, C.c_char_p]),
     "mg_batch_set_launch": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     "mg_batch_set_limits": (C.c_int, [_P, C.c_longlong, C.c_double]),
+    "mg_mlp_set_activation": (C.c_int, [_P, C.c_int]),
     "mg_batch_relax": (C.c_int, [_P, _P]),
     "mg_batch_cell_result": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mg_min_lbfgs": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _P, _P]),
@@ -316,6 +319,9 @@ class System:
         return out
 
     # ---- learned form ------------------------------------------------------
+    def mlp_set_activation(self, act):
+        _check(load_library().mg_mlp_set_activation(self.h, act))
+
     def mlp_init(self, r_lo=1.8, r_hi=5.0, w_lo=0.05, w_hi=0.20, seed=1):
         _check(load_library().mg_mlp_init(self.h, r_lo, r_hi, w_lo, w_hi, seed))
 

@@ -16,8 +16,8 @@ OUT = os.path.join(HERE, "libmapp_b200.so")
 BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["mg_api.cu", "mg_atoms.cu", "mg_eam.cu", "mg_dmd.cu", "mg_dmd32.cu", "mg_mlp.cu", "mg_noalloc.cu", "mg_batch.cu", "mg_cfg.cu", "mg_md.cu", "mg_clock.cu"]
-HEADERS = ["mg_internal.h", "mg_reduce.cuh", "mg_dmd_common.cuh"]
+SOURCES = ["mg_api.cu", "mg_atoms.cu", "mg_eam.cu", "mg_dmd.cu", "mg_dmd32.cu", "mg_mlp.cu", "mg_mlp_tc.cu", "mg_noalloc.cu", "mg_batch.cu", "mg_cfg.cu", "mg_md.cu", "mg_clock.cu"]
+HEADERS = ["mg_internal.h", "mg_reduce.cuh", "mg_dmd_common.cuh", "mg_mlp_common.cuh", "mg_split.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off",

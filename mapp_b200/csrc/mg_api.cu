@@ -982,7 +982,8 @@ int mg_destroy(mg_system* s)
                     s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};
     for (void* p : ptrs)
         if (p) cudaFree(p);
-    void* mptrs[] = {s->mlp.par, s->mlp.wbf, s->mlp.m, s->mlp.v, s->mlp.gpart, s->mlp.audit, s->mlp_loss};
+    void* mptrs[] = {s->mlp.par, s->mlp.wbf, s->mlp.m, s->mlp.v, s->mlp.gpart, s->mlp.audit, s->mlp_loss,
+                     s->mlp.row_in, s->mlp.row_id, s->mlp.row_r, s->mlp.row_n};
     for (void* p : mptrs)
         if (p) cudaFree(p);
     if (s->ev0) cudaEventDestroy(s->ev0);
@@ -1339,7 +1340,17 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
             CU(launch_dmd_force_f32(d, st_clc, &rows, s->st, s->evk));
             s->prf_stale = true;
         } else if (s->form == MG_FORM_MLP) {
+            // the network-row list holds every row of the list at most
+            const long long need = d.npairs * s->nt * s->nt;
+            if (need > s->mlp.row_cap) {
+                const long long cap = need + need / 5 + 1024;
+                CHK(dalloc(&s->mlp.row_in, (size_t)cap));
+                CHK(dalloc(&s->mlp.row_id, (size_t)cap));
+                CHK(dalloc(&s->mlp.row_r, (size_t)cap));
+                s->mlp.row_cap = cap;
+            }
             CU(cudaMemsetAsync(s->mlp.audit, 0, 16 * sizeof(float), s->st));
+            CU(cudaMemsetAsync(d.status + 5, 0, sizeof(int), s->st));
             CU(launch_dmd_force_mlp(d, s->mlp, 0x51ed270b3a5d4e1ull + 0x9e37ull * (++s->mlp_calls), st_clc, &rows,
                                     s->st, s->evk));
             s->prf_stale = false;
@@ -1350,12 +1361,15 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     CU(launch_reduce_partials(d, rows, 7, s->red_out, s->st));
     CHK(timed_end(s));
     CU(cudaMemcpyAsync(tot, s->red_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
-    int icut_over = 0;
+    int icut_over = 0, tc_timeout = 0;
     if (s->dmd && s->form == MG_FORM_FP32)
         CU(cudaMemcpyAsync(&icut_over, d.status + 4, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    if (s->dmd && s->form == MG_FORM_MLP)
+        CU(cudaMemcpyAsync(&tc_timeout, d.status + 5, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CHK(copy_out(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
     CU(cudaStreamSynchronize(s->st));
     if (icut_over) return fail(MG_ERR_CAPACITY, "precision form: in-cut pair list overflow");
+    if (tc_timeout) return fail(MG_ERR_TIMEOUT, "learned form: a tensor-core wait ran out");
     CHK(timed_read(s, &s->t_force));
     if (s->dmd)
         for (int k = 0; k < 3; k++) {
@@ -1612,6 +1626,14 @@ static int mlp_upload_params(mg_system* s, const std::vector<float>& par)
 
 int mg_mlp_nparam(void) { return mlp_nparam(); }
 
+int mg_mlp_set_activation(mg_system* s, int act)
+{
+    CHK(check_sys(s));
+    if (act != MG_MLP_ACT_POLY && act != MG_MLP_ACT_TANH) return fail(MG_ERR_ARG, "unknown activation %d", act);
+    s->mlp.act = act;
+    return MG_OK;
+}
+
 int mg_mlp_init(mg_system* s, double r_lo, double r_hi, double w_lo, double w_hi, unsigned long long seed)
 {
     CHK(check_sys(s));
@@ -1627,6 +1649,7 @@ int mg_mlp_init(mg_system* s, double r_lo, double r_hi, double w_lo, double w_hi
     CHK(dalloc(&M.v, np));
     CHK(dalloc(&M.gpart, (size_t)npart * 4096));  // up to 4096 tiles of 64 rows per step
     CHK(dalloc(&M.audit, 16));
+    if (!M.row_n) CHK(dalloc(&M.row_n, 1));
     CU(cudaMemset(M.m, 0, np * sizeof(float)));
     CU(cudaMemset(M.v, 0, np * sizeof(float)));
     M.box.r_lo = (float)r_lo;

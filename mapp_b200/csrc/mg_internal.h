@@ -103,7 +103,8 @@ struct Dev {
     // reductions
     double* partial;   // [nblocks][8]
     int* status;       // [0] overflow of nbr, [1] needed maxnb, [2] overflow crd, [3] needed maxcrd,
-                       // [4] overflow of the precision form's in-cut list
+                       // [4] overflow of the precision form's in-cut list, [5] a learned-form
+                       // tensor-core wait ran out
     // tables (device)
     int nr, nrho;
     double dr, drho, dr_inv, drho_inv, rho_max, cut_sq, cut_sq_mod, rc;
@@ -197,6 +198,15 @@ struct MlpState {
     float* audit;           // [0..5] max |network - quadrature| per output, [6..7] audited rows (u64), [8..9] fallback rows (u64)
     MlpBox box;
     float out_mean[6], out_scale[6];
+    int act;                // activation: 0 silu_p (FMA-pipe polynomial), 1 SiLU through tanh.approx
+    // deployment: the rows (site pair, species pair) that go through the
+    // network, listed by k_mlp_rows: normalised inputs, (pair, a*nt+b), r;
+    // row_n of them, capacity row_cap
+    float4* row_in;
+    int2* row_id;
+    float* row_r;
+    unsigned* row_n;
+    long long row_cap;
 };
 
 // ---- launchers (defined in the .cu files) ---------------------------------

@@ -31,13 +31,31 @@ def bf16(a):
     return v.view(np.float32).astype(np.float64)
 
 
+# the network's activation silu_p: z times a degree-13 odd polynomial stand-in
+# for the logistic function on z / 7 clamped to [-1, 1] (mapp_b200/csrc/
+# mg_mlp_common.cuh; the same coefficients)
+SIG_Q = np.array([1.733397424e+00, -6.256158375e+00, 2.008515691e+01, -4.197323551e+01,
+                  5.177145032e+01, -3.392468509e+01, 9.064074321e+00])
+
+
+def sigma_p(z):
+    x = np.clip(np.asarray(z, dtype=np.float64) / 7.0, -1.0, 1.0)
+    return np.clip(0.5 + x * np.polynomial.polynomial.polyval(x * x, SIG_Q), 0.0, 1.0)
+
+
 def silu(z):
-    return z / (1.0 + np.exp(-z))
+    return z * sigma_p(z)
 
 
 def dsilu(z):
-    s = 1.0 / (1.0 + np.exp(-z))
-    return s * (1.0 + z * (1.0 - s))
+    z = np.asarray(z, dtype=np.float64)
+    xr = z / 7.0
+    x = np.clip(xr, -1.0, 1.0)
+    u = x * x
+    q = np.polynomial.polynomial.polyval(u, SIG_Q)
+    dq = np.polynomial.polynomial.polyval(u, SIG_Q[1:] * np.arange(1, 7))
+    ds = np.where(np.abs(xr) < 1.0, (q + 2.0 * u * dq) / 7.0, 0.0)
+    return sigma_p(z) + z * ds
 
 
 def inputs(x, box):
