@@ -153,12 +153,15 @@ int mg_mlp_nparam(void);
 /* allocate the network for the training box r in [r_lo, r_hi] A and
    w_i, w_j in [w_lo, w_hi] A; random initial weights from `seed` */
 /* activation of the learned form's network (before mg_mlp_train: training and
-   deployment use the same one): MG_MLP_ACT_POLY (default) is z times a
-   degree-13 polynomial stand-in for the logistic function on the FP32 FMA
-   pipe (|sigma_p - sigma| <= 9.3e-4); MG_MLP_ACT_TANH is SiLU with the
-   logistic from the transcendental unit (tanh.approx). */
+   deployment use the same one): MG_MLP_ACT_POLY is z times a
+   degree-15 polynomial stand-in for the logistic function on the FP32 FMA
+   pipe (|sigma_p - sigma| <= 9.2e-4); MG_MLP_ACT_TANH is SiLU with the
+   logistic from the transcendental unit (tanh.approx); MG_MLP_ACT_SPLIT uses
+   the second on the first 48 units of each hidden layer and the first on the
+   other 16, so that both pipes evaluate activations at once (default). */
 #define MG_MLP_ACT_POLY 0
 #define MG_MLP_ACT_TANH 1
+#define MG_MLP_ACT_SPLIT 2
 int mg_mlp_set_activation(mg_system* s, int act);
 int mg_mlp_init(mg_system* s, double r_lo, double r_hi, double w_lo, double w_hi, unsigned long long seed);
 /* label nsamples seeded samples with the FP64 quadrature of the loaded tables

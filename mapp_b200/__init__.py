@@ -27,6 +27,7 @@ MG_LAUNCH_WHOLE_GPU = -1
 MG_ERR_TIMEOUT = 8
 MG_MLP_ACT_POLY = 0
 MG_MLP_ACT_TANH = 1
+MG_MLP_ACT_SPLIT = 2
 ERRORS = {1: "ARG", 2: "FILE", 3: "FORMAT", 4: "STATE", 5: "CUDA", 6: "CAPACITY", 7: "UNSUPPORTED", 8: "TIMEOUT", 9: "DOMAIN"}
 
 # Every exported entry point of include/mapp_b200.h with its ctypes signature.

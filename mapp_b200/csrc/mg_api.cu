@@ -947,6 +947,7 @@ int mg_create(const char* style, int device, mg_system** out)
     s->style = st;
     s->dmd = st >= STYLE_DMD_I;
     s->device = device;
+    s->mlp.act = MG_MLP_ACT_SPLIT;
     if (cudaSetDevice(device) != cudaSuccess) {
         delete s;
         return fail(MG_ERR_CUDA, "cudaSetDevice failed");
@@ -983,7 +984,7 @@ int mg_destroy(mg_system* s)
     for (void* p : ptrs)
         if (p) cudaFree(p);
     void* mptrs[] = {s->mlp.par, s->mlp.wbf, s->mlp.m, s->mlp.v, s->mlp.gpart, s->mlp.audit, s->mlp_loss,
-                     s->mlp.row_in, s->mlp.row_id, s->mlp.row_r, s->mlp.row_n};
+                     s->mlp.row_in, s->mlp.row_id, s->mlp.row_r, s->mlp.row_n, s->mlp.audit_rows};
     for (void* p : mptrs)
         if (p) cudaFree(p);
     if (s->ev0) cudaEventDestroy(s->ev0);
@@ -1347,7 +1348,12 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
                 CHK(dalloc(&s->mlp.row_in, (size_t)cap));
                 CHK(dalloc(&s->mlp.row_id, (size_t)cap));
                 CHK(dalloc(&s->mlp.row_r, (size_t)cap));
+                // the hashed 1% audit: 2% plus a margin holds any realistic draw;
+                // rows beyond the capacity are not audited
+                const long long acap = cap / 50 + 4096;
+                CHK(dalloc(&s->mlp.audit_rows, (size_t)acap));
                 s->mlp.row_cap = cap;
+                s->mlp.audit_cap = acap;
             }
             CU(cudaMemsetAsync(s->mlp.audit, 0, 16 * sizeof(float), s->st));
             CU(cudaMemsetAsync(d.status + 5, 0, sizeof(int), s->st));
@@ -1629,7 +1635,8 @@ int mg_mlp_nparam(void) { return mlp_nparam(); }
 int mg_mlp_set_activation(mg_system* s, int act)
 {
     CHK(check_sys(s));
-    if (act != MG_MLP_ACT_POLY && act != MG_MLP_ACT_TANH) return fail(MG_ERR_ARG, "unknown activation %d", act);
+    if (act != MG_MLP_ACT_POLY && act != MG_MLP_ACT_TANH && act != MG_MLP_ACT_SPLIT)
+        return fail(MG_ERR_ARG, "unknown activation %d", act);
     s->mlp.act = act;
     return MG_OK;
 }
@@ -1649,7 +1656,7 @@ int mg_mlp_init(mg_system* s, double r_lo, double r_hi, double w_lo, double w_hi
     CHK(dalloc(&M.v, np));
     CHK(dalloc(&M.gpart, (size_t)npart * 4096));  // up to 4096 tiles of 64 rows per step
     CHK(dalloc(&M.audit, 16));
-    if (!M.row_n) CHK(dalloc(&M.row_n, 1));
+    if (!M.row_n) CHK(dalloc(&M.row_n, 4));
     CU(cudaMemset(M.m, 0, np * sizeof(float)));
     CU(cudaMemset(M.v, 0, np * sizeof(float)));
     M.box.r_lo = (float)r_lo;

@@ -198,15 +198,20 @@ struct MlpState {
     float* audit;           // [0..5] max |network - quadrature| per output, [6..7] audited rows (u64), [8..9] fallback rows (u64)
     MlpBox box;
     float out_mean[6], out_scale[6];
-    int act;                // activation: 0 silu_p (FMA-pipe polynomial), 1 SiLU through tanh.approx
-    // deployment: the rows (site pair, species pair) that go through the
-    // network, listed by k_mlp_rows: normalised inputs, (pair, a*nt+b), r;
-    // row_n of them, capacity row_cap
+    int act;                // activation kind (MG_MLP_ACT_*): 0 silu_p, 1 silu_t, 2 split
+    // deployment: the rows (site pair, species pair) listed by k_mlp_rows.
+    // Network rows fill the list from the front (normalised inputs / 8,
+    // (pair, a*nt+b), r), quadrature-fallback rows from the back (row_id
+    // only); row_cap entries.  row_n: [0] network rows, [1] audited rows
+    // (indices into the list, in audit_rows, capacity audit_cap), [2] fallback
+    // rows.
     float4* row_in;
     int2* row_id;
     float* row_r;
     unsigned* row_n;
     long long row_cap;
+    int* audit_rows;
+    long long audit_cap;
 };
 
 // ---- launchers (defined in the .cu files) ---------------------------------

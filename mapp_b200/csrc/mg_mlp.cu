@@ -109,17 +109,17 @@ __device__ void forward(Tile& T, int act)
     cta_gemm<kRows, H, 16>([&](int m, int k) { return T.x[m][k]; }, [&](int k, int n) { return T.w1[k][n]; },
                            [&](int m, int n, float v) { T.z[0][m][n] = v + T.b1[n]; });
     __syncthreads();
-    for (int e = threadIdx.x; e < kRows * H; e += blockDim.x) (&T.h[0][0][0])[e] = __float2bfloat16(act_rt(act, (&T.z[0][0][0])[e]));
+    for (int e = threadIdx.x; e < kRows * H; e += blockDim.x) (&T.h[0][0][0])[e] = __float2bfloat16(act_rt(act, e & (H - 1), (&T.z[0][0][0])[e]));
     __syncthreads();
     cta_gemm<kRows, H, H>([&](int m, int k) { return T.h[0][m][k]; }, [&](int k, int n) { return T.w2[k][n]; },
                           [&](int m, int n, float v) { T.z[1][m][n] = v + T.b2[n]; });
     __syncthreads();
-    for (int e = threadIdx.x; e < kRows * H; e += blockDim.x) (&T.h[1][0][0])[e] = __float2bfloat16(act_rt(act, (&T.z[1][0][0])[e]));
+    for (int e = threadIdx.x; e < kRows * H; e += blockDim.x) (&T.h[1][0][0])[e] = __float2bfloat16(act_rt(act, e & (H - 1), (&T.z[1][0][0])[e]));
     __syncthreads();
     cta_gemm<kRows, H, H>([&](int m, int k) { return T.h[1][m][k]; }, [&](int k, int n) { return T.w3[k][n]; },
                           [&](int m, int n, float v) { T.z[2][m][n] = v + T.b3[n]; });
     __syncthreads();
-    for (int e = threadIdx.x; e < kRows * H; e += blockDim.x) (&T.h[2][0][0])[e] = __float2bfloat16(act_rt(act, (&T.z[2][0][0])[e]));
+    for (int e = threadIdx.x; e < kRows * H; e += blockDim.x) (&T.h[2][0][0])[e] = __float2bfloat16(act_rt(act, e & (H - 1), (&T.z[2][0][0])[e]));
     __syncthreads();
     cta_gemm<kRows, 8, H>([&](int m, int k) { return T.h[2][m][k]; }, [&](int k, int n) { return T.w4[k][n]; },
                           [&](int m, int n, float v) { T.y[m][n] = v + T.b4[n]; });
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_train(MlpState S, const flo
     }
     cta_gemm<kRows, H, 16>([&](int m, int k) { return dy[m][k]; },
                            [&](int k, int n2) { return k < 8 ? T.w4[n2][k] : __float2bfloat16(0.f); },
-                           [&](int m, int n2, float v) { T.z[2][m][n2] = v * dact_rt(S.act, T.z[2][m][n2]); });
+                           [&](int m, int n2, float v) { T.z[2][m][n2] = v * dact_rt(S.act, n2, T.z[2][m][n2]); });
     __syncthreads();
     // layers 3, 2, 1: z[l] now holds dL/dz_l
     for (int l = 2; l >= 0; l--) {
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_train(MlpState S, const flo
                                   [&](int m, int n2, float v) { gp[ow + m * H + n2] = v; });
             const __nv_bfloat16(*W)[H] = l == 2 ? T.w3 : T.w2;
             cta_gemm<kRows, H, H>([&](int m, int k) { return dzb[m][k]; }, [&](int k, int n2) { return W[n2][k]; },
-                                  [&](int m, int n2, float v) { T.z[l - 1][m][n2] = v * dact_rt(S.act, T.z[l - 1][m][n2]); });
+                                  [&](int m, int n2, float v) { T.z[l - 1][m][n2] = v * dact_rt(S.act, n2, T.z[l - 1][m][n2]); });
         } else {
             cta_gemm<16, H, kRows>([&](int m, int k) { return T.x[k][m]; }, [&](int k, int n2) { return dzb[k][n2]; },
                                    [&](int m, int n2, float v) { gp[OW1 + m * H + n2] = v; });

@@ -30,25 +30,33 @@ constexpr int OW1 = 0, OB1 = OW1 + 16 * H, OW2 = OB1 + H, OB2 = OW2 + H * H, OW3
 
 // Activation silu_p(z) = z * sigma_p(z), with sigma_p a polynomial stand-in for
 // the logistic function that runs on the FP32 FMA pipe (no transcendental
-// unit): x = clamp(z / 7, -1, 1), u = x^2,
-//     sigma_p(z) = 1/2 + x Q(u),   Q(u) = sum_k q_k u^k  (degree 6),
+// unit): x = z / 8, u = min(x^2, 1),
+//     sigma_p(z) = clamp(1/2 + x Q(u), 0, 1),   Q(u) = sum_k q_k u^k  (degree 7),
 // Q fitted here by iteratively reweighted least squares (a near-minimax fit)
-// to sigma(7x) - 1/2 on [-1, 1] under the constraint Q(1) = 1/2, so that
-// sigma_p(z) is 0 for z <= -7 and 1 for z >= 7 (to the rounding of the
-// coefficients) and silu_p(z) vanishes for large negative z.  Bounds (checked
-// against the exp-based logistic on a dense grid, FP32 evaluation):
-//     |sigma_p(z) - sigma(z)| <= 9.3e-4,  |silu_p(z) - silu(z)| <= 6.4e-3
-// for every z (the second is at most 9.3e-4 |z|), below the 2^-9 relative
+// to sigma(8x) - 1/2 on [-1, 1] under the constraint Q(1) = 1/2, so that
+// sigma_p(z) is 0 for z <= -8 and 1 for z >= 8 (to the rounding of the
+// coefficients, 1e-7) and silu_p(z) vanishes for large negative z.  (For |x| > 1, u = 1 and 1/2 + x/2 lies outside [0, 1]:
+// the clamp alone gives the two tails.)  Bounds (checked against the
+// exp-based logistic on a dense grid, FP32 evaluation):
+//     |sigma_p(z) - sigma(z)| <= 9.2e-4,  |silu_p(z) - silu(z)| <= 7.3e-3
+// for every z (the second is at most 9.2e-4 |z|), below the 2^-9 relative
 // rounding the BF16 activations carry.  Training and deployment use the same
 // function, so the network is fitted with the activation it runs.
-constexpr float kSigQ0 = 1.733397424e+00f, kSigQ1 = -6.256158375e+00f, kSigQ2 = 2.008515691e+01f,
-                kSigQ3 = -4.197323551e+01f, kSigQ4 = 5.177145032e+01f, kSigQ5 = -3.392468509e+01f,
-                kSigQ6 = 9.064074321e+00f;
-constexpr float kSigInvZ = 1.0f / 7.0f;
+//
+// The scale 8 is a power of two so that deployment can run the network on
+// x = z / 8 instead of z with every value scaled exactly (no extra rounding):
+// silu_p(z) / 8 = x sigma(x) with sigma a function of x alone, so the
+// tensor-core pass feeds the inputs and biases of layer 1 divided by 8, the
+// biases of layers 2 and 3 divided by 8, and multiplies layer 4 by 8.
+constexpr float kSigQ0 = 1.981310478e+00f, kSigQ1 = -9.368737072e+00f, kSigQ2 = 3.989676019e+01f,
+                kSigQ3 = -1.137893481e+02f, kSigQ4 = 2.023527075e+02f, kSigQ5 = -2.133724498e+02f,
+                kSigQ6 = 1.215064055e+02f, kSigQ7 = -2.870664878e+01f;
+constexpr float kSigZ = 8.0f, kSigInvZ = 0.125f;
 
 __host__ __device__ __forceinline__ float sig_q(float u)
 {
-    float q = kSigQ6;
+    float q = kSigQ7;
+    q = fmaf(q, u, kSigQ6);
     q = fmaf(q, u, kSigQ5);
     q = fmaf(q, u, kSigQ4);
     q = fmaf(q, u, kSigQ3);
@@ -58,35 +66,41 @@ __host__ __device__ __forceinline__ float sig_q(float u)
     return q;
 }
 
-__host__ __device__ __forceinline__ float sigma_p(float z)
+// sigma_p as a function of x = z / 8
+__host__ __device__ __forceinline__ float sigma_x(float x)
 {
-    const float x = fminf(fmaxf(z * kSigInvZ, -1.0f), 1.0f);
-    return fminf(fmaxf(fmaf(x, sig_q(x * x), 0.5f), 0.0f), 1.0f);
+    const float u = fminf(x * x, 1.0f);
+    return fminf(fmaxf(fmaf(x, sig_q(u), 0.5f), 0.0f), 1.0f);
 }
+
+__host__ __device__ __forceinline__ float sigma_p(float z) { return sigma_x(z * kSigInvZ); }
 
 __host__ __device__ __forceinline__ float silu_p(float z) { return z * sigma_p(z); }
 
-// d silu_p / dz = sigma_p + z sigma_p'; sigma_p' = (Q(u) + 2u Q'(u)) / 7
-// inside |z| < 7, 0 outside
+// d silu_p / dz = sigma_p + z sigma_p'; sigma_p' = (Q(u) + 2u Q'(u)) / 8
+// where |z| < 8 and the clamp of sigma_p is not active, 0 elsewhere (the
+// fitted polynomial reaches 0 and 1 slightly inside |z| = 8)
 __host__ __device__ __forceinline__ float dsilu_p(float z)
 {
-    const float xr = z * kSigInvZ;
-    const float x = fminf(fmaxf(xr, -1.0f), 1.0f), u = x * x;
+    const float x = z * kSigInvZ;
+    const float u = fminf(x * x, 1.0f);
     const float q = sig_q(u);
-    float dq = 6.0f * kSigQ6;
+    float dq = 7.0f * kSigQ7;
+    dq = fmaf(dq, u, 6.0f * kSigQ6);
     dq = fmaf(dq, u, 5.0f * kSigQ5);
     dq = fmaf(dq, u, 4.0f * kSigQ4);
     dq = fmaf(dq, u, 3.0f * kSigQ3);
     dq = fmaf(dq, u, 2.0f * kSigQ2);
     dq = fmaf(dq, u, kSigQ1);
-    const float s = fminf(fmaxf(fmaf(x, q, 0.5f), 0.0f), 1.0f);
-    const float ds = (fabsf(xr) < 1.0f) ? (q + 2.0f * u * dq) * kSigInvZ : 0.0f;
+    const float su = fmaf(x, q, 0.5f);
+    const float s = fminf(fmaxf(su, 0.0f), 1.0f);
+    const float ds = (fabsf(x) < 1.0f && su > 0.0f && su < 1.0f) ? (q + 2.0f * u * dq) * kSigInvZ : 0.0f;
     return s + z * ds;
 }
 
-// The alternative activation (MlpState::act = 1): SiLU with the logistic
-// function from the transcendental unit, sigma(z) = (1 + tanh(z / 2)) / 2
-// with tanh.approx.f32 (absolute error about 2^-11).
+// The other activation: SiLU with the logistic function from the
+// transcendental unit, sigma(z) = (1 + tanh(z / 2)) / 2 with tanh.approx.f32
+// (absolute error about 2^-11).
 __device__ __forceinline__ float tanh_hw(float x)
 {
     float y;
@@ -100,11 +114,47 @@ __device__ __forceinline__ float dsilu_t(float z)
     return s * (1.0f + z * (1.0f - s));
 }
 
-// activation of kind act (0: silu_p, 1: silu_t) and its derivative
+// Activation kinds (MlpState::act, MG_MLP_ACT_*): 0 silu_p on every hidden
+// unit; 1 silu_t on every hidden unit; 2 split: silu_t on the first
+// kSplitTanh units of each hidden layer, silu_p on the rest.  The split keeps
+// both pipes that can evaluate an activation busy at once: per element silu_t
+// costs one transcendental-unit operation (that unit runs at an eighth of the
+// FMA pipe's rate) and 4 FMA-pipe operations, silu_p 11 FMA-pipe operations:
+// with a fraction f of silu_t units the FMA pipe carries 11 - 7f and the
+// transcendental unit 8f FMA-equivalents per element, equal at f = 11/15,
+// so 48 of 64.
+constexpr int kSplitTanh = 48;
+
+__device__ __forceinline__ bool tanh_unit(int act, int col) { return act == 1 || (act == 2 && col < kSplitTanh); }
+__device__ __forceinline__ float act_rt(int act, int col, float z) { return tanh_unit(act, col) ? silu_t(z) : silu_p(z); }
+__device__ __forceinline__ float dact_rt(int act, int col, float z)
+{
+    return tanh_unit(act, col) ? dsilu_t(z) : dsilu_p(z);
+}
+
+// ---- deployment forms on x = z / 8 (see above) --------------------------------
+// g(x) = silu(8x) / 8.  Polynomial units: u = x^2 saturated to [0, 1], the
+// Horner steps, the final fma saturated to [0, 1] (the same values as
+// sigma_x: the .sat modifier is the clamp); tanh units: x (1 + tanh(4x)) / 2.
+__device__ __forceinline__ float mul_sat(float a, float b)
+{
+    float d;
+    asm("mul.rn.sat.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float fma_sat(float a, float b, float c)
+{
+    float d;
+    asm("fma.rn.sat.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float gx_poly(float x) { return x * fma_sat(x, sig_q(mul_sat(x, x)), 0.5f); }
+__device__ __forceinline__ float gx_tanh(float x) { return x * fmaf(0.5f, tanh_hw(4.0f * x), 0.5f); }
 template <int ACT>
-__device__ __forceinline__ float act_f(float z) { return ACT == 0 ? silu_p(z) : silu_t(z); }
-__device__ __forceinline__ float act_rt(int act, float z) { return act == 0 ? silu_p(z) : silu_t(z); }
-__device__ __forceinline__ float dact_rt(int act, float z) { return act == 0 ? dsilu_p(z) : dsilu_t(z); }
+__device__ __forceinline__ float gx(int col, float x)
+{
+    return (ACT == 1 || (ACT == 2 && col < kSplitTanh)) ? gx_tanh(x) : gx_poly(x);
+}
 
 __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi)
 {

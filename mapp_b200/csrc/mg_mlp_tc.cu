@@ -4,22 +4,27 @@
 // inside its training box.
 //
 // k_mlp_rows classifies every row: rows beyond the smeared cut store zeros,
-// rows outside the training box store the FP32 quadrature of the precision
-// form, rows inside are appended to the network-row list.
-// k_mlp_tc runs the network on that list, one CTA of 128 threads per 128-row
-// tile at a time (persistent):
+// rows inside the training box are appended to the front of the row list
+// (and a hashed 1% of them to the audit list), pairs with rows outside it to
+// the back.  k_mlp_fallback gives those rows the FP32 quadrature of the
+// precision form, every lane on a fallback pair (no divergence against
+// network rows).
+// k_mlp_tc runs the network on the front rows, one tile of 128 rows per
+// warpgroup at a time (persistent):
 //   * thread t puts row t of the tile into the BF16 A operand of layer 1 in
 //     shared memory (its TMEM lane is t);
 //   * one thread issues the layer's tcgen05.mma instructions (M = 128,
 //     N = 64, K = 16 each, BF16 operands from shared-memory descriptors, FP32
 //     accumulator in TMEM) and commits them to an mbarrier;
 //   * every thread reads its row's accumulators back with tcgen05.ld, adds
-//     the bias, applies the activation (silu_p on the FMA pipe, or SiLU
-//     through tanh.approx) and writes the BF16 row into the next layer's A
-//     operand; layer 4 (N = 16, 6 used) gives the corrections, to which the
-//     unsmeared spline values at r are added;
-//   * a hashed 1% of network rows is also evaluated by the FP64 quadrature
-//     and the largest deviation per output is recorded (mg_mlp_audit).
+//     the bias, applies the activation and writes the BF16 row into the next
+//     layer's A operand; layer 4 (N = 16, 6 used) gives the corrections, to
+//     which the unsmeared spline values at r are added.
+// The network runs on x = z / 8 (mg_mlp_common.cuh): inputs and biases of
+// the hidden layers are stored divided by 8 and the output layer's scale
+// multiplied by 8, all exact, so the activation needs no scaling.
+// k_mlp_audit evaluates the audit list by the FP64 quadrature and records
+// the largest deviation per output (mg_mlp_audit).
 // Per-pair results go to the FP32 pair scratch in the precision form's
 // layout; densities (k_mlp_densities), the embedding and pass 2 follow.
 //
@@ -60,7 +65,8 @@ struct TcSmem {
     // layer's epilogue overwrites the operand its own MMAs have finished reading)
     __nv_bfloat16 a0[kPipes][kTile * 16];
     __nv_bfloat16 a1[kPipes][kTile * H];
-    float b1[H], b2[H], b3[H], b4[kN4];
+    float b1[H], b2[H], b3[H];  // biases / 8
+    float s4[kN4], m4[kN4];     // output q = s4[q] acc + m4[q] (+ the spline base)
     unsigned long long bar[kPipes];  // mbarriers of MMA completion
     unsigned int tmem_base;
 };
@@ -143,8 +149,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 }
 
 // one layer's epilogue for this thread's row: bias + activation of 64
-// accumulators, 16 columns per TMEM load, BF16 into the K-major A operand `a`
-// of the next layer
+// accumulators (x = z / 8), 16 columns per TMEM load, BF16 into the K-major
+// A operand `a` of the next layer
 template <int ACT>
 __device__ __forceinline__ void epilogue64(uint32_t taddr, const float* __restrict__ bias, __nv_bfloat16* a, int row)
 {
@@ -154,8 +160,10 @@ __device__ __forceinline__ void epilogue64(uint32_t taddr, const float* __restri
         tmem_ld16(taddr + 16 * c, v);
         uint32_t w[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++)
-            w[k] = pack2f(act_f<ACT>(v[2 * k] + bias[16 * c + 2 * k]), act_f<ACT>(v[2 * k + 1] + bias[16 * c + 2 * k + 1]));
+        for (int k = 0; k < 8; k++) {
+            const int col = 16 * c + 2 * k;
+            w[k] = pack2f(gx<ACT>(col, v[2 * k] + bias[col]), gx<ACT>(col + 1, v[2 * k + 1] + bias[col + 1]));
+        }
         *reinterpret_cast<uint4*>(reinterpret_cast<char*>(a) + kmaj_off(kTile, row, 16 * c)) =
             make_uint4(w[0], w[1], w[2], w[3]);
         *reinterpret_cast<uint4*>(reinterpret_cast<char*>(a) + kmaj_off(kTile, row, 16 * c + 8)) =
@@ -277,14 +285,20 @@ __device__ __forceinline__ void issue_layer(uint32_t tmem, const __nv_bfloat16* 
              s > 0 ? 1u : 0u);
 }
 
-// ---- the rows: classification and the network-row list --------------------
+// ---- the rows: classification and the row lists ---------------------------
+// 1% audit selection of network row (pair p, species pair ab)
+__device__ __forceinline__ bool audited(unsigned long long seed, long long p, int ab, int rp)
+{
+    return (mix64(seed ^ ((unsigned long long)p * rp + (unsigned long long)ab)) >> 40) % 100 == 0;
+}
+
 // One thread per listed pair: a pair beyond the smeared cut stores zero
 // densities and pair energies; of an in-cut pair's NT^2 rows (ordered species
-// pairs), those outside the training box store the FP32 quadrature of the
-// precision form (split table), those inside are appended to the
-// network-row list (one atomic per block and round).
-template <int NT, int NQ>
-__global__ void __launch_bounds__(kFFBlock) k_mlp_rows(Dev d, MlpState S)
+// pairs), those inside the training box go to the front of the row list (one
+// atomic per block and round); a pair with rows outside it goes to the back
+// with the mask of those rows (one atomic per warp and round).
+template <int NT>
+__global__ void __launch_bounds__(kFFBlock) k_mlp_rows(Dev d, MlpState S, unsigned long long audit_seed)
 {
     using SL = Slots<NT>;
     constexpr int RP = NT * NT;
@@ -293,10 +307,9 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_rows(Dev d, MlpState S)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const SplitK k = split_consts(d);
     const size_t mp = (size_t)d.maxp;
-    unsigned long long n_fallback = 0;
     for (long long base = (long long)blockIdx.x * kFFBlock; base < d.npairs; base += (long long)gridDim.x * kFFBlock) {
         const long long p = base + threadIdx.x;
-        unsigned net = 0;  // bit ab: row (a, b) goes through the network
+        unsigned net = 0, fb = 0;  // bit ab: row (a, b) goes through the network / the quadrature
         float4 in[RP];
         float r = 0.f;
         if (p < d.npairs) {
@@ -312,16 +325,13 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_rows(Dev d, MlpState S)
                 for (int q = 0; q < SL::NC; q++) out[(SL::PHI + q) * mp] = 0.0f;
             } else {
                 const float rsqf = (float)rsq;
-                const float r_inv = rsqrtf(rsqf);
-                r = rsqf * r_inv;
-                const bool below_rc = rsq < d.cut_sq;
+                r = rsqf * rsqrtf(rsqf);
                 float ai[NT], aj[NT];
 #pragma unroll
                 for (int a = 0; a < NT; a++) {
                     ai[a] = (float)d.alpha[(size_t)i * NT + a];
                     aj[a] = (float)d.alpha[(size_t)j * NT + a];
                 }
-                const Knot k0 = knot_at(r, k);
 #pragma unroll
                 for (int a = 0; a < NT; a++)
 #pragma unroll
@@ -335,22 +345,34 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_rows(Dev d, MlpState S)
                         if (inbox) {
                             float v[4];
                             net_inputs(S.box, r, wi, wj, NT == 1 ? 0 : (a == b ? 2 * a : 1), v);
-                            in[ab] = make_float4(v[0], v[1], v[2], v[3]);
+                            in[ab] = make_float4(v[0] * kSigInvZ, v[1] * kSigInvZ, v[2] * kSigInvZ, v[3] * kSigInvZ);
                             net |= 1u << ab;
-                        } else {
-                            const float4* tr = d.pkS + (size_t)ab * d.nrS;
-                            const float4* tp = d.pkS + (size_t)(NT * NT + comp_idx(a, b)) * d.nrS;
-                            VDer g, f;
-                            if (a >= b) smear_full<NQ, true, false>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
-                            else smear_full<NQ, false, false>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
-                            const float o[6] = {f.v, g.v, f.dr, g.dr, f.da, g.da};
-                            store_row<NT>(d, p, a, b, o);
-                            n_fallback++;
-                        }
+                        } else
+                            fb |= 1u << ab;
                     }
             }
         }
-        // network rows: block-wide slots, one atomic per block
+        // pairs with fallback rows: the back of the list, (pair, row mask), one
+        // atomic per warp
+        {
+            const int cnt = fb ? 1 : 0;
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int tot = __shfl_sync(0xffffffffu, incl, 31);
+            unsigned wbase = 0;
+            if (lane == 31 && tot) wbase = atomicAdd(S.row_n + 2, (unsigned)tot);
+            wbase = __shfl_sync(0xffffffffu, wbase, 31);
+            const long long slot = (long long)wbase + incl - cnt;
+            if (cnt) {
+                if (slot < S.row_cap) S.row_id[S.row_cap - 1 - slot] = make_int2((int)p, (int)fb);
+                else d.status[5] = 2;
+            }
+        }
+        // network rows: block-wide slots at the front, one atomic per block
         const int cnt = __popc(net);
         int incl = cnt;
 #pragma unroll
@@ -378,14 +400,64 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_rows(Dev d, MlpState S)
                     S.row_in[slot] = in[ab];
                     S.row_id[slot] = make_int2((int)p, ab);
                     S.row_r[slot] = r;
+                    if (audited(audit_seed, p, ab, RP)) {
+                        const unsigned ka = atomicAdd(S.row_n + 1, 1u);
+                        if (ka < S.audit_cap) S.audit_rows[ka] = (int)slot;
+                    }
                 } else
                     d.status[5] = 2;
                 slot++;
             }
         __syncthreads();
     }
-    for (int off = 16; off > 0; off >>= 1) n_fallback += __shfl_xor_sync(0xffffffffu, n_fallback, off);
-    if (lane == 0 && n_fallback) atomicAdd(reinterpret_cast<unsigned long long*>(S.audit + 8), n_fallback);
+}
+
+// The fallback rows (back of the row list: pair, mask of its fallback rows):
+// the FP32 quadrature of the precision form (split table), one pair per
+// thread.
+template <int NT, int NQ>
+__global__ void __launch_bounds__(kFFBlock) k_mlp_fallback(Dev d, MlpState S)
+{
+    const SplitK k = split_consts(d);
+    const long long nfb = min((long long)S.row_n[2], S.row_cap);
+    unsigned long long nrows = 0;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nfb; e += (long long)gridDim.x * blockDim.x) {
+        const int2 id = S.row_id[S.row_cap - 1 - e];
+        const long long p = id.x;
+        const int i = d.pair_i[p], j = d.pair_j[p];
+        const double4 xi = d.pos[i], xj = d.pos[j];
+        const double dx0 = xi.x - xj.x, dx1 = xi.y - xj.y, dx2 = xi.z - xj.z;
+        const double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx0, dx0), __dmul_rn(dx1, dx1)), __dmul_rn(dx2, dx2));
+        const float rsqf = (float)rsq;
+        const float r_inv = rsqrtf(rsqf);
+        const float r = rsqf * r_inv;
+        const bool below_rc = rsq < d.cut_sq;
+        const Knot k0 = knot_at(r, k);
+        float ai[NT], aj[NT];
+#pragma unroll
+        for (int a = 0; a < NT; a++) {
+            ai[a] = (float)d.alpha[(size_t)i * NT + a];
+            aj[a] = (float)d.alpha[(size_t)j * NT + a];
+        }
+#pragma unroll
+        for (int a = 0; a < NT; a++)
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                const int ab = a * NT + b;
+                if (!(id.y >> ab & 1)) continue;
+                const float alpha = __fdividef(ai[a] * aj[b], ai[a] + aj[b]);
+                const float4* tr = d.pkS + (size_t)ab * d.nrS;
+                const float4* tp = d.pkS + (size_t)(NT * NT + comp_idx(a, b)) * d.nrS;
+                VDer g, f;
+                if (a >= b) smear_full<NQ, true, false>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
+                else smear_full<NQ, false, false>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
+                const float o[6] = {f.v, g.v, f.dr, g.dr, f.da, g.da};
+                store_row<NT>(d, p, a, b, o);
+                nrows++;
+            }
+    }
+    for (int off = 16; off > 0; off >>= 1) nrows += __shfl_xor_sync(0xffffffffu, nrows, off);
+    if ((threadIdx.x & 31) == 0 && nrows) atomicAdd(reinterpret_cast<unsigned long long*>(S.audit + 8), nrows);
 }
 
 // ---- the network on the listed rows, 128 at a time -------------------------
@@ -406,11 +478,15 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(Dev d, MlpState S)
     load_b(T.w3, S.wbf + OW3, H, H, H);
     load_b(T.w4, S.wbf + OW4, kN4, 8, H);
     for (int k = tid; k < H; k += kTcThreads) {
-        T.b1[k] = S.par[OB1 + k];
-        T.b2[k] = S.par[OB2 + k];
-        T.b3[k] = S.par[OB3 + k];
+        T.b1[k] = S.par[OB1 + k] * kSigInvZ;
+        T.b2[k] = S.par[OB2 + k] * kSigInvZ;
+        T.b3[k] = S.par[OB3 + k] * kSigInvZ;
     }
-    if (tid < kN4) T.b4[tid] = tid < 8 ? S.par[OB4 + tid] : 0.0f;
+    // y = W4 silu(z3) + b4 = 8 W4 g3 + b4; output = y scale + mean
+    if (tid < kN4) {
+        T.s4[tid] = tid < 6 ? kSigZ * S.out_scale[tid] : 0.0f;
+        T.m4[tid] = tid < 6 ? fmaf(S.par[OB4 + tid], S.out_scale[tid], S.out_mean[tid]) : 0.0f;
+    }
     // layer 1's K = 16 columns: the 4 inputs, then zeros (the second 8-column
     // half is never rewritten)
     for (int e = tid; e < kPipes * kTile * 16; e += kTcThreads) (&T.a0[0][0])[e] = __float2bfloat16(0.0f);
@@ -493,7 +569,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(Dev d, MlpState S)
             float base[6], o[6];
             base_f32<NT>(d, aa, bb, cr, base);
 #pragma unroll
-            for (int q = 0; q < 6; q++) o[q] = fmaf(y[q] + T.b4[q], S.out_scale[q], S.out_mean[q]) + base[q];
+            for (int q = 0; q < 6; q++) o[q] = fmaf(y[q], T.s4[q], T.m4[q]) + base[q];
             store_row<NT>(d, p, a, b, o);
         }
     }
@@ -507,25 +583,23 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(Dev d, MlpState S)
 }
 
 // ---- the 1% audit: network rows against the FP64 quadrature ----------------
-// A hashed 1% of the listed network rows is evaluated by the FP64 quadrature
-// and compared with what the network stored; the largest deviation per output
-// and the number of audited rows go to MlpState::audit.
+// The audit list (a hashed 1% of the network rows, chosen by k_mlp_rows) is
+// evaluated by the FP64 quadrature and compared with what the network
+// stored; the largest deviation per output and the number of audited rows go
+// to MlpState::audit.
 template <int NT, int NQ>
-__global__ void __launch_bounds__(kFFBlock) k_mlp_audit(Dev d, MlpState S, unsigned long long audit_seed)
+__global__ void __launch_bounds__(kFFBlock) k_mlp_audit(Dev d, MlpState S)
 {
     using SL = Slots<NT>;
-    constexpr int RP = NT * NT;
     const int lane = threadIdx.x & 31;
     const F32Consts kc = f32_consts(d);
-    const long long nrows = min((long long)*S.row_n, S.row_cap);
+    const long long na = min((long long)S.row_n[1], S.audit_cap);
     const size_t mp = (size_t)d.maxp;
-    unsigned long long n_audit = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *reinterpret_cast<unsigned long long*>(S.audit + 6) = (unsigned long long)na;
     float audit_err[6] = {0, 0, 0, 0, 0, 0};
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nrows; k += (long long)gridDim.x * blockDim.x) {
-        const int2 id = S.row_id[k];
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < na; e += (long long)gridDim.x * blockDim.x) {
+        const int2 id = S.row_id[S.audit_rows[e]];
         const long long p = id.x;
-        const unsigned long long h = mix64(audit_seed ^ ((unsigned long long)p * RP + (unsigned long long)id.y));
-        if ((h >> 40) % 100 != 0) continue;
         const int a = id.y / NT, b = id.y - (id.y / NT) * NT;
         int aa, bb;
         trained_order(a, b, aa, bb);
@@ -548,7 +622,6 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_audit(Dev d, MlpState S, unsig
 #pragma unroll
         for (int q = 0; q < 6; q++)
             if (q & 1 || q < nq) audit_err[q] = fmaxf(audit_err[q], fabsf((float)(qv[q] - o[q])));
-        n_audit++;
     }
 #pragma unroll
     for (int q = 0; q < 6; q++) {
@@ -556,8 +629,6 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_audit(Dev d, MlpState S, unsig
         for (int off = 16; off > 0; off >>= 1) e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, off));
         if (lane == 0 && e > 0.f) atomicMax(reinterpret_cast<unsigned int*>(S.audit) + q, __float_as_uint(e));
     }
-    for (int off = 16; off > 0; off >>= 1) n_audit += __shfl_xor_sync(0xffffffffu, n_audit, off);
-    if (lane == 0 && n_audit) atomicAdd(reinterpret_cast<unsigned long long*>(S.audit + 6), n_audit);
 }
 
 // Densities E and pair energy from the pair scratch the learned pass wrote
@@ -619,7 +690,7 @@ template <int NT, int ACT>
 cudaError_t mlp_force_nt(const Dev& d, const MlpState& S, unsigned long long audit_seed, int st_clc, int* nb,
                          cudaStream_t st, cudaEvent_t* evs)
 {
-    if (!S.row_in || !S.row_id || !S.row_r || !S.row_n || S.row_cap < d.npairs * NT * NT)
+    if (!S.row_in || !S.row_id || !S.row_r || !S.row_n || !S.audit_rows || S.row_cap < d.npairs * NT * NT)
         return cudaErrorInvalidValue;
     const size_t sm = sizeof(TcSmem);
     static int attr_dev = -1;
@@ -633,23 +704,33 @@ cudaError_t mlp_force_nt(const Dev& d, const MlpState& S, unsigned long long aud
         if (e != cudaSuccess) return e;
         attr_dev = dev;
     }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_tc<NT, ACT>, kTcThreads, sm) != cudaSuccess ||
-        per_sm < 1)
-        return cudaErrorInvalidConfiguration;
-    // every resident CTA (the tile count is only known on the device)
+    // every resident CTA (the tile count is only known on the device): two
+    // per SM when their shared memory and registers fit (TMEM holds two
+    // 256-column allocations), from the kernel's own attributes
+    static int per_sm = 0;
+    if (!per_sm) {
+        cudaFuncAttributes fa;
+        int smem_sm = 0;
+        if (cudaFuncGetAttributes(&fa, k_mlp_tc<NT, ACT>) != cudaSuccess ||
+            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
+            return cudaErrorInvalidConfiguration;
+        const long long per_cta_smem = (long long)sm + fa.sharedSizeBytes + 1024;  // + the driver's reserve
+        const int by_smem = (int)(smem_sm / per_cta_smem), by_regs = 65536 / (fa.numRegs * kTcThreads);
+        per_sm = std::max(1, std::min(2, std::min(by_smem, by_regs)));
+    }
     const int g1 = num_sms() * per_sm;
     const int g0 = (int)std::min<long long>((d.npairs + kFFBlock - 1) / kFFBlock, (long long)num_sms() * 8);
     const bool nq3 = d.nq == 3 && d.xi_f[1] == 0.0f;
     const int gd = persistent_grid(d.npairs, 4);
-    cudaError_t e = cudaMemsetAsync(S.row_n, 0, sizeof(unsigned), st);
+    cudaError_t e = cudaMemsetAsync(S.row_n, 0, 4 * sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
     if (evs) cudaEventRecord(evs[0], st);
-    if (nq3) k_mlp_rows<NT, 3><<<std::max(g0, 1), kFFBlock, 0, st>>>(d, S);
-    else k_mlp_rows<NT, 0><<<std::max(g0, 1), kFFBlock, 0, st>>>(d, S);
+    k_mlp_rows<NT><<<std::max(g0, 1), kFFBlock, 0, st>>>(d, S, audit_seed);
+    if (nq3) k_mlp_fallback<NT, 3><<<num_sms() * 8, kFFBlock, 0, st>>>(d, S);
+    else k_mlp_fallback<NT, 0><<<num_sms() * 8, kFFBlock, 0, st>>>(d, S);
     k_mlp_tc<NT, ACT><<<g1, kTcThreads, sm, st>>>(d, S);
-    if (d.nq == 3) k_mlp_audit<NT, 3><<<num_sms() * 2, kFFBlock, 0, st>>>(d, S, audit_seed);
-    else k_mlp_audit<NT, 0><<<num_sms() * 2, kFFBlock, 0, st>>>(d, S, audit_seed);
+    if (d.nq == 3) k_mlp_audit<NT, 3><<<num_sms(), kFFBlock, 0, st>>>(d, S);
+    else k_mlp_audit<NT, 0><<<num_sms(), kFFBlock, 0, st>>>(d, S);
     k_mlp_densities<NT><<<gd, kFFBlock, 0, st>>>(d, 0);
     if (evs) cudaEventRecord(evs[1], st);
     int rows = 0;
@@ -664,10 +745,12 @@ cudaError_t launch_dmd_force_mlp(const Dev& d, const MlpState& S, unsigned long 
                                  cudaStream_t st, cudaEvent_t* evs)
 {
     if (d.npairs > 2147483647LL / 4) return cudaErrorInvalidValue;  // queued rows keep the pair index in an int
-    if (d.nt == 1) return S.act ? mlp_force_nt<1, 1>(d, S, audit_seed, st_clc, nb, st, evs)
-                                : mlp_force_nt<1, 0>(d, S, audit_seed, st_clc, nb, st, evs);
-    if (d.nt == 2) return S.act ? mlp_force_nt<2, 1>(d, S, audit_seed, st_clc, nb, st, evs)
-                                : mlp_force_nt<2, 0>(d, S, audit_seed, st_clc, nb, st, evs);
+    if (d.nt == 1) return S.act == 2   ? mlp_force_nt<1, 2>(d, S, audit_seed, st_clc, nb, st, evs)
+                          : S.act == 1 ? mlp_force_nt<1, 1>(d, S, audit_seed, st_clc, nb, st, evs)
+                                       : mlp_force_nt<1, 0>(d, S, audit_seed, st_clc, nb, st, evs);
+    if (d.nt == 2) return S.act == 2   ? mlp_force_nt<2, 2>(d, S, audit_seed, st_clc, nb, st, evs)
+                          : S.act == 1 ? mlp_force_nt<2, 1>(d, S, audit_seed, st_clc, nb, st, evs)
+                                       : mlp_force_nt<2, 0>(d, S, audit_seed, st_clc, nb, st, evs);
     return cudaErrorInvalidValue;
 }
 

@@ -28,8 +28,13 @@ def _system(tmp_path, n=4, sigma=0.03):
     return mb, w, mb.system_from_workload(w)
 
 
-def test_mlp_gradient_matches_cpu_reference(tmp_path):
+@pytest.mark.parametrize("kind", [0, 2])
+def test_mlp_gradient_matches_cpu_reference(tmp_path, kind):
+    """Loss and gradient of the GPU training kernels against the CPU FP64
+    reference, with the polynomial activation (kind 0) and the split one
+    (kind 2; its tanh.approx units are compared with the exact SiLU)."""
     mb, w, s = _system(tmp_path)
+    s.mlp_set_activation(kind)
     s.mlp_init(*BOX, seed=3)
     rng = np.random.default_rng(0)
     n = 128
@@ -39,7 +44,7 @@ def test_mlp_gradient_matches_cpu_reference(tmp_path):
     scaling = np.array([0.1, -0.2, 0.3, 0.0, 0.05, -0.1, 1.5, 0.7, 2.0, 1.0, 0.3, 0.9], dtype=np.float32)
     p, _ = s.mlp_state(scaling=scaling)
     g_gpu, loss_gpu = s.mlp_grad(x, y)
-    loss_cpu, g_cpu = ref.loss_and_grad(p, x, y, scaling, BOX)
+    loss_cpu, g_cpu = ref.loss_and_grad(p, x, y, scaling, BOX, kind)
     assert abs(loss_gpu - loss_cpu) <= 1e-3 * loss_cpu
     cos = float(g_gpu @ g_cpu / (np.linalg.norm(g_gpu) * np.linalg.norm(g_cpu)))
     rel = float(np.linalg.norm(g_gpu - g_cpu) / np.linalg.norm(g_cpu))
