@@ -934,12 +934,15 @@ def run_ours(args):
                                "frac": tflops(fB, call_ms) / peak, "flops_rule": flop_rules["force_call"]}}
     else:
         bf16 = float(peaks.get("bf16_tflops", 1590.0))
-        fm = MLP_FLOPS_PER_ROW * nt * nt * in_cut
-        roof = {"bound": "tensor", "kernel": "k_dmd_pass1_mlp", "achieved": tflops(fm, p1_ms), "peak": bf16,
+        _, mlp_counts = s.mlp_audit()
+        net_rows = nt * nt * in_cut - int(mlp_counts[1])
+        fm = MLP_FLOPS_PER_ROW * net_rows
+        roof = {"bound": "tensor", "kernel": "k_mlp_rows .. k_mlp_densities (the learned pass 1)",
+                "achieved": tflops(fm, p1_ms), "peak": bf16,
                 "unit": "TFLOP/s", "frac": tflops(fm, p1_ms) / bf16, "traffic": None, "launch_ms": p1_ms,
-                "flops_per_launch": fm,
-                "flops_rule": "network flops per evaluated row x nt^2 rows per half pair inside the smeared cut "
-                              "(rows outside the training box take the quadrature instead)",
+                "flops_per_launch": fm, "network_rows": net_rows,
+                "flops_rule": "network flops per row (17664) x rows inside the training box (nt^2 rows per half "
+                              "pair inside the smeared cut, less the quadrature-fallback rows the call counted)",
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json bf16_tflops)"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -956,8 +959,9 @@ def run_ours(args):
         "forms": forms,
         # library kernels per force call: plain pass 1, embedding, pass 2,
         # reduction; precision prep, density, embedding, force, merge,
-        # reduction; learned pass 1, embedding, pass 2, reduction
-        "gpu_launches": {"fp64": 4, "fp32": 6, "mlp": 4}[args.form] * args.steps,
+        # reduction; learned rows, fallback, network, audit, densities,
+        # embedding, force, merge, reduction
+        "gpu_launches": {"fp64": 4, "fp32": 6, "mlp": 9}[args.form] * args.steps,
         "phases_ms": {"force": t_dev / args.steps, "force.pass1": p1_ms, "force.embed": emb_ms,
                       "force.pass2": p2_ms, "list_rebuild": t_list,
                       "energy_calc": t_energy, "c_d_calc": t_cd, "calc_g": t_g},

@@ -91,3 +91,10 @@ def test_gather_over_two_gloo_ranks(tmp_path):
         assert float(r[2]) == costs[k]
     job = float([l for l in lines if l.startswith("job")][0].split()[1])
     assert job == max(sum(costs[k] for k in p) for p in parts)
+
+
+def test_gather_rejects_duplicate_and_missing_cells():
+    with pytest.raises(RuntimeError, match="two ranks"):
+        shard.gather_results([(0, "a"), (1, "b"), (0, "c")], 2)
+    with pytest.raises(RuntimeError, match="no rank"):
+        shard.gather_results([(0, "a")], 3)
