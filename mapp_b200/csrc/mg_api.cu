@@ -215,8 +215,6 @@ struct mg_system {
     bool own_stream = false;
     size_t cap = 0;          // per-atom capacity (owned + ghost)
     int cap_bins = 0;
-    int* flags = nullptr;
-    int* offs = nullptr;
     void* scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
     double* stage = nullptr;  // device staging for host arrays
@@ -243,6 +241,10 @@ struct mg_system {
     float* mlp_loss = nullptr;
     int mlp_loss_n = 0;
     unsigned long long mlp_calls = 0;
+    GhostCtl* gctl = nullptr;  // device control of the ghost passes (two, ping-pong)
+    unsigned* gtiles = nullptr;  // look-back words of the ghost passes (two halves)
+    int gtiles_cap = 0;
+    int* gticket = nullptr;
     double t_list = 0, t_force = 0, t_energy = 0, t_cd = 0, t_g = 0;
     double t_k[3] = {0, 0, 0};  // DMD force: pass 1, embedding, pass 2
     long long partial_rows = 0;
@@ -324,8 +326,6 @@ int ensure_atoms(mg_system* s, size_t need, size_t keep)
         CHK(dalloc(&d.dE32, cap * nt));
         CHK(dalloc(&d.facc, cap * 8));
     }
-    CHK(dalloc(&s->flags, cap));
-    CHK(dalloc(&s->offs, cap));
     size_t tb = scan_temp_bytes((int)cap);
     if (tb > s->scan_tmp_bytes) {
         CHK(dalloc((char**)&s->scan_tmp, tb));
@@ -442,48 +442,52 @@ int rebuild(mg_system* s)
     cudaStream_t st = s->st;
     CU(cudaEventRecord(s->ev0, st));
     int natms = s->natms, nph = 0;
-    int lo_dim = 0, hi_dim = natms;
     fill_dev_scalars(s);
-    CU(cudaMemsetAsync(d.status, 0, 8 * sizeof(int), st));
-    for (int dim = 0; dim < 3; dim++) {
-        for (int dir = 0; dir < 2; dir++) {
-            int lo = lo_dim, hi = hi_dim;
-            for (int pass = 0; pass < s->comm_need[dim]; pass++) {
-                int tmp_r = natms + nph;
-                int n = hi - lo;
-                int count = 0;
-                if (n > 0) {
-                    d.nph = nph;
-                    d.nall = natms + nph;
-                    CU(launch_ghost_flags(d, lo, hi, dim, dir, s->flags, st));
-                    CU(launch_exclusive_scan(s->flags, s->offs, n, s->scan_tmp, s->scan_tmp_bytes, st));
-                    int last[2];
-                    CU(cudaMemcpyAsync(&last[0], s->offs + n - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-                    CU(cudaMemcpyAsync(&last[1], s->flags + n - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-                    CU(cudaStreamSynchronize(st));
-                    count = last[0] + last[1];
-                    if ((size_t)(natms + nph + count) > s->cap) {
-                        // flags/offs are reallocated by ensure_atoms: recompute them after growing
-                        CHK(ensure_atoms(s, natms + nph + count, natms + nph));
-                        CU(launch_ghost_flags(d, lo, hi, dim, dir, s->flags, st));
-                        CU(launch_exclusive_scan(s->flags, s->offs, n, s->scan_tmp, s->scan_tmp_bytes, st));
-                    }
-                    CU(launch_ghost_scatter(d, lo, hi, dim, dir, s->flags, s->offs, natms + nph, st));
-                }
-                nph += count;
-                hi = natms + nph;
-                lo = tmp_r;
-            }
+    if (!s->gctl) CHK(dalloc(&s->gctl, 2));
+    if (!s->gticket) CHK(dalloc(&s->gticket, 2));
+    // The ghost passes run back to back on the device (bounds and counts in
+    // GhostCtl, one launch per pass); the host reads the final count once.
+    // Ghosts that do not fit the arrays are counted, the arrays grow and the
+    // build runs again.
+    for (int attempt = 0;; attempt++) {
+        const int cap = (int)s->cap, nt_tiles = ghost_tiles(cap);
+        if (2 * nt_tiles > s->gtiles_cap) {
+            CHK(dalloc(&s->gtiles, (size_t)2 * nt_tiles));
+            s->gtiles_cap = 2 * nt_tiles;
         }
-        lo_dim = 0;
-        hi_dim = natms + nph;
+        CU(cudaMemsetAsync(d.status, 0, 8 * sizeof(int), st));
+        CU(cudaMemsetAsync(s->gtiles, 0, (size_t)2 * nt_tiles * sizeof(unsigned), st));
+        CU(cudaMemsetAsync(s->gticket, 0, 2 * sizeof(int), st));
+        CU(launch_ghost_init(d, s->gctl, st));
+        int cur = 0;
+        for (int dim = 0; dim < 3; dim++)
+            for (int dir = 0; dir < 2; dir++)
+                for (int pass = 0; pass < s->comm_need[dim]; pass++) {
+                    const int next_mode = pass + 1 < s->comm_need[dim] ? 0 : (dir == 0 ? 1 : 2);
+                    CU(launch_ghost_pass(d, s->gctl + cur, s->gctl + (cur ^ 1), s->gtiles + cur * nt_tiles,
+                                         s->gtiles + (cur ^ 1) * nt_tiles, s->gticket + cur, s->gticket + (cur ^ 1),
+                                         cap, dim, dir, next_mode, st));
+                    cur ^= 1;
+                }
+        GhostCtl gc;
+        int st_h[8];
+        CU(cudaMemcpyAsync(&gc, s->gctl + cur, sizeof(GhostCtl), cudaMemcpyDeviceToHost, st));
+        CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        if (st_h[4])
+            return fail(MG_ERR_CAPACITY, "ghost image chain deeper than %d swaps (box too small for the cut-off)",
+                        kMaxChain);
+        if (st_h[6]) return fail(MG_ERR_TIMEOUT, "ghost build: a compaction wait ran out");
+        if (gc.over <= 0) {
+            nph = gc.nph;
+            break;
+        }
+        if (attempt == 4) return fail(MG_ERR_CAPACITY, "ghost arrays could not be grown to fit");
+        // the owned atoms are kept; every ghost is rebuilt
+        CHK(ensure_atoms(s, (size_t)natms + (size_t)gc.nph + (size_t)gc.over + s->cap / 2, natms));
     }
     d.nph = nph;
     d.nall = natms + nph;
-    int st_h[8];
-    CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
-    if (st_h[4]) return fail(MG_ERR_CAPACITY, "ghost image chain deeper than %d swaps (box too small for the cut-off)", kMaxChain);
     // bins
     if (d.tot_bin + 1 > s->cap_bins) {
         CHK(dalloc(&d.cell_count, d.tot_bin + 1));
@@ -501,11 +505,18 @@ int rebuild(mg_system* s)
     CU(launch_exclusive_scan(d.cell_count, d.cell_start, d.tot_bin + 1, s->scan_tmp, s->scan_tmp_bytes, st));
     CU(cudaMemsetAsync(s->cursor, 0, (d.tot_bin + 1) * sizeof(int), st));
     CU(launch_cell_fill(d, s->cursor, st));
-    // half list, growing the per-atom capacity on overflow
+    // half list, growing the per-atom capacity on overflow; the scan of the
+    // per-atom counts is queued behind it so that one synchronisation reads
+    // both the overflow word and the pair count
+    int np_h = 0;
     for (int attempt = 0; attempt < 4; attempt++) {
+        int st_h[8];
         CU(cudaMemsetAsync(d.status, 0, 8 * sizeof(int), st));
         CU(launch_neigh(d, st));
+        CU(cudaMemsetAsync(d.nnb + natms, 0, sizeof(int), st));
+        CU(launch_exclusive_scan(d.nnb, d.poff, natms + 1, s->scan_tmp, s->scan_tmp_bytes, st));
         CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CU(cudaMemcpyAsync(&np_h, d.poff + natms, sizeof(int), cudaMemcpyDeviceToHost, st));
         CU(cudaStreamSynchronize(st));
         if (!st_h[0]) break;
         int need = st_h[1] + 16;
@@ -513,11 +524,6 @@ int rebuild(mg_system* s)
         if (attempt == 3) return fail(MG_ERR_CAPACITY, "neighbour list capacity could not be met");
     }
     // compact CSR pair list (pairs sorted by i)
-    CU(cudaMemsetAsync(d.nnb + natms, 0, sizeof(int), st));
-    CU(launch_exclusive_scan(d.nnb, d.poff, natms + 1, s->scan_tmp, s->scan_tmp_bytes, st));
-    int np_h = 0;
-    CU(cudaMemcpyAsync(&np_h, d.poff + natms, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
     CHK(ensure_compact(s, np_h));
     // partial rows: every launcher's grid is at most one block per 256 pairs (or
     // 4 * SMs for the persistent learned-form pass) plus per-atom grids
@@ -980,7 +986,7 @@ int mg_destroy(mg_system* s)
     void* ptrs[] = {d.prf, s->d_pkT, s->d_pk64, s->d_pkS, d.icut, d.icut_n, d.srec, d.dE32, d.facc, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
                     d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status, d.act_j, d.act_slot, d.nact,
-                    s->flags, s->offs, s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor};
+                    s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor, s->gctl, s->gtiles, s->gticket};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     void* mptrs[] = {s->mlp.par, s->mlp.wbf, s->mlp.m, s->mlp.v, s->mlp.gpart, s->mlp.audit, s->mlp_loss,

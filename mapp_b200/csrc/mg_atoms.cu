@@ -67,40 +67,173 @@ __global__ void k_x2s(Dev d)
     d.gchain[i] = 0ull;
 }
 
-// One swap pass of Atoms::ph_setup: flag atoms of [lo, hi) whose s in `dim`
-// lies in the low (dir 0) or high (dir 1) phantom shell.
-__global__ void k_ghost_flags(Dev d, int lo, int hi, int dim, int dir, int* __restrict__ flags)
+// One swap pass of Atoms::ph_setup (atoms.cpp:317-372): the atoms of
+// [lo, hi) whose s in `dim` lies in the low (dir 0) or high (dir 1) phantom
+// shell are appended, in order, as new ghosts: s[dim] shifted by +1 (dir 0)
+// or -1 (dir 1), the phantom vectors copied, (dim, dir) appended to the image
+// chain. The pass's bounds and the ghost count live in a GhostCtl on the
+// device, written by the previous pass, so the passes run back to back
+// without the host.
+//
+// One launch per pass: a stable compaction by decoupled look-back. Each
+// block takes the next tile of kGhostTile atoms (a ticket, so every earlier
+// tile belongs to a block that already runs), counts its flagged atoms,
+// publishes the count, and walks back over the earlier tiles' published
+// counts until it meets an inclusive prefix; then it publishes its own
+// inclusive prefix and scatters. Status words: value in the low 30 bits,
+// bit 30 "count of this tile", bit 31 "prefix through this tile". The block
+// of the last tile writes the next pass's control: next_mode 0 = another
+// pass of this direction (over the ghosts just made), 1 = the other
+// direction of this dimension (over [0, hi_dim)), 2 = the next dimension
+// (over every atom so far). Ghosts beyond `cap` are counted in `over` and not
+// written; the host then grows the arrays and builds again. The tile words
+// and the ticket of the next pass (the other half of the ping-pong) are
+// zeroed here. A look-back wait is bounded; if it runs out, status[6] is set
+// and the host reports the build as failed.
+constexpr int kGhostTile = 2 * kBlock;
+constexpr unsigned kTileAgg = 1u << 30, kTilePrefix = 1u << 31, kTileVal = (1u << 30) - 1;
+
+__global__ void __launch_bounds__(kBlock) k_ghost_pass(Dev d, const GhostCtl* __restrict__ c, GhostCtl* __restrict__ nx,
+                                                       unsigned* __restrict__ tiles, unsigned* __restrict__ tiles_next,
+                                                       int* __restrict__ ticket, int* __restrict__ ticket_next, int cap,
+                                                       int dim, int dir, int next_mode)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= hi - lo) return;
-    double sv = comp3(d.sfr[lo + k], dim);
-    int take = dir == 0 ? (sv <= d.s_ph_lo[dim]) : (d.s_ph_hi[dim] <= sv);
-    flags[k] = take;
+    __shared__ int s_tile, s_excl;
+    __shared__ int s_warp[kBlock / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // the other half of the ping-pong, for the next pass
+    tiles_next[blockIdx.x] = 0u;
+    if (blockIdx.x == 0 && tid == 0) *ticket_next = 0;
+    const int lo = c->lo, n = min(c->hi, cap) - lo, nph = c->nph;
+    const int base = d.natms + nph;
+    const int ntiles = n > 0 ? (n + kGhostTile - 1) / kGhostTile : 0;
+    if (tid == 0) s_tile = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int tile = s_tile;
+    if (ntiles == 0 && tile == 0 && tid == 0) {
+        // nothing to scan: the next pass's control with no new ghosts
+        GhostCtl o;
+        o.nph = nph;
+        o.over = c->over;
+        o.lo = next_mode == 0 ? base : 0;
+        o.hi = next_mode == 1 ? c->hi_dim : d.natms + nph;
+        o.hi_dim = next_mode == 2 ? d.natms + nph : c->hi_dim;
+        *nx = o;
+    }
+    if (tile >= ntiles) return;
+    // flags of this thread's two atoms
+    const int k0 = tile * kGhostTile + 2 * tid;
+    int f[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int k = k0 + q;
+        f[q] = 0;
+        if (k < n) {
+            const double sv = comp3(d.sfr[lo + k], dim);
+            f[q] = dir == 0 ? (sv <= d.s_ph_lo[dim]) : (d.s_ph_hi[dim] <= sv);
+        }
+    }
+    // block-wide exclusive scan of the counts
+    const int mine = f[0] + f[1];
+    int incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < kBlock / 32 ? s_warp[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < kBlock / 32) s_warp[lane] = wi - w;  // exclusive offset of each warp
+        if (lane == kBlock / 32 - 1) {
+            // lane holding the block total: publish, look back, publish the prefix
+            const unsigned total = (unsigned)wi;
+            unsigned excl = 0;
+            bool ok = true;
+            if (tile == 0) {
+                atomicExch(&tiles[0], kTilePrefix | total);
+            } else {
+                atomicExch(&tiles[tile], kTileAgg | total);
+                for (int j = tile - 1; j >= 0;) {
+                    unsigned v = 0;
+                    for (int it = 0; it < (1 << 22); it++) {
+                        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(tiles + j) : "memory");
+                        if (v) break;
+                        __nanosleep(64);
+                    }
+                    if (!v) {
+                        ok = false;
+                        break;
+                    }
+                    excl += v & kTileVal;
+                    if (v & kTilePrefix) break;
+                    j--;
+                }
+                atomicExch(&tiles[tile], kTilePrefix | (excl + total));
+            }
+            if (!ok) atomicExch(&d.status[6], 1);
+            s_excl = (int)excl;
+            if (tile == ntiles - 1) {
+                GhostCtl o;
+                o.nph = nph + (int)(excl + total);
+                o.over = max(c->over, d.natms + o.nph - cap);
+                if (next_mode == 0) {
+                    o.lo = base;
+                    o.hi = d.natms + o.nph;
+                    o.hi_dim = c->hi_dim;
+                } else if (next_mode == 1) {
+                    o.lo = 0;
+                    o.hi = c->hi_dim;
+                    o.hi_dim = c->hi_dim;
+                } else {
+                    o.lo = 0;
+                    o.hi = d.natms + o.nph;
+                    o.hi_dim = o.hi;
+                }
+                *nx = o;
+            }
+        }
+    }
+    __syncthreads();
+    int slot = s_excl + s_warp[warp] + incl - mine;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        if (!f[q]) continue;
+        const int src = lo + k0 + q, g = base + slot++;
+        if (g >= cap) continue;
+        double4 s = d.sfr[src];
+        double v = comp3(s, dim);
+        set3(s, dim, dir == 0 ? dadd(v, 1.0) : dsub(v, 1.0));
+        d.sfr[g] = s;
+        for (int a = 0; a < d.x_dim - 3; a++) d.alpha[(size_t)g * d.nt + a] = d.alpha[(size_t)src * d.nt + a];
+        if (d.c)
+            for (int a = 0; a < d.nt; a++) d.c[(size_t)g * d.nt + a] = d.c[(size_t)src * d.nt + a];
+        if (d.type) d.type[g] = d.type[src];
+        d.root[g] = d.root[src];
+        unsigned long long ch = d.gchain[src];
+        int used = __popcll(ch & 0x8888888888888888ull);
+        if (used < kMaxChain) ch |= (unsigned long long)(8 | (dim << 1) | dir) << (4 * used);
+        else atomicExch(&d.status[4], 1);  // chain too deep: reported as a capacity error
+        d.gchain[g] = ch;
+    }
 }
 
-// Stable scatter of the flagged atoms to new ghost slots base + offs[k]:
-// copy the phantom vectors, shift s[dim] by +1 (dir 0) or -1 (dir 1) and
-// append (dim, dir) to the image chain.
-__global__ void k_ghost_scatter(Dev d, int lo, int hi, int dim, int dir, const int* __restrict__ flags,
-                                const int* __restrict__ offs, int base)
+__global__ void k_ghost_ctl_init(Dev d, GhostCtl* c)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= hi - lo || !flags[k]) return;
-    int src = lo + k, g = base + offs[k];
-    double4 s = d.sfr[src];
-    double v = comp3(s, dim);
-    set3(s, dim, dir == 0 ? dadd(v, 1.0) : dsub(v, 1.0));
-    d.sfr[g] = s;
-    for (int a = 0; a < d.x_dim - 3; a++) d.alpha[(size_t)g * d.nt + a] = d.alpha[(size_t)src * d.nt + a];
-    if (d.c)
-        for (int a = 0; a < d.nt; a++) d.c[(size_t)g * d.nt + a] = d.c[(size_t)src * d.nt + a];
-    if (d.type) d.type[g] = d.type[src];
-    d.root[g] = d.root[src];
-    unsigned long long ch = d.gchain[src];
-    int used = __popcll(ch & 0x8888888888888888ull);
-    if (used < kMaxChain) ch |= (unsigned long long)(8 | (dim << 1) | dir) << (4 * used);
-    else atomicExch(&d.status[4], 1);  // chain too deep: reported as a capacity error
-    d.gchain[g] = ch;
+    GhostCtl o;
+    o.lo = 0;
+    o.hi = d.natms;
+    o.nph = 0;
+    o.hi_dim = d.natms;
+    o.over = 0;
+    *c = o;
 }
 
 // Neighbor::s2bin for every atom, then Atoms::s2x (owned + ghost), counting
@@ -325,16 +458,19 @@ cudaError_t launch_x2s(const Dev& d, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t launch_ghost_flags(const Dev& d, int lo, int hi, int dim, int dir, int* flags, cudaStream_t st)
+cudaError_t launch_ghost_init(const Dev& d, GhostCtl* ctl, cudaStream_t st)
 {
-    if (hi > lo) k_ghost_flags<<<div_up(hi - lo, kBlock), kBlock, 0, st>>>(d, lo, hi, dim, dir, flags);
+    k_ghost_ctl_init<<<1, 1, 0, st>>>(d, ctl);
     return cudaGetLastError();
 }
 
-cudaError_t launch_ghost_scatter(const Dev& d, int lo, int hi, int dim, int dir, const int* flags, const int* offs,
-                                 int base, cudaStream_t st)
+int ghost_tiles(int cap) { return (cap + kGhostTile - 1) / kGhostTile; }
+
+cudaError_t launch_ghost_pass(const Dev& d, const GhostCtl* ctl, GhostCtl* next, unsigned* tiles, unsigned* tiles_next,
+                              int* ticket, int* ticket_next, int cap, int dim, int dir, int next_mode, cudaStream_t st)
 {
-    if (hi > lo) k_ghost_scatter<<<div_up(hi - lo, kBlock), kBlock, 0, st>>>(d, lo, hi, dim, dir, flags, offs, base);
+    k_ghost_pass<<<std::max(ghost_tiles(cap), 1), kBlock, 0, st>>>(d, ctl, next, tiles, tiles_next, ticket,
+                                                                   ticket_next, cap, dim, dir, next_mode);
     return cudaGetLastError();
 }
 

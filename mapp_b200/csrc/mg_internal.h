@@ -103,8 +103,9 @@ struct Dev {
     // reductions
     double* partial;   // [nblocks][8]
     int* status;       // [0] overflow of nbr, [1] needed maxnb, [2] overflow crd, [3] needed maxcrd,
-                       // [4] overflow of the precision form's in-cut list, [5] a learned-form
-                       // tensor-core wait ran out
+                       // [4] overflow of the precision form's in-cut list (in a rebuild: ghost
+                       // chain too deep), [5] a learned-form tensor-core wait ran out, [6] a
+                       // ghost pass's look-back wait ran out
     // tables (device)
     int nr, nrho;
     double dr, drho, dr_inv, drho_inv, rho_max, cut_sq, cut_sq_mod, rc;
@@ -218,9 +219,18 @@ struct MlpState {
 // atoms / neighbour
 cudaError_t launch_x2s(const Dev& d, cudaStream_t st);
 cudaError_t launch_split_x(const Dev& d, const double* x_aos, int frac, cudaStream_t st);
-cudaError_t launch_ghost_flags(const Dev& d, int lo, int hi, int dim, int dir, int* flags, cudaStream_t st);
-cudaError_t launch_ghost_scatter(const Dev& d, int lo, int hi, int dim, int dir, const int* flags,
-                                 const int* offs, int base, cudaStream_t st);
+// bounds of one ghost pass ([lo, hi) scanned), the ghost count so far, the
+// end of the range the current dimension's passes start from, and the number
+// of ghosts that did not fit
+struct GhostCtl {
+    int lo, hi, nph, hi_dim, over;
+};
+cudaError_t launch_ghost_init(const Dev& d, GhostCtl* ctl, cudaStream_t st);
+// one ghost pass: tile words and tickets of this pass and of the next
+// (ping-pong halves, ghost_tiles(cap) words each)
+int ghost_tiles(int cap);
+cudaError_t launch_ghost_pass(const Dev& d, const GhostCtl* ctl, GhostCtl* next, unsigned* tiles, unsigned* tiles_next,
+                              int* ticket, int* ticket_next, int cap, int dim, int dir, int next_mode, cudaStream_t st);
 cudaError_t launch_bin_and_s2x(const Dev& d, cudaStream_t st);
 cudaError_t launch_cell_fill(const Dev& d, int* cursor, cudaStream_t st);
 cudaError_t launch_neigh(const Dev& d, cudaStream_t st);
