@@ -244,7 +244,6 @@ struct mg_system {
     GhostCtl* gctl = nullptr;  // device control of the ghost passes (two, ping-pong)
     unsigned* gtiles = nullptr;  // look-back words of the ghost passes (two halves)
     int gtiles_cap = 0;
-    int* gticket = nullptr;
     double t_list = 0, t_force = 0, t_energy = 0, t_cd = 0, t_g = 0;
     double t_k[3] = {0, 0, 0};  // DMD force: pass 1, embedding, pass 2
     long long partial_rows = 0;
@@ -444,20 +443,23 @@ int rebuild(mg_system* s)
     int natms = s->natms, nph = 0;
     fill_dev_scalars(s);
     if (!s->gctl) CHK(dalloc(&s->gctl, 2));
-    if (!s->gticket) CHK(dalloc(&s->gticket, 2));
     // The ghost passes run back to back on the device (bounds and counts in
-    // GhostCtl, one launch per pass); the host reads the final count once.
-    // Ghosts that do not fit the arrays are counted, the arrays grow and the
-    // build runs again.
+    // GhostCtl, one launch per pass), and so do binning and the half list,
+    // which read the ghost count from the device. One synchronisation reads
+    // the ghost count, the list's overflow word and the pair count; ghosts that
+    // did not fit the arrays make them grow and the build run again, a list
+    // overflow makes the per-atom list capacity grow and the list run again.
+    int np_h = 0;
     for (int attempt = 0;; attempt++) {
         const int cap = (int)s->cap, nt_tiles = ghost_tiles(cap);
-        if (2 * nt_tiles > s->gtiles_cap) {
-            CHK(dalloc(&s->gtiles, (size_t)2 * nt_tiles));
-            s->gtiles_cap = 2 * nt_tiles;
+        // the tile words of both halves, then the two tickets: one memset
+        if (2 * nt_tiles + 2 > s->gtiles_cap) {
+            CHK(dalloc(&s->gtiles, (size_t)2 * nt_tiles + 2));
+            s->gtiles_cap = 2 * nt_tiles + 2;
         }
+        int* gticket = reinterpret_cast<int*>(s->gtiles + 2 * nt_tiles);
         CU(cudaMemsetAsync(d.status, 0, 8 * sizeof(int), st));
-        CU(cudaMemsetAsync(s->gtiles, 0, (size_t)2 * nt_tiles * sizeof(unsigned), st));
-        CU(cudaMemsetAsync(s->gticket, 0, 2 * sizeof(int), st));
+        CU(cudaMemsetAsync(s->gtiles, 0, ((size_t)2 * nt_tiles + 2) * sizeof(unsigned), st));
         CU(launch_ghost_init(d, s->gctl, st));
         int cur = 0;
         for (int dim = 0; dim < 3; dim++)
@@ -465,64 +467,62 @@ int rebuild(mg_system* s)
                 for (int pass = 0; pass < s->comm_need[dim]; pass++) {
                     const int next_mode = pass + 1 < s->comm_need[dim] ? 0 : (dir == 0 ? 1 : 2);
                     CU(launch_ghost_pass(d, s->gctl + cur, s->gctl + (cur ^ 1), s->gtiles + cur * nt_tiles,
-                                         s->gtiles + (cur ^ 1) * nt_tiles, s->gticket + cur, s->gticket + (cur ^ 1),
+                                         s->gtiles + (cur ^ 1) * nt_tiles, gticket + cur, gticket + (cur ^ 1),
                                          cap, dim, dir, next_mode, st));
                     cur ^= 1;
                 }
-        GhostCtl gc;
-        int st_h[8];
-        CU(cudaMemcpyAsync(&gc, s->gctl + cur, sizeof(GhostCtl), cudaMemcpyDeviceToHost, st));
-        CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
-        CU(cudaStreamSynchronize(st));
-        if (st_h[4])
-            return fail(MG_ERR_CAPACITY, "ghost image chain deeper than %d swaps (box too small for the cut-off)",
-                        kMaxChain);
-        if (st_h[6]) return fail(MG_ERR_TIMEOUT, "ghost build: a compaction wait ran out");
-        if (gc.over <= 0) {
-            nph = gc.nph;
-            break;
+        const GhostCtl* gfin = s->gctl + cur;
+        // bins
+        if (d.tot_bin + 1 > s->cap_bins) {
+            CHK(dalloc(&d.cell_count, 2 * ((size_t)d.tot_bin + 1)));
+            CHK(dalloc(&d.cell_start, d.tot_bin + 1));
+            s->cap_bins = d.tot_bin + 1;
+            size_t tb = scan_temp_bytes(d.tot_bin + 1);
+            if (tb > s->scan_tmp_bytes) {
+                CHK(dalloc((char**)&s->scan_tmp, tb));
+                s->scan_tmp_bytes = tb;
+            }
         }
-        if (attempt == 4) return fail(MG_ERR_CAPACITY, "ghost arrays could not be grown to fit");
-        // the owned atoms are kept; every ghost is rebuilt
-        CHK(ensure_atoms(s, (size_t)natms + (size_t)gc.nph + (size_t)gc.over + s->cap / 2, natms));
+        // the fill cursors sit right after this build's counts (the allocation
+        // holds two arrays of cap_bins), so one memset zeroes both
+        s->cursor = d.cell_count + d.tot_bin + 1;
+        CU(cudaMemsetAsync(d.cell_count, 0, 2 * ((size_t)d.tot_bin + 1) * sizeof(int), st));
+        CU(launch_bin_and_s2x(d, gfin, cap, st));
+        CU(launch_exclusive_scan(d.cell_count, d.cell_start, d.tot_bin + 1, s->scan_tmp, s->scan_tmp_bytes, st));
+        CU(launch_cell_fill(d, s->cursor, gfin, cap, st));
+        // half list, then the scan of the per-atom counts
+        bool regrow_ghosts = false;
+        for (int attempt_nb = 0;; attempt_nb++) {
+            GhostCtl gc;
+            int st_h[8];
+            // (the list kernel zeroes nnb[natms], the scan's last element)
+            if (attempt_nb) CU(cudaMemsetAsync(d.status, 0, 2 * sizeof(int), st));
+            CU(launch_neigh(d, st));
+            CU(launch_exclusive_scan(d.nnb, d.poff, natms + 1, s->scan_tmp, s->scan_tmp_bytes, st));
+            CU(cudaMemcpyAsync(&gc, gfin, sizeof(GhostCtl), cudaMemcpyDeviceToHost, st));
+            CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CU(cudaMemcpyAsync(&np_h, d.poff + natms, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CU(cudaStreamSynchronize(st));
+            if (st_h[4])
+                return fail(MG_ERR_CAPACITY, "ghost image chain deeper than %d swaps (box too small for the cut-off)",
+                            kMaxChain);
+            if (st_h[6]) return fail(MG_ERR_TIMEOUT, "ghost build: a compaction wait ran out");
+            if (gc.over > 0) {
+                if (attempt == 4) return fail(MG_ERR_CAPACITY, "ghost arrays could not be grown to fit");
+                // the owned atoms are kept; every ghost is rebuilt
+                CHK(ensure_atoms(s, (size_t)natms + (size_t)gc.nph + (size_t)gc.over + s->cap / 2, natms));
+                regrow_ghosts = true;
+                break;
+            }
+            nph = gc.nph;
+            if (!st_h[0]) break;
+            if (attempt_nb == 3) return fail(MG_ERR_CAPACITY, "neighbour list capacity could not be met");
+            CHK(ensure_pairs(s, st_h[1] + 16));
+        }
+        if (!regrow_ghosts) break;
     }
     d.nph = nph;
     d.nall = natms + nph;
-    // bins
-    if (d.tot_bin + 1 > s->cap_bins) {
-        CHK(dalloc(&d.cell_count, d.tot_bin + 1));
-        CHK(dalloc(&d.cell_start, d.tot_bin + 1));
-        CHK(dalloc(&s->cursor, d.tot_bin + 1));
-        s->cap_bins = d.tot_bin + 1;
-        size_t tb = scan_temp_bytes(d.tot_bin + 1);
-        if (tb > s->scan_tmp_bytes) {
-            CHK(dalloc((char**)&s->scan_tmp, tb));
-            s->scan_tmp_bytes = tb;
-        }
-    }
-    CU(cudaMemsetAsync(d.cell_count, 0, (d.tot_bin + 1) * sizeof(int), st));
-    CU(launch_bin_and_s2x(d, st));
-    CU(launch_exclusive_scan(d.cell_count, d.cell_start, d.tot_bin + 1, s->scan_tmp, s->scan_tmp_bytes, st));
-    CU(cudaMemsetAsync(s->cursor, 0, (d.tot_bin + 1) * sizeof(int), st));
-    CU(launch_cell_fill(d, s->cursor, st));
-    // half list, growing the per-atom capacity on overflow; the scan of the
-    // per-atom counts is queued behind it so that one synchronisation reads
-    // both the overflow word and the pair count
-    int np_h = 0;
-    for (int attempt = 0; attempt < 4; attempt++) {
-        int st_h[8];
-        CU(cudaMemsetAsync(d.status, 0, 8 * sizeof(int), st));
-        CU(launch_neigh(d, st));
-        CU(cudaMemsetAsync(d.nnb + natms, 0, sizeof(int), st));
-        CU(launch_exclusive_scan(d.nnb, d.poff, natms + 1, s->scan_tmp, s->scan_tmp_bytes, st));
-        CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
-        CU(cudaMemcpyAsync(&np_h, d.poff + natms, sizeof(int), cudaMemcpyDeviceToHost, st));
-        CU(cudaStreamSynchronize(st));
-        if (!st_h[0]) break;
-        int need = st_h[1] + 16;
-        CHK(ensure_pairs(s, need));
-        if (attempt == 3) return fail(MG_ERR_CAPACITY, "neighbour list capacity could not be met");
-    }
     // compact CSR pair list (pairs sorted by i)
     CHK(ensure_compact(s, np_h));
     // partial rows: every launcher's grid is at most one block per 256 pairs (or
@@ -986,7 +986,7 @@ int mg_destroy(mg_system* s)
     void* ptrs[] = {d.prf, s->d_pkT, s->d_pk64, s->d_pkS, d.icut, d.icut_n, d.srec, d.dE32, d.facc, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
                     d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status, d.act_j, d.act_slot, d.nact,
-                    s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->cursor, s->gctl, s->gtiles, s->gticket};
+                    s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->gctl, s->gtiles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     void* mptrs[] = {s->mlp.par, s->mlp.wbf, s->mlp.m, s->mlp.v, s->mlp.gpart, s->mlp.audit, s->mlp_loss,

@@ -236,12 +236,19 @@ __global__ void k_ghost_ctl_init(Dev d, GhostCtl* c)
     *c = o;
 }
 
+// owned + ghost atoms: from the ghost build's control on the device (at
+// most cap) when given, else d.nall
+__device__ __forceinline__ int nall_of(const Dev& d, const GhostCtl* gc, int cap)
+{
+    return gc ? min(d.natms + gc->nph, cap) : d.nall;
+}
+
 // Neighbor::s2bin for every atom, then Atoms::s2x (owned + ghost), counting
 // atoms per bin.
-__global__ void k_bin_s2x(Dev d)
+__global__ void k_bin_s2x(Dev d, const GhostCtl* __restrict__ gc, int cap)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.nall) return;
+    if (i >= nall_of(d, gc, cap)) return;
     double4 s = d.sfr[i];
     int no = 0;
     for (int k = 0; k < 3; k++) {
@@ -267,10 +274,10 @@ __device__ __forceinline__ double pack_idx(int idx, int type)
 __device__ __forceinline__ int unpack_idx(double w) { return (int)(__double_as_longlong(w) & 0xffffffffll); }
 __device__ __forceinline__ int unpack_type(double w) { return (int)(__double_as_longlong(w) >> 32); }
 
-__global__ void k_cell_fill(Dev d, int* __restrict__ cursor)
+__global__ void k_cell_fill(Dev d, int* __restrict__ cursor, const GhostCtl* __restrict__ gc, int cap)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.nall) return;
+    if (i >= nall_of(d, gc, cap)) return;
     int b = d.bin[i];
     int slot = d.cell_start[b] + atomicAdd(&cursor[b], 1);
     double4 p = d.pos[i];
@@ -331,6 +338,7 @@ __global__ void __launch_bounds__(kBlock) k_neigh(Dev d)
     }
     if (lane == 0) {
         d.nnb[i] = min(cnt, d.maxnb);
+        if (i == 0) d.nnb[d.natms] = 0;  // the scan's extra element (pair count at poff[natms])
         if (cnt > d.maxnb) {
             d.status[0] = 1;
             atomicMax(&d.status[1], cnt);
@@ -474,15 +482,17 @@ cudaError_t launch_ghost_pass(const Dev& d, const GhostCtl* ctl, GhostCtl* next,
     return cudaGetLastError();
 }
 
-cudaError_t launch_bin_and_s2x(const Dev& d, cudaStream_t st)
+cudaError_t launch_bin_and_s2x(const Dev& d, const GhostCtl* gc, int cap, cudaStream_t st)
 {
-    if (d.nall) k_bin_s2x<<<div_up(d.nall, kBlock), kBlock, 0, st>>>(d);
+    const int n = gc ? cap : d.nall;
+    if (n) k_bin_s2x<<<div_up(n, kBlock), kBlock, 0, st>>>(d, gc, cap);
     return cudaGetLastError();
 }
 
-cudaError_t launch_cell_fill(const Dev& d, int* cursor, cudaStream_t st)
+cudaError_t launch_cell_fill(const Dev& d, int* cursor, const GhostCtl* gc, int cap, cudaStream_t st)
 {
-    if (d.nall) k_cell_fill<<<div_up(d.nall, kBlock), kBlock, 0, st>>>(d, cursor);
+    const int n = gc ? cap : d.nall;
+    if (n) k_cell_fill<<<div_up(n, kBlock), kBlock, 0, st>>>(d, cursor, gc, cap);
     return cudaGetLastError();
 }
 

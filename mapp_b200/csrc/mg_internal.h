@@ -231,8 +231,10 @@ cudaError_t launch_ghost_init(const Dev& d, GhostCtl* ctl, cudaStream_t st);
 int ghost_tiles(int cap);
 cudaError_t launch_ghost_pass(const Dev& d, const GhostCtl* ctl, GhostCtl* next, unsigned* tiles, unsigned* tiles_next,
                               int* ticket, int* ticket_next, int cap, int dim, int dir, int next_mode, cudaStream_t st);
-cudaError_t launch_bin_and_s2x(const Dev& d, cudaStream_t st);
-cudaError_t launch_cell_fill(const Dev& d, int* cursor, cudaStream_t st);
+// over owned + ghost atoms, their count from gc (the ghost build's control,
+// clamped to cap) when gc is given, else d.nall
+cudaError_t launch_bin_and_s2x(const Dev& d, const GhostCtl* gc, int cap, cudaStream_t st);
+cudaError_t launch_cell_fill(const Dev& d, int* cursor, const GhostCtl* gc, int cap, cudaStream_t st);
 cudaError_t launch_neigh(const Dev& d, cudaStream_t st);
 cudaError_t launch_pairs_compact(const Dev& d, cudaStream_t st);
 cudaError_t launch_store_x0(const Dev& d, cudaStream_t st);
