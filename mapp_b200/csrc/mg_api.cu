@@ -1903,6 +1903,19 @@ int mg::system_enqueue_calc_g(mg_system* s, int chk, double alpha, int* rows)
     CU(launch_reduce_partials(d, *rows, 1, s->red_out, s->st));
     return MG_OK;
 }
+int mg::system_enqueue_calc_g_dev(mg_system* s, const int* chk_dev, const double* alpha_dev, int* rows)
+{
+    if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "calc_g needs a DMD force field");
+    if (!s->crd_built) return fail(MG_ERR_STATE, "create_2nd_neigh_lst must run before calc_g");
+    CHK(ensure_pair_values(s));
+    Dev d = s->d;
+    d.g_chk = chk_dev;
+    d.g_alpha = alpha_dev;
+    CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
+    CU(launch_dmd_calc_g(d, 0, 0.0, rows, s->st));
+    CU(launch_reduce_partials(d, *rows, 1, s->red_out, s->st));
+    return MG_OK;
+}
 int mg::system_set_active_pairs(mg_system* s, bool on)
 {
     Dev& d = s->d;

@@ -351,6 +351,181 @@ __global__ void __launch_bounds__(kCkBlock) k_bdf_hilo(CkView V, BdfVecs B, BdfH
     }
 }
 
+// ---- Clock_BDF::solve's line search, steered on the device ------------------
+// The conjugate-gradient iterations of Clock_BDF::solve (clock_bdf.cpp:
+// 727-828) run as one CUDA graph: a conditional WHILE node whose body is one
+// calc_g with its step set-up and its decision, so a solve synchronises with
+// the host once instead of once per calc_g. The scalar control (Armijo test,
+// step reduction, restore of c0, direction update) is the reference's,
+// evaluated by one thread in the same order of operations (explicitly
+// rounded: no contraction into fused multiply-adds), so the device takes the
+// steps the host loop took.
+struct SolveDev {
+    double tol, min_gamma, gamma_red, slope;  // m_tol * dof, and the options
+    double alpha;                             // calc_g's alpha (the step's beta)
+    double curr_cost, cost, g0_g0, g_h, bound, max_gamma, g_g, g_g0, ratio;
+    int max_iter, iter, chk;
+    int mode;       // the body's calc_g: 0 at a trial point, 1 after restoring c0
+    int calc_chk;   // calc_g's chk argument for the body (read by the g kernels)
+    int line_done;  // the line search ended with this calc_g
+    int need_next;  // a direction update follows (the line search succeeded)
+    int copy_hg;    // h = g (the updated direction pointed uphill)
+    int overrun;    // the iteration guard ended the loop
+    long long n_calc_g;
+};
+
+// more body iterations than max_iter line searches of at most
+// log(min_gamma) / log(gamma_red) trials each can take: a guard against a
+// loop that does not end, reported as MG_ERR_TIMEOUT
+constexpr long long kBsGuard = 100000;
+
+// the top of the outer loop: its test, then the next line search's start;
+// true when a calc_g follows, false when the solve is over
+__device__ bool bs_outer_top(SolveDev& S)
+{
+    for (;;) {
+        if (!(S.curr_cost > S.tol && S.iter < S.max_iter && S.max_gamma > S.min_gamma)) return false;
+        // min(0.99, the box bounds along h) (clock_bdf.cpp:744-759)
+        const double gamma = S.bound < 0.99 ? S.bound : 0.99;
+        S.max_gamma = dmul(gamma, 0.9);
+        S.chk = 1;
+        S.cost = S.curr_cost;
+        if (S.max_gamma > S.min_gamma) {
+            S.mode = 0;
+            S.calc_chk = 0;
+            return true;
+        }
+        S.iter++;  // an empty line search: chk stays 1, no direction update
+    }
+}
+
+// after the first calc_g and the first direction (k_ck_first_dir)
+__global__ void k_bs_init(SolveDev* S, const double* red_out, const double* sc, cudaGraphConditionalHandle h)
+{
+    if (threadIdx.x) return;
+    S->curr_cost = dmul(red_out[0], 0.25);
+    S->g0_g0 = sc[SC_G0G0];
+    S->g_h = S->g0_g0;
+    S->bound = sc[SC_GAMMA];
+    S->max_gamma = 1.0;
+    S->iter = 0;
+    S->n_calc_g = 0;
+    S->overrun = 0;
+    cudaGraphSetConditional(h, bs_outer_top(*S) ? 1u : 0u);
+}
+
+// the body's point: c0 + max_gamma h, or c0 itself after a failed line
+// search; ghosts from their owners (what the reference's refresh copies)
+__global__ void __launch_bounds__(kCkBlock) k_bs_trial(CkView V, const SolveDev* S)
+{
+    const int i = blockIdx.x * kCkBlock + threadIdx.x;
+    const bool restore = S->mode == 1;
+    const double gamma = S->max_gamma;
+    if (i < V.n) {
+        V.c[i] = restore ? V.c0[i] : dadd(V.c0[i], dmul(gamma, V.h[i]));
+        return;
+    }
+    const int k = i - V.n;
+    if (k >= V.nph * V.nt) return;
+    const int gq = k / V.nt, a = k - gq * V.nt;
+    const size_t o = (size_t)V.root[V.natms + gq] * V.nt + a;
+    V.c[(size_t)(V.natms + gq) * V.nt + a] = restore ? V.c0[o] : dadd(V.c0[o], dmul(gamma, V.h[o]));
+}
+
+// the Armijo test of the body's calc_g and the step reduction
+// (clock_bdf.cpp:760-806)
+__global__ void k_bs_post(SolveDev* S, const double* red_out, const double* sc)
+{
+    if (threadIdx.x) return;
+    S->n_calc_g++;
+    S->curr_cost = dmul(red_out[0], 0.25);
+    S->g_g0 = sc[SC_GG0];
+    S->g_g = sc[SC_GG];
+    S->need_next = 0;
+    S->line_done = 1;
+    if (S->mode == 0) {
+        const double ideal = dsub(S->cost, dmul(dmul(S->slope, S->max_gamma), S->g_h));
+        if (S->curr_cost < ideal) S->chk = 0;
+        S->max_gamma = dmul(S->max_gamma, S->gamma_red);
+        if (S->max_gamma <= S->min_gamma) {
+            // restore c0 and take the cost there (calc_g with chk = 1)
+            S->mode = 1;
+            S->calc_chk = 1;
+            S->line_done = 0;
+            return;
+        }
+        if (S->chk) {
+            S->calc_chk = 0;
+            S->line_done = 0;
+            return;
+        }
+    }
+    if (S->chk == 0) {
+        S->ratio = ddiv(dsub(S->g_g, S->g_g0), S->g0_g0);
+        S->g0_g0 = S->g_g;
+        S->need_next = 1;
+    }
+}
+
+// the direction update when the line search succeeded (k_ck_next_dir)
+__global__ void __launch_bounds__(kCkBlock) k_bs_next_dir(CkView V, const SolveDev* S)
+{
+    if (!S->need_next) return;
+    const double ratio = S->ratio;
+    const int i = blockIdx.x * kCkBlock + threadIdx.x;
+    double v[3] = {0.0, 1.0, 1.0};
+    if (i < V.n) {
+        const double gi = V.g[i], ci = V.c[i];
+        const double hi = dadd(dmul(V.h[i], ratio), gi);
+        V.h[i] = hi;
+        V.g0[i] = gi;
+        V.c0[i] = ci;
+        v[0] = dmul(hi, gi);
+        v[1] = box_bound(ci, dadd(ci, hi), 1.0);
+        v[2] = box_bound(ci, dadd(ci, gi), 1.0);
+    }
+    double tot[3];
+    if (reduce_last<3, 6u>(v, V, tot) && threadIdx.x == 0) {
+        V.sc[SC_GH] = tot[0];
+        V.sc[SC_GAMMA] = tot[1];
+        V.sc[SC_B] = tot[2];
+    }
+}
+
+// the end of an outer iteration: h.g, the step bounds, the restart from g
+// when h.g < 0 (clock_bdf.cpp:810-828), then the outer loop's test
+__global__ void k_bs_fin(SolveDev* S, const double* sc, cudaGraphConditionalHandle h)
+{
+    if (threadIdx.x) return;
+    bool go = true;
+    S->copy_hg = 0;
+    if (S->line_done) {
+        if (S->need_next) {
+            S->g_h = sc[SC_GH];
+            S->bound = sc[SC_GAMMA];
+            if (S->g_h < 0.0) {
+                S->copy_hg = 1;
+                S->g_h = S->g_g;
+                S->bound = sc[SC_B];
+            }
+        }
+        S->iter++;
+        go = bs_outer_top(*S);
+    }
+    if (go && S->n_calc_g >= kBsGuard) {
+        S->overrun = 1;
+        go = false;
+    }
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(kCkBlock) k_bs_copy(CkView V, const SolveDev* S)
+{
+    if (!S->copy_hg) return;
+    const int i = blockIdx.x * kCkBlock + threadIdx.x;
+    if (i < V.n) V.h[i] = V.g[i];
+}
+
 constexpr double kBeta[6][6] = {
     {1.0, 0, 0, 0, 0, 0},
     {1.0 / 2.0, 1.0 / 2.0, 0, 0, 0, 0},
@@ -492,7 +667,73 @@ struct Bdf {
     double alpha_y[kMaxBdfOrder + 1], dalpha_y[kMaxBdfOrder + 1], lwr_alpha[kMaxBdfOrder + 1];
     double alpha_dy_0 = 0, dalpha_dy_0 = 0, beta = 0, err = 0, lo_err = 0, hi_err = 0, eq_ratio = 0;
 
+    // the line search's graph (captured once per run) and its device state
+    SolveDev* S_dev = nullptr;
+    cudaGraph_t ls_graph = nullptr;
+    cudaGraphExec_t ls_exec = nullptr;
+    ~Bdf()
+    {
+        if (ls_exec) cudaGraphExecDestroy(ls_exec);
+        if (ls_graph) cudaGraphDestroy(ls_graph);
+        cudaFree(S_dev);
+    }
+
     int grid() const { return ck->V.nblocks; }
+
+    // one iteration of the line search: the point, calc_g (chk and alpha from
+    // the device state), the dot products, the Armijo test, the direction
+    // update, the outer loop's test
+    int enqueue_ls_body(cudaGraphConditionalHandle h)
+    {
+        k_bs_trial<<<ck->trial_grid(), kCkBlock, 0, ck->st>>>(ck->V, S_dev);
+        KCU(cudaGetLastError());
+        int rows = 0;
+        KCHK(system_enqueue_calc_g_dev(ck->s, &S_dev->calc_chk, &S_dev->alpha, &rows));
+        k_ck_dots<<<grid(), kCkBlock, 0, ck->st>>>(ck->V);
+        k_bs_post<<<1, 32, 0, ck->st>>>(S_dev, system_red_out(ck->s), ck->V.sc);
+        k_bs_next_dir<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, S_dev);
+        k_bs_fin<<<1, 32, 0, ck->st>>>(S_dev, ck->V.sc, h);
+        k_bs_copy<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, S_dev);
+        KCU(cudaGetLastError());
+        return MG_OK;
+    }
+
+    // graph: k_bs_init, then WHILE (condition set by k_bs_init and k_bs_fin)
+    int build_ls_graph()
+    {
+        KCU(cudaMalloc(&S_dev, sizeof(SolveDev)));
+        KCU(cudaGraphCreate(&ls_graph, 0));
+        cudaGraphConditionalHandle h;
+        KCU(cudaGraphConditionalHandleCreate(&h, ls_graph, 0, cudaGraphCondAssignDefault));
+        SolveDev* S = S_dev;
+        const double* red = system_red_out(ck->s);
+        const double* sc = ck->V.sc;
+        void* args[] = {&S, &red, &sc, &h};
+        cudaKernelNodeParams kp = {};
+        kp.func = (void*)k_bs_init;
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(32);
+        kp.sharedMemBytes = 0;
+        kp.kernelParams = args;
+        cudaGraphNode_t init;
+        KCU(cudaGraphAddKernelNode(&init, ls_graph, nullptr, 0, &kp));
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        KCU(cudaGraphAddNode(&node, ls_graph, &init, 1, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        KCU(cudaStreamBeginCaptureToGraph(ck->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        const int rc = enqueue_ls_body(h);
+        cudaGraph_t out = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(ck->st, &out);
+        if (rc != MG_OK) return rc;
+        KCU(e);
+        KCU(cudaGraphInstantiate(&ls_exec, ls_graph, 0));
+        return MG_OK;
+    }
 
     // Clock_BDF::interpolate (clock_bdf.cpp:295-368) -> 1 or -1
     int interpolate(double del_t, int q, int* ret)
@@ -532,79 +773,47 @@ struct Bdf {
     }
 
     // Clock_BDF::solve (clock_bdf.cpp:677-884); *out = the cost ratio.  The
-    // error estimate there reads an uninitialised local curr_t
-    // (clock_bdf.cpp:838-854) which the reference built with gcc -O2
-    // evaluates as 0.0; so does this.
+    // predictor, the first calc_g and the first direction are enqueued, then
+    // the line search runs as one graph launch (k_bs_*), and the error sums
+    // come back with its state in one synchronisation.  The error estimate
+    // there reads an uninitialised local curr_t (clock_bdf.cpp:838-854) which
+    // the reference built with gcc -O2 evaluates as 0.0; so does this.
     int solve(double del_t, int q, double* out)
     {
         const mg_bdf_opts& o = p;
-        double gamma, max_gamma = 1.0, ratio, g0_g0, g_g, g_g0, g_h, curr_cost, ideal_cost, cost;
-        int chk;
         k_bdf_predict_bound<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, y[0], B.dy, del_t);
         k_bdf_predict<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, y[0], B.dy, del_t);
         KCU(cudaGetLastError());
         KCHK(ck->refresh_c());
-        KCHK(ck->calc_g(0, beta, &curr_cost));
+        int rows = 0;
+        KCHK(system_enqueue_calc_g(ck->s, 0, beta, &rows));
+        ck->n_calc_g++;
         // h = g, and the first iteration's g0, c0 and step bound with it
         k_ck_first_dir<<<grid(), kCkBlock, 0, ck->st>>>(ck->V);
         KCU(cudaGetLastError());
+        SolveDev hs{};
+        hs.tol = o.m_tol * (double)dof_tot;
+        hs.min_gamma = o.min_gamma;
+        hs.gamma_red = o.gamma_red;
+        hs.slope = o.slope;
+        hs.alpha = beta;
+        hs.max_iter = o.max_iter;
+        KCU(cudaMemcpyAsync(S_dev, &hs, sizeof(SolveDev), cudaMemcpyHostToDevice, ck->st));
+        KCU(cudaGraphLaunch(ls_exec, ck->st));
+        k_bdf_err<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, B);
+        KCU(cudaGetLastError());
+        SolveDev r{};
+        KCU(cudaMemcpyAsync(&r, S_dev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ck->st));
         KCHK(ck->read_scalars());
-        g0_g0 = ck->host_sc[SC_G0G0];
-        g_h = g0_g0;
-        double bound = ck->host_sc[SC_GAMMA];
-        int iter = 0;
-        while (curr_cost > o.m_tol * (double)dof_tot && iter < o.max_iter && max_gamma > o.min_gamma) {
-            // min(0.99, the box bounds along h) (clock_bdf.cpp:744-759)
-            gamma = bound < 0.99 ? bound : 0.99;
-            max_gamma = gamma * 0.9;
-            chk = 1;
-            cost = curr_cost;
-            while (chk && max_gamma > o.min_gamma) {
-                k_ck_trial<<<ck->trial_grid(), kCkBlock, 0, ck->st>>>(ck->V, max_gamma);
-                KCU(cudaGetLastError());
-                // the dot products g.g0, g.g ride along with the cost readback
-                KCHK(ck->calc_g(0, beta, &curr_cost, true));
-                ideal_cost = cost - o.slope * max_gamma * g_h;
-                if (curr_cost < ideal_cost) chk = 0;
-                max_gamma *= o.gamma_red;
-                if (max_gamma <= o.min_gamma) {
-                    KCU(cudaMemcpyAsync(ck->V.c, ck->V.c0, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice,
-                                        ck->st));
-                    KCHK(ck->refresh_c());
-                    // the cost-only call zeroes g, so the dots become 0
-                    KCHK(ck->calc_g(1, beta, &curr_cost, true));
-                }
-            }
-            if (chk == 0) {
-                g_g0 = ck->host_sc[SC_GG0];
-                g_g = ck->host_sc[SC_GG];
-                ratio = (g_g - g_g0) / g0_g0;
-                g0_g0 = g_g;
-                // the new direction, and the next iteration's g0, c0 and bound
-                // (a failed line search ends the loop: max_gamma <= min_gamma)
-                k_ck_next_dir<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, ratio);
-                KCU(cudaGetLastError());
-                KCHK(ck->read_scalars());
-                g_h = ck->host_sc[SC_GH];
-                bound = ck->host_sc[SC_GAMMA];
-                if (g_h < 0.0) {
-                    KCU(cudaMemcpyAsync(ck->V.h, ck->V.g, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice,
-                                        ck->st));
-                    g_h = g_g;
-                    bound = ck->host_sc[SC_B];
-                }
-            }
-            iter++;
-        }
+        ck->n_calc_g += r.n_calc_g;
+        if (r.overrun) return internal_fail(MG_ERR_TIMEOUT, "BDF clock: the line search did not end");
+        const double curr_cost = r.curr_cost;
         double a_1 = 1.0, curr_t = 0.0, l1_q = 0.0, err_pre_fac;
         for (int i = 0; i < q; i++) {
             l1_q += 1.0 / (curr_t - t[i]);
             if (i != 0) a_1 *= (curr_t - t[i]) / (t[0] - t[i]);
         }
         err_pre_fac = -1.0 / (l1_q * (1.0 + a_1));
-        k_bdf_err<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, B);
-        KCU(cudaGetLastError());
-        KCHK(ck->read_scalars());
         eq_ratio = sqrt(ck->host_sc[SC_GG] / (double)dof_tot) / o.e_tol;
         err = sqrt(ck->host_sc[SC_GG0] / ((double)dof_tot * o.a_tol));
         err *= fabs(err_pre_fac);
@@ -888,6 +1097,7 @@ extern "C" int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, d
     ck.V.nph = d.nph;
     ck.V.nt = nt;
     KCU(cudaMemsetAsync(ck.block, 0, total * sizeof(double), ck.st));
+    KCHK(b.build_ls_graph());
     KCHK(system_enqueue_c_d(s));
     const size_t bytes = (size_t)n * sizeof(double);
     double initial_del_t = o.initial_del_t;

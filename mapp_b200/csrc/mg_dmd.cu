@@ -594,6 +594,7 @@ __global__ void k_g_sinit(Dev d, int mode)
 template <int NT, int G>
 __global__ void __launch_bounds__(kFFBlock) k_g_srates(Dev d, double alpha)
 {
+    if (d.g_alpha) alpha = *d.g_alpha;
     int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
@@ -636,6 +637,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_srates(Dev d, double alpha)
 template <int NT>
 __global__ void __launch_bounds__(kFFBlock) k_g_cost(Dev d, int row0, int chk)
 {
+    if (d.g_chk) chk = *d.g_chk;
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     if (idx < d.natms * NT) {
@@ -655,6 +657,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_cost(Dev d, int row0, int chk)
 template <int NT, int G>
 __global__ void __launch_bounds__(kFFBlock) k_g_trates(Dev d, double alpha)
 {
+    if (d.g_chk && *d.g_chk) return;  // cost-only call: no g terms
+    if (d.g_alpha) alpha = *d.g_alpha;
     int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
@@ -723,6 +727,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_trates(Dev d, double alpha)
 template <int NT, typename P, int G>
 __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
 {
+    if (d.g_chk && *d.g_chk) return;  // cost-only call: no g terms
+    if (d.g_alpha) alpha = *d.g_alpha;
     using S = Slots<NT>;
     int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     int lane = threadIdx.x & (G - 1);
@@ -784,6 +790,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
 template <int NT, typename P, int G>
 __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
 {
+    if (d.g_chk && *d.g_chk) return;  // cost-only call: no g terms
+    if (d.g_alpha) alpha = *d.g_alpha;
     int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
@@ -914,7 +922,7 @@ cudaError_t dmd_calc_g_ntp(const Dev& d, int chk, double alpha, int* nb, cudaStr
     k_g_srates<NT, kCrdLanes><<<gc, kFFBlock, 0, st>>>(d, alpha);
     k_g_cost<NT><<<gs, kFFBlock, 0, st>>>(d, 0, chk);
     *nb = gs;
-    if (!chk) {
+    if (!chk || d.g_chk) {
         k_g_trates<NT, kCrdLanes><<<gc, kFFBlock, 0, st>>>(d, alpha);
         k_g_vpass<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d, alpha);
         k_g_last<NT, P, kNbrLanes><<<gw, kFFBlock, 0, st>>>(d, alpha);

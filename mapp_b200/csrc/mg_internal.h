@@ -100,6 +100,12 @@ struct Dev {
     long long* act_slot;
     int* nact;
     int act_on;
+    // calc_g's chk and alpha read from device memory (a device-steered solve
+    // changes them between graph iterations) when set, else the launch's
+    // arguments; with g_chk set the g passes are always enqueued and return
+    // at once when *g_chk is non-zero
+    const int* g_chk;
+    const double* g_alpha;
     // reductions
     double* partial;   // [nblocks][8]
     int* status;       // [0] overflow of nbr, [1] needed maxnb, [2] overflow crd, [3] needed maxcrd,
@@ -324,6 +330,9 @@ double* system_red_out(mg_system* s);
 // enqueue calc_g's device work on the system's a_in (cost * 4 left in red_out[0],
 // g in the system's g unless chk) and c_d_calc's (c_d in the system's c_d); capturable
 int system_enqueue_calc_g(mg_system* s, int chk, double alpha, int* rows);
+// the same with chk and alpha read from device memory at run time (for a
+// captured loop whose iterations change them)
+int system_enqueue_calc_g_dev(mg_system* s, const int* chk_dev, const double* alpha_dev, int* rows);
 int system_enqueue_c_d(mg_system* s);
 // builds the active-pair sublist from the last force_calc's pair values and
 // makes c_d_calc / calc_g walk it (on), or walk the full list again (off);
