@@ -220,7 +220,7 @@ struct mg_system {
     double* stage = nullptr;  // device staging for host arrays
     size_t stage_cap = 0;
     size_t act_cap = 0;   // capacity of the active-pair sublist (entries)
-    size_t nact_cap = 0;  // and of its per-site counts (sites)
+    size_t nact_cap = 0;  // and of its per-site counts and offsets (sites + 1)
     double* red_out = nullptr;  // 8 doubles
     double* d_rhoT = nullptr;
     double* d_phiT = nullptr;
@@ -985,7 +985,7 @@ int mg_destroy(mg_system* s)
     Dev& d = s->d;
     void* ptrs[] = {d.prf, s->d_pkT, s->d_pk64, s->d_pkS, d.icut, d.icut_n, d.srec, d.dE32, d.facc, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
-                    d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status, d.act_j, d.act_slot, d.nact,
+                    d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status, d.act_pj, d.act_pv, d.act_off, d.nact,
                     s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->gctl, s->gtiles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1924,18 +1924,27 @@ int mg::system_set_active_pairs(mg_system* s, bool on)
         return MG_OK;
     }
     if (!s->dmd || s->form != MG_FORM_FP64 || s->natms == 0) return MG_OK;
-    const size_t cap = (size_t)s->natms * d.maxnb;
-    if (cap > s->act_cap) {
-        CHK(dalloc(&d.act_j, cap));
-        CHK(dalloc(&d.act_slot, cap));
-        s->act_cap = cap;
-    }
-    if ((size_t)s->natms > s->nact_cap) {
-        CHK(dalloc(&d.nact, (size_t)s->natms));
-        s->nact_cap = (size_t)s->natms;
+    if ((size_t)s->natms + 1 > s->nact_cap) {
+        CHK(dalloc(&d.nact, (size_t)s->natms + 1));
+        CHK(dalloc(&d.act_off, (size_t)s->natms + 1));
+        s->nact_cap = (size_t)s->natms + 1;
     }
     d.act_on = 0;
-    CU(launch_active_pairs(d, s->st));
+    CHK(ensure_pair_values(s));
+    CU(launch_active_count(d, s->st));
+    CU(launch_exclusive_scan(d.nact, d.act_off, s->natms + 1, s->scan_tmp, s->scan_tmp_bytes, s->st));
+    int total = 0;
+    CU(cudaMemcpyAsync(&total, d.act_off + s->natms, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    const int nvals = s->nt * s->nt + s->nt * (s->nt + 1) / 2;
+    if ((size_t)total + 1 > s->act_cap) {
+        const size_t cap = (size_t)total + (size_t)total / 8 + 64;
+        CHK(dalloc(&d.act_pj, cap));
+        CHK(dalloc(&d.act_pv, cap * nvals));
+        s->act_cap = cap;
+    }
+    d.act_cap = (long long)s->act_cap;
+    CU(launch_active_fill(d, s->st));
     d.act_on = 1;
     return MG_OK;
 }

@@ -383,6 +383,7 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
     int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
+    const PairVals<NT, P> pv(d);
     double ci[NT], Ei[NT];
 #pragma unroll
     for (int a = 0; a < NT; a++) {
@@ -391,9 +392,8 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
     }
     int nn = d.act_on ? d.nact[i] : d.nnb[i];
     for (int k = lane; k < nn; k += G) {
-        const size_t q = (size_t)i * d.maxnb + k;
-        long long slot = d.act_on ? d.act_slot[q] : (long long)d.poff[i] + k;
-        int j = d.act_on ? d.act_j[q] : d.nbr[q];
+        const long long slot = (d.act_on ? (long long)d.act_off[i] : (long long)d.poff[i]) + k;
+        const int j = d.act_on ? d.act_pj[slot] : d.pair_j[slot];
         double cj[NT], Ej[NT];
 #pragma unroll
         for (int b = 0; b < NT; b++) {
@@ -404,8 +404,8 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_E(Dev d)
         for (int a = 0; a < NT; a++)
 #pragma unroll
             for (int b = 0; b < NT; b++) {
-                Ei[a] += cj[b] * (double)pr_ptr<P>(d)[(size_t)(a * NT + b) * d.maxp + slot];
-                Ej[b] += ci[a] * (double)pr_ptr<P>(d)[(size_t)(b * NT + a) * d.maxp + slot];
+                Ei[a] += cj[b] * pv.rho(a * NT + b, slot);
+                Ej[b] += ci[a] * pv.rho(b * NT + a, slot);
             }
         if (j < d.natms) {
 #pragma unroll
@@ -452,6 +452,7 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
     int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
+    const PairVals<NT, P> pv(d);
     double ci[NT], ni[NT], dEi_q[NT];
 #pragma unroll
     for (int a = 0; a < NT; a++) {
@@ -461,9 +462,8 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
     }
     int nn = d.act_on ? d.nact[i] : d.nnb[i];
     for (int k = lane; k < nn; k += G) {
-        const size_t q = (size_t)i * d.maxnb + k;
-        long long slot = d.act_on ? d.act_slot[q] : (long long)d.poff[i] + k;
-        int j = d.act_on ? d.act_j[q] : d.nbr[q];
+        const long long slot = (d.act_on ? (long long)d.act_off[i] : (long long)d.poff[i]) + k;
+        const int j = d.act_on ? d.act_pj[slot] : d.pair_j[slot];
         double cj[NT], nj[NT], dEj_q[NT];
 #pragma unroll
         for (int b = 0; b < NT; b++) {
@@ -475,10 +475,9 @@ __global__ void __launch_bounds__(kFFBlock) k_mu_npairs(Dev d)
         for (int a = 0; a < NT; a++)
 #pragma unroll
             for (int b = 0; b < NT; b++) {
-                const P* pr = pr_ptr<P>(d);
-                double ph = pr[(size_t)(S::PHI + comp_idx(a, b)) * d.maxp + slot];
-                ni[a] += cj[b] * ((double)pr[(size_t)(b * NT + a) * d.maxp + slot] * dEj_q[b] + ph);
-                nj[b] += ci[a] * ((double)pr[(size_t)(a * NT + b) * d.maxp + slot] * dEi_q[a] + ph);
+                double ph = pv.phi(comp_idx(a, b), slot);
+                ni[a] += cj[b] * (pv.rho(b * NT + a, slot) * dEj_q[b] + ph);
+                nj[b] += ci[a] * (pv.rho(a * NT + b, slot) * dEi_q[a] + ph);
             }
         if (j < d.natms) {
 #pragma unroll
@@ -733,6 +732,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
     int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
+    const PairVals<NT, P> pv(d);
     double dEi[NT], ti[NT], vi[NT], gi[NT];
 #pragma unroll
     for (int a = 0; a < NT; a++) {
@@ -743,9 +743,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
     double ba = d.beta * alpha;
     int nn = d.act_on ? d.nact[i] : d.nnb[i];
     for (int k = lane; k < nn; k += G) {
-        const size_t q = (size_t)i * d.maxnb + k;
-        long long slot = d.act_on ? d.act_slot[q] : (long long)d.poff[i] + k;
-        int j = d.act_on ? d.act_j[q] : d.nbr[q];
+        const long long slot = (d.act_on ? (long long)d.act_off[i] : (long long)d.poff[i]) + k;
+        const int j = d.act_on ? d.act_pj[slot] : d.pair_j[slot];
         int oj = owner(d, j);
         double dEj[NT], tj[NT], vj[NT], gj[NT];
 #pragma unroll
@@ -758,10 +757,9 @@ __global__ void __launch_bounds__(kFFBlock) k_g_vpass(Dev d, double alpha)
         for (int a = 0; a < NT; a++)
 #pragma unroll
             for (int b = 0; b < NT; b++) {
-                const P* pr = pr_ptr<P>(d);
-                double r_ab = pr[(size_t)(a * NT + b) * d.maxp + slot];  // type2rho[jtype][itype]
-                double r_ba = pr[(size_t)(b * NT + a) * d.maxp + slot];  // type2rho[itype][jtype]
-                double tmp0 = (double)pr[(size_t)(S::PHI + comp_idx(b, a)) * d.maxp + slot] + r_ab * dEi[a] + r_ba * dEj[b];
+                double r_ab = pv.rho(a * NT + b, slot);  // type2rho[jtype][itype]
+                double r_ba = pv.rho(b * NT + a, slot);  // type2rho[itype][jtype]
+                double tmp0 = pv.phi(comp_idx(b, a), slot) + r_ab * dEi[a] + r_ba * dEj[b];
                 tmp0 *= ba;
                 vi[a] += r_ab * tj[b];
                 gi[a] += tmp0 * tj[b];
@@ -795,6 +793,7 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
     int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     int lane = threadIdx.x & (G - 1);
     if (i >= d.natms) return;
+    const PairVals<NT, P> pv(d);
     double wi[NT], gi[NT];
     double ab = alpha * d.beta;
 #pragma unroll
@@ -805,9 +804,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
     }
     int nn = d.act_on ? d.nact[i] : d.nnb[i];
     for (int k = lane; k < nn; k += G) {
-        const size_t q = (size_t)i * d.maxnb + k;
-        long long slot = d.act_on ? d.act_slot[q] : (long long)d.poff[i] + k;
-        int j = d.act_on ? d.act_j[q] : d.nbr[q];
+        const long long slot = (d.act_on ? (long long)d.act_off[i] : (long long)d.poff[i]) + k;
+        const int j = d.act_on ? d.act_pj[slot] : d.pair_j[slot];
         int oj = owner(d, j);
         double wj[NT], gj[NT];
 #pragma unroll
@@ -820,8 +818,8 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
         for (int a = 0; a < NT; a++)
 #pragma unroll
             for (int b = 0; b < NT; b++) {
-                gi[a] += ab * (double)pr_ptr<P>(d)[(size_t)(b * NT + a) * d.maxp + slot] * wj[b];
-                gj[b] += ab * (double)pr_ptr<P>(d)[(size_t)(a * NT + b) * d.maxp + slot] * wi[a];
+                gi[a] += ab * pv.rho(b * NT + a, slot) * wj[b];
+                gj[b] += ab * pv.rho(a * NT + b, slot) * wi[a];
             }
         if (j < d.natms) {
 #pragma unroll
@@ -838,29 +836,53 @@ __global__ void __launch_bounds__(kFFBlock) k_g_last(Dev d, double alpha)
 
 // the active sublist (Dev::act_*): a listed pair is active when any of its
 // stored densities or pair energies (the only per-pair values c_d_calc and
-// calc_g read) is non-zero; an inactive pair adds exact zeros there
+// calc_g read) is non-zero; an inactive pair adds exact zeros there.
+// Pass 1 counts each owned site's active pairs (nact, with nact[natms] = 0 so
+// that the scan's last element is the total); pass 2, after the scan into
+// act_off, copies their partners and values to the CSR arrays.
 template <int NT>
-__global__ void k_active_pairs(Dev d)
+__device__ __forceinline__ bool pair_active(const Dev& d, long long slot)
+{
+    using S = Slots<NT>;
+    bool on = false;
+#pragma unroll
+    for (int q = 0; q < NT * NT; q++) on |= d.pr[(size_t)(S::RHO + q) * d.maxp + slot] != 0.0;
+#pragma unroll
+    for (int q = 0; q < S::NC; q++) on |= d.pr[(size_t)(S::PHI + q) * d.maxp + slot] != 0.0;
+    return on;
+}
+
+template <int NT>
+__global__ void k_active_count(Dev d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) d.nact[d.natms] = 0;
+    if (i >= d.natms) return;
+    const int nn = d.nnb[i];
+    int m = 0;
+    for (int k = 0; k < nn; k++) m += pair_active<NT>(d, (long long)d.poff[i] + k) ? 1 : 0;
+    d.nact[i] = m;
+}
+
+template <int NT>
+__global__ void k_active_fill(Dev d)
 {
     using S = Slots<NT>;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.natms) return;
     const int nn = d.nnb[i];
-    int m = 0;
+    long long o = d.act_off[i];
     for (int k = 0; k < nn; k++) {
         const long long slot = (long long)d.poff[i] + k;
-        bool on = false;
+        if (!pair_active<NT>(d, slot)) continue;
+        d.act_pj[o] = d.pair_j[slot];
 #pragma unroll
-        for (int q = 0; q < NT * NT; q++) on |= d.pr[(size_t)(S::RHO + q) * d.maxp + slot] != 0.0;
+        for (int q = 0; q < NT * NT; q++) d.act_pv[(size_t)q * d.act_cap + o] = d.pr[(size_t)(S::RHO + q) * d.maxp + slot];
 #pragma unroll
-        for (int q = 0; q < S::NC; q++) on |= d.pr[(size_t)(S::PHI + q) * d.maxp + slot] != 0.0;
-        if (on) {
-            const size_t o = (size_t)i * d.maxnb + m++;
-            d.act_j[o] = d.nbr[(size_t)i * d.maxnb + k];
-            d.act_slot[o] = slot;
-        }
+        for (int q = 0; q < S::NC; q++)
+            d.act_pv[(size_t)(NT * NT + q) * d.act_cap + o] = d.pr[(size_t)(S::PHI + q) * d.maxp + slot];
+        o++;
     }
-    d.nact[i] = m;
 }
 
 template <int NT>
@@ -979,14 +1001,27 @@ cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st)
     }
 }
 
-cudaError_t launch_active_pairs(const Dev& d, cudaStream_t st)
+cudaError_t launch_active_count(const Dev& d, cudaStream_t st)
+{
+    const int g = div_up(d.natms + 1, kFFBlock);
+    switch (d.nt) {
+    case 1: k_active_count<1><<<g, kFFBlock, 0, st>>>(d); break;
+    case 2: k_active_count<2><<<g, kFFBlock, 0, st>>>(d); break;
+    case 3: k_active_count<3><<<g, kFFBlock, 0, st>>>(d); break;
+    case 4: k_active_count<4><<<g, kFFBlock, 0, st>>>(d); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_active_fill(const Dev& d, cudaStream_t st)
 {
     const int g = div_up(d.natms, kFFBlock);
     switch (d.nt) {
-    case 1: k_active_pairs<1><<<g, kFFBlock, 0, st>>>(d); break;
-    case 2: k_active_pairs<2><<<g, kFFBlock, 0, st>>>(d); break;
-    case 3: k_active_pairs<3><<<g, kFFBlock, 0, st>>>(d); break;
-    case 4: k_active_pairs<4><<<g, kFFBlock, 0, st>>>(d); break;
+    case 1: k_active_fill<1><<<g, kFFBlock, 0, st>>>(d); break;
+    case 2: k_active_fill<2><<<g, kFFBlock, 0, st>>>(d); break;
+    case 3: k_active_fill<3><<<g, kFFBlock, 0, st>>>(d); break;
+    case 4: k_active_fill<4><<<g, kFFBlock, 0, st>>>(d); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

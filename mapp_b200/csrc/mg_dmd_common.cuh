@@ -299,5 +299,30 @@ __device__ __forceinline__ const double* pr_ptr<double>(const Dev& d) { return d
 template <>
 __device__ __forceinline__ const float* pr_ptr<float>(const Dev& d) { return d.prf; }
 
+// the per-pair densities (q = b*nt+a of species pair (a, b)) and pair energies
+// (q = COMP(a, b)) that c_d_calc and calc_g read, at a list entry's slot: the
+// pair scratch of the force call at the compact pair index, or, while the
+// active sublist is on, its contiguous copy at the entry's CSR index
+template <int NT, typename P>
+struct PairVals {
+    const P* pr;
+    const double* av;
+    long long pstride, astride;
+    bool act;
+    __device__ __forceinline__ explicit PairVals(const Dev& d)
+        : pr(pr_ptr<P>(d)), av(d.act_pv), pstride(d.maxp), astride(d.act_cap), act(d.act_on != 0)
+    {
+    }
+    __device__ __forceinline__ double rho(int q, long long slot) const
+    {
+        return act ? av[(size_t)q * astride + slot] : (double)pr[(size_t)(Slots<NT>::RHO + q) * pstride + slot];
+    }
+    __device__ __forceinline__ double phi(int q, long long slot) const
+    {
+        return act ? av[(size_t)(NT * NT + q) * astride + slot]
+                   : (double)pr[(size_t)(Slots<NT>::PHI + q) * pstride + slot];
+    }
+};
+
 }  // namespace
 }  // namespace mg

@@ -93,12 +93,17 @@ struct Dev {
     // per-pair scratch
     double* pr;    // EAM/FS: drhoi[maxp], drhoj[maxp]; DMD: 21 SoA blocks of maxp
     long long maxp;
-    // while act_on: per owned site the listed pairs whose stored densities and
-    // pair energies are not all zero (site j, pair slot), [natms][maxnb], and
-    // their count; c_d_calc and calc_g then walk these instead of the list
-    int* act_j;
-    long long* act_slot;
+    // while act_on: the listed pairs whose stored densities and pair
+    // energies are not all zero, as CSR over the owned sites (act_off[i],
+    // nact[i] entries): the partner act_pj and the pair's NT^2 densities and
+    // NC pair energies copied contiguously (value q of entry k at
+    // act_pv[q * act_cap + k], densities first); c_d_calc and calc_g then
+    // stream these instead of the list and its per-pair buffers
+    int* act_pj;
+    double* act_pv;
+    int* act_off;
     int* nact;
+    long long act_cap;
     int act_on;
     // calc_g's chk and alpha read from device memory (a device-steered solve
     // changes them between graph iterations) when set, else the launch's
@@ -288,7 +293,10 @@ cudaError_t launch_dmd_force_mlp(const Dev& d, const MlpState& S, unsigned long 
 cudaError_t launch_dmd_crd(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_cdot(const Dev& d, cudaStream_t st);
 cudaError_t launch_dmd_calc_g(const Dev& d, int chk, double alpha, int* nblocks_out, cudaStream_t st);
-cudaError_t launch_active_pairs(const Dev& d, cudaStream_t st);
+// the active sublist: per-site counts (nact, nact[natms] = 0), then, after the
+// caller's scan into act_off and with act_cap set, the CSR copy
+cudaError_t launch_active_count(const Dev& d, cudaStream_t st);
+cudaError_t launch_active_fill(const Dev& d, cudaStream_t st);
 
 // One NVTX range per hot-path entry point, named after it, so a profiler's
 // timeline shows force_calc, calc_g, list builds and solver runs the way the
