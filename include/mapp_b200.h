@@ -78,7 +78,11 @@ int mg_atoms_set(mg_system* s, int natms, const double* x_frac, const int* type,
 /* Atoms::update_0(0,1,...) (atoms.cpp:1780-1865) after the caller wrote the
    owned Cartesian x (natms * x_dim): skin check against the positions at the
    last rebuild, then either a ghost refresh or x2s + ghost build + list
-   rebuild.  *rebuilt (may be NULL) reports which. */
+   rebuild.  *rebuilt reports which, and the call waits for the test.  With
+   rebuilt NULL the call does not wait: the test is read by the next entry
+   point that needs the positions, ghosts or list (mg_ff_force_calc reads it
+   with its results and, when the skin was exceeded, rebuilds and evaluates
+   again), with the same outcome as the waiting call. */
 int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt);
 /* Owned c written, then Atoms::update(c_n) ghost refresh. */
 int mg_atoms_update_c(mg_system* s, const double* c);

@@ -270,8 +270,15 @@ class System:
         _check(load_library().mg_ff_fin(self.h))
 
     # ---- Atoms -----------------------------------------------------------
-    def update_x(self, x):
+    def update_x(self, x, report=True):
+        """Atoms::update_0 with new positions. With report the call waits for
+        the skin test and returns whether the list was rebuilt; without, the
+        test is settled by the next call that needs the list (force_calc reads
+        it with its results) and None is returned."""
         xx = x if not isinstance(x, np.ndarray) else np.ascontiguousarray(x, dtype=np.float64)
+        if not report:
+            _check(load_library().mg_atoms_update_x(self.h, _ptr(xx), None))
+            return None
         r = C.c_int(0)
         _check(load_library().mg_atoms_update_x(self.h, _ptr(xx), C.byref(r)))
         return r.value

@@ -241,6 +241,7 @@ struct mg_system {
     float* mlp_loss = nullptr;
     int mlp_loss_n = 0;
     unsigned long long mlp_calls = 0;
+    bool skin_pending = false;  // update_x's skin test not yet read (status[7])
     GhostCtl* gctl = nullptr;  // device control of the ghost passes (two, ping-pong)
     unsigned* gtiles = nullptr;  // look-back words of the ghost passes (two halves)
     int gtiles_cap = 0;
@@ -256,11 +257,39 @@ struct mg_system {
 
 namespace {
 
-int check_sys(mg_system* s)
+int rebuild(mg_system* s);
+
+// the argument check of every entry point, without settling a pending skin
+// test (update_x, update_c and force_calc take care of it themselves)
+int check_sys_nores(mg_system* s)
 {
     if (!s) return fail(MG_ERR_ARG, "null mg_system");
     if (cudaSetDevice(s->device) != cudaSuccess) return fail(MG_ERR_CUDA, "cudaSetDevice(%d) failed", s->device);
     return MG_OK;
+}
+
+// update_x called without asking whether it rebuilt leaves its skin test on
+// the device (status[7]); the next entry point that reads positions, ghosts or
+// lists settles it first: the flag is read and, when some site moved more than
+// the skin since the last build, the list is rebuilt, as update_0 would have
+int resolve_skin(mg_system* s)
+{
+    if (!s->skin_pending) return MG_OK;
+    s->skin_pending = false;
+    int flag = 0;
+    CU(cudaMemcpyAsync(&flag, s->d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    if (flag) {
+        CU(launch_x2s(s->d, s->st));
+        CHK(rebuild(s));
+    }
+    return MG_OK;
+}
+
+int check_sys(mg_system* s)
+{
+    CHK(check_sys_nores(s));
+    return resolve_skin(s);
 }
 
 int stage_in(mg_system* s, const void* src, size_t bytes, const void** dev_out)
@@ -1245,8 +1274,9 @@ int mg_ff_init(mg_system* s)
 int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
 {
     MG_NVTX("mg_atoms_update_x");
-    CHK(check_sys(s));
+    CHK(check_sys_nores(s));
     if (!s->initialized) return fail(MG_ERR_STATE, "init must run before update_0");
+    CHK(resolve_skin(s));  // an earlier update_x whose test nothing has read yet
     if (s->natms == 0) {
         if (rebuilt) *rebuilt = 0;
         return MG_OK;
@@ -1257,27 +1287,35 @@ int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
         CHK(stage_in(s, x, (size_t)s->natms * s->x_dim * sizeof(double), &dx));
         CU(launch_split_x(d, (const double*)dx, 0, s->st));
     }
-    CU(cudaMemsetAsync(d.status + 5, 0, sizeof(int), s->st));
-    CU(launch_skin_check(d, s->skin * s->skin, d.status + 5, s->st));
-    int flag = 0;
-    CU(cudaMemcpyAsync(&flag, d.status + 5, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaMemsetAsync(d.status + 7, 0, sizeof(int), s->st));
+    CU(launch_skin_check(d, s->skin * s->skin, d.status + 7, s->st));
     // the ghost refresh is queued before the flag is known: it only writes
-    // the ghost slots, which a rebuild recreates anyway, and in the usual
-    // no-rebuild case it runs while the host waits for the flag
+    // the ghost slots, which a rebuild recreates anyway
     CU(launch_refresh_x(d, s->st));
+    if (!rebuilt) {
+        // nobody asked: the test is settled by the next entry point that needs
+        // the lists, so the host does not wait here (force_calc reads it
+        // with its results)
+        s->skin_pending = true;
+        return MG_OK;
+    }
+    int flag = 0;
+    CU(cudaMemcpyAsync(&flag, d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
     if (flag) {
         CU(launch_x2s(d, s->st));
         CHK(rebuild(s));
     }
-    if (rebuilt) *rebuilt = flag;
+    *rebuilt = flag;
     return MG_OK;
 }
 
 int mg_atoms_update_c(mg_system* s, const double* c)
 {
     MG_NVTX("mg_atoms_update_c");
-    CHK(check_sys(s));
+    // (a pending skin test may stay pending: a rebuild copies the new c to
+    // the ghosts it makes)
+    CHK(check_sys_nores(s));
     if (!s->dmd) return fail(MG_ERR_UNSUPPORTED, "c exists only in DMD mode");
     if (!s->initialized) return fail(MG_ERR_STATE, "init must run first");
     if (s->natms == 0) return MG_OK;
@@ -1324,7 +1362,11 @@ int mg_atoms_get_ghosts(mg_system* s, double* x, int* owner)
 int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
 {
     MG_NVTX("mg_ff_force_calc");
-    CHK(check_sys(s));
+    CHK(check_sys_nores(s));
+    // with update_x's skin test pending the force is computed on the current
+    // list and the test read with the results; if some site moved more than
+    // the skin, the list is rebuilt and the force computed again
+    const bool speculative = s->skin_pending;
     if (!s->initialized) return fail(MG_ERR_STATE, "force_calc before init");
     if (s->natms == 0) {
         if (en_st)
@@ -1379,7 +1421,17 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     if (s->dmd && s->form == MG_FORM_MLP)
         CU(cudaMemcpyAsync(&tc_timeout, d.status + 5, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CHK(copy_out(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
+    int skin = 0;
+    if (speculative) CU(cudaMemcpyAsync(&skin, d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
+    if (speculative) {
+        s->skin_pending = false;
+        if (skin) {
+            CU(launch_x2s(d, s->st));
+            CHK(rebuild(s));
+            return mg_ff_force_calc(s, st_clc, f, en_st);
+        }
+    }
     if (icut_over) return fail(MG_ERR_CAPACITY, "precision form: in-cut pair list overflow");
     if (tc_timeout) return fail(MG_ERR_TIMEOUT, "learned form: a tensor-core wait ran out");
     CHK(timed_read(s, &s->t_force));

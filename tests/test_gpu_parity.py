@@ -151,6 +151,50 @@ def test_gpu_matches_oracle(tmp_path, kind, kw):
         assert rel(s.c_d_calc(), o.c_d()) <= TOL
 
 
+@pytest.mark.parametrize("kind,kw", [("eam", dict(n=4)), ("dmd", dict(n=4, sigma=0.02, style="DMD_I"))],
+                         ids=["eam", "dmd"])
+def test_gpu_update_x_without_waiting(tmp_path, kind, kw):
+    """update_x with no rebuilt flag asked for leaves the skin test pending:
+    force_calc reads it with its results and, past the skin, rebuilds and
+    evaluates again; other entry points settle it first. Forces, lists and
+    ghosts match the oracle's update_0 either way."""
+    mb = _lib_or_skip()
+    from oracle.restated import Oracle
+
+    w = fx.write_workload(str(tmp_path / "w"), kind, **kw)
+    s = mb.system_from_workload(w)
+    o = Oracle(w)
+    N = w["cfg"].natms
+    dmd = w["cfg"].dmd
+    x0 = s.get_x()
+    rng = np.random.default_rng(11)
+    x1 = x0.copy()
+    x1[:, :3] += rng.normal(0, 0.05, (N, 3))
+    assert s.update_x(x1, report=False) is None
+    assert o.update_x(x1) == 0
+    check_forces(s, o, dmd)
+    check_state(s, o)
+    # past the skin: force_calc finds out and rebuilds
+    x2 = x1.copy()
+    x2[: max(1, N // 50), :3] += 0.7
+    s.update_x(x2, report=False)
+    assert o.update_x(x2) == 1
+    check_forces(s, o, dmd)
+    check_state(s, o)
+    # past the skin again, settled by a list query instead of force_calc
+    x3 = x2.copy()
+    x3[-max(1, N // 50):, :3] -= 0.7
+    s.update_x(x3, report=False)
+    assert o.update_x(x3) == 1
+    check_state(s, o)
+    check_forces(s, o, dmd)
+    # two updates in a row: the second settles the first
+    s.update_x(x2, report=False)
+    s.update_x(x3, report=False)
+    assert o.update_x(x2) == 1 and o.update_x(x3) == 1
+    check_forces(s, o, dmd)
+
+
 BOXES = [
     ("eam", dict(n=4, sigma=0.05), 4 * 3.615, (1.3, -0.9, 0.7)),
     ("dmd", dict(n=4, sigma=0.02, style="DMD_I"), 4 * 3.58, (0.8, 0.0, -0.6)),
