@@ -7,11 +7,12 @@
 // vector across the boundary tens of times per step.  Here the vector work is
 // a handful of kernels over the natms * nt concentrations (forming a, the
 // predictor, the conjugate-gradient direction, the box-constrained step
-// bound) and the force field's own calc_g / c_d_calc kernels; only the scalars
-// that steer the solve (costs, dot products, step bounds) come back to the
-// host, which runs the reference's control flow on them unchanged.  Dot
-// products and minima are deterministic: per-block partials reduced in a
-// fixed order by the last block to finish.
+// bound) and the force field's own calc_g / c_d_calc kernels.  A solve's line
+// searches run on the device as one conditional graph (k_bs_*), steered by
+// the reference's scalar control flow evaluated there; the step-size and
+// order control of the BDF clock stays on the host, one synchronisation per
+// solve.  Dot products and minima are deterministic: per-block partials
+// reduced in a fixed order by the last block to finish.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -154,23 +155,6 @@ __global__ void __launch_bounds__(kCkBlock) k_ck_predict(CkView V, double dt)
     V.c[i] = dadd(V.c[i], dmul(dmul(V.c_d[i], dt), r));
 }
 
-// trial point c = c0 + gamma h (clock_adams.cpp:322-323), ghosts included:
-// a ghost takes its owner's trial value, computed the same way, which is what
-// the ghost refresh that follows in the reference (atoms->update(c_n)) copies
-__global__ void __launch_bounds__(kCkBlock) k_ck_trial(CkView V, double gamma)
-{
-    const int i = blockIdx.x * kCkBlock + threadIdx.x;
-    if (i < V.n) {
-        V.c[i] = dadd(V.c0[i], dmul(gamma, V.h[i]));
-        return;
-    }
-    const int k = i - V.n;
-    if (k >= V.nph * V.nt) return;
-    const int gq = k / V.nt, a = k - gq * V.nt;
-    const size_t o = (size_t)V.root[V.natms + gq] * V.nt + a;
-    V.c[(size_t)(V.natms + gq) * V.nt + a] = dadd(V.c0[o], dmul(gamma, V.h[o]));
-}
-
 // g.g0 and g.g after the line search (clock_adams.cpp:340-352)
 __global__ void __launch_bounds__(kCkBlock) k_ck_dots(CkView V)
 {
@@ -207,32 +191,6 @@ __global__ void __launch_bounds__(kCkBlock) k_ck_first_dir(CkView V)
     if (reduce_last<2, 2u>(v, V, tot) && threadIdx.x == 0) {
         V.sc[SC_G0G0] = tot[0];
         V.sc[SC_GAMMA] = tot[1];
-    }
-}
-
-// the direction update h = h ratio + g with h.g (clock_adams.cpp:356-366,
-// clock_bdf.cpp:810-828), fused with the start of the next iteration:
-// g0 = g, c0 = c, and the box bounds along the new h and along g (the
-// direction restarts from g when h.g < 0)
-__global__ void __launch_bounds__(kCkBlock) k_ck_next_dir(CkView V, double ratio)
-{
-    const int i = blockIdx.x * kCkBlock + threadIdx.x;
-    double v[3] = {0.0, 1.0, 1.0};
-    if (i < V.n) {
-        const double gi = V.g[i], ci = V.c[i];
-        const double hi = dadd(dmul(V.h[i], ratio), gi);
-        V.h[i] = hi;
-        V.g0[i] = gi;
-        V.c0[i] = ci;
-        v[0] = dmul(hi, gi);
-        v[1] = box_bound(ci, dadd(ci, hi), 1.0);
-        v[2] = box_bound(ci, dadd(ci, gi), 1.0);
-    }
-    double tot[3];
-    if (reduce_last<3, 6u>(v, V, tot) && threadIdx.x == 0) {
-        V.sc[SC_GH] = tot[0];
-        V.sc[SC_GAMMA] = tot[1];
-        V.sc[SC_B] = tot[2];
     }
 }
 
@@ -351,21 +309,29 @@ __global__ void __launch_bounds__(kCkBlock) k_bdf_hilo(CkView V, BdfVecs B, BdfH
     }
 }
 
-// ---- Clock_BDF::solve's line search, steered on the device ------------------
+// ---- the clocks' line searches, steered on the device ------------------------
 // The conjugate-gradient iterations of Clock_BDF::solve (clock_bdf.cpp:
-// 727-828) run as one CUDA graph: a conditional WHILE node whose body is one
-// calc_g with its step set-up and its decision, so a solve synchronises with
-// the host once instead of once per calc_g. The scalar control (Armijo test,
-// step reduction, restore of c0, direction update) is the reference's,
-// evaluated by one thread in the same order of operations (explicitly
-// rounded: no contraction into fused multiply-adds), so the device takes the
-// steps the host loop took.
+// 727-828) and Clock_Adams::solve (clock_adams.cpp:316-365) run as one CUDA
+// graph: a conditional WHILE node whose body is one calc_g with its step
+// set-up and its decision, so a solve synchronises with the host once instead
+// of once per calc_g. The scalar control (Armijo test, step reduction, restore
+// of c0, direction update) is the reference's, evaluated by one thread in the
+// same order of operations (explicitly rounded: no contraction into fused
+// multiply-adds), so the device takes the steps the host loop took. The two
+// solves differ in three places: the BDF clock starts a line search at
+// 0.9 min(0.99, bound), the Adams clock at the bound; the BDF clock's trials
+// take the full calc_g and a failed search restores c0, the Adams clock's
+// trials take the cost only and every line search ends with a full calc_g at
+// the last point; the BDF clock updates the direction after a successful
+// search only, the Adams clock after every search.
 struct SolveDev {
-    double tol, min_gamma, gamma_red, slope;  // m_tol * dof, and the options
-    double alpha;                             // calc_g's alpha (the step's beta)
+    double tol, min_gamma, gamma_red, slope;  // the cost tolerance, and the options
+    double alpha;                             // calc_g's alpha
     double curr_cost, cost, g0_g0, g_h, bound, max_gamma, g_g, g_g0, ratio;
     int max_iter, iter, chk;
-    int mode;       // the body's calc_g: 0 at a trial point, 1 after restoring c0
+    int adams;      // Clock_Adams::solve's variant of the loop
+    int mode;       // the body's calc_g: 0 at a trial point, 1 after restoring c0 (BDF),
+                    // 2 the full calc_g at the last point after a line search (Adams)
     int calc_chk;   // calc_g's chk argument for the body (read by the g kernels)
     int line_done;  // the line search ended with this calc_g
     int need_next;  // a direction update follows (the line search succeeded)
@@ -385,13 +351,23 @@ __device__ bool bs_outer_top(SolveDev& S)
 {
     for (;;) {
         if (!(S.curr_cost > S.tol && S.iter < S.max_iter && S.max_gamma > S.min_gamma)) return false;
-        // min(0.99, the box bounds along h) (clock_bdf.cpp:744-759)
-        const double gamma = S.bound < 0.99 ? S.bound : 0.99;
-        S.max_gamma = dmul(gamma, 0.9);
+        if (S.adams) {
+            S.max_gamma = S.bound;
+        } else {
+            // min(0.99, the box bounds along h) (clock_bdf.cpp:744-759)
+            const double gamma = S.bound < 0.99 ? S.bound : 0.99;
+            S.max_gamma = dmul(gamma, 0.9);
+        }
         S.chk = 1;
         S.cost = S.curr_cost;
         if (S.max_gamma > S.min_gamma) {
             S.mode = 0;
+            S.calc_chk = S.adams ? 1 : 0;
+            return true;
+        }
+        if (S.adams) {
+            // an empty line search still ends with the full calc_g
+            S.mode = 2;
             S.calc_chk = 0;
             return true;
         }
@@ -418,6 +394,7 @@ __global__ void k_bs_init(SolveDev* S, const double* red_out, const double* sc, 
 // search; ghosts from their owners (what the reference's refresh copies)
 __global__ void __launch_bounds__(kCkBlock) k_bs_trial(CkView V, const SolveDev* S)
 {
+    if (S->mode == 2) return;  // the full calc_g at the last point
     const int i = blockIdx.x * kCkBlock + threadIdx.x;
     const bool restore = S->mode == 1;
     const double gamma = S->max_gamma;
@@ -443,6 +420,23 @@ __global__ void k_bs_post(SolveDev* S, const double* red_out, const double* sc)
     S->g_g = sc[SC_GG];
     S->need_next = 0;
     S->line_done = 1;
+    if (S->adams) {
+        if (S->mode == 0) {
+            const double ideal = dsub(S->cost, dmul(dmul(S->slope, S->max_gamma), S->g_h));
+            if (S->curr_cost < ideal) S->chk = 0;
+            S->max_gamma = dmul(S->max_gamma, S->gamma_red);
+            // the search goes on, or the full calc_g at this point follows
+            S->mode = (S->chk && S->max_gamma > S->min_gamma) ? 0 : 2;
+            S->calc_chk = S->mode == 0 ? 1 : 0;
+            S->line_done = 0;
+            return;
+        }
+        // after the full calc_g: the direction update, whatever the search gave
+        S->ratio = ddiv(dsub(S->g_g, S->g_g0), S->g0_g0);
+        S->g0_g0 = S->g_g;
+        S->need_next = 1;
+        return;
+    }
     if (S->mode == 0) {
         const double ideal = dsub(S->cost, dmul(dmul(S->slope, S->max_gamma), S->g_h));
         if (S->curr_cost < ideal) S->chk = 0;
@@ -467,7 +461,10 @@ __global__ void k_bs_post(SolveDev* S, const double* red_out, const double* sc)
     }
 }
 
-// the direction update when the line search succeeded (k_ck_next_dir)
+// the direction update h = h ratio + g with h.g (clock_adams.cpp:356-366,
+// clock_bdf.cpp:810-828), fused with the start of the next iteration: g0 = g,
+// c0 = c, and the box bounds along the new h and along g (the direction
+// restarts from g when h.g < 0); only when the body's post step asked for it
 __global__ void __launch_bounds__(kCkBlock) k_bs_next_dir(CkView V, const SolveDev* S)
 {
     if (!S->need_next) return;
@@ -559,26 +556,73 @@ struct Clock {
     double* block = nullptr;  // one allocation for every vector and the scalars
     long long n_calc_g = 0;
     double host_sc[SC_COUNT];
-    ~Clock() { cudaFree(block); }
+    // the line search's graph (captured once per run) and its device state
+    SolveDev* S_dev = nullptr;
+    cudaGraph_t ls_graph = nullptr;
+    cudaGraphExec_t ls_exec = nullptr;
+    ~Clock()
+    {
+        if (ls_exec) cudaGraphExecDestroy(ls_exec);
+        if (ls_graph) cudaGraphDestroy(ls_graph);
+        cudaFree(S_dev);
+        cudaFree(block);
+    }
 
     int grid() const { return V.nblocks; }
     int trial_grid() const { return div_up(V.n + V.nph * V.nt, kCkBlock); }
 
-    // calc_g(chk, alpha, a, g) -> cost (one synchronisation)
-    int calc_g(int chk, double alpha, double* cost, bool with_dots = false)
+    // one iteration of the line search: the point, calc_g (chk and alpha from
+    // the device state), the dot products, the Armijo test, the direction
+    // update, the outer loop's test
+    int enqueue_ls_body(cudaGraphConditionalHandle h)
     {
+        k_bs_trial<<<trial_grid(), kCkBlock, 0, st>>>(V, S_dev);
+        KCU(cudaGetLastError());
         int rows = 0;
-        KCHK(system_enqueue_calc_g(s, chk, alpha, &rows));
-        n_calc_g++;
-        if (with_dots) {
-            k_ck_dots<<<grid(), kCkBlock, 0, st>>>(V);
-            KCU(cudaGetLastError());
-        }
-        double r[1];
-        KCU(cudaMemcpyAsync(r, system_red_out(s), sizeof(double), cudaMemcpyDeviceToHost, st));
-        if (with_dots) KCU(cudaMemcpyAsync(host_sc, V.sc, SC_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
-        KCU(cudaStreamSynchronize(st));
-        *cost = r[0] * 0.25;
+        KCHK(system_enqueue_calc_g_dev(s, &S_dev->calc_chk, &S_dev->alpha, &rows));
+        k_ck_dots<<<grid(), kCkBlock, 0, st>>>(V);
+        k_bs_post<<<1, 32, 0, st>>>(S_dev, system_red_out(s), V.sc);
+        k_bs_next_dir<<<grid(), kCkBlock, 0, st>>>(V, S_dev);
+        k_bs_fin<<<1, 32, 0, st>>>(S_dev, V.sc, h);
+        k_bs_copy<<<grid(), kCkBlock, 0, st>>>(V, S_dev);
+        KCU(cudaGetLastError());
+        return MG_OK;
+    }
+
+    // graph: k_bs_init, then WHILE (condition set by k_bs_init and k_bs_fin)
+    int build_ls_graph()
+    {
+        KCU(cudaMalloc(&S_dev, sizeof(SolveDev)));
+        KCU(cudaGraphCreate(&ls_graph, 0));
+        cudaGraphConditionalHandle h;
+        KCU(cudaGraphConditionalHandleCreate(&h, ls_graph, 0, cudaGraphCondAssignDefault));
+        SolveDev* S = S_dev;
+        const double* red = system_red_out(s);
+        const double* sc = V.sc;
+        void* args[] = {&S, &red, &sc, &h};
+        cudaKernelNodeParams kp = {};
+        kp.func = (void*)k_bs_init;
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(32);
+        kp.sharedMemBytes = 0;
+        kp.kernelParams = args;
+        cudaGraphNode_t init;
+        KCU(cudaGraphAddKernelNode(&init, ls_graph, nullptr, 0, &kp));
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        KCU(cudaGraphAddNode(&node, ls_graph, &init, 1, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        KCU(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        const int rc = enqueue_ls_body(h);
+        cudaGraph_t out = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &out);
+        if (rc != MG_OK) return rc;
+        KCU(e);
+        KCU(cudaGraphInstantiate(&ls_exec, ls_graph, 0));
         return MG_OK;
     }
 
@@ -595,13 +639,16 @@ struct Clock {
         return MG_OK;
     }
 
-    // Clock_Adams::solve (clock_adams.cpp:246-365)
+    // Clock_Adams::solve (clock_adams.cpp:246-365): the first calc_g, c_d, the
+    // bounded predictor and the first direction are enqueued, then the line
+    // searches run as one graph launch (k_bs_*, the Adams variant), and the
+    // final cost comes back in one synchronisation
     int solve(double delta_t, double bet, double* out_cost)
     {
-        const double min_gamma = 1.0e-16, slope = 0.4, gamma_red = 0.8, alpha = delta_t * bet;
-        double max_gamma = 1.0, ratio, g0_g0, g_g, g_g0, g_h, curr_cost, ideal_cost, cost;
-        int chk;
-        KCHK(calc_g(0, alpha, &curr_cost));
+        const double alpha = delta_t * bet;
+        int rows = 0;
+        KCHK(system_enqueue_calc_g(s, 0, alpha, &rows));
+        n_calc_g++;
         KCHK(system_enqueue_c_d(s));
         k_ck_predict_bound<<<grid(), kCkBlock, 0, st>>>(V, delta_t);
         k_ck_predict<<<grid(), kCkBlock, 0, st>>>(V, delta_t);
@@ -610,44 +657,22 @@ struct Clock {
         // h = g, and the first iteration's g0, c0 and step bound with it
         k_ck_first_dir<<<grid(), kCkBlock, 0, st>>>(V);
         KCU(cudaGetLastError());
-        KCHK(read_scalars());
-        g0_g0 = host_sc[SC_G0G0];
-        g_h = g0_g0;
-        double bound = host_sc[SC_GAMMA];
-        int iter = 0;
-        while (curr_cost > 1.0e-8 && iter < 50 && max_gamma > min_gamma) {
-            max_gamma = bound;
-            chk = 1;
-            cost = curr_cost;
-            while (chk && max_gamma > min_gamma) {
-                k_ck_trial<<<trial_grid(), kCkBlock, 0, st>>>(V, max_gamma);
-                KCU(cudaGetLastError());
-                KCHK(calc_g(1, alpha, &curr_cost));
-                ideal_cost = cost - slope * max_gamma * g_h;
-                if (curr_cost < ideal_cost) chk = 0;
-                max_gamma *= gamma_red;
-                // the reference restores c0 when max_gamma <= 0, which the
-                // positive factor gamma_red never reaches
-            }
-            KCHK(calc_g(0, alpha, &curr_cost, true));
-            g_g0 = host_sc[SC_GG0];
-            g_g = host_sc[SC_GG];
-            ratio = (g_g - g_g0) / g0_g0;
-            g0_g0 = g_g;
-            // the new direction, and the next iteration's g0, c0 and bound
-            k_ck_next_dir<<<grid(), kCkBlock, 0, st>>>(V, ratio);
-            KCU(cudaGetLastError());
-            KCHK(read_scalars());
-            g_h = host_sc[SC_GH];
-            bound = host_sc[SC_GAMMA];
-            if (g_h < 0.0) {
-                KCU(cudaMemcpyAsync(V.h, V.g, (size_t)V.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-                g_h = g_g;
-                bound = host_sc[SC_B];
-            }
-            iter++;
-        }
-        *out_cost = curr_cost;
+        SolveDev hs{};
+        hs.tol = 1.0e-8;
+        hs.min_gamma = 1.0e-16;
+        hs.gamma_red = 0.8;
+        hs.slope = 0.4;
+        hs.alpha = alpha;
+        hs.max_iter = 50;
+        hs.adams = 1;
+        KCU(cudaMemcpyAsync(S_dev, &hs, sizeof(SolveDev), cudaMemcpyHostToDevice, st));
+        KCU(cudaGraphLaunch(ls_exec, st));
+        SolveDev r{};
+        KCU(cudaMemcpyAsync(&r, S_dev, sizeof(SolveDev), cudaMemcpyDeviceToHost, st));
+        KCU(cudaStreamSynchronize(st));
+        n_calc_g += r.n_calc_g;
+        if (r.overrun) return internal_fail(MG_ERR_TIMEOUT, "Adams clock: the line search did not end");
+        *out_cost = r.curr_cost;
         return MG_OK;
     }
 };
@@ -667,73 +692,7 @@ struct Bdf {
     double alpha_y[kMaxBdfOrder + 1], dalpha_y[kMaxBdfOrder + 1], lwr_alpha[kMaxBdfOrder + 1];
     double alpha_dy_0 = 0, dalpha_dy_0 = 0, beta = 0, err = 0, lo_err = 0, hi_err = 0, eq_ratio = 0;
 
-    // the line search's graph (captured once per run) and its device state
-    SolveDev* S_dev = nullptr;
-    cudaGraph_t ls_graph = nullptr;
-    cudaGraphExec_t ls_exec = nullptr;
-    ~Bdf()
-    {
-        if (ls_exec) cudaGraphExecDestroy(ls_exec);
-        if (ls_graph) cudaGraphDestroy(ls_graph);
-        cudaFree(S_dev);
-    }
-
     int grid() const { return ck->V.nblocks; }
-
-    // one iteration of the line search: the point, calc_g (chk and alpha from
-    // the device state), the dot products, the Armijo test, the direction
-    // update, the outer loop's test
-    int enqueue_ls_body(cudaGraphConditionalHandle h)
-    {
-        k_bs_trial<<<ck->trial_grid(), kCkBlock, 0, ck->st>>>(ck->V, S_dev);
-        KCU(cudaGetLastError());
-        int rows = 0;
-        KCHK(system_enqueue_calc_g_dev(ck->s, &S_dev->calc_chk, &S_dev->alpha, &rows));
-        k_ck_dots<<<grid(), kCkBlock, 0, ck->st>>>(ck->V);
-        k_bs_post<<<1, 32, 0, ck->st>>>(S_dev, system_red_out(ck->s), ck->V.sc);
-        k_bs_next_dir<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, S_dev);
-        k_bs_fin<<<1, 32, 0, ck->st>>>(S_dev, ck->V.sc, h);
-        k_bs_copy<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, S_dev);
-        KCU(cudaGetLastError());
-        return MG_OK;
-    }
-
-    // graph: k_bs_init, then WHILE (condition set by k_bs_init and k_bs_fin)
-    int build_ls_graph()
-    {
-        KCU(cudaMalloc(&S_dev, sizeof(SolveDev)));
-        KCU(cudaGraphCreate(&ls_graph, 0));
-        cudaGraphConditionalHandle h;
-        KCU(cudaGraphConditionalHandleCreate(&h, ls_graph, 0, cudaGraphCondAssignDefault));
-        SolveDev* S = S_dev;
-        const double* red = system_red_out(ck->s);
-        const double* sc = ck->V.sc;
-        void* args[] = {&S, &red, &sc, &h};
-        cudaKernelNodeParams kp = {};
-        kp.func = (void*)k_bs_init;
-        kp.gridDim = dim3(1);
-        kp.blockDim = dim3(32);
-        kp.sharedMemBytes = 0;
-        kp.kernelParams = args;
-        cudaGraphNode_t init;
-        KCU(cudaGraphAddKernelNode(&init, ls_graph, nullptr, 0, &kp));
-        cudaGraphNodeParams np = {};
-        np.type = cudaGraphNodeTypeConditional;
-        np.conditional.handle = h;
-        np.conditional.type = cudaGraphCondTypeWhile;
-        np.conditional.size = 1;
-        cudaGraphNode_t node;
-        KCU(cudaGraphAddNode(&node, ls_graph, &init, 1, &np));
-        cudaGraph_t body = np.conditional.phGraph_out[0];
-        KCU(cudaStreamBeginCaptureToGraph(ck->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        const int rc = enqueue_ls_body(h);
-        cudaGraph_t out = nullptr;
-        const cudaError_t e = cudaStreamEndCapture(ck->st, &out);
-        if (rc != MG_OK) return rc;
-        KCU(e);
-        KCU(cudaGraphInstantiate(&ls_exec, ls_graph, 0));
-        return MG_OK;
-    }
 
     // Clock_BDF::interpolate (clock_bdf.cpp:295-368) -> 1 or -1
     int interpolate(double del_t, int q, int* ret)
@@ -798,12 +757,12 @@ struct Bdf {
         hs.slope = o.slope;
         hs.alpha = beta;
         hs.max_iter = o.max_iter;
-        KCU(cudaMemcpyAsync(S_dev, &hs, sizeof(SolveDev), cudaMemcpyHostToDevice, ck->st));
-        KCU(cudaGraphLaunch(ls_exec, ck->st));
+        KCU(cudaMemcpyAsync(ck->S_dev, &hs, sizeof(SolveDev), cudaMemcpyHostToDevice, ck->st));
+        KCU(cudaGraphLaunch(ck->ls_exec, ck->st));
         k_bdf_err<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, B);
         KCU(cudaGetLastError());
         SolveDev r{};
-        KCU(cudaMemcpyAsync(&r, S_dev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ck->st));
+        KCU(cudaMemcpyAsync(&r, ck->S_dev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ck->st));
         KCHK(ck->read_scalars());
         ck->n_calc_g += r.n_calc_g;
         if (r.overrun) return internal_fail(MG_ERR_TIMEOUT, "BDF clock: the line search did not end");
@@ -994,6 +953,7 @@ extern "C" int mg_clock_adams(mg_system* s, int order, int nsteps, double delta_
     ck.V.nph = d.nph;
     ck.V.nt = nt;
     KCU(cudaMemsetAsync(ck.V.counter, 0, 8 * sizeof(double), ck.st));
+    KCHK(ck.build_ls_graph());
     const double* beta = kBeta[order - 1];
     std::vector<int> slot(m);
     for (int j = 0; j < m; j++) slot[j] = j;
@@ -1097,7 +1057,7 @@ extern "C" int mg_clock_bdf(mg_system* s, int nsteps, const mg_bdf_opts* opts, d
     ck.V.nph = d.nph;
     ck.V.nt = nt;
     KCU(cudaMemsetAsync(ck.block, 0, total * sizeof(double), ck.st));
-    KCHK(b.build_ls_graph());
+    KCHK(ck.build_ls_graph());
     KCHK(system_enqueue_c_d(s));
     const size_t bytes = (size_t)n * sizeof(double);
     double initial_del_t = o.initial_del_t;
