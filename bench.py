@@ -55,7 +55,8 @@ def parse():
     p.add_argument("--eam-cells", type=int, default=0,
                    help="instead: time EAM force_calc (the MD crystal's potential) on FCC n^3 atoms (profiling)")
     p.add_argument("--clock", default="", choices=["", "adams", "bdf"],
-                   help="instead: run only the 32000-site Adams or BDF clock line, without the CPU reference (profiling)")
+                   help="instead: run only the Adams (32000 sites) or BDF (--cells, default 32000 sites) clock line, "
+                        "without the CPU reference (profiling)")
     return p.parse_args()
 
 
@@ -687,8 +688,9 @@ def run_adams(mb, w, device, order=2, steps=20, ref_steps=1, with_reference=True
     return out
 
 
-def run_bdf(mb, fx, device, steps=100, ref_steps=5, with_reference=True):
-    """BDF clock (mg_clock_bdf) of the 32000-site binary DMD system with the
+def run_bdf(mb, fx, device, steps=100, ref_steps=5, with_reference=True, cells=20):
+    """BDF clock (mg_clock_bdf) of the FCC cells^3 (default 20^3 = 32000-site)
+    binary DMD system with the
     DMD_II force field: "clock bdf 100 max_order 2 initial_del_t 1e-3 tau"
     (tau = 1 / rms(c_d) at the start), the reference's own step-size and
     order control, timed on the host clock around the call (crd list,
@@ -699,7 +701,7 @@ def run_bdf(mb, fx, device, steps=100, ref_steps=5, with_reference=True):
     loop never ends.  Beside it the reference's Clock_BDF for the first
     ref_steps steps on one core, and ours over the same steps."""
     d = tempfile.mkdtemp(prefix="mapp_bdf_")
-    w = fx.write_workload(d, "dmd", n=20, a=WORKLOAD["a"], sigma=0.0, style="DMD_II", seed=4321)
+    w = fx.write_workload(d, "dmd", n=cells, a=WORKLOAD["a"], sigma=0.0, style="DMD_II", seed=4321)
     s = mb.system_from_workload(w, device=device)
     s.create_2nd_neigh_lst()
     s.force_calc(1)
@@ -1028,7 +1030,7 @@ def main():
 
         torch.cuda.set_device(0)
         if args.clock == "bdf":
-            out = run_bdf(mb, fx, 0, with_reference=False)
+            out = run_bdf(mb, fx, 0, with_reference=False, cells=args.cells)
         else:
             w = fx.write_workload(tempfile.mkdtemp(prefix="mapp_adams_w_"), "dmd", n=WORKLOAD["n"], a=WORKLOAD["a"],
                                   sigma=WORKLOAD["sigma"], style="DMD_I", seed=4321)
