@@ -938,7 +938,8 @@ int build_all(mg_batch* b)
         BCHK(b->facc.exact((size_t)NT * 8));
     } else
         BCHK(b->pr.exact(maxp * nblk));
-    const long long rows = 2LL * div_up(pair_fill, kFFBlock) + div_up((long long)NT, kFFBlock) + 64;
+    // pass 1 and pass 2 at one thread per pair at most, the embedding at one per (site, species)
+    const long long rows = 2LL * div_up(pair_fill, kFFBlock) + div_up((long long)NT * nt, kFFBlock) + 64;
     BCHK(b->partial.exact((size_t)rows * 8));
     BCHK(b->cell_E.exact((size_t)ncells));
     BCHK(b->active.exact((size_t)ncells));

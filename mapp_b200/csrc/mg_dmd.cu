@@ -117,25 +117,25 @@ __global__ void __launch_bounds__(kFFBlock, MG_DMD_MINB) k_dmd_pass1(Dev d, int 
 }
 
 // ---- per-site embedding, entropy and alpha terms (ff_dmd_I.cpp:322-351) ---
+// One thread per (site, species), so that twice as many warps hide the
+// table gather and the logarithms as with one thread per site.
 template <int NT>
 __global__ void __launch_bounds__(kFFBlock) k_dmd_embed(Dev d, int with_force, int row0)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = idx / NT, a = idx - (idx / NT) * NT;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     double e = 0.0;
     if (i < d.natms && site_active(d, i)) {
-#pragma unroll
-        for (int a = 0; a < NT; a++) {
-            double tmp0, tmp1;
-            embed_F(d, a, d.E[(size_t)i * NT + a], tmp0, tmp1, nullptr);
-            double ca = d.c[(size_t)i * NT + a], al = d.alpha[(size_t)i * NT + a];
-            d.E[(size_t)i * NT + a] = tmp0;
-            if (with_force) d.dE[(size_t)i * NT + a] = tmp1;
-            e += ca * tmp0;
-            e += d.kbT * calc_ent(ca);
-            e += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
-            if (with_force) d.f[(size_t)i * d.x_dim + 3 + a] -= 1.5 * d.kbT * ca / al;
-        }
+        double tmp0, tmp1;
+        embed_F(d, a, d.E[(size_t)idx], tmp0, tmp1, nullptr);
+        const double ca = d.c[(size_t)idx], al = d.alpha[(size_t)idx];
+        d.E[(size_t)idx] = tmp0;
+        if (with_force) d.dE[(size_t)idx] = tmp1;
+        e += ca * tmp0;
+        e += d.kbT * calc_ent(ca);
+        e += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
+        if (with_force) d.f[(size_t)i * d.x_dim + 3 + a] -= 1.5 * d.kbT * ca / al;
     }
     if (d.site_cell) cell_energy_add(d, i < d.natms ? i : -1, e);
     else acc[0] += e;
@@ -888,7 +888,7 @@ __global__ void k_active_fill(Dev d)
 template <int NT>
 cudaError_t dmd_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, cudaEvent_t* evs)
 {
-    int g1 = persistent_grid(d.npairs, d.tune_bps > 0 ? d.tune_bps : MG_DMD_MINB), g2 = div_up(d.natms, kFFBlock);
+    int g1 = persistent_grid(d.npairs, d.tune_bps > 0 ? d.tune_bps : MG_DMD_MINB), g2 = div_up(d.natms * NT, kFFBlock);
     int g3 = persistent_grid(d.npairs, d.tune_bps2 > 0 ? d.tune_bps2 : MG_DMD_MINB);
     if (evs) cudaEventRecord(evs[0], st);
     if (d.nq == 3) k_dmd_pass1<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
@@ -905,7 +905,7 @@ cudaError_t dmd_force_nt(const Dev& d, int st_clc, int* nb, cudaStream_t st, cud
 template <int NT>
 cudaError_t dmd_energy_nt(const Dev& d, int* nb, cudaStream_t st)
 {
-    int g1 = persistent_grid(d.npairs, MG_DMD_MINB), g2 = div_up(d.natms, kFFBlock);
+    int g1 = persistent_grid(d.npairs, MG_DMD_MINB), g2 = div_up(d.natms * NT, kFFBlock);
     if (d.nq == 3) k_dmd_energy_pass<NT, 3><<<g1, kFFBlock, 0, st>>>(d, 0);
     else k_dmd_energy_pass<NT, 0><<<g1, kFFBlock, 0, st>>>(d, 0);
     k_dmd_embed<NT><<<g2, kFFBlock, 0, st>>>(d, 0, g1);
