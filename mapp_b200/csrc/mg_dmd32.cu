@@ -138,14 +138,6 @@ __device__ __forceinline__ double4 pos_ld(const Dev& d, int i)
     return r;
 }
 
-// copies the first nslots slots of the split table into shared memory
-__device__ __forceinline__ void load_split_table(const Dev& d, float4* sh, int nslots)
-{
-    const int n = nslots * d.nrS;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) sh[k] = __ldg(d.pkS + k);
-    __syncthreads();
-}
-
 // alpha and c of site j from its FP32 record (srec: {alpha_0.., c_0..})
 template <int NT>
 __device__ __forceinline__ void load_rec(const Dev& d, int j, float (&al)[NT], float (&cc)[NT])
@@ -303,9 +295,11 @@ __global__ void MG_DENS_BOUNDS k_dmd32_dens(Dev d, int K)
             // region: per pair {i, j, owner of j} and {dx, dy, dz, rsq}
             if (nbt < K) {
                 const int oj = on ? owner(d, e.y) : -1;
-                int4* o = region + ((size_t)nbt * 32 + lane) * 2;
+                // (a batch's 32 first halves, then its 32 second halves: each
+                // store instruction writes 512 contiguous bytes)
+                int4* o = region + (size_t)nbt * 64 + lane;
                 o[0] = make_int4(e.x, e.y, oj, 0);
-                o[1] = make_int4(__float_as_int(gx.x), __float_as_int(gx.y), __float_as_int(gx.z), __float_as_int(gx.w));
+                o[32] = make_int4(__float_as_int(gx.x), __float_as_int(gx.y), __float_as_int(gx.z), __float_as_int(gx.w));
             } else if (lane == 0)
                 d.status[4] = 1;
             nbt++;
@@ -388,8 +382,8 @@ __global__ void MG_FORCE_BOUNDS k_dmd32_force(Dev d, int st_clc, int row0, int W
     for (long long t = (long long)blockIdx.x * kFFWarps + (threadIdx.x >> 5); t < nslot; t += wstride) {
         const long long rg = t / K;
         if (t - rg * K >= (long long)__ldg(d.icut_n + rg)) continue;  // past the region's last batch
-        const int4 e = d.icut[(size_t)t * 64 + lane * 2];
-        const int4 ex = d.icut[(size_t)t * 64 + lane * 2 + 1];
+        const int4 e = d.icut[(size_t)t * 64 + lane];
+        const int4 ex = d.icut[(size_t)t * 64 + 32 + lane];
         const bool on = e.x >= 0;
         float fi[3 + NT];
 #pragma unroll

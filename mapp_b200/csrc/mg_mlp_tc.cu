@@ -304,6 +304,11 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_rows(Dev d, MlpState S, unsign
     constexpr int RP = NT * NT;
     __shared__ int warp_n[kFFWarps];
     __shared__ unsigned blk_base;
+    // a warp's network rows of one round, in slot order, so that they leave
+    // for the row list with coalesced stores
+    __shared__ float4 st_in[kFFWarps][32 * RP];
+    __shared__ int2 st_id[kFFWarps][32 * RP];
+    __shared__ float st_r[kFFWarps][32 * RP];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const SplitK k = split_consts(d);
     const size_t mp = (size_t)d.maxp;
@@ -392,22 +397,32 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_rows(Dev d, MlpState S, unsign
             blk_base = tot ? atomicAdd(S.row_n, (unsigned)tot) : 0u;
         }
         __syncthreads();
-        long long slot = (long long)blk_base + warp_n[warp] + incl - cnt;
+        int q = incl - cnt;  // this lane's first row in the warp's staging
 #pragma unroll
         for (int ab = 0; ab < RP; ab++)
             if (net >> ab & 1u) {
-                if (slot < S.row_cap) {
-                    S.row_in[slot] = in[ab];
-                    S.row_id[slot] = make_int2((int)p, ab);
-                    S.row_r[slot] = r;
-                    if (audited(audit_seed, p, ab, RP)) {
-                        const unsigned ka = atomicAdd(S.row_n + 1, 1u);
-                        if (ka < S.audit_cap) S.audit_rows[ka] = (int)slot;
-                    }
-                } else
-                    d.status[5] = 2;
-                slot++;
+                st_in[warp][q] = in[ab];
+                st_id[warp][q] = make_int2((int)p, ab);
+                st_r[warp][q] = r;
+                q++;
             }
+        __syncwarp();
+        const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+        const long long wbase = (long long)blk_base + warp_n[warp];
+        for (int e = lane; e < wtot; e += 32) {
+            const long long slot = wbase + e;
+            if (slot < S.row_cap) {
+                const int2 id = st_id[warp][e];
+                S.row_in[slot] = st_in[warp][e];
+                S.row_id[slot] = id;
+                S.row_r[slot] = st_r[warp][e];
+                if (audited(audit_seed, id.x, id.y, RP)) {
+                    const unsigned ka = atomicAdd(S.row_n + 1, 1u);
+                    if (ka < S.audit_cap) S.audit_rows[ka] = (int)slot;
+                }
+            } else
+                d.status[5] = 2;
+        }
         __syncthreads();
     }
 }
@@ -418,6 +433,9 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_rows(Dev d, MlpState S, unsign
 template <int NT, int NQ>
 __global__ void __launch_bounds__(kFFBlock) k_mlp_fallback(Dev d, MlpState S)
 {
+    // the split table in shared memory, as the precision form's force pass has it
+    extern __shared__ float4 tab[];
+    load_split_table(d, tab, NT * NT + Slots<NT>::NC);
     const SplitK k = split_consts(d);
     const long long nfb = min((long long)S.row_n[2], S.row_cap);
     unsigned long long nrows = 0;
@@ -446,8 +464,8 @@ __global__ void __launch_bounds__(kFFBlock) k_mlp_fallback(Dev d, MlpState S)
                 const int ab = a * NT + b;
                 if (!(id.y >> ab & 1)) continue;
                 const float alpha = __fdividef(ai[a] * aj[b], ai[a] + aj[b]);
-                const float4* tr = d.pkS + (size_t)ab * d.nrS;
-                const float4* tp = d.pkS + (size_t)(NT * NT + comp_idx(a, b)) * d.nrS;
+                const float4* tr = tab + (size_t)ab * d.nrS;
+                const float4* tp = tab + (size_t)(NT * NT + comp_idx(a, b)) * d.nrS;
                 VDer g, f;
                 if (a >= b) smear_full<NQ, true, false>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
                 else smear_full<NQ, false, false>(d, tr, tp, k, r, r_inv, below_rc, alpha, k0, g, f);
@@ -726,8 +744,14 @@ cudaError_t mlp_force_nt(const Dev& d, const MlpState& S, unsigned long long aud
     if (e != cudaSuccess) return e;
     if (evs) cudaEventRecord(evs[0], st);
     k_mlp_rows<NT><<<std::max(g0, 1), kFFBlock, 0, st>>>(d, S, audit_seed);
-    if (nq3) k_mlp_fallback<NT, 3><<<num_sms() * 8, kFFBlock, 0, st>>>(d, S);
-    else k_mlp_fallback<NT, 0><<<num_sms() * 8, kFFBlock, 0, st>>>(d, S);
+    const size_t smF = (size_t)(NT * NT + NT * (NT + 1) / 2) * d.nrS * sizeof(float4);
+    if (smF > 48 * 1024) {
+        e = cudaFuncSetAttribute(nq3 ? k_mlp_fallback<NT, 3> : k_mlp_fallback<NT, 0>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smF);
+        if (e != cudaSuccess) return e;
+    }
+    if (nq3) k_mlp_fallback<NT, 3><<<num_sms() * 4, kFFBlock, smF, st>>>(d, S);
+    else k_mlp_fallback<NT, 0><<<num_sms() * 4, kFFBlock, smF, st>>>(d, S);
     k_mlp_tc<NT, ACT><<<g1, kTcThreads, sm, st>>>(d, S);
     if (d.nq == 3) k_mlp_audit<NT, 3><<<num_sms(), kFFBlock, 0, st>>>(d, S);
     else k_mlp_audit<NT, 0><<<num_sms(), kFFBlock, 0, st>>>(d, S);

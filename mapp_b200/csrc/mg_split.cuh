@@ -17,6 +17,14 @@ struct SplitK {
     float rc, dr_inv, top, alpha_min, alpha_max;
 };
 
+// copies the first nslots slots of the split table into shared memory
+__device__ __forceinline__ void load_split_table(const Dev& d, float4* sh, int nslots)
+{
+    const int n = nslots * d.nrS;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) sh[k] = __ldg(d.pkS + k);
+    __syncthreads();
+}
+
 __device__ __forceinline__ SplitK split_consts(const Dev& d)
 {
     SplitK k;
