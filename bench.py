@@ -441,6 +441,24 @@ def run_batched(mb, fx, device, ncells=512):
     return out
 
 
+def run_e2e_client(mb, w, steps, device, warmup=3):
+    """Runs mapp_b200/mapp_e2e (built with the library) on the workload w;
+    returns its JSON line, or None when it is missing or fails."""
+    client = os.path.join(os.path.dirname(os.path.abspath(mb.__file__)), "mapp_e2e")
+    if not os.path.exists(client):
+        return None
+    cmd = [client, w["style"], w["cfg_path"], str(steps), str(warmup), str(device), str(w.get("skin", 0.5)),
+           *w["coef"]]
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    except (OSError, subprocess.TimeoutExpired):
+        return None
+    if p.returncode != 0 or not p.stdout.strip():
+        print(f"e2e client failed: {p.stderr.strip()[-300:]}", file=sys.stderr)
+        return None
+    return json.loads(p.stdout.strip().splitlines()[-1])
+
+
 def run_batched_sharded(mb, fx, device, rank, world, ncells=512):
     """The batched form's 512 cells split over the job's GPUs
     (mapp_b200.shard): each rank relaxes its share (FP64, one graph launch,
@@ -863,7 +881,20 @@ def run_ours(args):
     ev1.record(e2e_stream)
     torch.cuda.synchronize()
     t_e2e = job_max(ev0.elapsed_time(ev1) * 1e-3, "cuda")
-    e2e_value = job_rate(natms, e2e_steps, t_e2e, ws)
+    e2e_py = job_rate(natms, e2e_steps, t_e2e, ws)
+    _, en_py = s.force_calc(1, f=f_host)
+    # the same steps from a C++ caller of the C ABI (mapp_b200/client/mapp_e2e.cpp),
+    # as MAPP's force loop would make them: set up from the same CFG file and
+    # ff_coef arguments, pinned host buffers, events on the library's stream
+    e2e_client = run_e2e_client(mb, w, e2e_steps, local) if args.form == "fp64" else None
+    t_client = job_max(e2e_client["ms"] * 1e-3 if e2e_client else float("inf"), "cuda")
+    if np.isfinite(t_client):
+        e2e_value = job_rate(natms, e2e_steps, t_client, ws)
+        e2e_path = ("C++ client of the C ABI (mapp_b200/client/mapp_e2e.cpp): mg_atoms_update_x (rebuilt flag not "
+                    "asked for, as MAPP's callers) + mg_atoms_update_c + mg_ff_force_calc, pinned host buffers")
+    else:
+        e2e_value, e2e_client = e2e_py, None
+        e2e_path = "mg_atoms_update_x + mg_atoms_update_c + mg_ff_force_calc through ctypes, pinned host buffers"
 
     # side measurements (list build, energy_calc, c_d_calc, calc_g)
     s.rebuild_list()
@@ -959,7 +990,10 @@ def run_ours(args):
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": natms * (s.x_dim + nt) * 8, "d2h_bytes_per_step": natms * s.x_dim * 8 + 56,
-                "steps": e2e_steps, "path": "mg_atoms_update_x + mg_atoms_update_c + mg_ff_force_calc, pinned host buffers"},
+                "steps": e2e_steps, "path": e2e_path,
+                "python_ctypes": {"value": e2e_py, "path": "the same calls from Python through ctypes"},
+                "client_energy_rel_diff": (abs(e2e_client["energy"] - float(en_py[0])) / abs(float(en_py[0]))
+                                           if e2e_client else None)},
         "forms": forms,
         # library kernels per force call: plain pass 1, embedding, pass 2,
         # reduction; precision prep, density, embedding, force, merge,

@@ -19,6 +19,10 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SOURCES = ["mg_api.cu", "mg_atoms.cu", "mg_eam.cu", "mg_dmd.cu", "mg_dmd32.cu", "mg_mlp.cu", "mg_mlp_tc.cu", "mg_noalloc.cu", "mg_batch.cu", "mg_cfg.cu", "mg_md.cu", "mg_clock.cu"]
 HEADERS = ["mg_internal.h", "mg_reduce.cuh", "mg_dmd_common.cuh", "mg_mlp_common.cuh", "mg_split.cuh"]
 
+# a C++ client of the C ABI (the end-to-end measurement of bench.py)
+CLIENT_SRC = os.path.join(HERE, "client", "mapp_e2e.cpp")
+CLIENT = os.path.join(HERE, "mapp_e2e")
+
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off",
          "-I" + os.path.join(HERE, "..", "include")]
@@ -53,6 +57,12 @@ def build(verbose: bool = False, extra_flags=(), jobs: int = 4) -> str:
             raise RuntimeError(f"nvcc failed on {name}")
     if _stale(OUT, objs):
         cmd = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+    if _stale(CLIENT, [CLIENT_SRC, OUT, hdrs[-1]]):
+        cmd = [NVCC, *ARCH, "-O2", "-std=c++17", "-cudart", "shared", "-I" + os.path.join(HERE, "..", "include"),
+               CLIENT_SRC, "-o", CLIENT, "-L" + HERE, "-lmapp_b200", "-Xlinker", "-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
