@@ -998,8 +998,8 @@ def run_ours(args):
         # library kernels per force call: plain pass 1, embedding, pass 2,
         # reduction; precision prep, density, embedding, force, merge,
         # reduction; learned rows, fallback, network, audit, densities,
-        # embedding, force, merge, reduction
-        "gpu_launches": {"fp64": 4, "fp32": 6, "mlp": 9}[args.form] * args.steps,
+        # embedding, pass 2, reduction
+        "gpu_launches": {"fp64": 4, "fp32": 6, "mlp": 8}[args.form] * args.steps,
         "phases_ms": {"force": t_dev / args.steps, "force.pass1": p1_ms, "force.embed": emb_ms,
                       "force.pass2": p2_ms, "list_rebuild": t_list,
                       "energy_calc": t_energy, "c_d_calc": t_cd, "calc_g": t_g},
