@@ -42,6 +42,21 @@ def test_assignment_is_the_largest_first_rule():
         shard.assign_cells(costs, 0)
 
 
+def test_assignment_with_more_ranks_than_cells():
+    costs = [3, 1, 2]
+    parts = shard.assign_cells(costs, 5)
+    # one cell per rank, largest first to the lowest empty rank; the rest idle
+    assert parts == [[0], [2], [1], [], []]
+
+
+def test_job_time_and_rate_on_one_rank():
+    """bench.job_rate / job_max: without a process group the job is this rank."""
+    import bench
+
+    assert bench.job_max(2.5) == 2.5
+    assert bench.job_rate(1000, 10, 2.0, 1) == 1000 * 10 / 2.0
+
+
 def test_gather_without_process_group_is_local():
     out = shard.gather_results([(1, "b"), (0, "a")], 2)
     assert out == ["a", "b"]
