@@ -954,7 +954,12 @@ def run_ours(args):
                              "algorithmic_bytes_rule": f"{PASS1_ALG_BYTES_PER_SITE} B per owned site "
                                                        "(x, alpha, c read; E written)",
                              "traffic_note": "pass 1 writes the per-pair scratch the reference keeps (21 FP64 "
-                                             "values per listed pair); that is most of its DRAM traffic"}}
+                                             "values per listed pair); that is most of its DRAM traffic"},
+                # what does bind the kernel, from its ncu capture (not measured in this run)
+                "binding_resource": {"resource": "L1/TEX data pipe (one wavefront per lane for the knot "
+                                                 "and site gathers, about 30 per in-cut pair)",
+                                     "utilisation": 0.74, "fp64_pipe": 0.30,
+                                     "source": "profiles/k_dmd_pass1_32k.md (ncu --set full, 32000 sites)"}}
     elif args.form == "fp32":
         peak = measure_fp32_peak()
         fB = f1 + f2  # the force pass evaluates the whole smearing and the projection
