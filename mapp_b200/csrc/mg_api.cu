@@ -221,7 +221,22 @@ struct mg_system {
     size_t stage_cap = 0;
     size_t act_cap = 0;   // capacity of the active-pair sublist (entries)
     size_t nact_cap = 0;  // and of its per-site counts and offsets (sites + 1)
-    double* red_out = nullptr;  // 8 doubles
+    // one device block of 8 doubles (the reduced totals) followed by the 8
+    // status words, d.status pointing into it, so that one copy reads both
+    double* red_out = nullptr;
+    // Page-locked host block for the small results the entry points read back.
+    // A copy into pageable memory blocks the host until the stream has
+    // drained, so a pageable read of a total before the force copy would leave
+    // the GPU idle for a host round trip; into this block every copy is
+    // asynchronous and the one synchronisation at the end of a call covers them
+    // all.  Its first two members mirror the device block above.
+    struct HostPin {
+        double tot[8];
+        int status[8];
+        GhostCtl gc;
+        int count;
+    };
+    HostPin* hp = nullptr;
     double* d_rhoT = nullptr;
     double* d_phiT = nullptr;
     double* d_FT = nullptr;
@@ -276,10 +291,9 @@ int resolve_skin(mg_system* s)
 {
     if (!s->skin_pending) return MG_OK;
     s->skin_pending = false;
-    int flag = 0;
-    CU(cudaMemcpyAsync(&flag, s->d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaMemcpyAsync(&s->hp->status[7], s->d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
-    if (flag) {
+    if (s->hp->status[7]) {
         CU(launch_x2s(s->d, s->st));
         CHK(rebuild(s));
     }
@@ -522,16 +536,17 @@ int rebuild(mg_system* s)
         // half list, then the scan of the per-atom counts
         bool regrow_ghosts = false;
         for (int attempt_nb = 0;; attempt_nb++) {
-            GhostCtl gc;
-            int st_h[8];
+            const GhostCtl& gc = s->hp->gc;
+            const int* st_h = s->hp->status;
             // (the list kernel zeroes nnb[natms], the scan's last element)
             if (attempt_nb) CU(cudaMemsetAsync(d.status, 0, 2 * sizeof(int), st));
             CU(launch_neigh(d, st));
             CU(launch_exclusive_scan(d.nnb, d.poff, natms + 1, s->scan_tmp, s->scan_tmp_bytes, st));
-            CU(cudaMemcpyAsync(&gc, gfin, sizeof(GhostCtl), cudaMemcpyDeviceToHost, st));
-            CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
-            CU(cudaMemcpyAsync(&np_h, d.poff + natms, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CU(cudaMemcpyAsync(&s->hp->gc, gfin, sizeof(GhostCtl), cudaMemcpyDeviceToHost, st));
+            CU(cudaMemcpyAsync(s->hp->status, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CU(cudaMemcpyAsync(&s->hp->count, d.poff + natms, sizeof(int), cudaMemcpyDeviceToHost, st));
             CU(cudaStreamSynchronize(st));
+            np_h = s->hp->count;
             if (st_h[4])
                 return fail(MG_ERR_CAPACITY, "ghost image chain deeper than %d swaps (box too small for the cut-off)",
                             kMaxChain);
@@ -996,9 +1011,22 @@ int mg_create(const char* style, int device, mg_system** out)
     cudaEventCreate(&s->ev1);
     for (int k = 0; k < 4; k++) cudaEventCreate(&s->evk[k]);
     memset(&s->d, 0, sizeof(Dev));
-    int r = dalloc(&s->d.status, 8);
-    if (!r) r = dalloc(&s->red_out, 8);
+    int r = dalloc(&s->red_out, 12);  // 8 totals, then 8 ints of status
+    if (!r) {
+        s->d.status = reinterpret_cast<int*>(s->red_out + 8);
+        if (cudaMallocHost((void**)&s->hp, sizeof(mg_system::HostPin)) != cudaSuccess) {
+            cudaGetLastError();
+            s->hp = nullptr;
+            r = fail(MG_ERR_CAPACITY, "cudaMallocHost of the result block failed");
+        } else
+            memset(s->hp, 0, sizeof(mg_system::HostPin));
+    }
     if (r) {
+        if (s->red_out) cudaFree(s->red_out);
+        for (int k = 0; k < 4; k++) cudaEventDestroy(s->evk[k]);
+        cudaEventDestroy(s->ev0);
+        cudaEventDestroy(s->ev1);
+        cudaStreamDestroy(s->st);
         delete s;
         return r;
     }
@@ -1014,7 +1042,7 @@ int mg_destroy(mg_system* s)
     Dev& d = s->d;
     void* ptrs[] = {d.prf, s->d_pkT, s->d_pk64, s->d_pkS, d.icut, d.icut_n, d.srec, d.dE32, d.facc, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
-                    d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.status, d.act_pj, d.act_pv, d.act_off, d.nact,
+                    d.dE, d.ddE, d.n, d.s, d.t, d.v, d.c_d, d.a_in, d.g, d.pr, d.partial, d.act_pj, d.act_pv, d.act_off, d.nact,
                     s->scan_tmp, s->stage, s->red_out, s->d_rhoT, s->d_phiT, s->d_FT, s->gctl, s->gtiles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1027,6 +1055,7 @@ int mg_destroy(mg_system* s)
     for (int k = 0; k < 4; k++)
         if (s->evk[k]) cudaEventDestroy(s->evk[k]);
     if (s->own_stream && s->st) cudaStreamDestroy(s->st);
+    if (s->hp) cudaFreeHost(s->hp);
     delete s;
     return MG_OK;
 }
@@ -1282,16 +1311,13 @@ int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
         return MG_OK;
     }
     Dev& d = s->d;
-    if (s->natms) {
-        const void* dx = nullptr;
-        CHK(stage_in(s, x, (size_t)s->natms * s->x_dim * sizeof(double), &dx));
-        CU(launch_split_x(d, (const double*)dx, 0, s->st));
-    }
+    const void* dx = nullptr;
+    CHK(stage_in(s, x, (size_t)s->natms * s->x_dim * sizeof(double), &dx));
     CU(cudaMemsetAsync(d.status + 7, 0, sizeof(int), s->st));
-    CU(launch_skin_check(d, s->skin * s->skin, d.status + 7, s->st));
-    // the ghost refresh is queued before the flag is known: it only writes
-    // the ghost slots, which a rebuild recreates anyway
-    CU(launch_refresh_x(d, s->st));
+    // new x, the skin test and the ghost refresh in one launch (the refresh
+    // runs before the flag is known: it only writes the ghost slots, which a
+    // rebuild recreates anyway)
+    CU(launch_update_x(d, (const double*)dx, s->skin * s->skin, d.status + 7, s->st));
     if (!rebuilt) {
         // nobody asked: the test is settled by the next entry point that needs
         // the lists, so the host does not wait here (force_calc reads it
@@ -1299,9 +1325,9 @@ int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
         s->skin_pending = true;
         return MG_OK;
     }
-    int flag = 0;
-    CU(cudaMemcpyAsync(&flag, d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaMemcpyAsync(&s->hp->status[7], d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
+    const int flag = s->hp->status[7];
     if (flag) {
         CU(launch_x2s(d, s->st));
         CHK(rebuild(s));
@@ -1411,22 +1437,19 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
         } else
             CU(launch_dmd_force(d, st_clc, &rows, s->st, s->evk));
     }
-    double tot[8] = {0};
     CU(launch_reduce_partials(d, rows, 7, s->red_out, s->st));
     CHK(timed_end(s));
-    CU(cudaMemcpyAsync(tot, s->red_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
-    int icut_over = 0, tc_timeout = 0;
-    if (s->dmd && s->form == MG_FORM_FP32)
-        CU(cudaMemcpyAsync(&icut_over, d.status + 4, sizeof(int), cudaMemcpyDeviceToHost, s->st));
-    if (s->dmd && s->form == MG_FORM_MLP)
-        CU(cudaMemcpyAsync(&tc_timeout, d.status + 5, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    // the forces first, then the totals and every status word in one copy;
+    // both asynchronous, one synchronisation
     CHK(copy_out(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
-    int skin = 0;
-    if (speculative) CU(cudaMemcpyAsync(&skin, d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaMemcpyAsync(s->hp, s->red_out, 8 * sizeof(double) + 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
+    const double* tot = s->hp->tot;
+    const int icut_over = s->dmd && s->form == MG_FORM_FP32 ? s->hp->status[4] : 0;
+    const int tc_timeout = s->dmd && s->form == MG_FORM_MLP ? s->hp->status[5] : 0;
     if (speculative) {
         s->skin_pending = false;
-        if (skin) {
+        if (s->hp->status[7]) {
             CU(launch_x2s(d, s->st));
             CHK(rebuild(s));
             return mg_ff_force_calc(s, st_clc, f, en_st);
@@ -1469,13 +1492,12 @@ int mg_ff_energy_calc(mg_system* s, double* energy)
         CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
         CU(launch_dmd_energy(d, &rows, s->st));
     }
-    double tot[8] = {0};
     CU(launch_reduce_partials(d, rows, 1, s->red_out, s->st));
     CHK(timed_end(s));
-    CU(cudaMemcpyAsync(tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaMemcpyAsync(s->hp->tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
     CHK(timed_read(s, &s->t_energy));
-    if (energy) *energy = tot[0];
+    if (energy) *energy = s->hp->tot[0];
     return MG_OK;
 }
 
@@ -1494,8 +1516,8 @@ int mg_ff_create_2nd_neigh_lst(mg_system* s)
         CU(cudaMemsetAsync(d.crd, 0, (size_t)d.nall * sizeof(int), s->st));
         CU(cudaMemsetAsync(d.status, 0, 8 * sizeof(int), s->st));
         CU(launch_dmd_crd(d, s->st));
-        int st_h[8];
-        CU(cudaMemcpyAsync(st_h, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+        const int* st_h = s->hp->status;
+        CU(cudaMemcpyAsync(s->hp->status, d.status, 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
         CU(cudaStreamSynchronize(s->st));
         if (!st_h[2]) break;
         d.maxcrd = st_h[3] + 8;
@@ -1554,12 +1576,11 @@ int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g
     CU(launch_dmd_calc_g(d, chk, alpha, &rows, s->st));
     CU(launch_reduce_partials(d, rows, 1, s->red_out, s->st));
     CHK(timed_end(s));
-    double tot[2] = {0, 0};
-    CU(cudaMemcpyAsync(tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CHK(copy_out(s, g, d.g, bytes));
+    CU(cudaMemcpyAsync(s->hp->tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
     CHK(timed_read(s, &s->t_g));
-    if (cost) *cost = tot[0] * 0.25;
+    if (cost) *cost = s->hp->tot[0] * 0.25;
     return MG_OK;
 }
 
@@ -1985,9 +2006,9 @@ int mg::system_set_active_pairs(mg_system* s, bool on)
     CHK(ensure_pair_values(s));
     CU(launch_active_count(d, s->st));
     CU(launch_exclusive_scan(d.nact, d.act_off, s->natms + 1, s->scan_tmp, s->scan_tmp_bytes, s->st));
-    int total = 0;
-    CU(cudaMemcpyAsync(&total, d.act_off + s->natms, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaMemcpyAsync(&s->hp->count, d.act_off + s->natms, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
+    const int total = s->hp->count;
     const int nvals = s->nt * s->nt + s->nt * (s->nt + 1) / 2;
     if ((size_t)total + 1 > s->act_cap) {
         const size_t cap = (size_t)total + (size_t)total / 8 + 64;

@@ -365,26 +365,30 @@ __global__ void k_store_x0(Dev d)
     if (i < d.natms) d.pos0[i] = d.pos[i];
 }
 
-__global__ void k_skin_check(Dev d, double sq_skin, int* __restrict__ flag)
+// Atoms::update for x (update_0) in one launch.  Owned sites take the new x
+// (position and alpha) and test their displacement since the last build
+// against the skin (Neighbor's rebuild test); each ghost is its root's new x
+// with the chain of +-H[dim][0..dim] additions applied in creation order, read
+// straight from the caller's x (roots are owned sites), so no second launch has
+// to wait for the owned copy.
+__global__ void k_update_x(Dev d, const double* __restrict__ x, double sq_skin, int* __restrict__ flag)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.natms) return;
-    double4 p = d.pos[i], q = d.pos0[i];
-    double dx0 = dsub(p.x, q.x), dx1 = dsub(p.y, q.y), dx2 = dsub(p.z, q.z);
-    double sq = dadd(dadd(dmul(dx0, dx0), dmul(dx1, dx1)), dmul(dx2, dx2));
-    if (sq > sq_skin) atomicOr(flag, 1);
-}
-
-// Atoms::update for x: each ghost = its root's x with the chain of +-H[dim][0..dim]
-// additions applied in creation order; alpha (the rest of vector x) is copied.
-__global__ void k_refresh_x(Dev d)
-{
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d.nph) return;
-    int g = d.natms + k;
-    int r = d.root[g];
-    d.pos[g] = ghost_image(d, d.gchain[g], d.pos[r]);
-    for (int a = 0; a < d.x_dim - 3; a++) d.alpha[(size_t)g * d.nt + a] = d.alpha[(size_t)r * d.nt + a];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < d.natms) {
+        const double* p = x + (size_t)k * d.x_dim;
+        const double4 v = make_double4(p[0], p[1], p[2], 0.0);
+        d.pos[k] = v;
+        for (int a = 0; a < d.x_dim - 3; a++) d.alpha[(size_t)k * d.nt + a] = p[3 + a];
+        const double4 q = d.pos0[k];
+        const double dx0 = dsub(v.x, q.x), dx1 = dsub(v.y, q.y), dx2 = dsub(v.z, q.z);
+        const double sq = dadd(dadd(dmul(dx0, dx0), dmul(dx1, dx1)), dmul(dx2, dx2));
+        if (sq > sq_skin) atomicOr(flag, 1);
+    } else if (k < d.natms + d.nph) {
+        const int r = d.root[k];
+        const double* p = x + (size_t)r * d.x_dim;
+        d.pos[k] = ghost_image(d, d.gchain[k], make_double4(p[0], p[1], p[2], 0.0));
+        for (int a = 0; a < d.x_dim - 3; a++) d.alpha[(size_t)k * d.nt + a] = p[3 + a];
+    }
 }
 
 __global__ void k_refresh_c(Dev d)
@@ -514,15 +518,10 @@ cudaError_t launch_store_x0(const Dev& d, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t launch_skin_check(const Dev& d, double sq_skin, int* flag, cudaStream_t st)
+cudaError_t launch_update_x(const Dev& d, const double* x_aos, double sq_skin, int* flag, cudaStream_t st)
 {
-    if (d.natms) k_skin_check<<<div_up(d.natms, kBlock), kBlock, 0, st>>>(d, sq_skin, flag);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_refresh_x(const Dev& d, cudaStream_t st)
-{
-    if (d.nph) k_refresh_x<<<div_up(d.nph, kBlock), kBlock, 0, st>>>(d);
+    const int n = d.natms + d.nph;
+    if (n) k_update_x<<<div_up(n, kBlock), kBlock, 0, st>>>(d, x_aos, sq_skin, flag);
     return cudaGetLastError();
 }
 
