@@ -90,6 +90,20 @@ bool is_device_ptr(const void* p)
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// where a caller's pointer lives: 0 pageable host memory (a device-to-host
+// copy into it blocks the host until the stream has drained), 1 page-locked
+// host memory, 2 device (or managed) memory
+int ptr_kind(const void* p)
+{
+    cudaPointerAttributes a;
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return 2;
+    return a.type == cudaMemoryTypeHost ? 1 : 0;
+}
+
 // ---- splines: interpolate (ff_eam.cpp:1323-1352) and interpolate_m
 // (ff_dmd_I.cpp:1794-1836), on rows of `w` doubles ---------------------------
 void spline_cubic(int n, double delta, double* s, int w)
@@ -213,6 +227,20 @@ struct mg_system {
     Dev d;
     cudaStream_t st = nullptr;
     bool own_stream = false;
+    // a second stream of the library's own for the copy of a final per-site
+    // array (forces, g) to the caller while the main stream reduces the
+    // totals; ev_fork / ev_join order it after the producing kernels and
+    // before the call returns
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool side_pending = false;
+    // a copy into pageable memory is not moved to the side stream (it would
+    // block the host before the reduction is queued): it waits for join_side
+    struct {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    } deferred{nullptr, nullptr, 0};
     size_t cap = 0;          // per-atom capacity (owned + ghost)
     int cap_bins = 0;
     void* scan_tmp = nullptr;
@@ -280,6 +308,13 @@ int check_sys_nores(mg_system* s)
 {
     if (!s) return fail(MG_ERR_ARG, "null mg_system");
     if (cudaSetDevice(s->device) != cudaSuccess) return fail(MG_ERR_CUDA, "cudaSetDevice(%d) failed", s->device);
+    s->deferred.dst = nullptr;  // (a failed call's copy into pageable memory is dropped)
+    if (s->side_pending) {
+        // a call that failed between its side copy and the join: nothing
+        // queued from here on may overwrite the array that copy reads
+        s->side_pending = false;
+        if (cudaStreamWaitEvent(s->st, s->ev_join, 0) != cudaSuccess) return fail(MG_ERR_CUDA, "stream join failed");
+    }
     return MG_OK;
 }
 
@@ -326,6 +361,42 @@ int copy_out(mg_system* s, void* dst, const void* dev_src, size_t bytes)
     if (!dst || !bytes) return MG_OK;
     cudaMemcpyKind k = is_device_ptr(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     CU(cudaMemcpyAsync(dst, dev_src, bytes, k, s->st));
+    return MG_OK;
+}
+
+// copy_out of an array that is final at this point of the main stream, run on
+// the side stream so it overlaps what the main stream queues next (the
+// reduction of the totals); join_side makes the main stream wait for it.  A
+// pageable destination is copied on the main stream by join_side instead.
+int copy_out_side(mg_system* s, void* dst, const void* dev_src, size_t bytes)
+{
+    if (!dst || !bytes) return MG_OK;
+    const int kind = ptr_kind(dst);
+    if (kind == 0) {
+        s->deferred.dst = dst;
+        s->deferred.src = dev_src;
+        s->deferred.bytes = bytes;
+        return MG_OK;
+    }
+    cudaMemcpyKind k = kind == 2 ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CU(cudaEventRecord(s->ev_fork, s->st));
+    CU(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
+    CU(cudaMemcpyAsync(dst, dev_src, bytes, k, s->side));
+    CU(cudaEventRecord(s->ev_join, s->side));
+    s->side_pending = true;
+    return MG_OK;
+}
+
+int join_side(mg_system* s)
+{
+    if (s->deferred.dst) {
+        void* dst = s->deferred.dst;
+        s->deferred.dst = nullptr;
+        CHK(copy_out(s, dst, s->deferred.src, s->deferred.bytes));
+    }
+    if (!s->side_pending) return MG_OK;
+    s->side_pending = false;
+    CU(cudaStreamWaitEvent(s->st, s->ev_join, 0));
     return MG_OK;
 }
 
@@ -1011,7 +1082,14 @@ int mg_create(const char* style, int device, mg_system** out)
     cudaEventCreate(&s->ev1);
     for (int k = 0; k < 4; k++) cudaEventCreate(&s->evk[k]);
     memset(&s->d, 0, sizeof(Dev));
-    int r = dalloc(&s->red_out, 12);  // 8 totals, then 8 ints of status
+    int r = MG_OK;
+    if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        r = fail(MG_ERR_CUDA, "side stream creation failed");
+    }
+    if (!r) r = dalloc(&s->red_out, 12);  // 8 totals, then 8 ints of status
     if (!r) {
         s->d.status = reinterpret_cast<int*>(s->red_out + 8);
         if (cudaMallocHost((void**)&s->hp, sizeof(mg_system::HostPin)) != cudaSuccess) {
@@ -1026,6 +1104,9 @@ int mg_create(const char* style, int device, mg_system** out)
         for (int k = 0; k < 4; k++) cudaEventDestroy(s->evk[k]);
         cudaEventDestroy(s->ev0);
         cudaEventDestroy(s->ev1);
+        if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+        if (s->ev_join) cudaEventDestroy(s->ev_join);
+        if (s->side) cudaStreamDestroy(s->side);
         cudaStreamDestroy(s->st);
         delete s;
         return r;
@@ -1039,6 +1120,7 @@ int mg_destroy(mg_system* s)
     if (!s) return MG_OK;
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->st);
+    if (s->side) cudaStreamSynchronize(s->side);
     Dev& d = s->d;
     void* ptrs[] = {d.prf, s->d_pkT, s->d_pk64, s->d_pkS, d.icut, d.icut_n, d.srec, d.dE32, d.facc, d.poff, d.pair_i, d.pair_j, d.pos, d.sfr, d.pos0, d.alpha, d.c, d.type, d.root, d.gchain, d.bin, d.cell_start,
                     d.cell_count, d.cell_pos, d.nbr, d.nnb, d.crdl, d.ncrd, d.crd, d.f, d.rho, d.E,
@@ -1055,6 +1137,9 @@ int mg_destroy(mg_system* s)
     for (int k = 0; k < 4; k++)
         if (s->evk[k]) cudaEventDestroy(s->evk[k]);
     if (s->own_stream && s->st) cudaStreamDestroy(s->st);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
+    if (s->side) cudaStreamDestroy(s->side);
     if (s->hp) cudaFreeHost(s->hp);
     delete s;
     return MG_OK;
@@ -1404,7 +1489,9 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     CHK(timed_begin(s));
     // the precision form's first kernel zeroes f and E itself
     const bool f32 = s->dmd && s->form == MG_FORM_FP32;
-    if (!f32) CU(cudaMemsetAsync(d.f, 0, (size_t)s->natms * s->x_dim * sizeof(double), s->st));
+    // (and the plain DMD form's embedding kernel writes f's first terms)
+    if (!f32 && !(s->dmd && s->form == MG_FORM_FP64))
+        CU(cudaMemsetAsync(d.f, 0, (size_t)s->natms * s->x_dim * sizeof(double), s->st));
     int rows = 0;
     if (s->style == STYLE_EAM || s->style == STYLE_FS) {
         CU(cudaMemsetAsync(d.rho, 0, (size_t)s->natms * sizeof(double), s->st));
@@ -1437,12 +1524,14 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
         } else
             CU(launch_dmd_force(d, st_clc, &rows, s->st, s->evk));
     }
+    // the forces are final: their copy runs beside the reduction of the
+    // totals, which are read with every status word in one more copy; all
+    // asynchronous, one synchronisation
+    CHK(copy_out_side(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
     CU(launch_reduce_partials(d, rows, 7, s->red_out, s->st));
     CHK(timed_end(s));
-    // the forces first, then the totals and every status word in one copy;
-    // both asynchronous, one synchronisation
-    CHK(copy_out(s, f, d.f, (size_t)s->natms * s->x_dim * sizeof(double)));
     CU(cudaMemcpyAsync(s->hp, s->red_out, 8 * sizeof(double) + 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CHK(join_side(s));
     CU(cudaStreamSynchronize(s->st));
     const double* tot = s->hp->tot;
     const int icut_over = s->dmd && s->form == MG_FORM_FP32 ? s->hp->status[4] : 0;
@@ -1574,10 +1663,11 @@ int mg_ff_calc_g(mg_system* s, int chk, double alpha, const double* a, double* g
     CU(cudaMemsetAsync(d.E, 0, bytes, s->st));
     int rows = 0;
     CU(launch_dmd_calc_g(d, chk, alpha, &rows, s->st));
+    CHK(copy_out_side(s, g, d.g, bytes));
     CU(launch_reduce_partials(d, rows, 1, s->red_out, s->st));
     CHK(timed_end(s));
-    CHK(copy_out(s, g, d.g, bytes));
     CU(cudaMemcpyAsync(s->hp->tot, s->red_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CHK(join_side(s));
     CU(cudaStreamSynchronize(s->st));
     CHK(timed_read(s, &s->t_g));
     if (cost) *cost = s->hp->tot[0] * 0.25;

@@ -135,7 +135,14 @@ __global__ void __launch_bounds__(kFFBlock) k_dmd_embed(Dev d, int with_force, i
         e += ca * tmp0;
         e += d.kbT * calc_ent(ca);
         e += 1.5 * d.kbT * ca * log(al) + ca * d.c0[a];
-        if (with_force) d.f[(size_t)i * d.x_dim + 3 + a] -= 1.5 * d.kbT * ca / al;
+        if (with_force) {
+            // with forces this kernel starts the site's force row (no memset
+            // before the call): zero position terms and the alpha entropy
+            // term, to which pass 2 adds the pair terms
+            double* fi = d.f + (size_t)i * d.x_dim;
+            if (a == 0) fi[0] = fi[1] = fi[2] = 0.0;
+            fi[3 + a] = 0.0 - 1.5 * d.kbT * ca / al;
+        }
     }
     if (d.site_cell) cell_energy_add(d, i < d.natms ? i : -1, e);
     else acc[0] += e;
