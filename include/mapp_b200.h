@@ -15,7 +15,11 @@
  *     returns the message of the last failure on the calling thread (the
  *     reference prints the same text and exits, error.cpp:29-43);
  *   - array arguments may be host or device memory (detected per call);
- *     host arrays are copied through the system's stream;
+ *     host arrays are copied through the system's stream, except that
+ *     force_calc and calc_g copy their finished per-site result (f, g) into
+ *     page-locked host or device memory on a second stream of the library's
+ *     own, beside the reduction of the totals, and join it before returning;
+ *     page-locked host buffers give the fastest calls;
  *   - per-atom arrays use the reference's layouts: x is natms * x_dim with
  *     x_dim = 3 (EAM, FS) or 3 + ntypes (DMD: x y z alpha_1..alpha_n),
  *     c is natms * ntypes, type is natms ints, f has the layout of x;

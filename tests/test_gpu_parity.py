@@ -254,3 +254,51 @@ def test_gpu_errors_are_reported(tmp_path):
     with pytest.raises(mb.MGError) as e:
         s.coef(["ff_coef", "SetFL", str(tmp_path / "missing.eam")])
     assert e.value.code == 2
+
+
+@pytest.mark.parametrize("kind,kw", [("eam", dict(n=4)), ("dmd", dict(n=4, sigma=0.02, style="DMD_I"))],
+                         ids=["eam", "dmd"])
+def test_gpu_result_buffers_of_every_kind(tmp_path, kind, kw):
+    """force_calc and calc_g copy their per-site result into pageable host
+    memory, page-locked host memory or device memory by different routes (a
+    side stream beside the reduction for the last two, the main stream after
+    it for the first). All three give the same bits, also right after an
+    update_x whose skin test is still pending, and also past the skin."""
+    mb = _lib_or_skip()
+    import torch
+
+    w = fx.write_workload(str(tmp_path / "w"), kind, **kw)
+    s = mb.system_from_workload(w)
+    N, xd = s.natms, s.x_dim
+    x0 = s.get_x()
+    rng = np.random.default_rng(5)
+
+    def buffers(cols):
+        return [np.zeros((N, cols)), torch.zeros((N, cols), dtype=torch.float64).pin_memory(),
+                torch.zeros((N, cols), dtype=torch.float64, device="cuda")]
+
+    def host(a):
+        return a if isinstance(a, np.ndarray) else a.cpu().numpy()
+
+    for shift in (0.05, 0.7):
+        x1 = x0.copy()
+        x1[: max(1, N // 10), :3] += rng.normal(0, shift, (max(1, N // 10), 3))
+        outs, ens = [], []
+        for f in buffers(xd):
+            s.update_x(x1, report=False)
+            _, en = s.force_calc(1, f=f)
+            outs.append(host(f))
+            ens.append(en.copy())
+        assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+        assert np.array_equal(ens[0], ens[1]) and np.array_equal(ens[0], ens[2])
+        assert np.abs(outs[0]).max() > 0
+    if kind == "dmd":
+        s.create_2nd_neigh_lst()
+        a = rng.uniform(-1e-3, 1e-3, (N, s.nt))
+        gs, costs = [], []
+        for g in buffers(s.nt):
+            cost, _ = s.calc_g(a, 0.1, 0, g=g)
+            gs.append(host(g))
+            costs.append(cost)
+        assert np.array_equal(gs[0], gs[1]) and np.array_equal(gs[0], gs[2])
+        assert costs[0] == costs[1] == costs[2]
