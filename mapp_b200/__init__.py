@@ -63,6 +63,7 @@ SIGNATURES = {
     "mg_get_vector": (C.c_int, [_P, C.c_char_p, _P]),
     "mg_get_int_vector": (C.c_int, [_P, C.c_char_p, _P]),
     "mg_last_time": (C.c_int, [_P, C.c_char_p, _D]),
+    "mg_set_phase_timing": (C.c_int, [_P, C.c_int]),
     "mg_fs_energy_noalloc": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
     "mg_mlp_nparam": (C.c_int, []),
     "mg_mlp_init": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_ulonglong]),
@@ -448,6 +449,11 @@ class System:
         ms = C.c_double(0.0)
         _check(load_library().mg_last_time(self.h, phase.encode(), C.byref(ms)))
         return ms.value
+
+    def set_phase_timing(self, on=True):
+        """Per-kernel events inside the DMD force call (off by default: each
+        costs the call a few microseconds); needed for last_time("force.*")."""
+        _check(load_library().mg_set_phase_timing(self.h, int(bool(on))))
 
 
 def fs_energy_noalloc(coeffs: "FsCoeffs", natms: int, nall: int, x, type, nbr_off, nbr, energy, stream: int = 0):

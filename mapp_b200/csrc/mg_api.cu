@@ -278,6 +278,10 @@ struct mg_system {
     long long pair_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};
+    // per-kernel events inside the DMD force call (mg_set_phase_timing): off
+    // by default, since each event between two kernels costs the call about
+    // 3 us at 32000 sites; t_k_valid says whether the last call took them
+    bool phase_timing = false, t_k_valid = false;
     // learned form
     MlpState mlp{};
     bool mlp_ready = false;
@@ -1486,6 +1490,7 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     }
     Dev& d = s->d;
     fill_dev_scalars(s);
+    cudaEvent_t* evk = s->phase_timing ? s->evk : nullptr;
     CHK(timed_begin(s));
     // the precision form's first kernel zeroes f and E itself
     const bool f32 = s->dmd && s->form == MG_FORM_FP32;
@@ -1499,7 +1504,7 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     } else {
         if (!f32) CU(cudaMemsetAsync(d.E, 0, (size_t)s->natms * s->nt * sizeof(double), s->st));
         if (f32) {
-            CU(launch_dmd_force_f32(d, st_clc, &rows, s->st, s->evk));
+            CU(launch_dmd_force_f32(d, st_clc, &rows, s->st, evk));
             s->prf_stale = true;
         } else if (s->form == MG_FORM_MLP) {
             // the network-row list holds every row of the list at most
@@ -1519,10 +1524,10 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
             CU(cudaMemsetAsync(s->mlp.audit, 0, 16 * sizeof(float), s->st));
             CU(cudaMemsetAsync(d.status + 5, 0, sizeof(int), s->st));
             CU(launch_dmd_force_mlp(d, s->mlp, 0x51ed270b3a5d4e1ull + 0x9e37ull * (++s->mlp_calls), st_clc, &rows,
-                                    s->st, s->evk));
+                                    s->st, evk));
             s->prf_stale = false;
         } else
-            CU(launch_dmd_force(d, st_clc, &rows, s->st, s->evk));
+            CU(launch_dmd_force(d, st_clc, &rows, s->st, evk));
     }
     // the forces are final: their copy runs beside the reduction of the
     // totals, which are read with every status word in one more copy; all
@@ -1547,10 +1552,11 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     if (icut_over) return fail(MG_ERR_CAPACITY, "precision form: in-cut pair list overflow");
     if (tc_timeout) return fail(MG_ERR_TIMEOUT, "learned form: a tensor-core wait ran out");
     CHK(timed_read(s, &s->t_force));
-    if (s->dmd)
+    s->t_k_valid = s->dmd && evk;
+    if (s->t_k_valid)
         for (int k = 0; k < 3; k++) {
             float ms = 0;
-            cudaEventElapsedTime(&ms, s->evk[k], s->evk[k + 1]);
+            CU(cudaEventElapsedTime(&ms, s->evk[k], s->evk[k + 1]));
             s->t_k[k] = ms;
         }
     if (en_st) {
@@ -1774,10 +1780,21 @@ int mg_last_time(mg_system* s, const char* phase, double* ms)
     else if (!strcmp(phase, "energy")) *ms = s->t_energy;
     else if (!strcmp(phase, "c_d")) *ms = s->t_cd;
     else if (!strcmp(phase, "calc_g")) *ms = s->t_g;
-    else if (!strcmp(phase, "force.pass1")) *ms = s->t_k[0];
-    else if (!strcmp(phase, "force.embed")) *ms = s->t_k[1];
-    else if (!strcmp(phase, "force.pass2")) *ms = s->t_k[2];
-    else return fail(MG_ERR_ARG, "unknown phase %s", phase);
+    else if (!strncmp(phase, "force.", 6)) {
+        int k = !strcmp(phase, "force.pass1") ? 0 : !strcmp(phase, "force.embed") ? 1 : !strcmp(phase, "force.pass2") ? 2 : -1;
+        if (k < 0) return fail(MG_ERR_ARG, "unknown phase %s", phase);
+        if (!s->t_k_valid)
+            return fail(MG_ERR_STATE, "%s: the last force_calc took no per-kernel times (mg_set_phase_timing)", phase);
+        *ms = s->t_k[k];
+    } else
+        return fail(MG_ERR_ARG, "unknown phase %s", phase);
+    return MG_OK;
+}
+
+int mg_set_phase_timing(mg_system* s, int on)
+{
+    CHK(check_sys(s));
+    s->phase_timing = on != 0;
     return MG_OK;
 }
 

@@ -555,7 +555,16 @@ struct Clock {
     std::vector<double*> y;
     double* block = nullptr;  // one allocation for every vector and the scalars
     long long n_calc_g = 0;
-    double host_sc[SC_COUNT];
+    // the scalars and the line search's final state as the host reads them,
+    // in page-locked memory: the copies are asynchronous, so one
+    // synchronisation brings both (a copy into pageable memory would block
+    // the host by itself, one more round trip per step)
+    struct HostOut {
+        double sc[SC_COUNT];
+        SolveDev r;
+    };
+    HostOut* hout = nullptr;
+    double* host_sc = nullptr;
     // the line search's graph (captured once per run) and its device state
     SolveDev* S_dev = nullptr;
     cudaGraph_t ls_graph = nullptr;
@@ -566,6 +575,7 @@ struct Clock {
         if (ls_graph) cudaGraphDestroy(ls_graph);
         cudaFree(S_dev);
         cudaFree(block);
+        if (hout) cudaFreeHost(hout);
     }
 
     int grid() const { return V.nblocks; }
@@ -593,6 +603,8 @@ struct Clock {
     int build_ls_graph()
     {
         KCU(cudaMalloc(&S_dev, sizeof(SolveDev)));
+        KCU(cudaMallocHost((void**)&hout, sizeof(HostOut)));
+        host_sc = hout->sc;
         KCU(cudaGraphCreate(&ls_graph, 0));
         cudaGraphConditionalHandle h;
         KCU(cudaGraphConditionalHandleCreate(&h, ls_graph, 0, cudaGraphCondAssignDefault));
@@ -667,9 +679,9 @@ struct Clock {
         hs.adams = 1;
         KCU(cudaMemcpyAsync(S_dev, &hs, sizeof(SolveDev), cudaMemcpyHostToDevice, st));
         KCU(cudaGraphLaunch(ls_exec, st));
-        SolveDev r{};
-        KCU(cudaMemcpyAsync(&r, S_dev, sizeof(SolveDev), cudaMemcpyDeviceToHost, st));
+        KCU(cudaMemcpyAsync(&hout->r, S_dev, sizeof(SolveDev), cudaMemcpyDeviceToHost, st));
         KCU(cudaStreamSynchronize(st));
+        const SolveDev& r = hout->r;
         n_calc_g += r.n_calc_g;
         if (r.overrun) return internal_fail(MG_ERR_TIMEOUT, "Adams clock: the line search did not end");
         *out_cost = r.curr_cost;
@@ -761,9 +773,10 @@ struct Bdf {
         KCU(cudaGraphLaunch(ck->ls_exec, ck->st));
         k_bdf_err<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, B);
         KCU(cudaGetLastError());
-        SolveDev r{};
-        KCU(cudaMemcpyAsync(&r, ck->S_dev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ck->st));
+        // the line search's state and the error sums in one synchronisation
+        KCU(cudaMemcpyAsync(&ck->hout->r, ck->S_dev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ck->st));
         KCHK(ck->read_scalars());
+        const SolveDev& r = ck->hout->r;
         ck->n_calc_g += r.n_calc_g;
         if (r.overrun) return internal_fail(MG_ERR_TIMEOUT, "BDF clock: the line search did not end");
         const double curr_cost = r.curr_cost;

@@ -307,3 +307,24 @@ def test_gpu_result_buffers_of_every_kind(tmp_path, kind, kw):
             assert np.abs(f_ref).max() > 0
             assert rel(host(f), f_ref) <= TOL
             assert rel(en, en_ref) <= TOL
+
+
+def test_gpu_phase_timing_switch(tmp_path):
+    """The DMD force call's per-kernel times exist only with phase timing on
+    (mg_set_phase_timing): without it mg_last_time("force.pass1") is an error,
+    with it the three kernels' times are positive and fit in the call's."""
+    mb = _lib_or_skip()
+    w = fx.write_workload(str(tmp_path / "w"), "dmd", n=4, sigma=0.02, style="DMD_I")
+    s = mb.system_from_workload(w)
+    f0, _ = s.force_calc(1)
+    with pytest.raises(mb.MGError):
+        s.last_time("force.pass1")
+    s.set_phase_timing(True)
+    f1, _ = s.force_calc(1)
+    t = [s.last_time(p) for p in ("force.pass1", "force.embed", "force.pass2")]
+    assert all(v > 0 for v in t) and sum(t) <= s.last_time("force")
+    s.set_phase_timing(False)
+    f2, _ = s.force_calc(1)
+    with pytest.raises(mb.MGError):
+        s.last_time("force.embed")
+    assert rel(f1, f0) <= TOL and rel(f2, f0) <= TOL
