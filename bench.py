@@ -328,7 +328,7 @@ def phase_times(s, f, steps, flush):
     microseconds each, so the throughput loops run without them."""
     import torch
 
-    s.set_phase_timing(True)
+    s.set_timing(2)
     t = [0.0, 0.0, 0.0, 0.0]
     for _ in range(steps):
         flush.zero_()
@@ -336,7 +336,7 @@ def phase_times(s, f, steps, flush):
         s.force_calc(1, f=f)
         for k, ph in enumerate(("force.pass1", "force.embed", "force.pass2", "force")):
             t[k] += s.last_time(ph)
-    s.set_phase_timing(False)
+    s.set_timing(1)
     return [v / steps for v in t]
 
 
@@ -894,7 +894,9 @@ def run_ours(args):
     e2e_stream = torch.cuda.Stream()
     s.set_stream(e2e_stream.cuda_stream)
     # update_x as a MAPP binding calls it (no rebuilt flag asked for: the
-    # skin test is read with force_calc's results)
+    # skin test is read with force_calc's results), and no timing events, as
+    # a production caller runs
+    s.set_timing(0)
     for _ in range(2):
         s.update_x(x_host, report=False)
         s.update_c(c_host)
@@ -912,6 +914,7 @@ def run_ours(args):
     t_e2e = job_max(ev0.elapsed_time(ev1) * 1e-3, "cuda")
     e2e_py = job_rate(natms, e2e_steps, t_e2e, ws)
     _, en_py = s.force_calc(1, f=f_host)
+    s.set_timing(1)
     # the same steps from a C++ caller of the C ABI (mapp_b200/client/mapp_e2e.cpp),
     # as MAPP's force loop would make them: set up from the same CFG file and
     # ff_coef arguments, pinned host buffers, events on the library's stream

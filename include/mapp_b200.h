@@ -144,17 +144,18 @@ int mg_get_vector(mg_system* s, const char* name, double* out);
 /* Per-atom int vectors: "crd" (owned + ghost). */
 int mg_get_int_vector(mg_system* s, const char* name, int* out);
 /* Device time in ms of the last call of each phase, measured with CUDA events
-   on the system's stream: "list", "force", "energy", "c_d", "calc_g", and for
-   DMD styles the three force kernels "force.pass1", "force.embed",
-   "force.pass2" (those only when the last force_calc ran with phase timing on;
-   MG_ERR_STATE otherwise). */
+   on the system's stream: "list" (always), "force", "energy", "c_d", "calc_g"
+   (timing level 1 or 2), and for DMD styles the three force kernels
+   "force.pass1", "force.embed", "force.pass2" (level 2); MG_ERR_STATE when the
+   last call of that phase was not timed. */
 int mg_last_time(mg_system* s, const char* phase, double* ms);
-/* Phase timing of the DMD force call (default off): with it on, force_calc
-   records an event between its kernels so that mg_last_time can report each
-   one; each such event costs the call a few microseconds. A profiling switch
-   of this library with no counterpart in the reference (whose force timer,
-   thermo_dynamics.cpp:188-206, times the whole call). */
-int mg_set_phase_timing(mg_system* s, int on);
+/* Device timing level: 0 no events, 1 (default) one event pair around the
+   whole call of force_calc, energy_calc, c_d_calc and calc_g, 2 also an event
+   between the kernels of the DMD force call. Each event costs a call a few
+   microseconds, so a production caller that does not read the times sets 0.
+   A profiling switch with no counterpart in the reference (whose force timer,
+   thermo_dynamics.cpp:188-206, times the whole call on the host). */
+int mg_set_timing(mg_system* s, int level);
 
 /* ---- learned form (MG_FORM_MLP) ------------------------------------------ */
 /* A 4 -> 64 -> 64 -> 64 -> 6 SiLU network replaces the Gauss-Hermite smearing

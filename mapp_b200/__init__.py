@@ -63,7 +63,7 @@ SIGNATURES = {
     "mg_get_vector": (C.c_int, [_P, C.c_char_p, _P]),
     "mg_get_int_vector": (C.c_int, [_P, C.c_char_p, _P]),
     "mg_last_time": (C.c_int, [_P, C.c_char_p, _D]),
-    "mg_set_phase_timing": (C.c_int, [_P, C.c_int]),
+    "mg_set_timing": (C.c_int, [_P, C.c_int]),
     "mg_fs_energy_noalloc": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
     "mg_mlp_nparam": (C.c_int, []),
     "mg_mlp_init": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_ulonglong]),
@@ -450,10 +450,11 @@ class System:
         _check(load_library().mg_last_time(self.h, phase.encode(), C.byref(ms)))
         return ms.value
 
-    def set_phase_timing(self, on=True):
-        """Per-kernel events inside the DMD force call (off by default: each
-        costs the call a few microseconds); needed for last_time("force.*")."""
-        _check(load_library().mg_set_phase_timing(self.h, int(bool(on))))
+    def set_timing(self, level):
+        """Device timing level: 0 none, 1 (default) whole calls, 2 also the
+        DMD force call's kernels (last_time("force.*")); each event costs a
+        call a few microseconds."""
+        _check(load_library().mg_set_timing(self.h, int(level)))
 
 
 def fs_energy_noalloc(coeffs: "FsCoeffs", natms: int, nall: int, x, type, nbr_off, nbr, energy, stream: int = 0):

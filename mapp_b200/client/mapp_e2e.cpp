@@ -88,6 +88,8 @@ int main(int argc, char** argv)
     cudaStream_t st;
     check_cuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
     check(mg_set_stream(s, st), "mg_set_stream");
+    // a production caller reads no per-call device times: no timing events
+    check(mg_set_timing(s, 0), "mg_set_timing");
 
     // pinned host buffers, as a caller keeping its arrays page-locked would
     const size_t nx = (size_t)natms * x_dim, nc = dmd ? (size_t)natms * nt : 0;

@@ -278,10 +278,12 @@ struct mg_system {
     long long pair_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};
-    // per-kernel events inside the DMD force call (mg_set_phase_timing): off
-    // by default, since each event between two kernels costs the call about
-    // 3 us at 32000 sites; t_k_valid says whether the last call took them
-    bool phase_timing = false, t_k_valid = false;
+    // device timing (mg_set_timing): 0 none, 1 (default) the whole call of
+    // each entry point, 2 also the kernels of the DMD force call; every event
+    // costs the call about 3 us at 32000 sites.  A phase time below zero, and
+    // t_k_valid false, mean the last call took none
+    int timing = 1;
+    bool t_k_valid = false;
     // learned form
     MlpState mlp{};
     bool mlp_ready = false;
@@ -1021,7 +1023,7 @@ int ensure_pair_values(mg_system* s)
 
 int timed_begin(mg_system* s)
 {
-    CU(cudaEventRecord(s->ev0, s->st));
+    if (s->timing > 0) CU(cudaEventRecord(s->ev0, s->st));
     return MG_OK;
 }
 
@@ -1030,12 +1032,16 @@ int timed_begin(mg_system* s)
 // queue behind the kernels without a host round trip between them
 int timed_end(mg_system* s)
 {
-    CU(cudaEventRecord(s->ev1, s->st));
+    if (s->timing > 0) CU(cudaEventRecord(s->ev1, s->st));
     return MG_OK;
 }
 
 int timed_read(mg_system* s, double* slot)
 {
+    if (s->timing <= 0) {
+        *slot = -1.0;
+        return MG_OK;
+    }
     CU(cudaEventSynchronize(s->ev1));
     float ms = 0;
     cudaEventElapsedTime(&ms, s->ev0, s->ev1);
@@ -1490,7 +1496,7 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     }
     Dev& d = s->d;
     fill_dev_scalars(s);
-    cudaEvent_t* evk = s->phase_timing ? s->evk : nullptr;
+    cudaEvent_t* evk = s->timing >= 2 ? s->evk : nullptr;
     CHK(timed_begin(s));
     // the precision form's first kernel zeroes f and E itself
     const bool f32 = s->dmd && s->form == MG_FORM_FP32;
@@ -1784,17 +1790,20 @@ int mg_last_time(mg_system* s, const char* phase, double* ms)
         int k = !strcmp(phase, "force.pass1") ? 0 : !strcmp(phase, "force.embed") ? 1 : !strcmp(phase, "force.pass2") ? 2 : -1;
         if (k < 0) return fail(MG_ERR_ARG, "unknown phase %s", phase);
         if (!s->t_k_valid)
-            return fail(MG_ERR_STATE, "%s: the last force_calc took no per-kernel times (mg_set_phase_timing)", phase);
+            return fail(MG_ERR_STATE, "%s: the last force_calc took no per-kernel times (mg_set_timing level 2)",
+                        phase);
         *ms = s->t_k[k];
     } else
         return fail(MG_ERR_ARG, "unknown phase %s", phase);
+    if (*ms < 0.0) return fail(MG_ERR_STATE, "%s: the last call was not timed (mg_set_timing level 0)", phase);
     return MG_OK;
 }
 
-int mg_set_phase_timing(mg_system* s, int on)
+int mg_set_timing(mg_system* s, int level)
 {
     CHK(check_sys(s));
-    s->phase_timing = on != 0;
+    if (level < 0 || level > 2) return fail(MG_ERR_ARG, "timing level %d is not 0, 1 or 2", level);
+    s->timing = level;
     return MG_OK;
 }
 

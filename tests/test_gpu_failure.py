@@ -50,7 +50,11 @@ def _relaxed(mb, builder, cells, launch=None):
 
 def _same(a, b):
     for (xa, fa, ra), (xb, fb, rb) in zip(a, b):
-        assert ra["iterations"] == rb["iterations"] and ra["code"] == rb["code"]
+        assert ra["iterations"] == rb["iterations"]
+        # the last line search can end on the minimum step (3) in one run and
+        # on the energy tolerance (5) in another: the energies it compares are
+        # sums of FP64 atomics, equal only to the last bits between runs
+        assert ra["code"] == rb["code"] or {ra["code"], rb["code"]} == {3, 5}
         assert np.max(np.abs(xa - xb)) <= 1e-9
 
 

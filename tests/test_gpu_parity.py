@@ -309,22 +309,31 @@ def test_gpu_result_buffers_of_every_kind(tmp_path, kind, kw):
             assert rel(en, en_ref) <= TOL
 
 
-def test_gpu_phase_timing_switch(tmp_path):
-    """The DMD force call's per-kernel times exist only with phase timing on
-    (mg_set_phase_timing): without it mg_last_time("force.pass1") is an error,
-    with it the three kernels' times are positive and fit in the call's."""
+def test_gpu_timing_levels(tmp_path):
+    """mg_set_timing: at level 1 (the default) only the whole force call is
+    timed and mg_last_time("force.pass1") is an error; level 2 adds the three
+    kernels' times, positive and within the call's; level 0 times nothing
+    (mg_last_time("force") is an error too). The forces do not change."""
     mb = _lib_or_skip()
     w = fx.write_workload(str(tmp_path / "w"), "dmd", n=4, sigma=0.02, style="DMD_I")
     s = mb.system_from_workload(w)
     f0, _ = s.force_calc(1)
+    assert s.last_time("force") > 0
     with pytest.raises(mb.MGError):
         s.last_time("force.pass1")
-    s.set_phase_timing(True)
+    s.set_timing(2)
     f1, _ = s.force_calc(1)
     t = [s.last_time(p) for p in ("force.pass1", "force.embed", "force.pass2")]
     assert all(v > 0 for v in t) and sum(t) <= s.last_time("force")
-    s.set_phase_timing(False)
+    s.set_timing(0)
     f2, _ = s.force_calc(1)
+    for p in ("force", "force.embed"):
+        with pytest.raises(mb.MGError):
+            s.last_time(p)
     with pytest.raises(mb.MGError):
-        s.last_time("force.embed")
-    assert rel(f1, f0) <= TOL and rel(f2, f0) <= TOL
+        s.set_timing(3)
+    s.set_timing(1)
+    f3, _ = s.force_calc(1)
+    assert s.last_time("force") > 0
+    for f in (f1, f2, f3):
+        assert rel(f, f0) <= TOL
