@@ -291,6 +291,9 @@ struct mg_system {
     int mlp_loss_n = 0;
     unsigned long long mlp_calls = 0;
     bool skin_pending = false;  // update_x's skin test not yet read (status[7])
+    // the value update_x's skin test writes to status[7] when some site moved
+    // more than the skin: a new one per update_x, so the word needs no reset
+    int skin_gen = 0;
     GhostCtl* gctl = nullptr;  // device control of the ghost passes (two, ping-pong)
     unsigned* gtiles = nullptr;  // look-back words of the ghost passes (two halves)
     int gtiles_cap = 0;
@@ -334,7 +337,7 @@ int resolve_skin(mg_system* s)
     s->skin_pending = false;
     CU(cudaMemcpyAsync(&s->hp->status[7], s->d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
-    if (s->hp->status[7]) {
+    if (s->hp->status[7] == s->skin_gen) {
         CU(launch_x2s(s->d, s->st));
         CHK(rebuild(s));
     }
@@ -1408,11 +1411,11 @@ int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
     Dev& d = s->d;
     const void* dx = nullptr;
     CHK(stage_in(s, x, (size_t)s->natms * s->x_dim * sizeof(double), &dx));
-    CU(cudaMemsetAsync(d.status + 7, 0, sizeof(int), s->st));
     // new x, the skin test and the ghost refresh in one launch (the refresh
     // runs before the flag is known: it only writes the ghost slots, which a
     // rebuild recreates anyway)
-    CU(launch_update_x(d, (const double*)dx, s->skin * s->skin, d.status + 7, s->st));
+    s->skin_gen = s->skin_gen % 0x7ffffffe + 1;
+    CU(launch_update_x(d, (const double*)dx, s->skin * s->skin, d.status + 7, s->skin_gen, s->st));
     if (!rebuilt) {
         // nobody asked: the test is settled by the next entry point that needs
         // the lists, so the host does not wait here (force_calc reads it
@@ -1422,7 +1425,7 @@ int mg_atoms_update_x(mg_system* s, const double* x, int* rebuilt)
     }
     CU(cudaMemcpyAsync(&s->hp->status[7], d.status + 7, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
-    const int flag = s->hp->status[7];
+    const int flag = s->hp->status[7] == s->skin_gen;
     if (flag) {
         CU(launch_x2s(d, s->st));
         CHK(rebuild(s));
@@ -1549,7 +1552,7 @@ int mg_ff_force_calc(mg_system* s, int st_clc, double* f, double* en_st)
     const int tc_timeout = s->dmd && s->form == MG_FORM_MLP ? s->hp->status[5] : 0;
     if (speculative) {
         s->skin_pending = false;
-        if (s->hp->status[7]) {
+        if (s->hp->status[7] == s->skin_gen) {
             CU(launch_x2s(d, s->st));
             CHK(rebuild(s));
             return mg_ff_force_calc(s, st_clc, f, en_st);

@@ -370,8 +370,9 @@ __global__ void k_store_x0(Dev d)
 // against the skin (Neighbor's rebuild test); each ghost is its root's new x
 // with the chain of +-H[dim][0..dim] additions applied in creation order, read
 // straight from the caller's x (roots are owned sites), so no second launch has
-// to wait for the owned copy.
-__global__ void k_update_x(Dev d, const double* __restrict__ x, double sq_skin, int* __restrict__ flag)
+// to wait for the owned copy.  A site past the skin writes `gen`, which the
+// caller makes new for every call, to *flag, so the word needs no reset.
+__global__ void k_update_x(Dev d, const double* __restrict__ x, double sq_skin, int* __restrict__ flag, int gen)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < d.natms) {
@@ -382,7 +383,7 @@ __global__ void k_update_x(Dev d, const double* __restrict__ x, double sq_skin, 
         const double4 q = d.pos0[k];
         const double dx0 = dsub(v.x, q.x), dx1 = dsub(v.y, q.y), dx2 = dsub(v.z, q.z);
         const double sq = dadd(dadd(dmul(dx0, dx0), dmul(dx1, dx1)), dmul(dx2, dx2));
-        if (sq > sq_skin) atomicOr(flag, 1);
+        if (sq > sq_skin) *flag = gen;  // (every writer stores the same value)
     } else if (k < d.natms + d.nph) {
         const int r = d.root[k];
         const double* p = x + (size_t)r * d.x_dim;
@@ -518,10 +519,10 @@ cudaError_t launch_store_x0(const Dev& d, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t launch_update_x(const Dev& d, const double* x_aos, double sq_skin, int* flag, cudaStream_t st)
+cudaError_t launch_update_x(const Dev& d, const double* x_aos, double sq_skin, int* flag, int gen, cudaStream_t st)
 {
     const int n = d.natms + d.nph;
-    if (n) k_update_x<<<div_up(n, kBlock), kBlock, 0, st>>>(d, x_aos, sq_skin, flag);
+    if (n) k_update_x<<<div_up(n, kBlock), kBlock, 0, st>>>(d, x_aos, sq_skin, flag, gen);
     return cudaGetLastError();
 }
 

@@ -252,7 +252,7 @@ cudaError_t launch_cell_fill(const Dev& d, int* cursor, const GhostCtl* gc, int 
 cudaError_t launch_neigh(const Dev& d, cudaStream_t st);
 cudaError_t launch_pairs_compact(const Dev& d, cudaStream_t st);
 cudaError_t launch_store_x0(const Dev& d, cudaStream_t st);
-cudaError_t launch_update_x(const Dev& d, const double* x_aos, double sq_skin, int* flag, cudaStream_t st);
+cudaError_t launch_update_x(const Dev& d, const double* x_aos, double sq_skin, int* flag, int gen, cudaStream_t st);
 cudaError_t launch_refresh_c(const Dev& d, cudaStream_t st);
 cudaError_t launch_merge_x(const Dev& d, double* x_aos, int first, int count, cudaStream_t st);
 cudaError_t launch_reduce_partials(const Dev& d, int nblocks, int nvals, double* out, cudaStream_t st);
