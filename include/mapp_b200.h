@@ -17,9 +17,9 @@
  *   - array arguments may be host or device memory (detected per call);
  *     host arrays are copied through the system's stream, except that
  *     force_calc and calc_g copy their finished per-site result (f, g) into
- *     page-locked host or device memory on a second stream of the library's
- *     own, beside the reduction of the totals, and join it before returning;
- *     page-locked host buffers give the fastest calls;
+ *     page-locked host memory on a second stream of the library's own,
+ *     beside the reduction of the totals, and join it before returning;
+ *     page-locked host buffers give the fastest calls from host memory;
  *   - per-atom arrays use the reference's layouts: x is natms * x_dim with
  *     x_dim = 3 (EAM, FS) or 3 + ntypes (DMD: x y z alpha_1..alpha_n),
  *     c is natms * ntypes, type is natms ints, f has the layout of x;

@@ -234,8 +234,8 @@ struct mg_system {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool side_pending = false;
-    // a copy into pageable memory is not moved to the side stream (it would
-    // block the host before the reduction is queued): it waits for join_side
+    // a copy into pageable or device memory is not moved to the side stream:
+    // it is queued on the main stream by join_side
     struct {
         void* dst;
         const void* src;
@@ -373,21 +373,23 @@ int copy_out(mg_system* s, void* dst, const void* dev_src, size_t bytes)
     return MG_OK;
 }
 
-// copy_out of an array that is final at this point of the main stream, run on
-// the side stream so it overlaps what the main stream queues next (the
-// reduction of the totals); join_side makes the main stream wait for it.  A
-// pageable destination is copied on the main stream by join_side instead.
+// copy_out of an array that is final at this point of the main stream: into
+// page-locked host memory it runs on the side stream, so it overlaps what the
+// main stream queues next (the reduction of the totals), and join_side makes
+// the main stream wait for it.  Into pageable memory (a copy that blocks the
+// host) or device memory (a copy of a microsecond, less than the fork event
+// between two kernels costs) it runs on the main stream, from join_side.
 int copy_out_side(mg_system* s, void* dst, const void* dev_src, size_t bytes)
 {
     if (!dst || !bytes) return MG_OK;
     const int kind = ptr_kind(dst);
-    if (kind == 0) {
+    if (kind != 1) {
         s->deferred.dst = dst;
         s->deferred.src = dev_src;
         s->deferred.bytes = bytes;
         return MG_OK;
     }
-    cudaMemcpyKind k = kind == 2 ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const cudaMemcpyKind k = cudaMemcpyDeviceToHost;
     CU(cudaEventRecord(s->ev_fork, s->st));
     CU(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
     CU(cudaMemcpyAsync(dst, dev_src, bytes, k, s->side));

@@ -261,8 +261,8 @@ def test_gpu_errors_are_reported(tmp_path):
 def test_gpu_result_buffers_of_every_kind(tmp_path, kind, kw):
     """force_calc and calc_g copy their per-site result into pageable host
     memory, page-locked host memory or device memory by different routes (a
-    side stream beside the reduction for the last two, the main stream after
-    it for the first). Each kind of buffer gets its own inputs, so a copy that
+    side stream beside the reduction for page-locked memory, the main stream
+    after it for the others). Each kind of buffer gets its own inputs, so a copy that
     ran before its results were final would return the previous inputs'
     values; each result is compared with a pageable-buffer call on the same
     inputs (to round-off: the sums end in atomics, whose order varies between
