@@ -377,8 +377,8 @@ int copy_out(mg_system* s, void* dst, const void* dev_src, size_t bytes)
 // page-locked host memory it runs on the side stream, so it overlaps what the
 // main stream queues next (the reduction of the totals), and join_side makes
 // the main stream wait for it.  Into pageable memory (a copy that blocks the
-// host) or device memory (a copy of a microsecond, less than the fork event
-// between two kernels costs) it runs on the main stream, from join_side.
+// host) or device memory (a copy of about a microsecond, nothing to hide) it
+// runs on the main stream, from join_side.
 int copy_out_side(mg_system* s, void* dst, const void* dev_src, size_t bytes)
 {
     if (!dst || !bytes) return MG_OK;
