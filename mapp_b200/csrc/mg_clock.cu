@@ -844,6 +844,10 @@ struct Bdf {
         P.lo = lo_ord_avail;
         k_bdf_hilo<<<grid(), kCkBlock, 0, ck->st>>>(ck->V, B, P);
         KCU(cudaGetLastError());
+        // the error sums only steer an order change: with neither order
+        // available the host has nothing to read (the kernel still updates
+        // e_n), so the step goes on without a synchronisation
+        if (!hi_ord_avail && !lo_ord_avail) return MG_OK;
         KCHK(ck->read_scalars());
         lo_err = sqrt(ck->host_sc[SC_GG] / ((double)dof_tot * p.a_tol));
         hi_err = sqrt(ck->host_sc[SC_GG0] / ((double)dof_tot * p.a_tol));
