@@ -1035,7 +1035,8 @@ def run_ours(args):
         "workload_counts": {"pairs": cnt["npairs"], "pairs_in_smeared_cut": in_cut, "ghosts": cnt["nph"]},
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": UNIT,
-                "h2d_bytes_per_step": natms * (s.x_dim + nt) * 8, "d2h_bytes_per_step": natms * s.x_dim * 8 + 56,
+                # down: f, then the 8 totals and 8 status words in one copy
+                "h2d_bytes_per_step": natms * (s.x_dim + nt) * 8, "d2h_bytes_per_step": natms * s.x_dim * 8 + 96,
                 "steps": e2e_steps, "path": e2e_path,
                 "python_ctypes": {"value": e2e_py, "path": "the same calls from Python through ctypes"},
                 "client_energy_rel_diff": (abs(e2e_client["energy"] - float(en_py[0])) / abs(float(en_py[0]))

@@ -120,7 +120,9 @@ int main(int argc, char** argv)
     check_cuda(cudaEventElapsedTime(&ms, e0, e1), "event");
     std::printf("{\"natms\": %d, \"steps\": %d, \"ms\": %.6f, \"h2d_bytes_per_step\": %zu, "
                 "\"d2h_bytes_per_step\": %zu, \"energy\": %.12e, \"f0\": [%.12e, %.12e, %.12e]}\n",
-                natms, steps, ms, (nx + nc) * sizeof(double), nx * sizeof(double) + 7 * sizeof(double), en[0], f[0],
+                // (down: f, then the library's one copy of 8 totals and 8 status words)
+                natms, steps, ms, (nx + nc) * sizeof(double), nx * sizeof(double) + 8 * sizeof(double) + 8 * sizeof(int),
+                en[0], f[0],
                 f[1], f[2]);
     mg_destroy(s);
     cudaFreeHost(x);
