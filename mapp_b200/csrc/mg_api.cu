@@ -79,17 +79,6 @@ int dgrow(T** p, size_t n, size_t keep, cudaStream_t st)
     return MG_OK;
 }
 
-bool is_device_ptr(const void* p)
-{
-    if (!p) return false;
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
 // where a caller's pointer lives: 0 pageable host memory (a device-to-host
 // copy into it blocks the host until the stream has drained), 1 page-locked
 // host memory, 2 device (or managed) memory
@@ -103,6 +92,8 @@ int ptr_kind(const void* p)
     if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return 2;
     return a.type == cudaMemoryTypeHost ? 1 : 0;
 }
+
+bool is_device_ptr(const void* p) { return ptr_kind(p) == 2; }
 
 // ---- splines: interpolate (ff_eam.cpp:1323-1352) and interpolate_m
 // (ff_dmd_I.cpp:1794-1836), on rows of `w` doubles ---------------------------
