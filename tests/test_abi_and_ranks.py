@@ -55,6 +55,29 @@ def test_python_mirror_binds_every_entry_point():
     assert set(declared_entry_points()) <= set(mapp_b200.SIGNATURES)
 
 
+def declared_arg_counts():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for name, args in re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(mg_\w+)\s*\(([^)]*)\)\s*;", text, flags=re.M | re.S):
+        args = " ".join(args.split())
+        out[name] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_python_mirror_argument_counts_match_the_header():
+    """Each ctypes signature of the mirror takes as many arguments as the
+    header's declaration, so a changed entry point cannot be called with a
+    stale argument list."""
+    import mapp_b200
+
+    counts = declared_arg_counts()
+    assert len(counts) == len(declared_entry_points())
+    wrong = {n: (c, len(mapp_b200.SIGNATURES[n][1])) for n, c in counts.items()
+             if len(mapp_b200.SIGNATURES[n][1]) != c}
+    assert not wrong, wrong
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
